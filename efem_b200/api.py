@@ -1,0 +1,336 @@
+"""Python access to libefem_b200.so (the C ABI declared in include/efem_gpu.h).
+
+The library is the product: C++ host set-up and hand-written sm_100a CUDA
+kernels.  This module only marshals arguments.  It never computes a result
+itself, and it raises when the library or a GPU is missing.
+
+``Simulator`` mirrors the reference's JSON-driven entry point
+(``Simulator::initial(path)`` / ``Simulator::start()``,
+src/simulation/Simulator.cpp:6-41).  ``Model`` exposes the hot-path calls one
+by one: ``residual`` (``SoftObjective::residual``), ``solve``
+(``LBFGSSolver::solve``), ``approx_jacobian_csr`` (``Constraint::getJacobi``)
+and ``precond_apply`` (the ``SimplicialLLT::solve`` of ``LBFGSMat::apply_Hv``).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libefem_b200.so")
+
+OK, ERR_ARG, ERR_CONFIG, ERR_MESH, ERR_CUDA, ERR_NAN, ERR_TIMEOUT, ERR_UNSUPPORTED, ERR_NO_DEVICE, ERR_FACE = range(10)
+STATUS_NAMES = {0: "OK", 1: "ERR_ARG", 2: "ERR_CONFIG", 3: "ERR_MESH", 4: "ERR_CUDA", 5: "ERR_NAN",
+                6: "ERR_TIMEOUT", 7: "ERR_UNSUPPORTED", 8: "ERR_NO_DEVICE", 9: "ERR_FACE"}
+NEO_HOOKEAN, MOONEY_RIVLIN, YEOH = 0, 1, 2
+LOAD_FIX, LOAD_FORCE, LOAD_PRESSURE, LOAD_DPRESSURE = 0, 1, 2, 3
+FP64, MIXED = 0, 1
+SOLVE_CONVERGED, SOLVE_PRECOND_FALLBACK, SOLVE_DX_CONVERGED, SOLVE_MAX_ITERS = 1, 2, 4, 8
+
+EXPORTED = ["efem_default_options", "efem_model_create_from_json", "efem_model_create", "efem_model_destroy",
+            "efem_get_options", "efem_set_options", "efem_get_model_info", "efem_dof_map", "efem_residual",
+            "efem_approx_jacobian_csr", "efem_precond_apply", "efem_solve", "efem_last_error", "efem_version"]
+
+
+class EfemError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int), ("integration", ctypes.c_int), ("nl_solver", ctypes.c_int),
+                ("m", ctypes.c_int), ("max_iterations", ctypes.c_int), ("max_linesearch", ctypes.c_int),
+                ("residual_criterion", ctypes.c_double), ("dx_criterion", ctypes.c_double),
+                ("device_ptrs", ctypes.c_int), ("deterministic", ctypes.c_int), ("device", ctypes.c_int)]
+
+
+class SolveInfo(ctypes.Structure):
+    _fields_ = [("niter", ctypes.c_int), ("n_residual_evals", ctypes.c_int), ("n_jacobian_evals", ctypes.c_int),
+                ("flags", ctypes.c_int), ("u_inf", ctypes.c_double), ("r_inf", ctypes.c_double),
+                ("ms_total", ctypes.c_double), ("ms_factor", ctypes.c_double), ("ms_residual", ctypes.c_double),
+                ("ms_precond", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class ModelInfo(ctypes.Structure):
+    _fields_ = [("n_nodes", ctypes.c_int), ("n_free_nodes", ctypes.c_int), ("n_dof", ctypes.c_int),
+                ("n_elements", ctypes.c_int), ("n_elements_skipped", ctypes.c_int), ("n_faces", ctypes.c_int),
+                ("n_force_nodes", ctypes.c_int), ("n_blocks", ctypes.c_int), ("factor_nnz", ctypes.c_longlong),
+                ("n_supernodes", ctypes.c_int), ("n_levels", ctypes.c_int), ("factor_gflop", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Material(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int), ("id", ctypes.c_int), ("C10", ctypes.c_double), ("C01", ctypes.c_double),
+                ("C20", ctypes.c_double), ("C30", ctypes.c_double), ("D1", ctypes.c_double),
+                ("density", ctypes.c_double)]
+
+
+class ElementBlock(ctypes.Structure):
+    _fields_ = [("nen", ctypes.c_int), ("n_elem", ctypes.c_int), ("conn", ctypes.POINTER(ctypes.c_int)),
+                ("material_id", ctypes.POINTER(ctypes.c_int))]
+
+
+class MeshDesc(ctypes.Structure):
+    _fields_ = [("n_nodes", ctypes.c_int), ("X", ctypes.POINTER(ctypes.c_double)), ("n_blocks", ctypes.c_int),
+                ("blocks", ctypes.POINTER(ElementBlock))]
+
+
+class LoadDesc(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int), ("n", ctypes.c_int), ("nodes", ctypes.POINTER(ctypes.c_int)),
+                ("face_ptr", ctypes.POINTER(ctypes.c_int)), ("value", ctypes.c_double * 3)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libefem_b200.so (built by ``__graft_entry__.build()``)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise EfemError(ERR_UNSUPPORTED, f"{LIB_PATH} is not built; run __graft_entry__.build()")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, dp, ip = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)
+        sig = {
+            "efem_default_options": [ctypes.POINTER(Options)],
+            "efem_model_create_from_json": [ctypes.c_char_p, ctypes.POINTER(vp)],
+            "efem_model_create": [ctypes.POINTER(MeshDesc), ctypes.POINTER(Material), ctypes.c_int,
+                                  ctypes.POINTER(LoadDesc), ctypes.c_int, ctypes.POINTER(Options), ctypes.POINTER(vp)],
+            "efem_model_destroy": [vp],
+            "efem_get_options": [vp, ctypes.POINTER(Options)],
+            "efem_set_options": [vp, ctypes.POINTER(Options)],
+            "efem_get_model_info": [vp, ctypes.POINTER(ModelInfo)],
+            "efem_dof_map": [vp, ip],
+            "efem_residual": [vp, vp, vp],
+            "efem_approx_jacobian_csr": [vp, ctypes.POINTER(ctypes.c_longlong), ip, ip, dp],
+            "efem_precond_apply": [vp, vp],
+            "efem_solve": [vp, vp, ctypes.POINTER(SolveInfo)],
+            "efem_last_error": [ctypes.c_char_p, ctypes.c_size_t],
+        }
+        for name, args in sig.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = ctypes.c_int
+        L.efem_version.restype = ctypes.c_char_p
+        _lib = L
+    return _lib
+
+
+def last_error():
+    buf = ctypes.create_string_buffer(2048)
+    lib().efem_last_error(buf, 2048)
+    return buf.value.decode(errors="replace")
+
+
+def check(status):
+    if status != OK:
+        raise EfemError(status, last_error())
+
+
+def default_options():
+    o = Options()
+    check(lib().efem_default_options(ctypes.byref(o)))
+    return o
+
+
+def _ptr(a, t=ctypes.c_double):
+    return a.ctypes.data_as(ctypes.POINTER(t))
+
+
+def _vec_ptr(v):
+    """Pointer of a float64 numpy array or a CUDA float64 torch tensor."""
+    if hasattr(v, "data_ptr"):
+        return ctypes.c_void_p(v.data_ptr())
+    return ctypes.c_void_p(v.ctypes.data)
+
+
+class Model:
+    """One problem on one GPU (the C ABI's opaque handle)."""
+
+    def __init__(self, handle):
+        self.h = ctypes.c_void_p(handle) if not isinstance(handle, ctypes.c_void_p) else handle
+        info = self.info()
+        self.n_dof = info["n_dof"]
+        self.n_free = info["n_free_nodes"]
+
+    # ------------------------------------------------------------------ creation
+    @classmethod
+    def from_json(cls, path):
+        h = ctypes.c_void_p()
+        check(lib().efem_model_create_from_json(os.fsencode(path), ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_arrays(cls, X, blocks, materials, loads, options=None):
+        """X (n,3); blocks: list of (conn (ne,nen) 0-based, material ids or None);
+        materials: dicts in the reference's JSON form; loads: list of
+        ("fix", nodes) / ("force", nodes, [fx,fy,fz]) / ("pressure", faces, p) /
+        ("dpressure", faces, [vx,vy,vz])."""
+        keep = []
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        keep.append(X)
+        eb = (ElementBlock * max(1, len(blocks)))()
+        for i, (conn, mids) in enumerate(blocks):
+            conn = np.ascontiguousarray(conn, dtype=np.int32)
+            keep.append(conn)
+            eb[i].nen = conn.shape[1]
+            eb[i].n_elem = conn.shape[0]
+            eb[i].conn = _ptr(conn, ctypes.c_int)
+            if mids is not None:
+                mids = np.ascontiguousarray(mids, dtype=np.int32)
+                keep.append(mids)
+                eb[i].material_id = _ptr(mids, ctypes.c_int)
+        mesh = MeshDesc(X.shape[0], _ptr(X), len(blocks), eb)
+        tmap = {"neo_hookean": NEO_HOOKEAN, "mo_riv": MOONEY_RIVLIN, "yeoh": YEOH}
+        mats = (Material * max(1, len(materials)))()
+        for i, mj in enumerate(materials):
+            mats[i] = Material(tmap[mj["type"]], int(mj.get("id", -1)), float(mj.get("C10", 0)),
+                               float(mj.get("C01", 0)) if mj["type"] == "mo_riv" else 0.0,
+                               float(mj.get("C20", 0)) if mj["type"] == "yeoh" else 0.0,
+                               float(mj.get("C30", 0)) if mj["type"] == "yeoh" else 0.0,
+                               float(mj.get("D1", 0)), float(mj.get("density", 0)))
+        lds = (LoadDesc * max(1, len(loads)))()
+        for i, ld in enumerate(loads):
+            kind = ld[0]
+            if kind in ("fix", "force"):
+                nodes = np.ascontiguousarray(ld[1], dtype=np.int32)
+                keep.append(nodes)
+                lds[i].type = LOAD_FIX if kind == "fix" else LOAD_FORCE
+                lds[i].n = nodes.shape[0]
+                lds[i].nodes = _ptr(nodes, ctypes.c_int)
+                if kind == "force":
+                    for c in range(3):
+                        lds[i].value[c] = float(ld[2][c])
+            else:
+                faces = ld[1]
+                ptr = np.zeros(len(faces) + 1, dtype=np.int32)
+                ptr[1:] = np.cumsum([len(f) for f in faces])
+                flat = np.ascontiguousarray(np.concatenate([np.asarray(f) for f in faces]) if faces else np.zeros(0),
+                                            dtype=np.int32)
+                keep += [ptr, flat]
+                lds[i].type = LOAD_PRESSURE if kind == "pressure" else LOAD_DPRESSURE
+                lds[i].n = len(faces)
+                lds[i].nodes = _ptr(flat, ctypes.c_int)
+                lds[i].face_ptr = _ptr(ptr, ctypes.c_int)
+                vals = [float(ld[2]), 0.0, 0.0] if kind == "pressure" else [float(v) for v in ld[2]]
+                for c in range(3):
+                    lds[i].value[c] = vals[c]
+        opts = options if options is not None else default_options()
+        h = ctypes.c_void_p()
+        check(lib().efem_model_create(ctypes.byref(mesh), mats, len(materials), lds, len(loads), ctypes.byref(opts),
+                                      ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_case(cls, case, options=None):
+        """Build from an ``efem_b200.meshgen.Case`` without writing files."""
+        loads = [("fix", case.fix)]
+        for value, nodes in case.force:
+            loads.append(("force", nodes, value))
+        for value, faces in case.pressure:
+            if isinstance(value, (list, tuple, np.ndarray)):
+                loads.append(("dpressure", faces, value))
+            else:
+                loads.append(("pressure", faces, value))
+        opts = options if options is not None else default_options()
+        opts.integration = 1 if case.integration == "reduced" else 0
+        return cls.from_arrays(case.mesh.X, [(case.mesh.conn, case.mesh.mat)], case.materials, loads, opts)
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            lib().efem_model_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------------ options / info
+    @property
+    def options(self):
+        o = Options()
+        check(lib().efem_get_options(self.h, ctypes.byref(o)))
+        return o
+
+    def set_options(self, **kw):
+        o = self.options
+        for k, v in kw.items():
+            setattr(o, k, v)
+        check(lib().efem_set_options(self.h, ctypes.byref(o)))
+
+    def info(self):
+        i = ModelInfo()
+        check(lib().efem_get_model_info(self.h, ctypes.byref(i)))
+        return i.as_dict()
+
+    def dof_map(self):
+        out = np.zeros(self.n_free, dtype=np.int32)
+        check(lib().efem_dof_map(self.h, _ptr(out, ctypes.c_int)))
+        return out
+
+    # ------------------------------------------------------------------ hot path
+    def residual(self, u, out=None):
+        """R(u) for a host float64 array, or for CUDA float64 tensors when the
+        model's ``device_ptrs`` option is set."""
+        if out is None:
+            out = np.zeros(self.n_dof) if not hasattr(u, "data_ptr") else u.new_zeros(self.n_dof)
+        if not hasattr(u, "data_ptr"):
+            u = np.ascontiguousarray(u, dtype=np.float64)
+        check(lib().efem_residual(self.h, _vec_ptr(u), _vec_ptr(out)))
+        return out
+
+    def solve(self, u0=None):
+        """L-BFGS solve from u0 (zeros by default); returns (u, info dict)."""
+        if u0 is None:
+            u = np.zeros(self.n_dof)
+        elif hasattr(u0, "data_ptr"):
+            u = u0
+        else:
+            u = np.array(u0, dtype=np.float64)
+        info = SolveInfo()
+        st = lib().efem_solve(self.h, _vec_ptr(u), ctypes.byref(info))
+        if st not in (OK,):
+            raise EfemError(st, last_error())
+        return u, info.as_dict()
+
+    def approx_jacobian_csr(self):
+        nnz = ctypes.c_longlong()
+        check(lib().efem_approx_jacobian_csr(self.h, ctypes.byref(nnz), None, None, None))
+        rp = np.zeros(self.n_free + 1, dtype=np.int32)
+        ci = np.zeros(nnz.value, dtype=np.int32)
+        v = np.zeros(nnz.value)
+        check(lib().efem_approx_jacobian_csr(self.h, ctypes.byref(nnz), _ptr(rp, ctypes.c_int), _ptr(ci, ctypes.c_int),
+                                             _ptr(v)))
+        return rp, ci, v
+
+    def precond_apply(self, v):
+        v = np.array(v, dtype=np.float64)
+        check(lib().efem_precond_apply(self.h, _vec_ptr(v)))
+        return v
+
+
+class Simulator:
+    """The reference's JSON-driven call: ``initial(path)`` then ``start()``."""
+
+    def __init__(self):
+        self.model = None
+        self.u = None
+        self.result = None
+
+    def initial(self, config_file_path):
+        self.model = Model.from_json(config_file_path)
+        return self
+
+    def start(self):
+        self.u, self.result = self.model.solve()
+        return self.result

@@ -1,0 +1,204 @@
+// Internal data model of the B200 EFEM library.
+//
+// Device layout (one model = one problem on one GPU):
+//   * node numbering: free nodes first, in the reference's DOF order
+//     (src/fe/Constraint.cpp:61-72), then fixed nodes.  A solver vector u of
+//     length 3*n_free is indexed u[3*dnode + c] for dnode < n_free.
+//   * element blocks, one per node count: connectivity SoA conn[a][e] (dnode
+//     ids), material index, V_e, and J0^{-1} per Gauss point AoS
+//     [e][g][9] (row-major 3x3), in FP64 and (for the mixed path) FP32.
+//   * pressure faces grouped by parent element kind: parent connectivity SoA,
+//     A0, J0^{-1} at each face point, and an index into small face tables
+//     (weights, N, dN/dxi at the face points).
+//   * f_ext: the nodal-force vector; every residual starts from r = -f_ext.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/efem_gpu.h"
+#include "elements.h"
+
+namespace efem {
+
+// ------------------------------------------------------------------ host input
+struct HostMaterial {
+    int type, id;
+    double C10, C01, C20, C30, D1, density;
+};
+
+struct HostBlock {
+    int nen = 0;
+    std::vector<int> conn;    // row-major (n, nen), original node ids
+    std::vector<int> mat_id;  // material id per element
+};
+
+struct HostLoad {
+    int type = 0;                   // efem_load_type
+    std::vector<int> nodes;         // FIX / FORCE nodes, or face nodes
+    std::vector<int> face_ptr;      // faces (CSR), PRESSURE / DPRESSURE
+    double value[3] = { 0, 0, 0 };
+};
+
+struct ModelInput {
+    std::vector<double> X;          // (n, 3)
+    std::vector<HostBlock> blocks;
+    std::vector<HostMaterial> materials;
+    std::vector<HostLoad> loads;
+    efem_options opts;
+};
+
+// ------------------------------------------------------------------ device
+// Material parameters as the kernels see them.
+template <typename T>
+struct MatParams {
+    int type;
+    T C10, C01, C20, C30, D1;
+};
+
+constexpr int MAX_MATS = 16;
+
+struct DevBlock {
+    int kind = 0, nen = 0, ngp = 0, n = 0;
+    int* conn = nullptr;          // [nen][n]
+    int* mat = nullptr;           // [n]
+    double* vol = nullptr;        // [n]
+    float* vol_f = nullptr;
+    double* J0inv = nullptr;      // [n][ngp][9]
+    float* J0inv_f = nullptr;
+    double* dN = nullptr;         // [ngp][nen][3]
+    float* dN_f = nullptr;
+    double* gw = nullptr;         // [ngp]
+    float* gw_f = nullptr;
+    // host copies used by set-up (Jacobian assembly, tests)
+    std::vector<int> h_conn;      // row-major (n, nen), dnode ids
+    std::vector<int> h_mat;
+    std::vector<double> h_vol, h_J0inv, h_dN, h_gw;
+};
+
+struct DevFaces {
+    int kind = 0, nen = 0, n = 0;
+    int* conn = nullptr;          // [nen][n] parent element nodes (dnode)
+    int* table = nullptr;         // [n]
+    double* A0 = nullptr;         // [n][3]
+    double* J0inv = nullptr;      // [n][MAX_FGP][9]
+    float* J0inv_f = nullptr;
+    double* load = nullptr;       // [n][4]: directed flag, value / vector
+    // face tables for this element kind
+    int n_tables = 0;
+    int* t_ngp = nullptr;         // [n_tables]
+    double* t_w = nullptr;        // [n_tables][MAX_FGP]
+    double* t_N = nullptr;        // [n_tables][MAX_FGP][nen]
+    double* t_dN = nullptr;       // [n_tables][MAX_FGP][nen][3]
+    float* t_w_f = nullptr;
+    float* t_N_f = nullptr;
+    float* t_dN_f = nullptr;
+    // host copies (set-up output; uploaded by ensure_device)
+    std::vector<int> h_conn, h_table, h_ngp;
+    std::vector<double> h_A0, h_J0inv, h_load, h_w, h_N, h_dN;
+};
+
+struct Precond;   // Cholesky preconditioner (chol.cu)
+struct SolverWS;  // L-BFGS workspace (solver.cu)
+
+struct Model {
+    efem_options opts;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+
+    int n_nodes = 0, n_free = 0, n_elements = 0, n_skipped = 0, n_force_nodes = 0;
+    std::vector<int> node_of_dnode;   // dnode -> original node
+    std::vector<int> dnode_of_node;   // original node -> dnode
+    std::vector<double> X;            // original order (n,3)
+
+    std::vector<HostMaterial> materials_used;  // index = material slot
+    std::vector<double> kappa;                 // elasticity_coeff per slot
+
+    // element input kept for rebuilding the integration tables
+    std::vector<HostBlock> in_blocks;
+    int built_integration = -1;
+    std::vector<DevBlock> blocks;
+    std::vector<DevFaces> faces;
+    int n_faces = 0;
+
+    MatParams<double>* d_mats = nullptr;
+    MatParams<float>* d_mats_f = nullptr;
+    std::vector<double> h_fext;       // [3*n_free]
+    bool on_device = false;
+    double* d_fext = nullptr;         // [3*n_free]
+    double* d_u = nullptr;            // staging for host-pointer calls
+    double* d_r = nullptr;
+
+    Precond* precond = nullptr;   // owned; freed by free_precond
+    SolverWS* ws = nullptr;       // owned; freed by free_solver
+
+    ~Model();
+};
+
+// ------------------------------------------------------------------ errors
+void set_error(const std::string& msg);
+const std::string& get_error();
+
+#define EFEM_CUDA(call)                                                                          \
+    do {                                                                                         \
+        cudaError_t _e = (call);                                                                 \
+        if (_e != cudaSuccess) {                                                                 \
+            efem::set_error(std::string(#call) + ": " + cudaGetErrorString(_e));                 \
+            return EFEM_ERR_CUDA;                                                                \
+        }                                                                                        \
+    } while (0)
+
+template <typename T>
+efem_status dev_alloc(T** p, size_t n)
+{
+    *p = nullptr;
+    if (n == 0) return EFEM_OK;
+    EFEM_CUDA(cudaMalloc(reinterpret_cast<void**>(p), n * sizeof(T)));
+    return EFEM_OK;
+}
+
+template <typename T>
+efem_status dev_upload(T** p, const std::vector<T>& h)
+{
+    efem_status s = dev_alloc(p, h.size());
+    if (s != EFEM_OK) return s;
+    if (!h.empty()) EFEM_CUDA(cudaMemcpy(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return EFEM_OK;
+}
+
+template <typename T>
+void dev_free(T*& p)
+{
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+// ------------------------------------------------------------------ set-up
+efem_status read_json_config(const char* path, ModelInput& in);
+efem_status build_model(ModelInput& in, Model& m);
+efem_status build_blocks(Model& m);   // (re)build the integration tables for opts.integration (host)
+efem_status ensure_device(Model& m);  // create the stream and upload everything not yet on the device
+
+// ------------------------------------------------------------------ kernels (residual.cu)
+// r = R(u) on the model's stream; u, r device pointers of length 3*n_free.
+efem_status launch_residual(Model& m, const double* d_u, double* d_r);
+
+// ------------------------------------------------------------------ solver (solver.cu)
+efem_status run_solve(Model& m, double* d_u, efem_solve_info* info);
+void free_solver(Model& m);
+
+// ------------------------------------------------------------------ preconditioner (chol.cu)
+// Build (once) the scalar approximate Jacobian L and its Cholesky factor.
+// Returns EFEM_OK with *ok = 0 when L is not positive definite.
+efem_status precond_setup(Model& m, int* ok, double* ms_factor);
+// v <- (L (x) I3)^{-1} v in place on the device (v: 3*n_free interleaved).
+efem_status precond_apply(Model& m, double* d_v);
+void free_precond(Model& m);
+void precond_info(const Model& m, efem_model_info* info);
+// Host assembly of L in CSR over free nodes (upper and lower triangle).
+void assemble_L_csr(const Model& m, std::vector<int>& rowptr, std::vector<int>& col, std::vector<double>& val);
+
+}  // namespace efem

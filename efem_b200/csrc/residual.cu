@@ -1,0 +1,303 @@
+// Residual R(u) = f_int(u) - f_ext(u) on the GPU.
+//
+//   element internal force   r_e = V_e sum_g w_g P(F_g) T_g
+//                            (src/fe/ElementConstraint.cpp:139-162)
+//   follower pressure        f_i = p sum_g w_g N_i(xi_g) cof(F_g) A0, r_i -= f_i
+//   directed pressure        f_i = v sum_g w_g N_i(xi_g) |cof(F_g) A0|
+//                            (src/fe/ExternalConstraint.cpp:829-959)
+//   nodal forces             r starts from -f_ext (:149-167)
+//
+// Element kernel: one CTA processes EPB elements in three phases.
+//   1. stage: threads (element, node) load conn (SoA, coalesced over elements)
+//      and gather u into shared memory;
+//   2. Gauss point: thread (element, gp) forms H = (u . dN) J0^{-1}, P(I+H) and
+//      S_g = V_e w_g P J0^{-T} (3x3) into shared memory;
+//   3. node: thread (element, node) reduces r_a = sum_g S_g dN_ga and adds it
+//      to the global residual with FP64 atomics (red.global.add.f64) or, in
+//      deterministic mode, writes it to a per-element buffer that a node-major
+//      gather kernel sums in a fixed order.
+// The arithmetic type T is double (FP64 path) or float (mixed path); the
+// global residual is always accumulated in FP64.
+#include <cuda_runtime.h>
+
+#include "efem_internal.h"
+#include "mechanics.cuh"
+
+namespace efem {
+
+namespace {
+
+constexpr int kBlock = 128;
+
+template <typename T>
+struct ElemArgs {
+    int n, n_free;
+    const int* __restrict__ conn;     // [NEN][n]
+    const int* __restrict__ mat;      // [n]
+    const T* __restrict__ vol;        // [n]
+    const T* __restrict__ J0inv;      // [n][NGP][9]
+    const T* __restrict__ dN;         // [NGP][NEN][3]
+    const T* __restrict__ gw;         // [NGP]
+    const MatParams<T>* __restrict__ mats;
+    const double* __restrict__ u;     // [3*n_free]
+    double* __restrict__ r;           // [3*n_free]
+};
+
+template <int NEN, int NGP, typename T>
+__global__ void __launch_bounds__(kBlock) k_elem_residual(ElemArgs<T> a)
+{
+    constexpr int EPB = (kBlock / NGP) > 0 ? (kBlock / NGP) : 1;
+    __shared__ T s_u[EPB][NEN][3];
+    __shared__ T s_S[EPB][NGP][9];
+    __shared__ T s_dN[NGP][NEN][3];
+    __shared__ int s_node[EPB][NEN];
+
+    const int tid = threadIdx.x;
+    for (int i = tid; i < NGP * NEN * 3; i += kBlock) (&s_dN[0][0][0])[i] = a.dN[i];
+    const int e0 = blockIdx.x * EPB;
+
+    // phase 1: stage node displacements
+    for (int i = tid; i < EPB * NEN; i += kBlock) {
+        const int el = i % EPB, nd = i / EPB, e = e0 + el;
+        int node = a.n_free;  // out-of-range marker
+        T v0 = 0, v1 = 0, v2 = 0;
+        if (e < a.n) {
+            node = __ldg(a.conn + static_cast<size_t>(nd) * a.n + e);
+            if (node < a.n_free) {
+                v0 = static_cast<T>(__ldg(a.u + 3 * node));
+                v1 = static_cast<T>(__ldg(a.u + 3 * node + 1));
+                v2 = static_cast<T>(__ldg(a.u + 3 * node + 2));
+            }
+        }
+        s_node[el][nd] = node;
+        s_u[el][nd][0] = v0;
+        s_u[el][nd][1] = v1;
+        s_u[el][nd][2] = v2;
+    }
+    __syncthreads();
+
+    // phase 2: one thread per (element, Gauss point)
+    if (tid < EPB * NGP) {
+        const int el = tid / NGP, g = tid % NGP, e = e0 + el;
+        if (e < a.n) {
+            T A[9];
+#pragma unroll
+            for (int k = 0; k < 9; k++) A[k] = 0;
+#pragma unroll 4
+            for (int q = 0; q < NEN; q++) {
+                const T u0 = s_u[el][q][0], u1 = s_u[el][q][1], u2 = s_u[el][q][2];
+                const T d0 = s_dN[g][q][0], d1 = s_dN[g][q][1], d2 = s_dN[g][q][2];
+                A[0] += u0 * d0; A[1] += u0 * d1; A[2] += u0 * d2;
+                A[3] += u1 * d0; A[4] += u1 * d1; A[5] += u1 * d2;
+                A[6] += u2 * d0; A[7] += u2 * d1; A[8] += u2 * d2;
+            }
+            const T* Jp = a.J0inv + (static_cast<size_t>(e) * NGP + g) * 9;
+            T Ji[9];
+#pragma unroll
+            for (int k = 0; k < 9; k++) Ji[k] = __ldg(Jp + k);
+            T H[9];
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+#pragma unroll
+                for (int j = 0; j < 3; j++) H[3 * i + j] = A[3 * i] * Ji[j] + A[3 * i + 1] * Ji[3 + j] + A[3 * i + 2] * Ji[6 + j];
+            const MatParams<T> mp = a.mats[__ldg(a.mat + e)];
+            T P[9];
+            piola(mp, H, P);
+            const T wv = __ldg(a.vol + e) * a.gw[g];
+            // S = wv P J0^{-T}
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+#pragma unroll
+                for (int j = 0; j < 3; j++)
+                    s_S[el][g][3 * i + j] = wv * (P[3 * i] * Ji[3 * j] + P[3 * i + 1] * Ji[3 * j + 1] + P[3 * i + 2] * Ji[3 * j + 2]);
+        }
+    }
+    __syncthreads();
+
+    // phase 3: one thread per (element, node): r_a = sum_g S_g dN_ga
+    for (int i = tid; i < EPB * NEN; i += kBlock) {
+        const int el = i % EPB, nd = i / EPB, e = e0 + el;
+        if (e >= a.n) continue;
+        const int node = s_node[el][nd];
+        if (node >= a.n_free) continue;
+        T r0 = 0, r1 = 0, r2 = 0;
+#pragma unroll 4
+        for (int g = 0; g < NGP; g++) {
+            const T d0 = s_dN[g][nd][0], d1 = s_dN[g][nd][1], d2 = s_dN[g][nd][2];
+            const T* S = s_S[el][g];
+            r0 += S[0] * d0 + S[1] * d1 + S[2] * d2;
+            r1 += S[3] * d0 + S[4] * d1 + S[5] * d2;
+            r2 += S[6] * d0 + S[7] * d1 + S[8] * d2;
+        }
+        atomicAdd(a.r + 3 * node, static_cast<double>(r0));
+        atomicAdd(a.r + 3 * node + 1, static_cast<double>(r1));
+        atomicAdd(a.r + 3 * node + 2, static_cast<double>(r2));
+    }
+}
+
+template <typename T>
+struct FaceArgs {
+    int n, n_free;
+    const int* __restrict__ conn;     // [NEN][n]
+    const int* __restrict__ table;    // [n]
+    const double* __restrict__ A0;    // [n][3]
+    const T* __restrict__ J0inv;      // [n][MAX_FGP][9]
+    const double* __restrict__ load;  // [n][4]
+    const int* __restrict__ t_ngp;
+    const T* __restrict__ t_w;        // [t][MAX_FGP]
+    const T* __restrict__ t_N;        // [t][MAX_FGP][NEN]
+    const T* __restrict__ t_dN;       // [t][MAX_FGP][NEN][3]
+    const double* __restrict__ u;
+    double* __restrict__ r;
+};
+
+// One thread per face: cof(F_g) A0 at every face point, then the nodal forces
+// of all element nodes.
+template <int NEN, typename T>
+__global__ void __launch_bounds__(kBlock) k_face_residual(FaceArgs<T> a)
+{
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= a.n) return;
+    const int t = a.table[f];
+    const int ngp = a.t_ngp[t];
+    int node[NEN];
+    T uu[NEN][3];
+#pragma unroll
+    for (int q = 0; q < NEN; q++) {
+        node[q] = a.conn[static_cast<size_t>(q) * a.n + f];
+        const bool fr = node[q] < a.n_free;
+        uu[q][0] = fr ? static_cast<T>(a.u[3 * node[q]]) : T(0);
+        uu[q][1] = fr ? static_cast<T>(a.u[3 * node[q] + 1]) : T(0);
+        uu[q][2] = fr ? static_cast<T>(a.u[3 * node[q] + 2]) : T(0);
+    }
+    const T A0[3] = { static_cast<T>(a.A0[3 * f]), static_cast<T>(a.A0[3 * f + 1]), static_cast<T>(a.A0[3 * f + 2]) };
+    const bool directed = a.load[4 * f] != 0.0;
+    T cA[MAX_FGP][3];
+    for (int g = 0; g < ngp; g++) {
+        const T* dN = a.t_dN + (static_cast<size_t>(t) * MAX_FGP + g) * NEN * 3;
+        T A[9] = { 0, 0, 0, 0, 0, 0, 0, 0, 0 };
+        for (int q = 0; q < NEN; q++)
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+#pragma unroll
+                for (int k = 0; k < 3; k++) A[3 * i + k] += uu[q][i] * dN[3 * q + k];
+        const T* Ji = a.J0inv + (static_cast<size_t>(f) * MAX_FGP + g) * 9;
+        T H[9];
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) H[3 * i + j] = A[3 * i] * Ji[j] + A[3 * i + 1] * Ji[3 + j] + A[3 * i + 2] * Ji[6 + j];
+        Kin<T> k;
+        kinematics(H, k);
+        // cof F A0 = (I + B) A0
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+            cA[g][i] = A0[i] + k.B[3 * i] * A0[0] + k.B[3 * i + 1] * A0[1] + k.B[3 * i + 2] * A0[2];
+        if (directed) {
+            const T nrm = sqrt(cA[g][0] * cA[g][0] + cA[g][1] * cA[g][1] + cA[g][2] * cA[g][2]);
+            cA[g][0] = nrm;
+        }
+    }
+    const double* L = a.load + 4 * f;
+    for (int q = 0; q < NEN; q++) {
+        if (node[q] >= a.n_free) continue;
+        T v0 = 0, v1 = 0, v2 = 0;
+        for (int g = 0; g < ngp; g++) {
+            const T wn = a.t_w[t * MAX_FGP + g] * a.t_N[(static_cast<size_t>(t) * MAX_FGP + g) * NEN + q];
+            if (directed) {
+                v0 += wn * cA[g][0];
+            } else {
+                v0 += wn * cA[g][0];
+                v1 += wn * cA[g][1];
+                v2 += wn * cA[g][2];
+            }
+        }
+        double f0, f1, f2;
+        if (directed) {
+            f0 = L[1] * static_cast<double>(v0);
+            f1 = L[2] * static_cast<double>(v0);
+            f2 = L[3] * static_cast<double>(v0);
+        } else {
+            f0 = L[1] * static_cast<double>(v0);
+            f1 = L[1] * static_cast<double>(v1);
+            f2 = L[1] * static_cast<double>(v2);
+        }
+        atomicAdd(a.r + 3 * node[q], -f0);
+        atomicAdd(a.r + 3 * node[q] + 1, -f1);
+        atomicAdd(a.r + 3 * node[q] + 2, -f2);
+    }
+}
+
+template <int NEN, int NGP, typename T>
+void launch_elem(const DevBlock& b, const MatParams<T>* mats, const T* vol, const T* J0, const T* dN, const T* gw,
+    int n_free, const double* u, double* r, cudaStream_t st)
+{
+    constexpr int EPB = (kBlock / NGP) > 0 ? (kBlock / NGP) : 1;
+    ElemArgs<T> a { b.n, n_free, b.conn, b.mat, vol, J0, dN, gw, mats, u, r };
+    const int grid = (b.n + EPB - 1) / EPB;
+    k_elem_residual<NEN, NGP, T><<<grid, kBlock, 0, st>>>(a);
+}
+
+template <typename T>
+void dispatch_elem(const DevBlock& b, const MatParams<T>* mats, const T* vol, const T* J0, const T* dN, const T* gw,
+    int n_free, const double* u, double* r, cudaStream_t st)
+{
+#define CASE(NEN, NGP)                                                            \
+    if (b.nen == NEN && b.ngp == NGP) {                                           \
+        launch_elem<NEN, NGP, T>(b, mats, vol, J0, dN, gw, n_free, u, r, st);     \
+        return;                                                                   \
+    }
+    CASE(4, 1)
+    CASE(10, 4)
+    CASE(10, 1)
+    CASE(8, 8)
+    CASE(8, 1)
+    CASE(20, 27)
+    CASE(20, 8)
+#undef CASE
+}
+
+template <typename T>
+void dispatch_face(const DevFaces& f, const T* J0, const T* tw, const T* tN, const T* tdN, int n_free, const double* u,
+    double* r, cudaStream_t st)
+{
+    FaceArgs<T> a { f.n, n_free, f.conn, f.table, f.A0, J0, f.load, f.t_ngp, tw, tN, tdN, u, r };
+    const int grid = (f.n + kBlock - 1) / kBlock;
+    switch (f.nen) {
+    case 4: k_face_residual<4, T><<<grid, kBlock, 0, st>>>(a); break;
+    case 8: k_face_residual<8, T><<<grid, kBlock, 0, st>>>(a); break;
+    case 10: k_face_residual<10, T><<<grid, kBlock, 0, st>>>(a); break;
+    case 20: k_face_residual<20, T><<<grid, kBlock, 0, st>>>(a); break;
+    }
+}
+
+}  // namespace
+
+efem_status launch_residual(Model& m, const double* d_u, double* d_r)
+{
+    const size_t n = 3 * static_cast<size_t>(m.n_free);
+    if (n == 0) return EFEM_OK;
+    EFEM_CUDA(cudaMemcpyAsync(d_r, m.d_fext, n * sizeof(double), cudaMemcpyDeviceToDevice, m.stream));
+    // r = -f_ext
+    extern void launch_scale(double* v, double s, size_t n, cudaStream_t st);
+    launch_scale(d_r, -1.0, n, m.stream);
+    const bool mixed = m.opts.precision == EFEM_MIXED;
+    for (auto& b : m.blocks) {
+        if (b.n == 0) continue;
+        if (mixed)
+            dispatch_elem<float>(b, m.d_mats_f, b.vol_f, b.J0inv_f, b.dN_f, b.gw_f, m.n_free, d_u, d_r, m.stream);
+        else
+            dispatch_elem<double>(b, m.d_mats, b.vol, b.J0inv, b.dN, b.gw, m.n_free, d_u, d_r, m.stream);
+    }
+    for (auto& f : m.faces) {
+        if (f.n == 0) continue;
+        if (mixed)
+            dispatch_face<float>(f, f.J0inv_f, f.t_w_f, f.t_N_f, f.t_dN_f, m.n_free, d_u, d_r, m.stream);
+        else
+            dispatch_face<double>(f, f.J0inv, f.t_w, f.t_N, f.t_dN, m.n_free, d_u, d_r, m.stream);
+    }
+    EFEM_CUDA(cudaGetLastError());
+    return EFEM_OK;
+}
+
+}  // namespace efem

@@ -1,0 +1,179 @@
+/*
+ * efem_gpu.h -- C ABI of the B200 (sm_100a) implementation of EFEM's hot path:
+ * the Total-Lagrangian hyperelastic residual, the L-BFGS solve preconditioned
+ * by the approximate-Jacobian Cholesky factor, and its adjoint.
+ *
+ * Plain C types only; every call returns an efem_status (0 = success) and
+ * never throws.  A model owns all of its device memory and one CUDA stream.
+ * Calls on different models may run from different threads; calls on one
+ * model must not overlap.
+ *
+ * Vectors u, r, ... are in the reference's free-DOF order: entry 3*id + c,
+ * id = the node's position among the non-fixed nodes in node-file order
+ * (src/fe/Constraint.cpp:61-72).  By default they are host pointers; with
+ * efem_options.device_ptrs = 1 they are device pointers on the model's GPU.
+ */
+#ifndef EFEM_GPU_H
+#define EFEM_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    EFEM_OK = 0,
+    EFEM_ERR_ARG = 1,          /* bad argument / handle */
+    EFEM_ERR_CONFIG = 2,       /* JSON config unreadable or invalid (reference: std::terminate, src/io/IO.cpp:47-59) */
+    EFEM_ERR_MESH = 3,         /* mesh / constraint file missing or malformed */
+    EFEM_ERR_CUDA = 4,         /* a CUDA call failed; efem_last_error() has the text */
+    EFEM_ERR_NAN = 5,          /* solution or residual not finite (reference: Integrator.cpp:28-34) */
+    EFEM_ERR_TIMEOUT = 6,      /* a bounded device-side wait ran out */
+    EFEM_ERR_UNSUPPORTED = 7,  /* a feature outside this library's scope */
+    EFEM_ERR_NO_DEVICE = 8,    /* no CUDA device: the library has no CPU fallback */
+    EFEM_ERR_FACE = 9          /* a pressure face does not lie on exactly one element */
+} efem_status;
+
+/* element material models, src/material/Material.h:9-16 */
+typedef enum { EFEM_NEO_HOOKEAN = 0, EFEM_MOONEY_RIVLIN = 1, EFEM_YEOH = 2 } efem_material_type;
+
+typedef struct {
+    int type;      /* efem_material_type */
+    int id;        /* material id matched against each element's id (-1 = default) */
+    double C10, C01, C20, C30, D1, density;
+} efem_material;
+
+/* One block of elements that share a node count (4 = C3D4, 8 = C3D8,
+ * 10 = C3D10, 20 = C3D20).  conn is row-major (n_elem, nen), 0-based. */
+typedef struct {
+    int nen;
+    int n_elem;
+    const int* conn;
+    const int* material_id;  /* n_elem ids, or NULL for -1 */
+} efem_element_block;
+
+typedef struct {
+    int n_nodes;
+    const double* X;         /* (n_nodes, 3) reference coordinates */
+    int n_blocks;
+    const efem_element_block* blocks;
+} efem_mesh_desc;
+
+typedef enum { EFEM_LOAD_FIX = 0, EFEM_LOAD_FORCE = 1, EFEM_LOAD_PRESSURE = 2, EFEM_LOAD_DPRESSURE = 3 } efem_load_type;
+
+/* A constraint as the reference's "constraint" JSON entries describe it
+ * (src/fe/ExternalConstraint.cpp:13-247).
+ *   FIX:       nodes[n]                      (0-based)
+ *   FORCE:     nodes[n], value[3]            (each listed occurrence adds value)
+ *   PRESSURE:  faces in CSR form, value[0] = follower pressure (> 0)
+ *   DPRESSURE: faces in CSR form, value[0..2] = directed pressure vector  */
+typedef struct {
+    int type;                /* efem_load_type */
+    int n;                   /* nodes (FIX, FORCE) or faces (PRESSURE, DPRESSURE) */
+    const int* nodes;        /* FIX / FORCE node list, or the concatenated face nodes */
+    const int* face_ptr;     /* n+1 offsets into nodes, PRESSURE / DPRESSURE only */
+    double value[3];
+} efem_load_desc;
+
+typedef enum { EFEM_FP64 = 0, EFEM_MIXED = 1 } efem_precision;
+
+typedef struct {
+    int precision;            /* efem_precision: element kernels in FP64 or FP32 */
+    int integration;          /* 0 full, 1 reduced (C3D4R/C3D10R/C3D8R/C3D20R rules) */
+    int nl_solver;            /* 0 "lbfgs_ah": H0 = approximate-Jacobian Cholesky;
+                                 1 "lbfgs": H0 = I/theta  (src/io/Config.cpp:25-33) */
+    int m;                    /* L-BFGS history length (src/simulation/nlsolver/Param.h:102) */
+    int max_iterations;       /* 0 = unlimited ("max_solver_iters"; "max_optim_iters" is accepted too) */
+    int max_linesearch;       /* trials per line search ("max_line_search") */
+    double residual_criterion;/* ||r||_inf <= eps or <= eps*||u||_inf ends the solve */
+    double dx_criterion;      /* reported flag only, as in src/simulation/Integrator.cpp:36 */
+    int device_ptrs;          /* 1: vector arguments are device pointers */
+    int deterministic;        /* 1: element scatter by ordered gather (bitwise repeatable) */
+    int device;               /* CUDA ordinal; -1 = current device */
+} efem_options;
+
+enum {
+    EFEM_SOLVE_CONVERGED = 1,      /* residual test passed */
+    EFEM_SOLVE_PRECOND_FALLBACK = 2,/* factorisation failed; H0 = I/theta used (LBFGS.h:76-79) */
+    EFEM_SOLVE_DX_CONVERGED = 4,   /* ||u||_inf < dx_criterion (the reference's return flag) */
+    EFEM_SOLVE_MAX_ITERS = 8
+};
+
+typedef struct {
+    int niter;                /* L-BFGS iterations (LBFGS.h:96-174 return value) */
+    int n_residual_evals;     /* SoftObjective::r_evalutes */
+    int n_jacobian_evals;     /* SoftObjective::j_evalutes */
+    int flags;                /* EFEM_SOLVE_* bits */
+    double u_inf, r_inf;      /* final ||u||_inf and ||r||_inf (Integrator.cpp:37-40) */
+    double ms_total, ms_factor, ms_residual, ms_precond;  /* device-timed phases */
+} efem_solve_info;
+
+typedef struct {
+    int n_nodes, n_free_nodes, n_dof;
+    int n_elements, n_elements_skipped;   /* skipped: undefined material id */
+    int n_faces, n_force_nodes;
+    int n_blocks;
+    long long factor_nnz;                 /* scalar Cholesky factor entries (0 before the first solve) */
+    int n_supernodes, n_levels;
+    double factor_gflop;
+} efem_model_info;
+
+/* --------------------------------------------------------------- lifetime */
+
+/* Fill *o with the reference's defaults (Config.h:18-48, Param.h:92-103). */
+efem_status efem_default_options(efem_options* o);
+
+/* Replaces `EFEM -f cfg.json` set-up: Simulator::initial(path)
+ * (src/simulation/Simulator.cpp:6-18) -> Config, Model, Constraint.
+ * Same keys and files; paths relative to the config file's directory. */
+efem_status efem_model_create_from_json(const char* cfg_path, void** model);
+
+/* Array form of the same set-up (ElementConstraintConfig / ExternalConstraintConfig,
+ * src/fe/ElementConstraint.cpp:11-67, src/fe/ExternalConstraint.cpp:13-247). */
+efem_status efem_model_create(const efem_mesh_desc* mesh, const efem_material* materials, int n_materials,
+    const efem_load_desc* loads, int n_loads, const efem_options* options, void** model);
+
+efem_status efem_model_destroy(void* model);
+
+efem_status efem_get_options(void* model, efem_options* o);
+efem_status efem_set_options(void* model, const efem_options* o);
+efem_status efem_get_model_info(void* model, efem_model_info* info);
+
+/* node_of_dof[id] = node index of free node id (length n_free_nodes). */
+efem_status efem_dof_map(void* model, int* node_of_dof);
+
+/* --------------------------------------------------------------- hot path */
+
+/* r = R(u): replaces SoftObjective::residual -> Constraint::assignDx +
+ * Constraint::getResidual (src/simulation/Integrator.cpp:49-55,
+ * src/fe/Constraint.cpp:93-126): element internal force, follower / directed
+ * pressure and nodal forces. */
+efem_status efem_residual(void* model, const double* u, double* r);
+
+/* Scalar approximate Jacobian L (K~ = L (x) I3) in CSR over free nodes:
+ * replaces Constraint::getJacobi triplets (src/fe/ElementConstraint.cpp:164-205,
+ * src/simulation/Integrator.cpp:57-70).  Call with vals == NULL to get nnz in
+ * *nnz; then with arrays of n_free_nodes+1 / nnz / nnz entries. */
+efem_status efem_approx_jacobian_csr(void* model, long long* nnz, int* rowptr, int* colidx, double* vals);
+
+/* Apply H0 = K~^{-1} (the Cholesky-preconditioner solve, LBFGSMat.h:119-120)
+ * to v in place.  Factorises on first use. */
+efem_status efem_precond_apply(void* model, double* v);
+
+/* Solve R(u) = 0 from u_inout: replaces Integrator::integral
+ * (src/simulation/Integrator.cpp:22-42) -> LBFGSSolver::solve (LBFGS.h:96-174). */
+efem_status efem_solve(void* model, double* u_inout, efem_solve_info* info);
+
+/* --------------------------------------------------------------- diagnostics */
+
+/* Copy the last error message of this thread into buf. */
+efem_status efem_last_error(char* buf, size_t len);
+
+/* Library version string. */
+const char* efem_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
