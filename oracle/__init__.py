@@ -176,6 +176,7 @@ def lib():
         L.orc_residual.argtypes = [ctypes.c_void_p, dp, dp]
         L.orc_approx_jacobian_dense.argtypes = [ctypes.c_void_p, dp]
         L.orc_solve.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Params), dp, ctypes.POINTER(_Info)]
+        L.orc_precond_apply.argtypes = [ctypes.c_void_p, dp]
         L.orc_piola.argtypes = [ctypes.c_int, dp, ctypes.c_int, dp, dp]
         L.orc_elasticity_coeff.restype = ctypes.c_double
         L.orc_elasticity_coeff.argtypes = [ctypes.c_int, dp]
@@ -244,6 +245,12 @@ class Oracle:
         lib().orc_solve(self.h, ctypes.byref(p), _p(u), ctypes.byref(info))
         return u, {"niter": info.niter, "r_evals": info.r_evals, "precond_ok": info.precond_ok,
                    "u_inf": info.u_inf, "r_inf": info.r_inf}
+
+    def precond_apply(self, v):
+        """H0 v with H0 the inverse approximate Jacobian; None if L is not SPD."""
+        v = np.array(v, dtype=np.float64)
+        ok = lib().orc_precond_apply(self.h, _p(v))
+        return v if ok else None
 
     def __del__(self):
         if getattr(self, "h", None):

@@ -988,6 +988,20 @@ static double inf_norm(const double* a, int n)
     return s;
 }
 
+/* H0 v = (L (x) I3)^{-1} v; returns 0 if L is not positive definite. */
+int orc_precond_apply(orc_model* m, double* v)
+{
+    skyline* sky = sky_build(m);
+    int ok = sky->n > 0 && sky_factor(sky);
+    if (ok) {
+        double* work = malloc(sizeof(double) * (m->n_free + 1));
+        sky_solve(sky, v, work);
+        free(work);
+    }
+    sky_free(sky);
+    return ok;
+}
+
 int orc_solve(orc_model* m, const orc_params* p, double* x, orc_info* info)
 {
     int n = 3 * m->n_free, mm = p->m;

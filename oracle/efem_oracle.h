@@ -53,6 +53,8 @@ void orc_residual(orc_model* m, const double* u, double* r);
  * reference's matrix is L (x) I3. */
 void orc_approx_jacobian_dense(orc_model* m, double* L);
 int orc_solve(orc_model* m, const orc_params* p, double* u, orc_info* info);
+/* v <- (L (x) I3)^{-1} v (the preconditioner solve); 0 if L is not SPD. */
+int orc_precond_apply(orc_model* m, double* v);
 /* First Piola-Kirchhoff stress of one material at n column-major 3x3 F. */
 void orc_piola(int type, const double* C, int n, const double* F, double* P);
 double orc_elasticity_coeff(int type, const double* C);

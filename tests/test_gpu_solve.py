@@ -1,6 +1,11 @@
-"""CUDA L-BFGS solve against the reference's converged displacements."""
-import json
+"""CUDA L-BFGS solve against the oracle and the reference's converged displacements.
 
+With the identity initial inverse Hessian (nl_solver "lbfgs") the problems are
+ill-conditioned: two runs that differ only in rounding stop at different points
+inside the ||r||_inf <= 1e-6 ball, up to ~1e-4 apart (relative L2).  Parity of
+the algorithm is therefore checked by converging both sides to 1e-10 (then the
+solutions must agree to 1e-7), and the reference tolerance run is checked by
+its true residual, evaluated independently by the oracle."""
 import numpy as np
 import pytest
 
@@ -13,13 +18,69 @@ CASES = golden_files()
 
 
 @pytest.mark.parametrize("path", CASES, ids=lambda p: p.split("/")[-1][5:-4])
-def test_solve_identity_h0_matches_oracle(path, tmp_path):
-    """nl_solver "lbfgs" (H0 = I/theta): GPU vs the oracle's identical algorithm."""
-    cfg, d = write_golden_case(path, tmp_path, nl_solver="lbfgs", max_solver_iters=4000)
+def test_solve_identity_h0_tight_matches_oracle(path, tmp_path):
+    cfg, d = write_golden_case(path, tmp_path, nl_solver="lbfgs", max_solver_iters=20000, residual_criterion=1e-10)
     m = api.Model.from_json(cfg)
     u, info = m.solve()
     o = oracle.Oracle(oracle.read_case(cfg))
     uo, io = o.solve()
-    assert info["flags"] & api.SOLVE_CONVERGED
+    assert info["flags"] & api.SOLVE_CONVERGED, info
+    err = np.linalg.norm(u - uo) / np.linalg.norm(uo)
+    assert err <= 1e-7, (err, info["niter"], io["niter"])
+
+
+@pytest.mark.parametrize("path", CASES[::3], ids=lambda p: p.split("/")[-1][5:-4])
+def test_solve_identity_h0_reference_tolerance(path, tmp_path):
+    cfg, d = write_golden_case(path, tmp_path, nl_solver="lbfgs", max_solver_iters=20000)
+    m = api.Model.from_json(cfg)
+    u, info = m.solve()
+    assert info["flags"] & api.SOLVE_CONVERGED and info["r_inf"] <= 1e-6
+    o = oracle.Oracle(oracle.read_case(cfg))
+    assert np.abs(o.residual(u)).max() <= 1.01e-6
+    # against the reference's preconditioned solution of the same problem
+    ref = d["u_solve"]
+    assert np.linalg.norm(u - ref) <= 1e-3 * np.linalg.norm(ref)
+
+
+@pytest.mark.parametrize("path", CASES, ids=lambda p: p.split("/")[-1][5:-4])
+def test_precond_apply_matches_oracle(path, tmp_path):
+    """H0 v through the GPU supernodal factor vs the oracle's envelope factor."""
+    cfg, d = write_golden_case(path, tmp_path)
+    m = api.Model.from_json(cfg)
+    o = oracle.Oracle(oracle.read_case(cfg))
+    v = d["v"]
+    hv = m.precond_apply(v)
+    ho = o.precond_apply(v)
+    assert np.linalg.norm(hv - ho) <= 1e-10 * np.linalg.norm(ho)
+
+
+@pytest.mark.parametrize("path", CASES, ids=lambda p: p.split("/")[-1][5:-4])
+def test_solve_matches_reference(path, tmp_path):
+    """The reference's configuration (lbfgs_ah, residual 1e-6): nodal
+    displacements within 1e-6 relative L2 of the reference's own solve."""
+    cfg, d = write_golden_case(path, tmp_path)
+    m = api.Model.from_json(cfg)
+    u, info = m.solve()
+    assert info["flags"] & api.SOLVE_CONVERGED and not info["flags"] & api.SOLVE_PRECOND_FALLBACK
     assert info["r_inf"] <= 1e-6
-    assert np.linalg.norm(u - uo) <= 1e-6 * np.linalg.norm(uo)
+    ref = d["u_solve"]
+    assert np.linalg.norm(u - ref) <= 1e-6 * np.linalg.norm(ref)
+
+
+def test_cantilever_c3d4_pressure_matches_reference(tmp_path):
+    path = golden_files("cantilever_c3d4_pressure.npz")[0]
+    cfg, d = write_golden_case(path, tmp_path)
+    m = api.Model.from_json(cfg)
+    u, info = m.solve()
+    ref = d["u_solve"]
+    assert info["r_inf"] <= 1e-6
+    assert np.linalg.norm(u - ref) <= 1e-6 * np.linalg.norm(ref)
+
+
+def test_c3d20_reduced_solve_matches_reference(tmp_path):
+    for path in golden_files("case_C3D20_*.npz"):
+        cfg, d = write_golden_case(path, tmp_path / path.split("/")[-1][:-4], "reduced")
+        m = api.Model.from_json(cfg)
+        u, info = m.solve()
+        ref = d["u_solve_reduced"]
+        assert np.linalg.norm(u - ref) <= 1e-6 * np.linalg.norm(ref)
