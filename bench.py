@@ -1,0 +1,285 @@
+"""Benchmark: time-to-converge and L-BFGS iterations/s of the hyperelastic solve.
+
+Workload (one step = one complete solve from u = 0 to ||r||_inf <= 1e-6, the
+reference's JSON-driven call): the C3D8 beam, 0.2 x 0.04 x 0.04 m on an
+80 x 16 x 16 hexahedral grid (20 480 elements, 23 409 nodes, 69 360 DOF),
+Mooney-Rivlin C10 = 80 kPa, C01 = 20 kPa, D1 = 1e-6, x = 0 fixed, nodal force
+[0, 0, -0.5] N on each of the 289 end-face nodes; FP64 element kernels (or the
+mixed FP32 path with --precision mixed).  Synthetic, seeded mesh in the
+reference's own file formats (efem_b200.meshgen).
+
+Each timed step includes the per-solve numeric factorisation of the
+approximate Jacobian (as LBFGSSolver::solve does once per solve); the mesh
+set-up (element tables, symbolic analysis of the factor) happens once, before
+the warm-up steps.
+
+--gpus N: N independent replicas (one process per GPU, the solve does not
+shard); value = iterations of all ranks / max-over-ranks time.
+--impl reference: the reference's own CPU solver (compiled from its sources in
+oracle/_ref), timed on the host cores on bounded samples of the same solve.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "L-BFGS iters/s (time-to-converge solve, C3D8 MR beam 20480 el)"
+UNIT = "iters/s"
+
+
+def workload_case():
+    from efem_b200 import meshgen as mg
+    return mg.cantilever_c3d8_force()
+
+
+def config_block(precision, n):
+    return {"workload": "C3D8 Mooney-Rivlin cantilever, 80x16x16 hex (20480 el, 69360 DOF), tip force, "
+                        "residual 1e-6, one full solve per step",
+            "precision": precision, "elements": 20480, "dof": 69360, "replicas": n,
+            "parallelism": f"replicas{n}", "l2": "flushed (256 MB write) before every step"}
+
+
+# --------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for ln in open(self.path):
+                p = [x.strip() for x in ln.split(",")]
+                if len(p) >= 9 and p[1].isdigit():
+                    rows.append(p)
+        except Exception:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = np.array([float(r[1]) for r in rows])
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(rows[0][2]), "reasons": reasons,
+                "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())}
+
+
+# --------------------------------------------------------------------------- reference arm
+def reference_sample(steps, warmup, ipstep=2):
+    """The reference's own solver on bounded samples of the workload: one-time
+    factorisation, then `warmup` + `steps` steps of `ipstep` L-BFGS iterations.
+    Returns (iters/s over the timed steps, details)."""
+    ref = os.path.join(ROOT, "oracle", "_ref", "efem_ref")
+    if not os.path.exists(ref):
+        return None, {"why": "oracle/_ref/efem_ref is not built"}
+    case = workload_case()
+    with tempfile.TemporaryDirectory() as td:
+        cfg = case.write(td)
+        t0 = time.time()
+        res = subprocess.run([ref, "bench", cfg, str(ipstep), str(warmup), str(steps)], capture_output=True,
+                             text=True, timeout=3600)
+        wall = time.time() - t0
+    if res.returncode != 0:
+        return None, {"why": res.stderr[-300:]}
+    meta = json.loads(res.stdout.strip().splitlines()[-1])
+    st = meta["step_s"]
+    if not st:
+        return None, {"why": "reference converged inside the warm-up"}
+    ips = ipstep * len(st) / sum(st)
+    meta.update(wall_s=wall)
+    return ips, meta
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    ips, meta = reference_sample(args.steps, args.warmup)
+    if ips is None:
+        print(json.dumps({"impl": "reference", "unavailable": meta.get("why", "reference failed")}))
+        return
+    cores = 1
+    line = {"impl": "reference", "metric": METRIC, "value": ips, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * meta["iters_per_step"] / ips,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_block("fp64", 1),
+            "cpu_baseline": {"value": ips, "unit": UNIT, "cores": cores, "kind": "reference",
+                             "sample": f"reference solver (oracle/_ref, unmodified sources, single-threaded as built "
+                                       f"upstream) on the same C3D8 beam: one-time approximate-Jacobian "
+                                       f"factorisation ({meta['factor_s']:.1f} s, outside the timed steps), then "
+                                       f"{args.steps} timed steps of {meta['iters_per_step']} L-BFGS iterations"},
+            "e2e": {"value": ips, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "reference_factor_s": meta["factor_s"]}
+    print(json.dumps(line))
+
+
+# --------------------------------------------------------------------------- GPU arm
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="efem_b200", choices=["efem_b200", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+    from efem_b200 import api
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    case = workload_case()
+    opts = api.default_options()
+    opts.precision = api.MIXED if args.precision == "mixed" else api.FP64
+    opts.device = local
+    t_setup = time.time()
+    model = api.Model.from_case(case, opts)
+    stream = torch.cuda.current_stream()
+    api.check(api.lib().efem_set_stream(model.h, api.ctypes.c_void_p(stream.cuda_stream)))
+    model.set_options(device_ptrs=1)
+    u = torch.zeros(model.n_dof, dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def one_solve():
+        u.zero_()
+        _, info = model.solve(u)
+        return info
+
+    first = one_solve()  # also builds the symbolic factor analysis
+    setup_s = time.time() - t_setup
+    for _ in range(args.warmup):
+        one_solve()
+    barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    infos = []
+    with ClockSampler(local) as clocks:
+        barrier()
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            ev[k][0].record(stream)
+            infos.append(one_solve())
+            ev[k][1].record(stream)
+        barrier()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = sum(step_ms)
+    iters = sum(i["niter"] for i in infos)
+    t = torch.tensor([total_ms, float(iters)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        tm = t.clone()
+        dist.all_reduce(tm[:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
+        total_ms_max, iters_all = float(tm[0]), float(t[1])
+    else:
+        total_ms_max, iters_all = total_ms, float(iters)
+    value = iters_all / (total_ms_max / 1000.0)
+
+    # ---- end to end through the C ABI with host buffers (pinned host input / output)
+    model.set_options(device_ptrs=0)
+    u_host = np.zeros(model.n_dof)
+    e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(max(1, args.steps // 2))]
+    e2e_iters = 0
+    barrier()
+    for a, b in e2e_ev:
+        u_host[:] = 0.0
+        a.record(stream)
+        _, info = model.solve(u_host)
+        b.record(stream)
+        e2e_iters += info["niter"]
+    barrier()
+    e2e_ms = sum(a.elapsed_time(b) for a, b in e2e_ev)
+    e2e_value = e2e_iters / (e2e_ms / 1000.0)
+    if world > 1:
+        te = torch.tensor([e2e_ms, float(e2e_iters)], dtype=torch.float64, device="cuda")
+        dist.all_reduce(te[:1], op=dist.ReduceOp.MAX)
+        ti = te[1:].clone()
+        dist.all_reduce(ti, op=dist.ReduceOp.SUM)
+        e2e_value = float(ti[0]) / (float(te[0]) / 1000.0)
+
+    # ---- roofline of the dominant kernel, measured live on the model's stream
+    from efem_b200 import profiling
+    roof, launches = profiling.roofline_report(model, case, infos, stream)
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "data": "synthetic (seeded structured mesh in the reference's input format)",
+            "config": config_block(args.precision, world),
+            "time_to_converge_ms": total_ms_max / args.steps,
+            "iterations_per_solve": iters / args.steps, "residual_evals_per_solve": sum(i["n_residual_evals"] for i in infos) / args.steps,
+            "final_r_inf": infos[-1]["r_inf"], "u_inf": infos[-1]["u_inf"],
+            "factor_ms": float(np.mean([i["ms_factor"] for i in infos])),
+            "setup_s": setup_s,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * model.n_dof,
+                    "d2h_bytes_per_step": 8 * model.n_dof},
+            "gpu_launches": int(launches * args.steps),
+            "roofline": roof,
+            "clocks": clocks.summary()}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        ips, meta = reference_sample(steps=3, warmup=1)
+        if ips is not None:
+            line["cpu_baseline"] = {"value": ips, "unit": UNIT, "cores": 1, "kind": "reference",
+                                    "sample": f"reference solver (oracle/_ref) on the same beam: approximate-Jacobian "
+                                              f"factorisation once ({meta['factor_s']:.1f} s, excluded), then 3 timed "
+                                              f"steps of {meta['iters_per_step']} L-BFGS iterations; single-threaded"}
+    if rank == 0:
+        print(json.dumps(line))
+    model.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

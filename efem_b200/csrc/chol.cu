@@ -35,8 +35,9 @@ namespace efem {
 
 struct Precond {
     Symbolic S;
-    bool ready = false;
-    bool ok = false;
+    bool ready = false;     // symbolic analysis done and uploaded
+    bool factored = false;  // numeric factor present
+    bool ok = false;        // factor is positive definite
     double ms_factor = 0;
     int max_r = 0, max_c = 0;
     std::vector<int> lev_max_r, lev_max_c;
@@ -385,13 +386,16 @@ void precond_info(const Model& m, efem_model_info* info)
     info->factor_gflop = S.flops * 1e-9;
 }
 
-efem_status precond_setup(Model& m, int* ok, double* ms_factor)
+static efem_status precond_factor(Model& m, int* ok, double* ms_factor);
+
+efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
 {
-    if (m.precond && m.precond->ready) {
+    if (m.precond && m.precond->ready && !refactor) {
         *ok = m.precond->ok;
         *ms_factor = 0.0;
         return EFEM_OK;
     }
+    if (m.precond && m.precond->ready) return precond_factor(m, ok, ms_factor);
     free_precond(m);
     m.precond = new Precond();
     Precond& P = *m.precond;
@@ -446,7 +450,19 @@ efem_status precond_setup(Model& m, int* ok, double* ms_factor)
     if ((st = dev_alloc(&P.d_upd, static_cast<size_t>(std::max<long long>(S.upd_size, 1)))) != EFEM_OK) return st;
     if ((st = dev_alloc(&P.d_w, 3 * static_cast<size_t>(std::max(S.n, 1)))) != EFEM_OK) return st;
     if ((st = dev_alloc(&P.d_fail, 1)) != EFEM_OK) return st;
-    // numeric factorisation
+    EFEM_CUDA(cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    EFEM_CUDA(cudaFuncSetAttribute(k_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    P.ready = true;  // analysed; the numeric factor follows
+    return precond_factor(m, ok, ms_factor);
+}
+
+// Numeric factorisation (every solve, like LBFGSSolver::updateApproxJacobi):
+// scatter L into the fronts, factor level by level, invert the diagonal blocks.
+static efem_status precond_factor(Model& m, int* ok, double* ms_factor)
+{
+    Precond& P = *m.precond;
+    const Symbolic& S = P.S;
+    const int nlev = static_cast<int>(S.level_ptr.size()) - 1;
     cudaEvent_t e0, e1;
     EFEM_CUDA(cudaEventCreate(&e0));
     EFEM_CUDA(cudaEventCreate(&e1));
@@ -473,12 +489,7 @@ efem_status precond_setup(Model& m, int* ok, double* ms_factor)
     cudaEventDestroy(e1);
     P.ms_factor = ms;
     P.ok = fail == 0;
-    P.ready = true;
-    dev_free(P.d_vals);
-    dev_free(P.d_a_pos);
-    dev_free(P.d_a_src);
-    EFEM_CUDA(cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    EFEM_CUDA(cudaFuncSetAttribute(k_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    P.factored = true;
     *ok = P.ok;
     *ms_factor = ms;
     return EFEM_OK;
@@ -486,7 +497,7 @@ efem_status precond_setup(Model& m, int* ok, double* ms_factor)
 
 efem_status precond_apply(Model& m, double* d_v)
 {
-    if (!m.precond || !m.precond->ready || !m.precond->ok) {
+    if (!m.precond || !m.precond->factored || !m.precond->ok) {
         set_error("preconditioner not factored");
         return EFEM_ERR_ARG;
     }

@@ -108,6 +108,7 @@ struct Model {
     efem_options opts;
     int device = 0;
     cudaStream_t stream = nullptr;
+    bool own_stream = false;          // false: the caller's stream (efem_set_stream)
 
     int n_nodes = 0, n_free = 0, n_elements = 0, n_skipped = 0, n_force_nodes = 0;
     std::vector<int> node_of_dnode;   // dnode -> original node
@@ -193,7 +194,7 @@ void free_solver(Model& m);
 // ------------------------------------------------------------------ preconditioner (chol.cu)
 // Build (once) the scalar approximate Jacobian L and its Cholesky factor.
 // Returns EFEM_OK with *ok = 0 when L is not positive definite.
-efem_status precond_setup(Model& m, int* ok, double* ms_factor);
+efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor);
 // v <- (L (x) I3)^{-1} v in place on the device (v: 3*n_free interleaved).
 efem_status precond_apply(Model& m, double* d_v);
 void free_precond(Model& m);

@@ -146,7 +146,7 @@ Model::~Model()
     dev_free(d_fext);
     dev_free(d_u);
     dev_free(d_r);
-    if (stream) cudaStreamDestroy(stream);
+    if (stream && own_stream) cudaStreamDestroy(stream);
 }
 
 // Host set-up shared by both creation paths.
@@ -499,7 +499,10 @@ efem_status ensure_device(Model& m)
         m.device = d;
     }
     EFEM_CUDA(cudaSetDevice(m.device));
-    if (!m.stream) EFEM_CUDA(cudaStreamCreateWithFlags(&m.stream, cudaStreamNonBlocking));
+    if (!m.stream) {
+        EFEM_CUDA(cudaStreamCreateWithFlags(&m.stream, cudaStreamNonBlocking));
+        m.own_stream = true;
+    }
     efem_status s;
 #define UP(ptr, vec)                          \
     if (!(ptr)) {                             \
@@ -875,7 +878,7 @@ efem_status efem_precond_apply(void* model, double* v)
     if (s != EFEM_OK) return s;
     int ok = 0;
     double ms = 0;
-    s = efem::precond_setup(*m, &ok, &ms);
+    s = efem::precond_setup(*m, false, &ok, &ms);
     if (s != EFEM_OK) return s;
     if (!ok) {
         efem::set_error("approximate Jacobian is not positive definite");
@@ -917,6 +920,25 @@ efem_status efem_solve(void* model, double* u_inout, efem_solve_info* info)
         EFEM_CUDA(cudaStreamSynchronize(m->stream));
     }
     return s;
+}
+
+efem_status efem_set_stream(void* model, void* cuda_stream)
+{
+    Model* m;
+    efem_status s = guard(model, &m);
+    if (s != EFEM_OK) return s;
+    s = efem::ensure_device(*m);
+    if (s != EFEM_OK) return s;
+    EFEM_CUDA(cudaStreamSynchronize(m->stream));
+    if (m->own_stream) cudaStreamDestroy(m->stream);
+    if (cuda_stream) {
+        m->stream = static_cast<cudaStream_t>(cuda_stream);
+        m->own_stream = false;
+    } else {
+        EFEM_CUDA(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
+        m->own_stream = true;
+    }
+    return EFEM_OK;
 }
 
 efem_status efem_last_error(char* buf, size_t len)

@@ -165,6 +165,11 @@ efem_status efem_precond_apply(void* model, double* v);
  * (src/simulation/Integrator.cpp:22-42) -> LBFGSSolver::solve (LBFGS.h:96-174). */
 efem_status efem_solve(void* model, double* u_inout, efem_solve_info* info);
 
+/* Run the model's device work on the caller's CUDA stream (a cudaStream_t);
+ * NULL gives the model its own stream again.  The reference has no streams;
+ * this lets a caller order the library's kernels with its own work. */
+efem_status efem_set_stream(void* model, void* cuda_stream);
+
 /* --------------------------------------------------------------- diagnostics */
 
 /* Copy the last error message of this thread into buf. */

@@ -14,6 +14,11 @@
 //                                                          src/simulation/nlsolver/LBFGS.h:96-174)
 //   efem_ref info     <cfg.json> <dofmap_out.i32>
 //       free-DOF numbering: node -> id (-1 fixed)         (src/fe/Constraint.cpp:61-72)
+//   efem_ref bench    <cfg.json> <iters_per_step> <warmup_steps> <steps>
+//       the same solve driven step by step through the reference's own
+//       components (SoftObjective, LBFGSMat, LineSearchFEA, SimplicialLLT),
+//       timing the one-time approximate-Jacobian factorisation and then each
+//       step of <iters_per_step> L-BFGS iterations separately
 //   efem_ref piola    <neo_hookean|mo_riv|yeoh> C10 C01 C20 C30 D1 <F.f64> <P_out.f64>
 //       Material::getFirstPiola on a batch of column-major 3x3 F
 //                                                         (src/material/*.cpp)
@@ -152,6 +157,67 @@ static int cmd_piola(int argc, char** argv)
     return 0;
 }
 
+// LBFGSSolver::solve (src/simulation/nlsolver/LBFGS.h:96-174) with its loop
+// cut into timed steps; every call below is the reference's own code.
+static int cmd_bench(Problem& p, int ipstep, int warm, int steps)
+{
+    using clk = std::chrono::steady_clock;
+    auto ac = p.config->analysisConfig();
+    NLSolverParam param;
+    param.epsilon = ac->residual_criterion;
+    param.epsilon_rel = ac->residual_criterion;
+    param.max_linesearch = ac->max_line_search;
+    param.config = p.config;
+    SoftObjective obj;
+    obj.constraint = p.constraint;
+    obj.dimens = p.constraint->getDimens();
+    const int n = obj.dimens;
+    Eigen::VectorXd x = Eigen::VectorXd::Zero(n), xp(n), r(n), rp(n), d(n);
+    LBFGSMat bfgs;
+    bfgs.reset(n, param.m);
+    obj.residual(x, r);
+    auto t0 = clk::now();
+    Eigen::SparseMatrix<double> K;
+    obj.jacobi(x, K);
+    auto llt = std::make_shared<Eigen::SimplicialLLT<Eigen::SparseMatrix<double>, Eigen::Upper>>();
+    llt->analyzePattern(K);
+    llt->factorize(K);
+    const bool ok = llt->info() == Eigen::Success;
+    if (!ok) llt.reset();
+    bfgs.setApproxJacobiSolverPtr(llt);
+    d = ok ? Eigen::VectorXd(-llt->solve(r)) : Eigen::VectorXd(-r);
+    auto t1 = clk::now();
+    int k = 1, converged_at = 0;
+    std::vector<double> st;
+    for (int step = 0; step < warm + steps && !converged_at; step++) {
+        auto a = clk::now();
+        int done = 0;
+        for (int it = 0; it < ipstep; it++) {
+            double s1 = 1.0;
+            xp = x;
+            rp = r;
+            LineSearchFEA::LineSearch(obj, x, r, s1, d, xp, param);
+            done++;
+            const double g = r.lpNorm<Eigen::Infinity>();
+            if (g <= param.epsilon || g <= param.epsilon_rel * x.lpNorm<Eigen::Infinity>()) {
+                converged_at = k;
+                break;
+            }
+            bfgs.add_correction(x - xp, r - rp);
+            bfgs.apply_Hv(r, -1.0, d);
+            k++;
+        }
+        auto b = clk::now();
+        if (step >= warm) st.push_back(std::chrono::duration<double>(b - a).count() / done * ipstep);
+    }
+    printf("{\"n_dof\": %d, \"factor_ok\": %d, \"factor_s\": %.6f, \"iters_per_step\": %d, \"converged_at\": %d, "
+           "\"r_evals\": %d, \"step_s\": [",
+        n, ok ? 1 : 0, std::chrono::duration<double>(t1 - t0).count(), ipstep, converged_at, obj.r_evalutes);
+    for (size_t i = 0; i < st.size(); i++) printf("%s%.6f", i ? ", " : "", st[i]);
+    printf("]}\n");
+    return 0;
+}
+
 int main(int argc, char** argv)
 {
     if (argc < 2) {
@@ -177,6 +243,10 @@ int main(int argc, char** argv)
     auto t1 = std::chrono::steady_clock::now();
     int n = p.constraint->getDimens();
 
+    if (cmd == "bench") {
+        if (argc < 6) return 1;
+        return cmd_bench(p, atoi(argv[3]), atoi(argv[4]), atoi(argv[5]));
+    }
     if (cmd == "info") {
         std::vector<int> ids;
         for (auto& body : p.model->getBodies())
