@@ -250,7 +250,7 @@ def main():
 
     # ---- roofline of the dominant kernel, measured live on the model's stream
     from efem_b200 import profiling
-    roof, launches = profiling.roofline_report(model, case, infos, stream)
+    roof, launches = profiling.roofline_report(model, infos)
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps, "higher_is_better": True,

@@ -31,7 +31,8 @@ SOLVE_CONVERGED, SOLVE_PRECOND_FALLBACK, SOLVE_DX_CONVERGED, SOLVE_MAX_ITERS = 1
 
 EXPORTED = ["efem_default_options", "efem_model_create_from_json", "efem_model_create", "efem_model_destroy",
             "efem_get_options", "efem_set_options", "efem_get_model_info", "efem_dof_map", "efem_residual",
-            "efem_approx_jacobian_csr", "efem_precond_apply", "efem_solve", "efem_last_error", "efem_version"]
+            "efem_approx_jacobian_csr", "efem_precond_apply", "efem_solve", "efem_set_stream", "efem_last_error",
+            "efem_version"]
 
 
 class EfemError(RuntimeError):
@@ -51,7 +52,8 @@ class SolveInfo(ctypes.Structure):
     _fields_ = [("niter", ctypes.c_int), ("n_residual_evals", ctypes.c_int), ("n_jacobian_evals", ctypes.c_int),
                 ("flags", ctypes.c_int), ("u_inf", ctypes.c_double), ("r_inf", ctypes.c_double),
                 ("ms_total", ctypes.c_double), ("ms_factor", ctypes.c_double), ("ms_residual", ctypes.c_double),
-                ("ms_precond", ctypes.c_double)]
+                ("ms_precond", ctypes.c_double), ("n_kernel_launches", ctypes.c_longlong),
+                ("n_precond_applies", ctypes.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -61,7 +63,9 @@ class ModelInfo(ctypes.Structure):
     _fields_ = [("n_nodes", ctypes.c_int), ("n_free_nodes", ctypes.c_int), ("n_dof", ctypes.c_int),
                 ("n_elements", ctypes.c_int), ("n_elements_skipped", ctypes.c_int), ("n_faces", ctypes.c_int),
                 ("n_force_nodes", ctypes.c_int), ("n_blocks", ctypes.c_int), ("factor_nnz", ctypes.c_longlong),
-                ("n_supernodes", ctypes.c_int), ("n_levels", ctypes.c_int), ("factor_gflop", ctypes.c_double)]
+                ("n_supernodes", ctypes.c_int), ("n_levels", ctypes.c_int), ("factor_gflop", ctypes.c_double),
+                ("factor_dinv_nnz", ctypes.c_longlong), ("residual_bytes", ctypes.c_longlong),
+                ("residual_flops", ctypes.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -114,6 +118,7 @@ def lib():
             "efem_precond_apply": [vp, vp],
             "efem_solve": [vp, vp, ctypes.POINTER(SolveInfo)],
             "efem_last_error": [ctypes.c_char_p, ctypes.c_size_t],
+            "efem_set_stream": [vp, vp],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -314,9 +319,16 @@ class Model:
         return rp, ci, v
 
     def precond_apply(self, v):
-        v = np.array(v, dtype=np.float64)
+        """H0 v (in place for a CUDA tensor when device_ptrs is set)."""
+        if not hasattr(v, "data_ptr"):
+            v = np.array(v, dtype=np.float64)
         check(lib().efem_precond_apply(self.h, _vec_ptr(v)))
         return v
+
+    def set_stream(self, cuda_stream_handle):
+        """Run on the caller's CUDA stream (an integer cudaStream_t, e.g.
+        torch.cuda.current_stream().cuda_stream); None for the model's own."""
+        check(lib().efem_set_stream(self.h, ctypes.c_void_p(cuda_stream_handle)))
 
 
 class Simulator:

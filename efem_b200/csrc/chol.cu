@@ -384,6 +384,9 @@ void precond_info(const Model& m, efem_model_info* info)
     info->n_supernodes = S.ns;
     info->n_levels = static_cast<int>(S.level_ptr.size()) - 1;
     info->factor_gflop = S.flops * 1e-9;
+    long long dn = 0;
+    for (int s = 0; s < S.ns; s++) dn += static_cast<long long>(S.ncol[s]) * (S.ncol[s] + 1) / 2;
+    info->factor_dinv_nnz = dn;
 }
 
 static efem_status precond_factor(Model& m, int* ok, double* ms_factor);
@@ -478,6 +481,7 @@ static efem_status precond_factor(Model& m, int* ok, double* ms_factor)
         k_factor<<<cnt, kFT, 0, m.stream>>>(a, S.level_ptr[l]);
     }
     k_inverse<<<S.ns, 128, 0, m.stream>>>(a, S.ns);
+    m.launches += 2 + nlev;
     EFEM_CUDA(cudaGetLastError());
     EFEM_CUDA(cudaEventRecord(e1, m.stream));
     int fail = 0;
@@ -520,6 +524,7 @@ efem_status precond_apply(Model& m, double* d_v)
         k_backward<<<cnt, kST, sm, m.stream>>>(a, S.level_ptr[l]);
     }
     k_scatter_sol<<<g, 256, 0, m.stream>>>(d_v, P.d_w, P.d_perm, n);
+    m.launches += 2 + 2 * nlev;
     EFEM_CUDA(cudaGetLastError());
     return EFEM_OK;
 }

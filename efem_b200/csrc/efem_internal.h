@@ -133,6 +133,7 @@ struct Model {
     double* d_u = nullptr;            // staging for host-pointer calls
     double* d_r = nullptr;
 
+    long long launches = 0;           // kernels launched by this model (diagnostics)
     Precond* precond = nullptr;   // owned; freed by free_precond
     SolverWS* ws = nullptr;       // owned; freed by free_solver
 

@@ -817,6 +817,27 @@ efem_status efem_get_model_info(void* model, efem_model_info* info)
     info->n_faces = m->n_faces;
     info->n_force_nodes = m->n_force_nodes;
     info->n_blocks = static_cast<int>(m->blocks.size());
+    // algorithmic traffic and work of one residual evaluation: every input read
+    // once (connectivity, material index, V_e, J0^{-1}, u, f_ext), r written
+    // once; flops = 2 per FMA (u.dN, H, P(F), S, and the nodal reduction)
+    const long long sz = m->opts.precision == EFEM_MIXED ? 4 : 8;
+    long long bytes = 3LL * 8 * m->n_free * 3;
+    double flops = 0;
+    for (auto& b : m->blocks) {
+        bytes += static_cast<long long>(b.n) * (4LL * b.nen + 4 + sz + sz * 9 * b.ngp);
+        double cmat = 0;
+        for (int e = 0; e < b.n; e++) {
+            const int t = m->materials_used[b.h_mat[e]].type;
+            cmat += t == EFEM_MOONEY_RIVLIN ? 510.0 : t == EFEM_YEOH ? 270.0 : 260.0;
+        }
+        flops += static_cast<double>(b.ngp) * (36.0 * b.nen * b.n + cmat);
+    }
+    for (auto& f : m->faces) {
+        bytes += static_cast<long long>(f.n) * (4LL * f.nen + 4 + 24 + 32 + sz * 9 * efem::MAX_FGP);
+        flops += static_cast<double>(f.n) * 9.0 * (24.0 * f.nen + 120.0);
+    }
+    info->residual_bytes = bytes;
+    info->residual_flops = flops;
     efem::precond_info(*m, info);
     return EFEM_OK;
 }

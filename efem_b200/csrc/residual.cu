@@ -281,9 +281,11 @@ efem_status launch_residual(Model& m, const double* d_u, double* d_r)
     // r = -f_ext
     extern void launch_scale(double* v, double s, size_t n, cudaStream_t st);
     launch_scale(d_r, -1.0, n, m.stream);
+    m.launches++;
     const bool mixed = m.opts.precision == EFEM_MIXED;
     for (auto& b : m.blocks) {
         if (b.n == 0) continue;
+        m.launches++;
         if (mixed)
             dispatch_elem<float>(b, m.d_mats_f, b.vol_f, b.J0inv_f, b.dN_f, b.gw_f, m.n_free, d_u, d_r, m.stream);
         else
@@ -291,6 +293,7 @@ efem_status launch_residual(Model& m, const double* d_u, double* d_r)
     }
     for (auto& f : m.faces) {
         if (f.n == 0) continue;
+        m.launches++;
         if (mixed)
             dispatch_face<float>(f, f.J0inv_f, f.t_w_f, f.t_N_f, f.t_dN_f, m.n_free, d_u, d_r, m.stream);
         else

@@ -256,7 +256,52 @@ int grid_for(size_t n) { return static_cast<int>(std::min<size_t>(kMaxBlocks, st
 
 }  // namespace
 
+// CUDA-event timing of the solve's phases: a pair of events around each
+// residual evaluation / H0 application, harvested after the host syncs the
+// line search already needs.
+struct PhaseTimer {
+    static constexpr int kPairs = 32;
+    cudaEvent_t ev[2 * kPairs] = {};
+    int kind[kPairs] = {};
+    int used = 0;
+    double acc[2] = { 0, 0 };
+    cudaError_t init()
+    {
+        for (auto& e : ev)
+            if (!e) {
+                cudaError_t s = cudaEventCreate(&e);
+                if (s != cudaSuccess) return s;
+            }
+        return cudaSuccess;
+    }
+    void destroy()
+    {
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+    }
+    int begin(int k, cudaStream_t st)
+    {
+        if (used == kPairs) return -1;  // pool full: this phase goes unmeasured
+        kind[used] = k;
+        cudaEventRecord(ev[2 * used], st);
+        return used++;
+    }
+    void end(int slot, cudaStream_t st)
+    {
+        if (slot >= 0) cudaEventRecord(ev[2 * slot + 1], st);
+    }
+    void harvest()  // call only after the stream has been synchronised
+    {
+        for (int i = 0; i < used; i++) {
+            float ms = 0;
+            if (cudaEventElapsedTime(&ms, ev[2 * i], ev[2 * i + 1]) == cudaSuccess) acc[kind[i]] += ms;
+        }
+        used = 0;
+    }
+};
+
 struct SolverWS {
+    PhaseTimer timer;
     size_t n = 0;
     int m = 0;
     double *r = nullptr, *xp = nullptr, *rp = nullptr, *d = nullptr, *q = nullptr;
@@ -288,6 +333,7 @@ void free_solver(Model& m)
     if (w.h_read) cudaFreeHost(w.h_read);
     for (auto& e : w.ev)
         if (e) cudaEventDestroy(e);
+    w.timer.destroy();
     delete m.ws;
     m.ws = nullptr;
 }
@@ -315,6 +361,7 @@ static efem_status alloc_ws(Model& m)
     EFEM_CUDA(cudaMemset(w.sc, 0, sizeof(Scalars)));
     EFEM_CUDA(cudaMallocHost(&w.h_read, sizeof(double) * 8));
     for (auto& e : w.ev) EFEM_CUDA(cudaEventCreate(&e));
+    EFEM_CUDA(w.timer.init());
     return EFEM_OK;
 }
 
@@ -329,17 +376,32 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
     cudaStream_t st = m.stream;
     const double eps = m.opts.residual_criterion;
     std::memset(info, 0, sizeof(*info));
+    const long long launches0 = m.launches;
     EFEM_CUDA(cudaEventRecord(w.ev[0], st));
     float ms_res = 0.f;
 
+    w.timer.used = 0;
+    w.timer.acc[0] = w.timer.acc[1] = 0;
     auto residual = [&](const double* xx) -> efem_status {
         info->n_residual_evals++;
-        return launch_residual(m, xx, w.r);
+        const int t = w.timer.begin(0, st);
+        efem_status rs = launch_residual(m, xx, w.r);
+        w.timer.end(t, st);
+        return rs;
+    };
+    auto precond = [&](double* v) -> efem_status {
+        info->n_precond_applies++;
+        const int t = w.timer.begin(1, st);
+        efem_status rs = precond_apply(m, v);
+        w.timer.end(t, st);
+        return rs;
     };
     auto read_ls = [&]() -> efem_status {
+        m.launches++;
         k_ls_reduce<<<G, kThreads, 0, st>>>(w.r, w.d, x, n, w.sc, w.partials);
         EFEM_CUDA(cudaMemcpyAsync(w.h_read, w.sc, sizeof(double) * 4, cudaMemcpyDeviceToHost, st));
         EFEM_CUDA(cudaStreamSynchronize(st));
+        w.timer.harvest();
         return EFEM_OK;
     };
 
@@ -366,17 +428,20 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
         if (!ok) info->flags |= EFEM_SOLVE_PRECOND_FALLBACK;
     }
     // initial direction d = -H0 r
+    m.launches++;
     k_neg_copy<<<G, kThreads, 0, st>>>(w.d, w.r, n);
-    if (ok && (s = precond_apply(m, w.d)) != EFEM_OK) return s;
+    if (ok && (s = precond(w.d)) != EFEM_OK) return s;
     {
         int ncorr = 0, ptr = mm;
         for (;;) {
+            m.launches++;
             k_ls_begin<<<G, kThreads, 0, st>>>(w.r, w.d, x, w.xp, w.rp, n, w.sc, w.partials);
             EFEM_CUDA(cudaMemcpyAsync(w.h_read + 4, &w.sc->dg0, sizeof(double), cudaMemcpyDeviceToHost, st));
             // residual-projection line search (LineSearchFEA.h:43-67); dg0 is read
             // together with the first trial's scalars
             double step = 1.0;
             for (int it = 0; it < m.opts.max_linesearch; it++) {
+                m.launches++;
                 k_trial<<<G, kThreads, 0, st>>>(x, w.xp, w.d, step, n);
                 if ((s = residual(x)) != EFEM_OK) return s;
                 if ((s = read_ls()) != EFEM_OK) return s;
@@ -397,25 +462,31 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
             }
             // add_correction (LBFGSMat.h:81-98)
             const int loc = ptr % mm;
+            m.launches++;
             k_correction<<<G, kThreads, 0, st>>>(x, w.xp, w.r, w.rp, w.S + loc * n, w.Y + loc * n, n, loc, w.sc, w.partials);
             if (ncorr < mm) ncorr++;
             ptr = loc + 1;
             // d = -H r, two-loop recursion (LBFGSMat.h:103-131)
+            m.launches++;
             k_neg_copy<<<G, kThreads, 0, st>>>(w.q, w.r, n);
             int j = ptr % mm, prev = -1;
             for (int i = 0; i < ncorr; i++) {
                 j = (j + mm - 1) % mm;
+                m.launches++;
                 k_loop1<<<G, kThreads, 0, st>>>(w.q, prev >= 0 ? w.Y + prev * n : nullptr, prev, w.S + j * n, j, n, w.sc, w.partials);
                 prev = j;
             }
+            m.launches++;
             k_loop1_tail<<<G, kThreads, 0, st>>>(w.q, prev >= 0 ? w.Y + prev * n : nullptr, prev, ok ? 0 : 1, n, w.sc);
-            if (ok && (s = precond_apply(m, w.q)) != EFEM_OK) return s;
+            if (ok && (s = precond(w.q)) != EFEM_OK) return s;
             prev = -1;
             for (int i = 0; i < ncorr; i++) {
+                m.launches++;
                 k_loop2<<<G, kThreads, 0, st>>>(w.q, prev >= 0 ? w.S + prev * n : nullptr, prev, w.Y + j * n, j, n, w.sc, w.partials);
                 prev = j;
                 j = (j + 1) % mm;
             }
+            m.launches++;
             k_loop2_tail<<<G, kThreads, 0, st>>>(w.d, w.q, prev >= 0 ? w.S + prev * n : nullptr, prev, n, w.sc);
             EFEM_CUDA(cudaGetLastError());
             k++;
@@ -424,15 +495,19 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
 done:
     EFEM_CUDA(cudaEventRecord(w.ev[1], st));
     EFEM_CUDA(cudaEventSynchronize(w.ev[1]));
+    w.timer.harvest();
     {
         float ms = 0;
         cudaEventElapsedTime(&ms, w.ev[0], w.ev[1]);
         info->ms_total = ms;
     }
+    info->ms_residual = w.timer.acc[0];
+    info->ms_precond = w.timer.acc[1];
     (void)ms_res;
     info->niter = k;
     info->u_inf = xinf;
     info->r_inf = rinf;
+    info->n_kernel_launches = m.launches - launches0;
     if (converged) info->flags |= EFEM_SOLVE_CONVERGED;
     if (xinf < m.opts.dx_criterion) info->flags |= EFEM_SOLVE_DX_CONVERGED;
     return EFEM_OK;

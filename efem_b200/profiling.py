@@ -1,0 +1,88 @@
+"""Roofline bookkeeping for bench.py.
+
+The solve reports device time per phase, taken with CUDA events on the
+model's stream around every residual evaluation and every H0 application
+(efem_solve_info.ms_residual / ms_precond).  From those and the algorithmic
+byte counts the library reports (efem_model_info), this module picks the
+dominant kernel group of the timed solves and forms
+
+    achieved = algorithmic bytes per launch / mean launch duration
+    frac     = achieved / measured HBM copy bandwidth (MEASURED_PEAKS.json)
+
+Algorithmic bytes per launch:
+  residual   every input read once (connectivity, material index, V_e,
+             J0^{-1} per Gauss point, u, f_ext) and r written once
+  H0 apply   the factor's panels (nnz(L) entries) and the inverted diagonal
+             blocks (their lower triangles), each read once in the forward and
+             once in the backward sweep, plus the 3-component work vectors
+"""
+from __future__ import annotations
+
+import json
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+FALLBACK_HBM_GBS = 6650.0
+
+
+def hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def measured_traffic(kernel_group):
+    """DRAM bytes per launch from a committed ncu summary, if one exists."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f).get(kernel_group)
+    except Exception:
+        return None
+
+
+def roofline_report(model, infos):
+    """Return (roofline dict, mean kernel launches per solve)."""
+    info = model.info()
+    n3 = model.n_dof
+    res_calls = sum(i["n_residual_evals"] for i in infos)
+    res_ms = sum(i["ms_residual"] for i in infos)
+    pc_calls = sum(i["n_precond_applies"] for i in infos)
+    pc_ms = sum(i["ms_precond"] for i in infos)
+    tot_ms = sum(i["ms_total"] for i in infos)
+    fac_ms = sum(i["ms_factor"] for i in infos)
+    res_bytes = float(info["residual_bytes"])
+    pc_bytes = 2.0 * 8.0 * (info["factor_nnz"] + info["factor_dinv_nnz"]) + 6.0 * 8.0 * n3
+    groups = {
+        "residual": (res_ms, res_calls, res_bytes),
+        "precond_apply": (pc_ms, pc_calls, pc_bytes),
+    }
+    dom = max(groups, key=lambda k: groups[k][0])
+    ms, calls, nbytes = groups[dom]
+    per_launch_s = (ms / max(calls, 1)) / 1000.0
+    achieved = nbytes / per_launch_s / 1e9 if per_launch_s > 0 else 0.0
+    peak, kind = hbm_peak()
+    roof = {
+        "kernel": dom,
+        "bound": "hbm",
+        "achieved": achieved,
+        "peak": peak,
+        "peak_source": kind,
+        "unit": "GB/s",
+        "frac": achieved / peak,
+        "traffic": measured_traffic(dom),
+        "algorithmic_bytes_per_launch": nbytes,
+        "launches_timed": calls,
+        "mean_launch_us": per_launch_s * 1e6,
+        "share_of_solve": {"residual": res_ms / tot_ms, "precond_apply": pc_ms / tot_ms,
+                           "factorisation": fac_ms / tot_ms,
+                           "other (line search, two-loop, host waits)": max(0.0, 1.0 - (res_ms + pc_ms + fac_ms) / tot_ms)},
+    }
+    if dom == "residual":
+        roof["residual_gflops_fp64"] = info["residual_flops"] / per_launch_s / 1e9
+    launches = sum(i["n_kernel_launches"] for i in infos) / len(infos)
+    return roof, launches

@@ -106,7 +106,12 @@ typedef struct {
     int n_jacobian_evals;     /* SoftObjective::j_evalutes */
     int flags;                /* EFEM_SOLVE_* bits */
     double u_inf, r_inf;      /* final ||u||_inf and ||r||_inf (Integrator.cpp:37-40) */
-    double ms_total, ms_factor, ms_residual, ms_precond;  /* device-timed phases */
+    double ms_total;          /* device time of the whole solve (CUDA events on the model's stream) */
+    double ms_factor;         /* numeric factorisation of the approximate Jacobian */
+    double ms_residual;       /* all residual evaluations (events around each) */
+    double ms_precond;        /* all H0 applications (events around each) */
+    long long n_kernel_launches;  /* this library's kernels launched by the solve */
+    int n_precond_applies;        /* H0 applications (ms_precond covers them) */
 } efem_solve_info;
 
 typedef struct {
@@ -117,6 +122,9 @@ typedef struct {
     long long factor_nnz;                 /* scalar Cholesky factor entries (0 before the first solve) */
     int n_supernodes, n_levels;
     double factor_gflop;
+    long long factor_dinv_nnz;            /* entries of the inverted diagonal blocks (lower triangles) */
+    long long residual_bytes;             /* algorithmic bytes of one residual evaluation */
+    double residual_flops;                /* algorithmic flops of one residual evaluation */
 } efem_model_info;
 
 /* --------------------------------------------------------------- lifetime */
