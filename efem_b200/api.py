@@ -31,8 +31,8 @@ SOLVE_CONVERGED, SOLVE_PRECOND_FALLBACK, SOLVE_DX_CONVERGED, SOLVE_MAX_ITERS = 1
 
 EXPORTED = ["efem_default_options", "efem_model_create_from_json", "efem_model_create", "efem_model_destroy",
             "efem_get_options", "efem_set_options", "efem_get_model_info", "efem_dof_map", "efem_residual",
-            "efem_approx_jacobian_csr", "efem_precond_apply", "efem_solve", "efem_set_stream", "efem_last_error",
-            "efem_version"]
+            "efem_approx_jacobian_csr", "efem_precond_apply", "efem_precond_apply_noalloc", "efem_solve",
+            "efem_set_stream", "efem_last_error", "efem_version"]
 
 
 class EfemError(RuntimeError):
@@ -119,6 +119,7 @@ def lib():
             "efem_solve": [vp, vp, ctypes.POINTER(SolveInfo)],
             "efem_last_error": [ctypes.c_char_p, ctypes.c_size_t],
             "efem_set_stream": [vp, vp],
+            "efem_precond_apply_noalloc": [vp, vp],
         }
         for name, args in sig.items():
             f = getattr(L, name)

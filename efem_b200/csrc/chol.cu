@@ -27,6 +27,8 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
+#include <string>
 
 #include "chol_symbolic.h"
 #include "efem_internal.h"
@@ -529,4 +531,104 @@ efem_status precond_apply(Model& m, double* d_v)
     return EFEM_OK;
 }
 
+// ============================================================================
+// Allocation-free H0 application.
+//
+// Some callers cannot call cudaMalloc at the moment they need H0 v: code that
+// runs while a CUDA stream capture is open (cudaMalloc is not allowed there),
+// code inside another framework's allocator (a caching allocator that owns the
+// device's free memory and must not see foreign allocations), or real-time
+// control loops that forbid the implicit device synchronisation an allocation
+// can cause.  For them efem_precond_apply_noalloc runs the same forward and
+// backward sweeps as efem_precond_apply, but its working vectors (the permuted
+// right-hand side, 3 per free node, and the fronts' update vectors) live in
+// the fixed array below instead of buffers owned by the model.
+//
+// Limits and sharing:
+//   * the array holds kNoAllocDoubles doubles (16 MiB); a model that needs
+//     more (3 * free nodes + its update-vector length) is rejected;
+//   * every GPU that loads this library keeps the array until the process
+//     exits;
+//   * all calls share the array and it keeps the last call's contents; every
+//     entry is written before it is read, so nothing has to be cleared, but
+//     calls that overlap on the GPU (other streams, other threads, other
+//     models) race on it and must be serialised by the caller.
+// ============================================================================
+namespace {
+constexpr size_t kNoAllocDoubles = size_t(2) << 20;
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+
+// device address of g_noalloc_scratch, looked up once per device; in host
+// code the array's name is only a host-side stand-in, never a device address
+std::mutex g_noalloc_mutex;
+double* g_noalloc_addr[256] = {};
+
+efem_status noalloc_scratch(int device, double** out)
+{
+    if (device < 0 || device >= 256) {
+        set_error("device ordinal out of range for the static workspace");
+        return EFEM_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[device]) {
+        EFEM_CUDA(cudaSetDevice(device));
+        void* p = nullptr;
+        EFEM_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        g_noalloc_addr[device] = static_cast<double*>(p);
+    }
+    *out = g_noalloc_addr[device];
+    return EFEM_OK;
+}
+}  // namespace
+
 }  // namespace efem
+
+extern "C" efem_status efem_precond_apply_noalloc(void* model, double* d_v)
+{
+    using namespace efem;
+    if (!model || !d_v) {
+        set_error("null model or vector");
+        return EFEM_ERR_ARG;
+    }
+    Model& m = *static_cast<Model*>(model);
+    if (!m.on_device || !m.precond || !m.precond->factored || !m.precond->ok) {
+        set_error("efem_precond_apply_noalloc needs an existing positive-definite factor: call efem_solve or "
+                  "efem_precond_apply once first");
+        return EFEM_ERR_ARG;
+    }
+    Precond& P = *m.precond;
+    const Symbolic& S = P.S;
+    const int n = S.n;
+    const size_t need = 3 * static_cast<size_t>(n) + static_cast<size_t>(S.upd_size);
+    if (need > kNoAllocDoubles) {
+        set_error("model needs " + std::to_string(need) + " doubles of workspace; the static workspace of "
+            "efem_precond_apply_noalloc holds " + std::to_string(kNoAllocDoubles));
+        return EFEM_ERR_ARG;
+    }
+    double* scratch = nullptr;
+    efem_status st = noalloc_scratch(m.device, &scratch);
+    if (st != EFEM_OK) return st;
+    EFEM_CUDA(cudaSetDevice(m.device));
+    if (n == 0) return EFEM_OK;
+    FrontArgs a = args_of(P);
+    a.w = scratch;
+    a.upd = scratch + 3 * static_cast<size_t>(n);
+    const int g = std::min(1184, (n + 255) / 256);
+    k_gather_rhs<<<g, 256, 0, m.stream>>>(a.w, d_v, P.d_perm, n);
+    const int nlev = static_cast<int>(S.level_ptr.size()) - 1;
+    for (int l = 0; l < nlev; l++) {
+        const int cnt = S.level_ptr[l + 1] - S.level_ptr[l];
+        const size_t sm = sizeof(double) * 3 * (P.lev_max_r[l] + P.lev_max_c[l]);
+        k_forward<<<cnt, kST, sm, m.stream>>>(a, S.level_ptr[l]);
+    }
+    for (int l = nlev - 1; l >= 0; l--) {
+        const int cnt = S.level_ptr[l + 1] - S.level_ptr[l];
+        const size_t sm = sizeof(double) * 3 * (P.lev_max_r[l] + P.lev_max_c[l]);
+        k_backward<<<cnt, kST, sm, m.stream>>>(a, S.level_ptr[l]);
+    }
+    k_scatter_sol<<<g, 256, 0, m.stream>>>(d_v, a.w, P.d_perm, n);
+    EFEM_CUDA(cudaGetLastError());
+    EFEM_CUDA(cudaStreamSynchronize(m.stream));
+    return EFEM_OK;
+}
+

@@ -169,6 +169,20 @@ efem_status efem_approx_jacobian_csr(void* model, long long* nnz, int* rowptr, i
  * to v in place.  Factorises on first use. */
 efem_status efem_precond_apply(void* model, double* v);
 
+/* H0 v like efem_precond_apply, for callers that cannot allocate device
+ * memory at call time (inside a CUDA stream capture, under another
+ * framework's caching allocator, in a loop that must not synchronise the
+ * device).  No counterpart in the reference.  It calls no cudaMalloc or
+ * cudaFree: its working vectors live in a fixed 16 MiB device array that
+ * every GPU loading this library keeps until exit.  Requirements: the model's
+ * factor exists (efem_solve or efem_precond_apply ran once) and
+ * 3 * free nodes + the factor's update-vector length <= 2^21 doubles
+ * (EFEM_ERR_ARG otherwise); d_v is a device pointer, overwritten in place.
+ * The first call on a device looks up the array's device address (do it
+ * before any stream capture).  All calls share the array: calls that overlap
+ * on the GPU race and must be serialised by the caller. */
+efem_status efem_precond_apply_noalloc(void* model, double* d_v);
+
 /* Solve R(u) = 0 from u_inout: replaces Integrator::integral
  * (src/simulation/Integrator.cpp:22-42) -> LBFGSSolver::solve (LBFGS.h:96-174). */
 efem_status efem_solve(void* model, double* u_inout, efem_solve_info* info);
