@@ -6,27 +6,34 @@
 // matrix L is factored (the same H0 = K~^{-1} up to rounding) and applied to
 // the three displacement components at once.
 //
-// Numeric factorisation, multifrontal, one level of the supernodal
-// elimination tree per launch (leaves first), one CTA per front:
-//   1. extend-add: the children's update blocks are added into the front
-//      through the precomputed relative indices (children in a fixed order, so
-//      the factor is bitwise repeatable);
-//   2. partial dense Cholesky of the r x r front: 32-column blocks, diagonal
-//      block in shared memory, panel TRSM row-parallel, trailing SYRK in 64x64
-//      register-blocked tiles.
-// Then each diagonal block L_JJ is inverted explicitly, so the triangular
-// solves are matrix-vector products.
+// Numeric factorisation (multifrontal, one level of the supernodal
+// elimination tree at a time, leaves first):
+//   k_extend_add  one CTA per front: add the children's update blocks through
+//                 the precomputed relative indices, children in a fixed order
+//                 (the factor is bitwise repeatable);
+//   per 32-column panel step of the level's fronts:
+//   k_panel       one CTA per front: Cholesky of the 32x32 diagonal block in
+//                 shared memory, then the panel TRSM, row-parallel;
+//   k_syrk        one CTA per 64x64 tile of every front's trailing lower
+//                 triangle: register-blocked rank-32 update.
+//   k_inverse     one warp per 32 columns of each diagonal block: L_JJ^{-1},
+//                 stored row-major, so the solves are matrix-vector products.
 //
-// Solves (3 right-hand sides interleaved per node), one launch per level:
-//   forward  (leaves -> root): f = [b_J; 0] + sum over children of their update
-//            vectors; y_J = L_JJ^{-1} f_J; update g = f_R - L_RJ y_J;
-//   backward (root -> leaves): x_J = L_JJ^{-T} (y_J - L_RJ^T x_R), x_R gathered
-//            from the ancestors' results.
-// No atomics anywhere: results are deterministic.
+// Solve H0 v (3 right-hand sides interleaved per node), per level and in
+// tiles of 32 rows (or columns) of a front, so that large fronts spread over
+// many CTAs:
+//   forward   k_fwd_y: y_J = L_JJ^{-1} f_J, f = b_J + children's updates
+//             k_fwd_g: g = f_R - L_RJ y_J (the update passed to the parent)
+//   backward  k_bwd_t: t_J = y_J - L_RJ^T x_R (x_R from the ancestors)
+//             k_bwd_x: x_J = L_JJ^{-T} t_J
+// Every sum is formed in a fixed order (no atomics): results are deterministic.
+// The whole solve (gather, 4 launches per level, scatter) is replayed as one
+// CUDA graph per input vector.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 
@@ -35,37 +42,75 @@
 
 namespace efem {
 
+namespace {
+constexpr int kFT = 256;  // factor threads
+constexpr int kNB = 32;   // factor panel width
+constexpr int kTS = 64;   // SYRK tile
+constexpr int kST = 128;  // solve threads
+constexpr int kRT = 32;   // solve tile (rows or columns)
+
+struct Tile {
+    int s;    // front
+    int off;  // first row / column of the tile (multiple of kRT)
+};
+}  // namespace
+
 struct Precond {
     Symbolic S;
     bool ready = false;     // symbolic analysis done and uploaded
     bool factored = false;  // numeric factor present
     bool ok = false;        // factor is positive definite
     double ms_factor = 0;
-    int max_r = 0, max_c = 0;
-    std::vector<int> lev_max_r, lev_max_c;
+    int max_r = 0, max_c = 0, max_m = 0, nlev = 0;
+    // solve schedule: tiles per level for the four solve kernels
+    std::vector<int> fy_off, fg_off, bt_off, bx_off;  // nlev + 1 offsets each
+    std::vector<int> lev_max_c, lev_max_m;
+    // factor schedule: per (level, step) the fronts with a panel at that step and the SYRK tiles
+    struct Step {
+        int level, k0, panel_off, panel_cnt, syrk_off, syrk_cnt;
+    };
+    std::vector<Step> steps;
+    std::vector<int> lev_first_step;  // index into steps, nlev + 1
+    int n_inv_tiles = 0;
     int *d_first = nullptr, *d_ncol = nullptr, *d_nrow = nullptr, *d_rows = nullptr, *d_child_ptr = nullptr,
-        *d_child_list = nullptr, *d_relind = nullptr, *d_level_list = nullptr, *d_perm = nullptr, *d_fail = nullptr;
+        *d_child_list = nullptr, *d_relind = nullptr, *d_level_list = nullptr, *d_perm = nullptr, *d_fail = nullptr,
+        *d_panel_list = nullptr;
     long long *d_front_off = nullptr, *d_rows_off = nullptr, *d_relind_off = nullptr, *d_dinv_off = nullptr,
               *d_upd_off = nullptr, *d_a_pos = nullptr, *d_a_src = nullptr;
-    double *d_front = nullptr, *d_dinv = nullptr, *d_upd = nullptr, *d_w = nullptr, *d_vals = nullptr;
+    Tile *d_fy = nullptr, *d_fg = nullptr, *d_bt = nullptr, *d_bx = nullptr, *d_inv = nullptr;
+    int4* d_syrk = nullptr;
+    double *d_front = nullptr, *d_dinv = nullptr, *d_upd = nullptr, *d_w = nullptr, *d_y = nullptr, *d_t = nullptr,
+           *d_vals = nullptr;
+    // graph replay of the solve, per (input vector, work buffers)
+    cudaStream_t capture = nullptr;
+    std::map<std::pair<double*, double*>, cudaGraphExec_t> graphs;
 };
 
 namespace {
-
-constexpr int kFT = 256;  // factor threads
-constexpr int kNB = 32;   // factor column block
-constexpr int kST = 128;  // solve threads
 
 struct FrontArgs {
     const int *first, *ncol, *nrow, *rows, *child_ptr, *child_list, *relind, *level_list;
     const long long *front_off, *rows_off, *relind_off, *dinv_off, *upd_off;
     double* front;
     double* dinv;
-    double* upd;
-    double* w;
     int* fail;
 };
 
+struct SolveBufs {
+    double* w;    // b, then x (permuted order, 3 per node)
+    double* y;    // forward result
+    double* t;    // backward intermediate
+    double* upd;  // fronts' update vectors
+};
+
+__device__ __forceinline__ double wsum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// ------------------------------------------------------------------ factorisation
 __global__ void k_scatter_a(double* __restrict__ front, const long long* __restrict__ pos,
     const long long* __restrict__ src, const double* __restrict__ vals, long long n)
 {
@@ -73,143 +118,154 @@ __global__ void k_scatter_a(double* __restrict__ front, const long long* __restr
         front[pos[k]] = vals[src[k]];
 }
 
-// extend-add of the children, then partial Cholesky of the front
-__global__ void __launch_bounds__(kFT) k_factor(FrontArgs a, int level_base)
+// children's update blocks into the front (children in list order)
+__global__ void __launch_bounds__(kFT) k_extend_add(FrontArgs a, int level_base)
 {
     const int s = a.level_list[level_base + blockIdx.x];
-    const int r = a.nrow[s], c = a.ncol[s];
+    const int r = a.nrow[s];
     double* F = a.front + a.front_off[s];
-    const int tid = threadIdx.x;
-
     for (int q = a.child_ptr[s]; q < a.child_ptr[s + 1]; q++) {
         const int ch = a.child_list[q];
         const int rc = a.nrow[ch], cc = a.ncol[ch], m = rc - cc;
         const int* ri = a.relind + a.relind_off[ch];
         const double* U = a.front + a.front_off[ch];
-        for (int idx = tid; idx < m * m; idx += kFT) {
-            const int i = idx % m, j = idx / m;
-            if (i < j) continue;
-            F[ri[i] + static_cast<long long>(ri[j]) * r] += U[(cc + i) + static_cast<long long>(cc + j) * rc];
+        for (int j = 0; j < m; j++) {
+            const long long dst = static_cast<long long>(ri[j]) * r;
+            const long long src = static_cast<long long>(cc + j) * rc + cc;
+            for (int i = j + threadIdx.x; i < m; i += kFT) F[ri[i] + dst] += U[i + src];
         }
         __syncthreads();
-    }
-
-    __shared__ double D[kNB][kNB + 1];
-    __shared__ double Pi[64][kNB + 1];
-    __shared__ double Pj[64][kNB + 1];
-    for (int k0 = 0; k0 < c; k0 += kNB) {
-        const int kb = min(kNB, c - k0);
-        // (a) diagonal block
-        for (int idx = tid; idx < kb * kb; idx += kFT) {
-            const int i = idx % kb, j = idx / kb;
-            D[i][j] = (i >= j) ? F[(k0 + i) + static_cast<long long>(k0 + j) * r] : 0.0;
-        }
-        __syncthreads();
-        for (int j = 0; j < kb; j++) {
-            if (tid == 0) {
-                double d = D[j][j];
-                if (!(d > 0.0)) {
-                    *a.fail = 1;
-                    d = 1.0;
-                }
-                D[j][j] = sqrt(d);
-            }
-            __syncthreads();
-            const double dj = D[j][j];
-            for (int i = j + 1 + tid; i < kb; i += kFT) D[i][j] /= dj;
-            __syncthreads();
-            const int t = kb - j - 1;
-            for (int idx = tid; idx < t * t; idx += kFT) {
-                const int ii = j + 1 + idx % t, kk = j + 1 + idx / t;
-                if (ii >= kk) D[ii][kk] -= D[ii][j] * D[kk][j];
-            }
-            __syncthreads();
-        }
-        for (int idx = tid; idx < kb * kb; idx += kFT) {
-            const int i = idx % kb, j = idx / kb;
-            if (i >= j) F[(k0 + i) + static_cast<long long>(k0 + j) * r] = D[i][j];
-        }
-        // (b) panel: rows below the block, x L^T = f
-        for (int i = k0 + kb + tid; i < r; i += kFT) {
-            double x[kNB];
-#pragma unroll
-            for (int j = 0; j < kNB; j++) x[j] = j < kb ? F[i + static_cast<long long>(k0 + j) * r] : 0.0;
-#pragma unroll
-            for (int j = 0; j < kNB; j++) {
-                if (j < kb) {
-                    double sum = x[j];
-#pragma unroll
-                    for (int k = 0; k < kNB; k++)
-                        if (k < j) sum -= x[k] * D[j][k];
-                    x[j] = sum / D[j][j];
-                }
-            }
-#pragma unroll
-            for (int j = 0; j < kNB; j++)
-                if (j < kb) F[i + static_cast<long long>(k0 + j) * r] = x[j];
-        }
-        __syncthreads();
-        // (c) trailing lower triangle -= P P^T, P = F[base:r, k0:k0+kb]
-        const int base = k0 + kb, m2 = r - base;
-        const int nt = (m2 + 63) / 64;
-        for (int tj = 0; tj < nt; tj++)
-            for (int ti = tj; ti < nt; ti++) {
-                for (int idx = tid; idx < 64 * kNB; idx += kFT) {
-                    const int p = idx % 64, k = idx / 64;
-                    const int gi = base + ti * 64 + p, gj = base + tj * 64 + p;
-                    Pi[p][k] = (k < kb && gi < r) ? F[gi + static_cast<long long>(k0 + k) * r] : 0.0;
-                    Pj[p][k] = (k < kb && gj < r) ? F[gj + static_cast<long long>(k0 + k) * r] : 0.0;
-                }
-                __syncthreads();
-                const int a0 = (tid % 16) * 4, b0 = (tid / 16) * 4;
-                double acc[4][4];
-#pragma unroll
-                for (int x = 0; x < 4; x++)
-#pragma unroll
-                    for (int y = 0; y < 4; y++) acc[x][y] = 0.0;
-                for (int k = 0; k < kb; k++) {
-                    double pa[4], pb[4];
-#pragma unroll
-                    for (int x = 0; x < 4; x++) {
-                        pa[x] = Pi[a0 + x][k];
-                        pb[x] = Pj[b0 + x][k];
-                    }
-#pragma unroll
-                    for (int x = 0; x < 4; x++)
-#pragma unroll
-                        for (int y = 0; y < 4; y++) acc[x][y] += pa[x] * pb[y];
-                }
-#pragma unroll
-                for (int x = 0; x < 4; x++)
-#pragma unroll
-                    for (int y = 0; y < 4; y++) {
-                        const int gi = base + ti * 64 + a0 + x, gj = base + tj * 64 + b0 + y;
-                        if (gi < r && gj < r && gi >= gj) F[gi + static_cast<long long>(gj) * r] -= acc[x][y];
-                    }
-                __syncthreads();
-            }
     }
 }
 
-// Dinv = L_JJ^{-1}, one thread per column of the inverse
-__global__ void k_inverse(FrontArgs a, int ns)
+// diagonal block and panel of step k0, one CTA per front in the step's list
+__global__ void __launch_bounds__(kFT) k_panel(FrontArgs a, const int* __restrict__ list, int k0)
 {
-    const int s = blockIdx.x;
-    if (s >= ns) return;
+    const int s = list[blockIdx.x];
     const int r = a.nrow[s], c = a.ncol[s];
-    const double* F = a.front + a.front_off[s];
-    double* X = a.dinv + a.dinv_off[s];
-    for (int j = threadIdx.x; j < c; j += blockDim.x) {
-        for (int i = 0; i < j; i++) X[i + static_cast<long long>(j) * c] = 0.0;
-        X[j + static_cast<long long>(j) * c] = 1.0 / F[j + static_cast<long long>(j) * r];
-        for (int i = j + 1; i < c; i++) {
-            double sum = 0.0;
-            for (int k = j; k < i; k++) sum += F[i + static_cast<long long>(k) * r] * X[k + static_cast<long long>(j) * c];
-            X[i + static_cast<long long>(j) * c] = -sum / F[i + static_cast<long long>(i) * r];
+    const int kb = min(kNB, c - k0);
+    double* F = a.front + a.front_off[s];
+    const int tid = threadIdx.x;
+    __shared__ double D[kNB][kNB + 1];
+    for (int idx = tid; idx < kb * kb; idx += kFT) {
+        const int i = idx % kb, j = idx / kb;
+        D[i][j] = (i >= j) ? F[(k0 + i) + static_cast<long long>(k0 + j) * r] : 0.0;
+    }
+    __syncthreads();
+    for (int j = 0; j < kb; j++) {
+        if (tid == 0) {
+            double d = D[j][j];
+            if (!(d > 0.0)) {
+                *a.fail = 1;
+                d = 1.0;
+            }
+            D[j][j] = sqrt(d);
         }
+        __syncthreads();
+        const double dj = D[j][j];
+        for (int i = j + 1 + tid; i < kb; i += kFT) D[i][j] /= dj;
+        __syncthreads();
+        const int t = kb - j - 1;
+        for (int idx = tid; idx < t * t; idx += kFT) {
+            const int ii = j + 1 + idx % t, kk = j + 1 + idx / t;
+            if (ii >= kk) D[ii][kk] -= D[ii][j] * D[kk][j];
+        }
+        __syncthreads();
+    }
+    for (int idx = tid; idx < kb * kb; idx += kFT) {
+        const int i = idx % kb, j = idx / kb;
+        if (i >= j) F[(k0 + i) + static_cast<long long>(k0 + j) * r] = D[i][j];
+    }
+    // rows below the block: x L^T = f
+    for (int i = k0 + kb + tid; i < r; i += kFT) {
+        double x[kNB];
+#pragma unroll
+        for (int j = 0; j < kNB; j++) x[j] = j < kb ? F[i + static_cast<long long>(k0 + j) * r] : 0.0;
+#pragma unroll
+        for (int j = 0; j < kNB; j++) {
+            if (j < kb) {
+                double sum = x[j];
+#pragma unroll
+                for (int k = 0; k < kNB; k++)
+                    if (k < j) sum -= x[k] * D[j][k];
+                x[j] = sum / D[j][j];
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kNB; j++)
+            if (j < kb) F[i + static_cast<long long>(k0 + j) * r] = x[j];
     }
 }
 
+// trailing lower triangle -= P P^T for one 64x64 tile; tile = (front, ti, tj)
+__global__ void __launch_bounds__(kFT) k_syrk(FrontArgs a, const int4* __restrict__ tiles, int k0)
+{
+    const int4 tl = tiles[blockIdx.x];
+    const int s = tl.x, ti = tl.y, tj = tl.z;
+    const int r = a.nrow[s], c = a.ncol[s];
+    const int kb = min(kNB, c - k0);
+    const int base = k0 + kb;
+    double* F = a.front + a.front_off[s];
+    const int tid = threadIdx.x;
+    __shared__ double Pi[kTS][kNB + 1];
+    __shared__ double Pj[kTS][kNB + 1];
+    for (int idx = tid; idx < kTS * kNB; idx += kFT) {
+        const int p = idx % kTS, k = idx / kTS;
+        const int gi = base + ti * kTS + p, gj = base + tj * kTS + p;
+        Pi[p][k] = (k < kb && gi < r) ? F[gi + static_cast<long long>(k0 + k) * r] : 0.0;
+        Pj[p][k] = (k < kb && gj < r) ? F[gj + static_cast<long long>(k0 + k) * r] : 0.0;
+    }
+    __syncthreads();
+    const int a0 = (tid % 16) * 4, b0 = (tid / 16) * 4;
+    double acc[4][4];
+#pragma unroll
+    for (int x = 0; x < 4; x++)
+#pragma unroll
+        for (int y = 0; y < 4; y++) acc[x][y] = 0.0;
+    for (int k = 0; k < kb; k++) {
+        double pa[4], pb[4];
+#pragma unroll
+        for (int x = 0; x < 4; x++) {
+            pa[x] = Pi[a0 + x][k];
+            pb[x] = Pj[b0 + x][k];
+        }
+#pragma unroll
+        for (int x = 0; x < 4; x++)
+#pragma unroll
+            for (int y = 0; y < 4; y++) acc[x][y] += pa[x] * pb[y];
+    }
+#pragma unroll
+    for (int x = 0; x < 4; x++)
+#pragma unroll
+        for (int y = 0; y < 4; y++) {
+            const int gi = base + ti * kTS + a0 + x, gj = base + tj * kTS + b0 + y;
+            if (gi < r && gj < r && gi >= gj) F[gi + static_cast<long long>(gj) * r] -= acc[x][y];
+        }
+}
+
+// Inverse of the diagonal block, row-major: X = L_JJ^{-1}.  One warp per 32
+// columns; lane j owns column j and reads only its own earlier entries.
+__global__ void __launch_bounds__(32) k_inverse(FrontArgs a, const Tile* __restrict__ tiles)
+{
+    const Tile tl = tiles[blockIdx.x];
+    const int s = tl.s, j0 = tl.off;
+    const int r = a.nrow[s], c = a.ncol[s];
+    const double* L = a.front + a.front_off[s];
+    double* X = a.dinv + a.dinv_off[s];
+    const int j = j0 + threadIdx.x;
+    const bool valid = j < c;
+    for (int i = 0; i < j0; i++)
+        if (valid) X[static_cast<long long>(i) * c + j] = 0.0;
+    for (int i = j0; i < c; i++) {
+        const double* Li = L + i;
+        double acc = 0.0;
+        for (int k = j0; k < i; k++) acc += Li[static_cast<long long>(k) * r] * (valid ? X[static_cast<long long>(k) * c + j] : 0.0);
+        const double lii = Li[static_cast<long long>(i) * r];
+        if (valid) X[static_cast<long long>(i) * c + j] = (i < j) ? 0.0 : (i == j ? 1.0 / lii : -acc / lii);
+    }
+}
+
+// ------------------------------------------------------------------ solves
 __global__ void k_gather_rhs(double* __restrict__ w, const double* __restrict__ v, const int* __restrict__ perm, int n)
 {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
@@ -230,94 +286,135 @@ __global__ void k_scatter_sol(double* __restrict__ v, const double* __restrict__
     }
 }
 
-__global__ void __launch_bounds__(kST) k_forward(FrontArgs a, int level_base)
+// y rows [i0, i0+32) of front s: assemble f_J (rows < i0+32), then y = L_JJ^{-1} f_J
+__global__ void __launch_bounds__(kST) k_fwd_y(FrontArgs a, SolveBufs b, const Tile* __restrict__ tiles)
 {
     extern __shared__ double sm[];
-    const int s = a.level_list[level_base + blockIdx.x];
-    const int r = a.nrow[s], c = a.ncol[s], m = r - c, f0 = a.first[s];
-    double* f = sm;          // [r][3]
-    double* y = sm + 3 * r;  // [c][3]
-    const int tid = threadIdx.x;
-    for (int k = tid; k < r; k += kST) {
-        const bool own = k < c;
-        f[3 * k] = own ? a.w[3 * (f0 + k)] : 0.0;
-        f[3 * k + 1] = own ? a.w[3 * (f0 + k) + 1] : 0.0;
-        f[3 * k + 2] = own ? a.w[3 * (f0 + k) + 2] : 0.0;
-    }
+    const Tile tl = tiles[blockIdx.x];
+    const int s = tl.s, i0 = tl.off;
+    const int c = a.ncol[s], f0 = a.first[s];
+    const int kmax = min(c, i0 + kRT);
+    double* f = sm;  // [kmax][3]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int k = tid; k < 3 * kmax; k += kST) f[k] = b.w[3 * f0 + k];
     __syncthreads();
     for (int q = a.child_ptr[s]; q < a.child_ptr[s + 1]; q++) {
         const int ch = a.child_list[q];
         const int mc = a.nrow[ch] - a.ncol[ch];
         const int* ri = a.relind + a.relind_off[ch];
-        const double* g = a.upd + a.upd_off[ch];
-        for (int k = tid; k < mc; k += kST) {
-            const int t = ri[k];
-            f[3 * t] += g[3 * k];
-            f[3 * t + 1] += g[3 * k + 1];
-            f[3 * t + 2] += g[3 * k + 2];
+        const double* g = b.upd + a.upd_off[ch];
+        for (int j = tid; j < mc; j += kST) {
+            const int t = ri[j];
+            if (t < kmax) {
+                f[3 * t] += g[3 * j];
+                f[3 * t + 1] += g[3 * j + 1];
+                f[3 * t + 2] += g[3 * j + 2];
+            }
         }
         __syncthreads();
     }
-    const double* Di = a.dinv + a.dinv_off[s];
-    for (int i = tid; i < c; i += kST) {
+    const double* X = a.dinv + a.dinv_off[s];
+    for (int i = i0 + warp; i < kmax; i += kST / 32) {
+        const double* row = X + static_cast<long long>(i) * c;
         double y0 = 0, y1 = 0, y2 = 0;
-        for (int k = 0; k <= i; k++) {
-            const double d = Di[i + static_cast<long long>(k) * c];
+        for (int k = lane; k <= i; k += 32) {
+            const double d = row[k];
             y0 += d * f[3 * k];
             y1 += d * f[3 * k + 1];
             y2 += d * f[3 * k + 2];
         }
-        y[3 * i] = y0;
-        y[3 * i + 1] = y1;
-        y[3 * i + 2] = y2;
-        a.w[3 * (f0 + i)] = y0;
-        a.w[3 * (f0 + i) + 1] = y1;
-        a.w[3 * (f0 + i) + 2] = y2;
-    }
-    __syncthreads();
-    const double* F = a.front + a.front_off[s];
-    double* g = a.upd + a.upd_off[s];
-    for (int k = tid; k < m; k += kST) {
-        double g0 = f[3 * (c + k)], g1 = f[3 * (c + k) + 1], g2 = f[3 * (c + k) + 2];
-        for (int j = 0; j < c; j++) {
-            const double l = F[(c + k) + static_cast<long long>(j) * r];
-            g0 -= l * y[3 * j];
-            g1 -= l * y[3 * j + 1];
-            g2 -= l * y[3 * j + 2];
+        y0 = wsum(y0);
+        y1 = wsum(y1);
+        y2 = wsum(y2);
+        if (lane == 0) {
+            b.y[3 * (f0 + i)] = y0;
+            b.y[3 * (f0 + i) + 1] = y1;
+            b.y[3 * (f0 + i) + 2] = y2;
         }
-        g[3 * k] = g0;
-        g[3 * k + 1] = g1;
-        g[3 * k + 2] = g2;
     }
 }
 
-__device__ __forceinline__ double wsum(double v)
-{
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
-__global__ void __launch_bounds__(kST) k_backward(FrontArgs a, int level_base)
+// update rows [k0, k0+32) of front s: g = f_R - L_RJ y_J
+__global__ void __launch_bounds__(kST) k_fwd_g(FrontArgs a, SolveBufs b, const Tile* __restrict__ tiles)
 {
     extern __shared__ double sm[];
-    const int s = a.level_list[level_base + blockIdx.x];
+    const Tile tl = tiles[blockIdx.x];
+    const int s = tl.s, k0 = tl.off;
     const int r = a.nrow[s], c = a.ncol[s], m = r - c, f0 = a.first[s];
-    double* xr = sm;          // [m][3]
-    double* t = sm + 3 * m;   // [c][3]
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = kST / 32;
-    const int* rows = a.rows + a.rows_off[s];
+    double* y = sm;                  // [c][3]
+    double* fr = sm + 3 * c;         // [32][3]
+    double* red = fr + 3 * kRT;      // [4][32][3]
+    const int tid = threadIdx.x;
+    for (int k = tid; k < 3 * c; k += kST) y[k] = b.y[3 * f0 + k];
+    for (int k = tid; k < 3 * kRT; k += kST) fr[k] = 0.0;
+    __syncthreads();
+    for (int q = a.child_ptr[s]; q < a.child_ptr[s + 1]; q++) {
+        const int ch = a.child_list[q];
+        const int mc = a.nrow[ch] - a.ncol[ch];
+        const int* ri = a.relind + a.relind_off[ch];
+        const double* g = b.upd + a.upd_off[ch];
+        for (int j = tid; j < mc; j += kST) {
+            const int t = ri[j] - c - k0;
+            if (t >= 0 && t < kRT) {
+                fr[3 * t] += g[3 * j];
+                fr[3 * t + 1] += g[3 * j + 1];
+                fr[3 * t + 2] += g[3 * j + 2];
+            }
+        }
+        __syncthreads();
+    }
+    const int row = tid % kRT, part = tid / kRT;
+    const int k = k0 + row;
+    double a0 = 0, a1 = 0, a2 = 0;
+    if (k < m) {
+        const double* F = a.front + a.front_off[s] + c + k;
+        for (int j = part; j < c; j += kST / kRT) {
+            const double l = F[static_cast<long long>(j) * r];
+            a0 += l * y[3 * j];
+            a1 += l * y[3 * j + 1];
+            a2 += l * y[3 * j + 2];
+        }
+    }
+    red[3 * (part * kRT + row)] = a0;
+    red[3 * (part * kRT + row) + 1] = a1;
+    red[3 * (part * kRT + row) + 2] = a2;
+    __syncthreads();
+    if (tid < kRT && k < m) {
+        double g0 = fr[3 * row], g1 = fr[3 * row + 1], g2 = fr[3 * row + 2];
+        for (int p = 0; p < kST / kRT; p++) {
+            g0 -= red[3 * (p * kRT + row)];
+            g1 -= red[3 * (p * kRT + row) + 1];
+            g2 -= red[3 * (p * kRT + row) + 2];
+        }
+        double* g = b.upd + a.upd_off[s] + 3 * k;
+        g[0] = g0;
+        g[1] = g1;
+        g[2] = g2;
+    }
+}
+
+// columns [j0, j0+32) of front s: t_J = y_J - L_RJ^T x_R
+__global__ void __launch_bounds__(kST) k_bwd_t(FrontArgs a, SolveBufs b, const Tile* __restrict__ tiles)
+{
+    extern __shared__ double sm[];
+    const Tile tl = tiles[blockIdx.x];
+    const int s = tl.s, j0 = tl.off;
+    const int r = a.nrow[s], c = a.ncol[s], m = r - c, f0 = a.first[s];
+    double* xr = sm;  // [m][3]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int* rows = a.rows + a.rows_off[s] + c;
     for (int k = tid; k < m; k += kST) {
-        const int g = rows[c + k];
-        xr[3 * k] = a.w[3 * g];
-        xr[3 * k + 1] = a.w[3 * g + 1];
-        xr[3 * k + 2] = a.w[3 * g + 2];
+        const int g = rows[k];
+        xr[3 * k] = b.w[3 * g];
+        xr[3 * k + 1] = b.w[3 * g + 1];
+        xr[3 * k + 2] = b.w[3 * g + 2];
     }
     __syncthreads();
-    const double* F = a.front + a.front_off[s];
-    for (int j = warp; j < c; j += nw) {
+    const double* F = a.front + a.front_off[s] + c;
+    const int jmax = min(c, j0 + kRT);
+    for (int j = j0 + warp; j < jmax; j += kST / 32) {
+        const double* col = F + static_cast<long long>(j) * r;
         double s0 = 0, s1 = 0, s2 = 0;
-        const double* col = F + static_cast<long long>(j) * r + c;
         for (int k = lane; k < m; k += 32) {
             const double l = col[k];
             s0 += l * xr[3 * k];
@@ -328,30 +425,51 @@ __global__ void __launch_bounds__(kST) k_backward(FrontArgs a, int level_base)
         s1 = wsum(s1);
         s2 = wsum(s2);
         if (lane == 0) {
-            t[3 * j] = a.w[3 * (f0 + j)] - s0;
-            t[3 * j + 1] = a.w[3 * (f0 + j) + 1] - s1;
-            t[3 * j + 2] = a.w[3 * (f0 + j) + 2] - s2;
+            b.t[3 * (f0 + j)] = b.y[3 * (f0 + j)] - s0;
+            b.t[3 * (f0 + j) + 1] = b.y[3 * (f0 + j) + 1] - s1;
+            b.t[3 * (f0 + j) + 2] = b.y[3 * (f0 + j) + 2] - s2;
         }
     }
+}
+
+// rows [i0, i0+32) of front s: x_J = L_JJ^{-T} t_J
+__global__ void __launch_bounds__(kST) k_bwd_x(FrontArgs a, SolveBufs b, const Tile* __restrict__ tiles)
+{
+    extern __shared__ double sm[];
+    const Tile tl = tiles[blockIdx.x];
+    const int s = tl.s, i0 = tl.off;
+    const int c = a.ncol[s], f0 = a.first[s];
+    double* t = sm;                         // [c - i0][3]
+    double* red = sm + 3 * (c - i0);        // [4][32][3]
+    const int tid = threadIdx.x;
+    for (int k = tid; k < 3 * (c - i0); k += kST) t[k] = b.t[3 * (f0 + i0) + k];
     __syncthreads();
-    const double* Di = a.dinv + a.dinv_off[s];
-    for (int i = warp; i < c; i += nw) {
-        double s0 = 0, s1 = 0, s2 = 0;
-        const double* col = Di + static_cast<long long>(i) * c;  // column i of L_JJ^{-1} = row i of its transpose
-        for (int k = i + lane; k < c; k += 32) {
-            const double d = col[k];
-            s0 += d * t[3 * k];
-            s1 += d * t[3 * k + 1];
-            s2 += d * t[3 * k + 2];
+    const double* X = a.dinv + a.dinv_off[s];
+    const int row = tid % kRT, part = tid / kRT;
+    const int i = i0 + row;
+    double a0 = 0, a1 = 0, a2 = 0;
+    if (i < c)
+        for (int k = i0 + part; k < c; k += kST / kRT) {
+            if (k < i) continue;
+            const double d = X[static_cast<long long>(k) * c + i];
+            a0 += d * t[3 * (k - i0)];
+            a1 += d * t[3 * (k - i0) + 1];
+            a2 += d * t[3 * (k - i0) + 2];
         }
-        s0 = wsum(s0);
-        s1 = wsum(s1);
-        s2 = wsum(s2);
-        if (lane == 0) {
-            a.w[3 * (f0 + i)] = s0;
-            a.w[3 * (f0 + i) + 1] = s1;
-            a.w[3 * (f0 + i) + 2] = s2;
+    red[3 * (part * kRT + row)] = a0;
+    red[3 * (part * kRT + row) + 1] = a1;
+    red[3 * (part * kRT + row) + 2] = a2;
+    __syncthreads();
+    if (tid < kRT && i < c) {
+        double x0 = 0, x1 = 0, x2 = 0;
+        for (int p = 0; p < kST / kRT; p++) {
+            x0 += red[3 * (p * kRT + row)];
+            x1 += red[3 * (p * kRT + row) + 1];
+            x2 += red[3 * (p * kRT + row) + 2];
         }
+        b.w[3 * (f0 + i)] = x0;
+        b.w[3 * (f0 + i) + 1] = x1;
+        b.w[3 * (f0 + i) + 2] = x2;
     }
 }
 
@@ -359,7 +477,32 @@ FrontArgs args_of(Precond& P)
 {
     return FrontArgs { P.d_first, P.d_ncol, P.d_nrow, P.d_rows, P.d_child_ptr, P.d_child_list, P.d_relind,
         P.d_level_list, P.d_front_off, P.d_rows_off, P.d_relind_off, P.d_dinv_off, P.d_upd_off, P.d_front, P.d_dinv,
-        P.d_upd, P.d_w, P.d_fail };
+        P.d_fail };
+}
+
+constexpr size_t kRed = 4 * kRT * 3;  // doubles of the per-tile partial sums
+
+// enqueue one H0 application (gather, levels, scatter) on stream st
+void enqueue_solve(const Precond& P, const FrontArgs& a, const SolveBufs& b, double* d_v, cudaStream_t st)
+{
+    const Symbolic& S = P.S;
+    const int n = S.n;
+    const int g = std::min(1184, (n + 255) / 256);
+    k_gather_rhs<<<g, 256, 0, st>>>(b.w, d_v, P.d_perm, n);
+    for (int l = 0; l < P.nlev; l++) {
+        const int ny = P.fy_off[l + 1] - P.fy_off[l];
+        k_fwd_y<<<ny, kST, sizeof(double) * 3 * P.lev_max_c[l], st>>>(a, b, P.d_fy + P.fy_off[l]);
+        const int ng = P.fg_off[l + 1] - P.fg_off[l];
+        if (ng > 0)
+            k_fwd_g<<<ng, kST, sizeof(double) * (3 * P.lev_max_c[l] + 3 * kRT + kRed), st>>>(a, b, P.d_fg + P.fg_off[l]);
+    }
+    for (int l = P.nlev - 1; l >= 0; l--) {
+        const int nt = P.bt_off[l + 1] - P.bt_off[l];
+        k_bwd_t<<<nt, kST, sizeof(double) * 3 * std::max(P.lev_max_m[l], 1), st>>>(a, b, P.d_bt + P.bt_off[l]);
+        const int nx = P.bx_off[l + 1] - P.bx_off[l];
+        k_bwd_x<<<nx, kST, sizeof(double) * (3 * P.lev_max_c[l] + kRed), st>>>(a, b, P.d_bx + P.bx_off[l]);
+    }
+    k_scatter_sol<<<g, 256, 0, st>>>(d_v, b.w, P.d_perm, n);
 }
 
 }  // namespace
@@ -368,12 +511,17 @@ void free_precond(Model& m)
 {
     if (!m.precond) return;
     Precond& P = *m.precond;
+    for (auto& kv : P.graphs) cudaGraphExecDestroy(kv.second);
+    P.graphs.clear();
+    if (P.capture) cudaStreamDestroy(P.capture);
     for (int** p : { &P.d_first, &P.d_ncol, &P.d_nrow, &P.d_rows, &P.d_child_ptr, &P.d_child_list, &P.d_relind,
-             &P.d_level_list, &P.d_perm, &P.d_fail })
+             &P.d_level_list, &P.d_perm, &P.d_fail, &P.d_panel_list })
         dev_free(*p);
     for (long long** p : { &P.d_front_off, &P.d_rows_off, &P.d_relind_off, &P.d_dinv_off, &P.d_upd_off, &P.d_a_pos, &P.d_a_src })
         dev_free(*p);
-    for (double** p : { &P.d_front, &P.d_dinv, &P.d_upd, &P.d_w, &P.d_vals }) dev_free(*p);
+    for (Tile** p : { &P.d_fy, &P.d_fg, &P.d_bt, &P.d_bx, &P.d_inv }) dev_free(*p);
+    dev_free(P.d_syrk);
+    for (double** p : { &P.d_front, &P.d_dinv, &P.d_upd, &P.d_w, &P.d_y, &P.d_t, &P.d_vals }) dev_free(*p);
     delete m.precond;
     m.precond = nullptr;
 }
@@ -395,7 +543,7 @@ static efem_status precond_factor(Model& m, int* ok, double* ms_factor);
 
 efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
 {
-    if (m.precond && m.precond->ready && !refactor) {
+    if (m.precond && m.precond->factored && !refactor) {
         *ok = m.precond->ok;
         *ms_factor = 0.0;
         return EFEM_OK;
@@ -413,17 +561,64 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
     for (int i = 0; i < m.n_free; i++)
         for (int k = 0; k < 3; k++) coords[3 * i + k] = m.X[3 * static_cast<size_t>(m.node_of_dnode[i]) + k];
     symbolic_analysis(m.n_free, rp, ci, coords.data(), S);
-    const int nlev = static_cast<int>(S.level_ptr.size()) - 1;
-    P.lev_max_r.assign(nlev, 0);
+    P.nlev = static_cast<int>(S.level_ptr.size()) - 1;
+    const int nlev = P.nlev;
+    // solve and factor schedules
+    std::vector<Tile> fy, fg, bt, bx, inv;
+    std::vector<int> panel_list;
+    std::vector<int4> syrk;
+    P.fy_off.assign(1, 0);
+    P.fg_off.assign(1, 0);
+    P.bt_off.assign(1, 0);
+    P.bx_off.assign(1, 0);
     P.lev_max_c.assign(nlev, 0);
-    for (int l = 0; l < nlev; l++)
+    P.lev_max_m.assign(nlev, 0);
+    P.lev_first_step.assign(1, 0);
+    for (int l = 0; l < nlev; l++) {
+        int maxc = 0;
         for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) {
             const int s = S.level_list[q];
-            P.lev_max_r[l] = std::max(P.lev_max_r[l], S.nrow[s]);
-            P.lev_max_c[l] = std::max(P.lev_max_c[l], S.ncol[s]);
+            const int c = S.ncol[s], mm = S.nrow[s] - c;
+            P.lev_max_c[l] = std::max(P.lev_max_c[l], c);
+            P.lev_max_m[l] = std::max(P.lev_max_m[l], mm);
             P.max_r = std::max(P.max_r, S.nrow[s]);
+            P.max_c = std::max(P.max_c, c);
+            P.max_m = std::max(P.max_m, mm);
+            maxc = std::max(maxc, c);
+            for (int o = 0; o < c; o += kRT) {
+                fy.push_back({ s, o });
+                bt.push_back({ s, o });
+                bx.push_back({ s, o });
+                inv.push_back({ s, o });
+            }
+            for (int o = 0; o < mm; o += kRT) fg.push_back({ s, o });
         }
-    if (static_cast<size_t>(P.max_r) * 6 * sizeof(double) > 200 * 1024) {
+        P.fy_off.push_back(static_cast<int>(fy.size()));
+        P.fg_off.push_back(static_cast<int>(fg.size()));
+        P.bt_off.push_back(static_cast<int>(bt.size()));
+        P.bx_off.push_back(static_cast<int>(bx.size()));
+        for (int k0 = 0; k0 < maxc; k0 += kNB) {
+            Precond::Step st { l, k0, static_cast<int>(panel_list.size()), 0, static_cast<int>(syrk.size()), 0 };
+            for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) {
+                const int s = S.level_list[q];
+                const int c = S.ncol[s], r = S.nrow[s];
+                if (c <= k0) continue;
+                panel_list.push_back(s);
+                const int kb = std::min(kNB, c - k0);
+                const int m2 = r - k0 - kb;
+                const int nt = (m2 + kTS - 1) / kTS;
+                for (int tj = 0; tj < nt; tj++)
+                    for (int ti = tj; ti < nt; ti++) syrk.push_back(make_int4(s, ti, tj, 0));
+            }
+            st.panel_cnt = static_cast<int>(panel_list.size()) - st.panel_off;
+            st.syrk_cnt = static_cast<int>(syrk.size()) - st.syrk_off;
+            P.steps.push_back(st);
+        }
+        P.lev_first_step.push_back(static_cast<int>(P.steps.size()));
+    }
+    P.n_inv_tiles = static_cast<int>(inv.size());
+    const size_t smem_need = sizeof(double) * (3 * static_cast<size_t>(std::max(P.max_c, P.max_m)) + 3 * kRT + kRed);
+    if (smem_need > 200 * 1024) {
         set_error("a front of the approximate-Jacobian factor is too large for the solve kernels ("
             + std::to_string(P.max_r) + " rows)");
         return EFEM_ERR_UNSUPPORTED;
@@ -449,14 +644,25 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
     UP(P.d_a_pos, S.a_pos);
     UP(P.d_a_src, S.a_src);
     UP(P.d_vals, vals);
+    UP(P.d_fy, fy);
+    UP(P.d_fg, fg);
+    UP(P.d_bt, bt);
+    UP(P.d_bx, bx);
+    UP(P.d_inv, inv);
+    UP(P.d_panel_list, panel_list);
+    UP(P.d_syrk, syrk);
 #undef UP
+    const size_t n3 = 3 * static_cast<size_t>(std::max(S.n, 1));
     if ((st = dev_alloc(&P.d_front, static_cast<size_t>(S.front_size))) != EFEM_OK) return st;
     if ((st = dev_alloc(&P.d_dinv, static_cast<size_t>(std::max<long long>(S.dinv_size, 1)))) != EFEM_OK) return st;
     if ((st = dev_alloc(&P.d_upd, static_cast<size_t>(std::max<long long>(S.upd_size, 1)))) != EFEM_OK) return st;
-    if ((st = dev_alloc(&P.d_w, 3 * static_cast<size_t>(std::max(S.n, 1)))) != EFEM_OK) return st;
+    if ((st = dev_alloc(&P.d_w, n3)) != EFEM_OK) return st;
+    if ((st = dev_alloc(&P.d_y, n3)) != EFEM_OK) return st;
+    if ((st = dev_alloc(&P.d_t, n3)) != EFEM_OK) return st;
     if ((st = dev_alloc(&P.d_fail, 1)) != EFEM_OK) return st;
-    EFEM_CUDA(cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    EFEM_CUDA(cudaFuncSetAttribute(k_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    for (const void* k : { (const void*)k_fwd_y, (const void*)k_fwd_g, (const void*)k_bwd_t, (const void*)k_bwd_x })
+        EFEM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    EFEM_CUDA(cudaStreamCreateWithFlags(&P.capture, cudaStreamNonBlocking));
     P.ready = true;  // analysed; the numeric factor follows
     return precond_factor(m, ok, ms_factor);
 }
@@ -467,7 +673,6 @@ static efem_status precond_factor(Model& m, int* ok, double* ms_factor)
 {
     Precond& P = *m.precond;
     const Symbolic& S = P.S;
-    const int nlev = static_cast<int>(S.level_ptr.size()) - 1;
     cudaEvent_t e0, e1;
     EFEM_CUDA(cudaEventCreate(&e0));
     EFEM_CUDA(cudaEventCreate(&e1));
@@ -477,13 +682,26 @@ static efem_status precond_factor(Model& m, int* ok, double* ms_factor)
     const long long na = static_cast<long long>(S.a_pos.size());
     k_scatter_a<<<static_cast<int>(std::min<long long>(1184, (na + 255) / 256 + 1)), 256, 0, m.stream>>>(
         P.d_front, P.d_a_pos, P.d_a_src, P.d_vals, na);
+    m.launches++;
     FrontArgs a = args_of(P);
-    for (int l = 0; l < nlev; l++) {
+    for (int l = 0; l < P.nlev; l++) {
         const int cnt = S.level_ptr[l + 1] - S.level_ptr[l];
-        k_factor<<<cnt, kFT, 0, m.stream>>>(a, S.level_ptr[l]);
+        k_extend_add<<<cnt, kFT, 0, m.stream>>>(a, S.level_ptr[l]);
+        m.launches++;
+        for (int q = P.lev_first_step[l]; q < P.lev_first_step[l + 1]; q++) {
+            const Precond::Step& stp = P.steps[q];
+            k_panel<<<stp.panel_cnt, kFT, 0, m.stream>>>(a, P.d_panel_list + stp.panel_off, stp.k0);
+            m.launches++;
+            if (stp.syrk_cnt > 0) {
+                k_syrk<<<stp.syrk_cnt, kFT, 0, m.stream>>>(a, P.d_syrk + stp.syrk_off, stp.k0);
+                m.launches++;
+            }
+        }
     }
-    k_inverse<<<S.ns, 128, 0, m.stream>>>(a, S.ns);
-    m.launches += 2 + nlev;
+    if (P.n_inv_tiles > 0) {
+        k_inverse<<<P.n_inv_tiles, 32, 0, m.stream>>>(a, P.d_inv);
+        m.launches++;
+    }
     EFEM_CUDA(cudaGetLastError());
     EFEM_CUDA(cudaEventRecord(e1, m.stream));
     int fail = 0;
@@ -501,6 +719,34 @@ static efem_status precond_factor(Model& m, int* ok, double* ms_factor)
     return EFEM_OK;
 }
 
+// One H0 application, replayed from a CUDA graph captured (once per input
+// vector and work buffers) on the preconditioner's private stream.
+static efem_status apply_with(Model& m, double* d_v, const SolveBufs& b)
+{
+    Precond& P = *m.precond;
+    if (P.S.n == 0) return EFEM_OK;
+    const auto key = std::make_pair(d_v, b.w);
+    auto it = P.graphs.find(key);
+    if (it == P.graphs.end()) {
+        if (P.graphs.size() >= 8) {  // callers passing many distinct vectors: start over
+            EFEM_CUDA(cudaStreamSynchronize(m.stream));
+            for (auto& kv : P.graphs) cudaGraphExecDestroy(kv.second);
+            P.graphs.clear();
+        }
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t ge = nullptr;
+        EFEM_CUDA(cudaStreamBeginCapture(P.capture, cudaStreamCaptureModeThreadLocal));
+        enqueue_solve(P, args_of(P), b, d_v, P.capture);
+        EFEM_CUDA(cudaStreamEndCapture(P.capture, &g));
+        EFEM_CUDA(cudaGraphInstantiate(&ge, g, 0));
+        cudaGraphDestroy(g);
+        it = P.graphs.emplace(key, ge).first;
+    }
+    EFEM_CUDA(cudaGraphLaunch(it->second, m.stream));
+    m.launches += 2 + 4LL * P.nlev;
+    return EFEM_OK;
+}
+
 efem_status precond_apply(Model& m, double* d_v)
 {
     if (!m.precond || !m.precond->factored || !m.precond->ok) {
@@ -508,27 +754,7 @@ efem_status precond_apply(Model& m, double* d_v)
         return EFEM_ERR_ARG;
     }
     Precond& P = *m.precond;
-    const Symbolic& S = P.S;
-    const int n = S.n;
-    if (n == 0) return EFEM_OK;
-    const int g = std::min(1184, (n + 255) / 256);
-    k_gather_rhs<<<g, 256, 0, m.stream>>>(P.d_w, d_v, P.d_perm, n);
-    FrontArgs a = args_of(P);
-    const int nlev = static_cast<int>(S.level_ptr.size()) - 1;
-    for (int l = 0; l < nlev; l++) {
-        const int cnt = S.level_ptr[l + 1] - S.level_ptr[l];
-        const size_t sm = sizeof(double) * 3 * (P.lev_max_r[l] + P.lev_max_c[l]);
-        k_forward<<<cnt, kST, sm, m.stream>>>(a, S.level_ptr[l]);
-    }
-    for (int l = nlev - 1; l >= 0; l--) {
-        const int cnt = S.level_ptr[l + 1] - S.level_ptr[l];
-        const size_t sm = sizeof(double) * 3 * (P.lev_max_r[l] + P.lev_max_c[l]);
-        k_backward<<<cnt, kST, sm, m.stream>>>(a, S.level_ptr[l]);
-    }
-    k_scatter_sol<<<g, 256, 0, m.stream>>>(d_v, P.d_w, P.d_perm, n);
-    m.launches += 2 + 2 * nlev;
-    EFEM_CUDA(cudaGetLastError());
-    return EFEM_OK;
+    return apply_with(m, d_v, SolveBufs { P.d_w, P.d_y, P.d_t, P.d_upd });
 }
 
 // ============================================================================
@@ -541,12 +767,13 @@ efem_status precond_apply(Model& m, double* d_v)
 // control loops that forbid the implicit device synchronisation an allocation
 // can cause.  For them efem_precond_apply_noalloc runs the same forward and
 // backward sweeps as efem_precond_apply, but its working vectors (the permuted
-// right-hand side, 3 per free node, and the fronts' update vectors) live in
-// the fixed array below instead of buffers owned by the model.
+// right-hand side and solution, the forward and backward intermediates, 3 per
+// free node each, and the fronts' update vectors) live in the fixed array
+// below instead of buffers owned by the model.
 //
 // Limits and sharing:
 //   * the array holds kNoAllocDoubles doubles (16 MiB); a model that needs
-//     more (3 * free nodes + its update-vector length) is rejected;
+//     more (9 * free nodes + its update-vector length) is rejected;
 //   * every GPU that loads this library keeps the array until the process
 //     exits;
 //   * all calls share the array and it keeps the last call's contents; every
@@ -598,8 +825,8 @@ extern "C" efem_status efem_precond_apply_noalloc(void* model, double* d_v)
     }
     Precond& P = *m.precond;
     const Symbolic& S = P.S;
-    const int n = S.n;
-    const size_t need = 3 * static_cast<size_t>(n) + static_cast<size_t>(S.upd_size);
+    const size_t n3 = 3 * static_cast<size_t>(S.n);
+    const size_t need = 3 * n3 + static_cast<size_t>(S.upd_size);
     if (need > kNoAllocDoubles) {
         set_error("model needs " + std::to_string(need) + " doubles of workspace; the static workspace of "
             "efem_precond_apply_noalloc holds " + std::to_string(kNoAllocDoubles));
@@ -609,26 +836,10 @@ extern "C" efem_status efem_precond_apply_noalloc(void* model, double* d_v)
     efem_status st = noalloc_scratch(m.device, &scratch);
     if (st != EFEM_OK) return st;
     EFEM_CUDA(cudaSetDevice(m.device));
-    if (n == 0) return EFEM_OK;
-    FrontArgs a = args_of(P);
-    a.w = scratch;
-    a.upd = scratch + 3 * static_cast<size_t>(n);
-    const int g = std::min(1184, (n + 255) / 256);
-    k_gather_rhs<<<g, 256, 0, m.stream>>>(a.w, d_v, P.d_perm, n);
-    const int nlev = static_cast<int>(S.level_ptr.size()) - 1;
-    for (int l = 0; l < nlev; l++) {
-        const int cnt = S.level_ptr[l + 1] - S.level_ptr[l];
-        const size_t sm = sizeof(double) * 3 * (P.lev_max_r[l] + P.lev_max_c[l]);
-        k_forward<<<cnt, kST, sm, m.stream>>>(a, S.level_ptr[l]);
-    }
-    for (int l = nlev - 1; l >= 0; l--) {
-        const int cnt = S.level_ptr[l + 1] - S.level_ptr[l];
-        const size_t sm = sizeof(double) * 3 * (P.lev_max_r[l] + P.lev_max_c[l]);
-        k_backward<<<cnt, kST, sm, m.stream>>>(a, S.level_ptr[l]);
-    }
-    k_scatter_sol<<<g, 256, 0, m.stream>>>(d_v, a.w, P.d_perm, n);
+    if (S.n == 0) return EFEM_OK;
+    const SolveBufs b { scratch, scratch + n3, scratch + 2 * n3, scratch + 3 * n3 };
+    enqueue_solve(P, args_of(P), b, d_v, m.stream);
     EFEM_CUDA(cudaGetLastError());
     EFEM_CUDA(cudaStreamSynchronize(m.stream));
     return EFEM_OK;
 }
-

@@ -176,7 +176,7 @@ efem_status efem_precond_apply(void* model, double* v);
  * cudaFree: its working vectors live in a fixed 16 MiB device array that
  * every GPU loading this library keeps until exit.  Requirements: the model's
  * factor exists (efem_solve or efem_precond_apply ran once) and
- * 3 * free nodes + the factor's update-vector length <= 2^21 doubles
+ * 9 * free nodes + the factor's update-vector length <= 2^21 doubles
  * (EFEM_ERR_ARG otherwise); d_v is a device pointer, overwritten in place.
  * The first call on a device looks up the array's device address (do it
  * before any stream capture).  All calls share the array: calls that overlap
