@@ -309,3 +309,146 @@ def small_case(etype: str, material: str, load: str, n=(3, 2, 2), size=(0.03, 0.
     else:
         raise ValueError(load)
     return case
+
+
+def cylinder_cap_c3d20(ri=0.020, ro=0.025, h=0.030, plate=0.005, n_theta=64, n_r=4, n_z=24, n_ring=19,
+                       n_plate=2, p=1.0e4, reduced=True) -> Case:
+    """Hollow cylinder closed by a top plate, C3D20 (reduced integration by default).
+
+    Shell: n_theta x n_r x n_z hexahedra between radii ri and ro, height h.
+    Plate (thickness `plate`, n_plate layers): a butterfly mesh -- a square core
+    of (n_theta/4)^2 hexahedra and an O-grid of n_ring layers from the core's
+    boundary out to ro.  The O-grid's outer n_r layers share the shell's top
+    nodes, and the angular index starts at the core's corner (-45 degrees).
+    Neo-Hookean C10 = 114 kPa, D1 = 1e-6; z = 0 fixed; follower pressure p on
+    the inner wall and on the plate's underside inside the cavity (a closed
+    cavity)."""
+    assert n_theta % 4 == 0 and n_ring > n_r
+    nc = n_theta // 4
+    nodes, index = [], {}
+
+    def node(key, xyz):
+        if key not in index:
+            index[key] = len(nodes)
+            nodes.append(xyz)
+        return index[key]
+
+    th = -np.pi / 4 + 2 * np.pi * np.arange(n_theta) / n_theta
+    shell_r = np.linspace(ri, ro, n_r + 1)
+    hw = 0.45 * ri / np.sqrt(2.0)  # half-width of the square core
+    n_blend = n_ring - n_r         # O-grid layers from the square to radius ri
+
+    def square_pt(j):
+        side, t = divmod(j % n_theta, nc)
+        u = -hw + 2 * hw * t / nc
+        return [(hw, u), (-u, hw), (-hw, -u), (u, -hw)][side]
+
+    def ring_xy(sidx, j):
+        if sidx >= n_blend:
+            r = shell_r[sidx - n_blend]
+            return r * np.cos(th[j]), r * np.sin(th[j])
+        t = sidx / n_blend
+        sq = square_pt(j)
+        return ((1 - t) * sq[0] + t * ri * np.cos(th[j]), (1 - t) * sq[1] + t * ri * np.sin(th[j]))
+
+    def core_to_ring(a, b):
+        """Square-grid boundary point (a, b) -> ring angular index, or None inside."""
+        if a == nc:
+            return b % n_theta
+        if b == nc:
+            return nc + (nc - a)
+        if a == 0:
+            return 2 * nc + (nc - b)
+        if b == 0:
+            return (3 * nc + a) % n_theta
+        return None
+
+    z_shell = np.linspace(0.0, h, n_z + 1)
+    z_plate = h + np.linspace(0.0, plate, n_plate + 1)
+    # plate level c = 0 is the shell's top, so shell nodes at iz = n_z use plate keys
+    def shell_node(a, j, iz):
+        if iz == n_z:
+            return plate_node(n_blend + a, j, 0)
+        r = shell_r[a]
+        return node(("s", a, j, iz), (r * np.cos(th[j]), r * np.sin(th[j]), z_shell[iz]))
+
+    def plate_node(sidx, j, c):
+        x, y = ring_xy(sidx, j)
+        return node(("r", sidx, j % n_theta, c), (x, y, z_plate[c]))
+
+    def core_node(a, b, c):
+        j = core_to_ring(a, b)
+        if j is not None:
+            return plate_node(0, j, c)
+        return node(("c", a, b, c), (-hw + 2 * hw * a / nc, -hw + 2 * hw * b / nc, z_plate[c]))
+
+    hexes = []
+    for iz in range(n_z):
+        for a in range(n_r):
+            for j in range(n_theta):
+                jn = (j + 1) % n_theta
+                hexes.append([shell_node(a, j, iz), shell_node(a + 1, j, iz), shell_node(a + 1, jn, iz),
+                              shell_node(a, jn, iz), shell_node(a, j, iz + 1), shell_node(a + 1, j, iz + 1),
+                              shell_node(a + 1, jn, iz + 1), shell_node(a, jn, iz + 1)])
+    for c in range(n_plate):
+        for sidx in range(n_ring):
+            for j in range(n_theta):
+                jn = (j + 1) % n_theta
+                hexes.append([plate_node(sidx, j, c), plate_node(sidx + 1, j, c), plate_node(sidx + 1, jn, c),
+                              plate_node(sidx, jn, c), plate_node(sidx, j, c + 1), plate_node(sidx + 1, j, c + 1),
+                              plate_node(sidx + 1, jn, c + 1), plate_node(sidx, jn, c + 1)])
+        for a in range(nc):
+            for b in range(nc):
+                hexes.append([core_node(a, b, c), core_node(a + 1, b, c), core_node(a + 1, b + 1, c),
+                              core_node(a, b + 1, c), core_node(a, b, c + 1), core_node(a + 1, b, c + 1),
+                              core_node(a + 1, b + 1, c + 1), core_node(a, b + 1, c + 1)])
+    X = np.array(nodes, dtype=np.float64)
+    conn = np.array(hexes, dtype=np.int64)
+    # orient every hexahedron so that its bottom loop 0-1-2-3 runs counter-clockwise seen from its top
+    a_, b_, d_, e_ = (X[conn[:, k]] for k in (0, 1, 3, 4))
+    neg = np.einsum("ij,ij->i", b_ - a_, np.cross(d_ - a_, e_ - a_)) < 0
+    conn[neg] = conn[neg][:, [0, 3, 2, 1, 4, 7, 6, 5]]
+    m = hex8_to_hex20(Mesh(X, conn))
+    tol = 1e-9
+    fix = nodes_where(m, lambda P: np.abs(P[:, 2]) < tol)
+    r_xy = lambda P: np.sqrt(P[:, 0] ** 2 + P[:, 1] ** 2)
+    inner_wall = lambda P: bool(np.all(np.abs(r_xy(P) - ri) < 1e-7) and np.all(P[:, 2] <= h + 1e-9))
+    underside = lambda P: bool(np.all(np.abs(P[:, 2] - h) < 1e-9) and np.all(r_xy(P) <= ri + 1e-7))
+    faces = boundary_faces(m, lambda P: inner_wall(P) or underside(P))
+    return Case(m, [mat_nh()], fix, pressure=[(p, faces)], integration="reduced" if reduced else "full")
+
+
+def finger_c3d10(L=0.080, W=0.015, H=0.015, nx=80, nyz=12, n_ch=8, ch_len=0.006, ch_w=0.010, pitch=0.009,
+                 p=3.0e4) -> tuple:
+    """Pneumatic finger: a block with n_ch internal rectangular chambers, voxel hex
+    grid -> 6 tets per voxel -> C3D10.  Yeoh C10 = 110 kPa, C20 = 20 kPa,
+    C30 = -300 Pa, D1 = 1e-6; x = 0 face fixed; follower pressure p on the
+    chamber walls.  Returns (case, tip node index) with the tip node at the
+    centre of the x = L face's bottom edge line (y = W/2, z = 0)."""
+    hx, hyz = L / nx, W / nyz
+    base = box_hex8(L, W, H, nx, nyz, nyz)
+    # voxel centres; remove the chambers
+    ci = np.arange(nx)
+    cj = np.arange(nyz)
+    K, J, I = np.meshgrid(cj, cj, ci, indexing="ij")
+    xc, yc, zc = (I.ravel() + 0.5) * hx, (J.ravel() + 0.5) * hyz, (K.ravel() + 0.5) * hyz
+    x0 = round(((L - ((n_ch - 1) * pitch + ch_len)) / 2) / hx) * hx
+    inside = np.zeros(xc.shape, dtype=bool)
+    for k in range(n_ch):
+        xa = x0 + k * pitch
+        inside |= (xc > xa) & (xc < xa + ch_len) & (np.abs(yc - W / 2) < ch_w / 2) & (np.abs(zc - H / 2) < ch_w / 2)
+    conn = base.conn[~inside]
+    used = np.unique(conn)
+    remap = -np.ones(base.X.shape[0], dtype=np.int64)
+    remap[used] = np.arange(used.shape[0])
+    m = hex8_to_tet4(Mesh(base.X[used], remap[conn]))
+    m = tet4_to_tet10(m)
+    tol = 1e-9
+    fix = nodes_where(m, lambda P: np.abs(P[:, 0]) < tol)
+    outer = lambda P: bool(np.all(np.abs(P[:, 0]) < tol) or np.all(np.abs(P[:, 0] - L) < tol)
+                           or np.all(np.abs(P[:, 1]) < tol) or np.all(np.abs(P[:, 1] - W) < tol)
+                           or np.all(np.abs(P[:, 2]) < tol) or np.all(np.abs(P[:, 2] - H) < tol))
+    faces = boundary_faces(m, lambda P: not outer(P))
+    tip = int(np.argmin(np.sum((m.X - np.array([L, W / 2, 0.0])) ** 2, axis=1)))
+    case = Case(m, [mat_yeoh()], fix, pressure=[(p, faces)])
+    return case, tip
