@@ -46,8 +46,9 @@ namespace {
 constexpr int kFT = 256;  // factor threads
 constexpr int kNB = 32;   // factor panel width
 constexpr int kTS = 64;   // SYRK tile
-constexpr int kST = 128;  // solve threads
-constexpr int kRT = 32;   // solve tile (rows or columns)
+constexpr int kST = 256;  // solve threads: one warp per output row / column
+constexpr int kSW = kST / 32;  // outputs per solve CTA
+constexpr int kRT = 32;   // columns per CTA of the inverse / transpose kernels
 
 struct Tile {
     int s;    // front
@@ -78,6 +79,9 @@ struct Precond {
     long long *d_front_off = nullptr, *d_rows_off = nullptr, *d_relind_off = nullptr, *d_dinv_off = nullptr,
               *d_upd_off = nullptr, *d_a_pos = nullptr, *d_a_src = nullptr;
     Tile *d_fy = nullptr, *d_fg = nullptr, *d_bt = nullptr, *d_bx = nullptr, *d_inv = nullptr;
+    int *d_contrib_ptr = nullptr, *d_contrib_idx = nullptr;
+    long long* d_lt_off = nullptr;
+    double *d_dinvT = nullptr, *d_lt = nullptr;
     int4* d_syrk = nullptr;
     double *d_front = nullptr, *d_dinv = nullptr, *d_upd = nullptr, *d_w = nullptr, *d_y = nullptr, *d_t = nullptr,
            *d_vals = nullptr;
@@ -89,10 +93,12 @@ struct Precond {
 namespace {
 
 struct FrontArgs {
-    const int *first, *ncol, *nrow, *rows, *child_ptr, *child_list, *relind, *level_list;
-    const long long *front_off, *rows_off, *relind_off, *dinv_off, *upd_off;
+    const int *first, *ncol, *nrow, *rows, *child_ptr, *child_list, *relind, *level_list, *contrib_ptr, *contrib_idx;
+    const long long *front_off, *rows_off, *relind_off, *dinv_off, *upd_off, *lt_off;
     double* front;
-    double* dinv;
+    double* dinv;   // L_JJ^{-1}, row-major
+    double* dinvT;  // its transpose, row-major
+    double* lt;     // L_RJ, row-major
     int* fail;
 };
 
@@ -252,16 +258,24 @@ __global__ void __launch_bounds__(32) k_inverse(FrontArgs a, const Tile* __restr
     const int r = a.nrow[s], c = a.ncol[s];
     const double* L = a.front + a.front_off[s];
     double* X = a.dinv + a.dinv_off[s];
+    double* XT = a.dinvT + a.dinv_off[s];
     const int j = j0 + threadIdx.x;
     const bool valid = j < c;
     for (int i = 0; i < j0; i++)
-        if (valid) X[static_cast<long long>(i) * c + j] = 0.0;
+        if (valid) {
+            X[static_cast<long long>(i) * c + j] = 0.0;
+            XT[static_cast<long long>(j) * c + i] = 0.0;
+        }
     for (int i = j0; i < c; i++) {
         const double* Li = L + i;
         double acc = 0.0;
         for (int k = j0; k < i; k++) acc += Li[static_cast<long long>(k) * r] * (valid ? X[static_cast<long long>(k) * c + j] : 0.0);
         const double lii = Li[static_cast<long long>(i) * r];
-        if (valid) X[static_cast<long long>(i) * c + j] = (i < j) ? 0.0 : (i == j ? 1.0 / lii : -acc / lii);
+        const double v = (i < j) ? 0.0 : (i == j ? 1.0 / lii : -acc / lii);
+        if (valid) {
+            X[static_cast<long long>(i) * c + j] = v;
+            XT[static_cast<long long>(j) * c + i] = v;
+        }
     }
 }
 
@@ -286,114 +300,104 @@ __global__ void k_scatter_sol(double* __restrict__ v, const double* __restrict__
     }
 }
 
-// y rows [i0, i0+32) of front s: assemble f_J (rows < i0+32), then y = L_JJ^{-1} f_J
+// Dot product of a contiguous row with a 3-component vector held in shared
+// memory, over k in [k0, k1); the 32 lanes stride the row with four loads in
+// flight each, then the warp reduces.
+__device__ __forceinline__ void warp_dot3(const double* __restrict__ row, const double* __restrict__ v, int k0, int k1,
+    int vbase, int lane, double& s0, double& s1, double& s2)
+{
+    double a0 = 0, a1 = 0, a2 = 0;
+    int k = k0 + lane;
+    for (; k + 96 < k1; k += 128) {
+        const double d0 = row[k], d1 = row[k + 32], d2 = row[k + 64], d3 = row[k + 96];
+        const double* v0 = v + 3 * (k - vbase);
+        a0 += d0 * v0[0] + d1 * v0[96] + d2 * v0[192] + d3 * v0[288];
+        a1 += d0 * v0[1] + d1 * v0[97] + d2 * v0[193] + d3 * v0[289];
+        a2 += d0 * v0[2] + d1 * v0[98] + d2 * v0[194] + d3 * v0[290];
+    }
+    for (; k < k1; k += 32) {
+        const double d = row[k];
+        const double* v0 = v + 3 * (k - vbase);
+        a0 += d * v0[0];
+        a1 += d * v0[1];
+        a2 += d * v0[2];
+    }
+    s0 = wsum(a0);
+    s1 = wsum(a1);
+    s2 = wsum(a2);
+}
+
+// f_t = (b_t for own columns) + the children's update entries landing on row t
+__device__ __forceinline__ void assemble_row(const FrontArgs& a, const SolveBufs& b, int s, int t, bool own, int f0,
+    double& f0v, double& f1v, double& f2v)
+{
+    double x0 = 0, x1 = 0, x2 = 0;
+    if (own) {
+        x0 = b.w[3 * (f0 + t)];
+        x1 = b.w[3 * (f0 + t) + 1];
+        x2 = b.w[3 * (f0 + t) + 2];
+    }
+    const long long row = a.rows_off[s] + t;
+    for (int q = a.contrib_ptr[row]; q < a.contrib_ptr[row + 1]; q++) {
+        const double* g = b.upd + 3LL * a.contrib_idx[q];
+        x0 += g[0];
+        x1 += g[1];
+        x2 += g[2];
+    }
+    f0v = x0;
+    f1v = x1;
+    f2v = x2;
+}
+
+// y rows [i0, i0+8) of front s: y_i = sum_{k<=i} (L_JJ^{-1})_ik f_k, one warp per row
 __global__ void __launch_bounds__(kST) k_fwd_y(FrontArgs a, SolveBufs b, const Tile* __restrict__ tiles)
 {
     extern __shared__ double sm[];
     const Tile tl = tiles[blockIdx.x];
     const int s = tl.s, i0 = tl.off;
     const int c = a.ncol[s], f0 = a.first[s];
-    const int kmax = min(c, i0 + kRT);
+    const int kmax = min(c, i0 + kSW);
     double* f = sm;  // [kmax][3]
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int k = tid; k < 3 * kmax; k += kST) f[k] = b.w[3 * f0 + k];
+    for (int k = tid; k < kmax; k += kST) assemble_row(a, b, s, k, true, f0, f[3 * k], f[3 * k + 1], f[3 * k + 2]);
     __syncthreads();
-    for (int q = a.child_ptr[s]; q < a.child_ptr[s + 1]; q++) {
-        const int ch = a.child_list[q];
-        const int mc = a.nrow[ch] - a.ncol[ch];
-        const int* ri = a.relind + a.relind_off[ch];
-        const double* g = b.upd + a.upd_off[ch];
-        for (int j = tid; j < mc; j += kST) {
-            const int t = ri[j];
-            if (t < kmax) {
-                f[3 * t] += g[3 * j];
-                f[3 * t + 1] += g[3 * j + 1];
-                f[3 * t + 2] += g[3 * j + 2];
-            }
-        }
-        __syncthreads();
-    }
-    const double* X = a.dinv + a.dinv_off[s];
-    for (int i = i0 + warp; i < kmax; i += kST / 32) {
-        const double* row = X + static_cast<long long>(i) * c;
-        double y0 = 0, y1 = 0, y2 = 0;
-        for (int k = lane; k <= i; k += 32) {
-            const double d = row[k];
-            y0 += d * f[3 * k];
-            y1 += d * f[3 * k + 1];
-            y2 += d * f[3 * k + 2];
-        }
-        y0 = wsum(y0);
-        y1 = wsum(y1);
-        y2 = wsum(y2);
-        if (lane == 0) {
-            b.y[3 * (f0 + i)] = y0;
-            b.y[3 * (f0 + i) + 1] = y1;
-            b.y[3 * (f0 + i) + 2] = y2;
-        }
+    const int i = i0 + warp;
+    if (i >= kmax) return;
+    double y0, y1, y2;
+    warp_dot3(a.dinv + a.dinv_off[s] + static_cast<long long>(i) * c, f, 0, i + 1, 0, lane, y0, y1, y2);
+    if (lane == 0) {
+        b.y[3 * (f0 + i)] = y0;
+        b.y[3 * (f0 + i) + 1] = y1;
+        b.y[3 * (f0 + i) + 2] = y2;
     }
 }
 
-// update rows [k0, k0+32) of front s: g = f_R - L_RJ y_J
+// update rows [k0, k0+8) of front s: g_k = f_{c+k} - (L_RJ)_k . y_J, one warp per row
 __global__ void __launch_bounds__(kST) k_fwd_g(FrontArgs a, SolveBufs b, const Tile* __restrict__ tiles)
 {
     extern __shared__ double sm[];
     const Tile tl = tiles[blockIdx.x];
     const int s = tl.s, k0 = tl.off;
     const int r = a.nrow[s], c = a.ncol[s], m = r - c, f0 = a.first[s];
-    double* y = sm;                  // [c][3]
-    double* fr = sm + 3 * c;         // [32][3]
-    double* red = fr + 3 * kRT;      // [4][32][3]
-    const int tid = threadIdx.x;
+    double* y = sm;  // [c][3]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int k = tid; k < 3 * c; k += kST) y[k] = b.y[3 * f0 + k];
-    for (int k = tid; k < 3 * kRT; k += kST) fr[k] = 0.0;
     __syncthreads();
-    for (int q = a.child_ptr[s]; q < a.child_ptr[s + 1]; q++) {
-        const int ch = a.child_list[q];
-        const int mc = a.nrow[ch] - a.ncol[ch];
-        const int* ri = a.relind + a.relind_off[ch];
-        const double* g = b.upd + a.upd_off[ch];
-        for (int j = tid; j < mc; j += kST) {
-            const int t = ri[j] - c - k0;
-            if (t >= 0 && t < kRT) {
-                fr[3 * t] += g[3 * j];
-                fr[3 * t + 1] += g[3 * j + 1];
-                fr[3 * t + 2] += g[3 * j + 2];
-            }
-        }
-        __syncthreads();
-    }
-    const int row = tid % kRT, part = tid / kRT;
-    const int k = k0 + row;
-    double a0 = 0, a1 = 0, a2 = 0;
-    if (k < m) {
-        const double* F = a.front + a.front_off[s] + c + k;
-        for (int j = part; j < c; j += kST / kRT) {
-            const double l = F[static_cast<long long>(j) * r];
-            a0 += l * y[3 * j];
-            a1 += l * y[3 * j + 1];
-            a2 += l * y[3 * j + 2];
-        }
-    }
-    red[3 * (part * kRT + row)] = a0;
-    red[3 * (part * kRT + row) + 1] = a1;
-    red[3 * (part * kRT + row) + 2] = a2;
-    __syncthreads();
-    if (tid < kRT && k < m) {
-        double g0 = fr[3 * row], g1 = fr[3 * row + 1], g2 = fr[3 * row + 2];
-        for (int p = 0; p < kST / kRT; p++) {
-            g0 -= red[3 * (p * kRT + row)];
-            g1 -= red[3 * (p * kRT + row) + 1];
-            g2 -= red[3 * (p * kRT + row) + 2];
-        }
+    const int k = k0 + warp;
+    if (k >= m) return;
+    double d0, d1, d2;
+    warp_dot3(a.lt + a.lt_off[s] + static_cast<long long>(k) * c, y, 0, c, 0, lane, d0, d1, d2);
+    if (lane == 0) {
+        double f0v, f1v, f2v;
+        assemble_row(a, b, s, c + k, false, f0, f0v, f1v, f2v);
         double* g = b.upd + a.upd_off[s] + 3 * k;
-        g[0] = g0;
-        g[1] = g1;
-        g[2] = g2;
+        g[0] = f0v - d0;
+        g[1] = f1v - d1;
+        g[2] = f2v - d2;
     }
 }
 
-// columns [j0, j0+32) of front s: t_J = y_J - L_RJ^T x_R
+// columns [j0, j0+8) of front s: t_j = y_j - (L_RJ)^T_j . x_R, one warp per column
 __global__ void __launch_bounds__(kST) k_bwd_t(FrontArgs a, SolveBufs b, const Tile* __restrict__ tiles)
 {
     extern __shared__ double sm[];
@@ -410,77 +414,58 @@ __global__ void __launch_bounds__(kST) k_bwd_t(FrontArgs a, SolveBufs b, const T
         xr[3 * k + 2] = b.w[3 * g + 2];
     }
     __syncthreads();
-    const double* F = a.front + a.front_off[s] + c;
-    const int jmax = min(c, j0 + kRT);
-    for (int j = j0 + warp; j < jmax; j += kST / 32) {
-        const double* col = F + static_cast<long long>(j) * r;
-        double s0 = 0, s1 = 0, s2 = 0;
-        for (int k = lane; k < m; k += 32) {
-            const double l = col[k];
-            s0 += l * xr[3 * k];
-            s1 += l * xr[3 * k + 1];
-            s2 += l * xr[3 * k + 2];
-        }
-        s0 = wsum(s0);
-        s1 = wsum(s1);
-        s2 = wsum(s2);
-        if (lane == 0) {
-            b.t[3 * (f0 + j)] = b.y[3 * (f0 + j)] - s0;
-            b.t[3 * (f0 + j) + 1] = b.y[3 * (f0 + j) + 1] - s1;
-            b.t[3 * (f0 + j) + 2] = b.y[3 * (f0 + j) + 2] - s2;
-        }
+    const int j = j0 + warp;
+    if (j >= c) return;
+    double s0, s1, s2;
+    warp_dot3(a.front + a.front_off[s] + static_cast<long long>(j) * r + c, xr, 0, m, 0, lane, s0, s1, s2);
+    if (lane == 0) {
+        b.t[3 * (f0 + j)] = b.y[3 * (f0 + j)] - s0;
+        b.t[3 * (f0 + j) + 1] = b.y[3 * (f0 + j) + 1] - s1;
+        b.t[3 * (f0 + j) + 2] = b.y[3 * (f0 + j) + 2] - s2;
     }
 }
 
-// rows [i0, i0+32) of front s: x_J = L_JJ^{-T} t_J
+// rows [i0, i0+8) of front s: x_i = sum_{k>=i} (L_JJ^{-1})_ki t_k, one warp per row
 __global__ void __launch_bounds__(kST) k_bwd_x(FrontArgs a, SolveBufs b, const Tile* __restrict__ tiles)
 {
     extern __shared__ double sm[];
     const Tile tl = tiles[blockIdx.x];
     const int s = tl.s, i0 = tl.off;
     const int c = a.ncol[s], f0 = a.first[s];
-    double* t = sm;                         // [c - i0][3]
-    double* red = sm + 3 * (c - i0);        // [4][32][3]
-    const int tid = threadIdx.x;
+    double* t = sm;  // [c - i0][3]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int k = tid; k < 3 * (c - i0); k += kST) t[k] = b.t[3 * (f0 + i0) + k];
     __syncthreads();
-    const double* X = a.dinv + a.dinv_off[s];
-    const int row = tid % kRT, part = tid / kRT;
-    const int i = i0 + row;
-    double a0 = 0, a1 = 0, a2 = 0;
-    if (i < c)
-        for (int k = i0 + part; k < c; k += kST / kRT) {
-            if (k < i) continue;
-            const double d = X[static_cast<long long>(k) * c + i];
-            a0 += d * t[3 * (k - i0)];
-            a1 += d * t[3 * (k - i0) + 1];
-            a2 += d * t[3 * (k - i0) + 2];
-        }
-    red[3 * (part * kRT + row)] = a0;
-    red[3 * (part * kRT + row) + 1] = a1;
-    red[3 * (part * kRT + row) + 2] = a2;
-    __syncthreads();
-    if (tid < kRT && i < c) {
-        double x0 = 0, x1 = 0, x2 = 0;
-        for (int p = 0; p < kST / kRT; p++) {
-            x0 += red[3 * (p * kRT + row)];
-            x1 += red[3 * (p * kRT + row) + 1];
-            x2 += red[3 * (p * kRT + row) + 2];
-        }
+    const int i = i0 + warp;
+    if (i >= c) return;
+    double x0, x1, x2;
+    warp_dot3(a.dinvT + a.dinv_off[s] + static_cast<long long>(i) * c, t, i, c, i0, lane, x0, x1, x2);
+    if (lane == 0) {
         b.w[3 * (f0 + i)] = x0;
         b.w[3 * (f0 + i) + 1] = x1;
         b.w[3 * (f0 + i) + 2] = x2;
     }
 }
 
+// row-major copy of every front's L_RJ, columns [j0, j0+32) per CTA
+__global__ void __launch_bounds__(256) k_transpose_lt(FrontArgs a, const Tile* __restrict__ tiles)
+{
+    const Tile tl = tiles[blockIdx.x];
+    const int s = tl.s, j0 = tl.off;
+    const int r = a.nrow[s], c = a.ncol[s], m = r - c;
+    const int j = j0 + (threadIdx.x & 31);
+    if (j >= c) return;
+    const double* F = a.front + a.front_off[s] + static_cast<long long>(j) * r + c;
+    double* LT = a.lt + a.lt_off[s] + j;
+    for (int k = threadIdx.x >> 5; k < m; k += 8) LT[static_cast<long long>(k) * c] = F[k];
+}
+
 FrontArgs args_of(Precond& P)
 {
     return FrontArgs { P.d_first, P.d_ncol, P.d_nrow, P.d_rows, P.d_child_ptr, P.d_child_list, P.d_relind,
-        P.d_level_list, P.d_front_off, P.d_rows_off, P.d_relind_off, P.d_dinv_off, P.d_upd_off, P.d_front, P.d_dinv,
-        P.d_fail };
+        P.d_level_list, P.d_contrib_ptr, P.d_contrib_idx, P.d_front_off, P.d_rows_off, P.d_relind_off, P.d_dinv_off,
+        P.d_upd_off, P.d_lt_off, P.d_front, P.d_dinv, P.d_dinvT, P.d_lt, P.d_fail };
 }
-
-constexpr size_t kRed = 4 * kRT * 3;  // doubles of the per-tile partial sums
 
 // enqueue one H0 application (gather, levels, scatter) on stream st
 void enqueue_solve(const Precond& P, const FrontArgs& a, const SolveBufs& b, double* d_v, cudaStream_t st)
@@ -490,17 +475,17 @@ void enqueue_solve(const Precond& P, const FrontArgs& a, const SolveBufs& b, dou
     const int g = std::min(1184, (n + 255) / 256);
     k_gather_rhs<<<g, 256, 0, st>>>(b.w, d_v, P.d_perm, n);
     for (int l = 0; l < P.nlev; l++) {
+        const size_t smc = sizeof(double) * 3 * std::max(P.lev_max_c[l], 1);
         const int ny = P.fy_off[l + 1] - P.fy_off[l];
-        k_fwd_y<<<ny, kST, sizeof(double) * 3 * P.lev_max_c[l], st>>>(a, b, P.d_fy + P.fy_off[l]);
+        k_fwd_y<<<ny, kST, smc, st>>>(a, b, P.d_fy + P.fy_off[l]);
         const int ng = P.fg_off[l + 1] - P.fg_off[l];
-        if (ng > 0)
-            k_fwd_g<<<ng, kST, sizeof(double) * (3 * P.lev_max_c[l] + 3 * kRT + kRed), st>>>(a, b, P.d_fg + P.fg_off[l]);
+        if (ng > 0) k_fwd_g<<<ng, kST, smc, st>>>(a, b, P.d_fg + P.fg_off[l]);
     }
     for (int l = P.nlev - 1; l >= 0; l--) {
         const int nt = P.bt_off[l + 1] - P.bt_off[l];
         k_bwd_t<<<nt, kST, sizeof(double) * 3 * std::max(P.lev_max_m[l], 1), st>>>(a, b, P.d_bt + P.bt_off[l]);
         const int nx = P.bx_off[l + 1] - P.bx_off[l];
-        k_bwd_x<<<nx, kST, sizeof(double) * (3 * P.lev_max_c[l] + kRed), st>>>(a, b, P.d_bx + P.bx_off[l]);
+        k_bwd_x<<<nx, kST, sizeof(double) * 3 * std::max(P.lev_max_c[l], 1), st>>>(a, b, P.d_bx + P.bx_off[l]);
     }
     k_scatter_sol<<<g, 256, 0, st>>>(d_v, b.w, P.d_perm, n);
 }
@@ -515,13 +500,15 @@ void free_precond(Model& m)
     P.graphs.clear();
     if (P.capture) cudaStreamDestroy(P.capture);
     for (int** p : { &P.d_first, &P.d_ncol, &P.d_nrow, &P.d_rows, &P.d_child_ptr, &P.d_child_list, &P.d_relind,
-             &P.d_level_list, &P.d_perm, &P.d_fail, &P.d_panel_list })
+             &P.d_level_list, &P.d_perm, &P.d_fail, &P.d_panel_list, &P.d_contrib_ptr, &P.d_contrib_idx })
         dev_free(*p);
-    for (long long** p : { &P.d_front_off, &P.d_rows_off, &P.d_relind_off, &P.d_dinv_off, &P.d_upd_off, &P.d_a_pos, &P.d_a_src })
+    for (long long** p : { &P.d_front_off, &P.d_rows_off, &P.d_relind_off, &P.d_dinv_off, &P.d_upd_off, &P.d_a_pos,
+             &P.d_a_src, &P.d_lt_off })
         dev_free(*p);
     for (Tile** p : { &P.d_fy, &P.d_fg, &P.d_bt, &P.d_bx, &P.d_inv }) dev_free(*p);
     dev_free(P.d_syrk);
-    for (double** p : { &P.d_front, &P.d_dinv, &P.d_upd, &P.d_w, &P.d_y, &P.d_t, &P.d_vals }) dev_free(*p);
+    for (double** p : { &P.d_front, &P.d_dinv, &P.d_dinvT, &P.d_lt, &P.d_upd, &P.d_w, &P.d_y, &P.d_t, &P.d_vals })
+        dev_free(*p);
     delete m.precond;
     m.precond = nullptr;
 }
@@ -585,13 +572,13 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
             P.max_c = std::max(P.max_c, c);
             P.max_m = std::max(P.max_m, mm);
             maxc = std::max(maxc, c);
-            for (int o = 0; o < c; o += kRT) {
+            for (int o = 0; o < c; o += kSW) {
                 fy.push_back({ s, o });
                 bt.push_back({ s, o });
                 bx.push_back({ s, o });
-                inv.push_back({ s, o });
             }
-            for (int o = 0; o < mm; o += kRT) fg.push_back({ s, o });
+            for (int o = 0; o < c; o += kRT) inv.push_back({ s, o });
+            for (int o = 0; o < mm; o += kSW) fg.push_back({ s, o });
         }
         P.fy_off.push_back(static_cast<int>(fy.size()));
         P.fg_off.push_back(static_cast<int>(fg.size()));
@@ -617,7 +604,7 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
         P.lev_first_step.push_back(static_cast<int>(P.steps.size()));
     }
     P.n_inv_tiles = static_cast<int>(inv.size());
-    const size_t smem_need = sizeof(double) * (3 * static_cast<size_t>(std::max(P.max_c, P.max_m)) + 3 * kRT + kRed);
+    const size_t smem_need = sizeof(double) * 3 * static_cast<size_t>(std::max(P.max_c, P.max_m));
     if (smem_need > 200 * 1024) {
         set_error("a front of the approximate-Jacobian factor is too large for the solve kernels ("
             + std::to_string(P.max_r) + " rows)");
@@ -641,6 +628,9 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
     UP(P.d_relind_off, S.relind_off);
     UP(P.d_dinv_off, S.dinv_off);
     UP(P.d_upd_off, S.upd_off);
+    UP(P.d_lt_off, S.lt_off);
+    UP(P.d_contrib_ptr, S.contrib_ptr);
+    UP(P.d_contrib_idx, S.contrib_idx);
     UP(P.d_a_pos, S.a_pos);
     UP(P.d_a_src, S.a_src);
     UP(P.d_vals, vals);
@@ -655,6 +645,8 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
     const size_t n3 = 3 * static_cast<size_t>(std::max(S.n, 1));
     if ((st = dev_alloc(&P.d_front, static_cast<size_t>(S.front_size))) != EFEM_OK) return st;
     if ((st = dev_alloc(&P.d_dinv, static_cast<size_t>(std::max<long long>(S.dinv_size, 1)))) != EFEM_OK) return st;
+    if ((st = dev_alloc(&P.d_dinvT, static_cast<size_t>(std::max<long long>(S.dinv_size, 1)))) != EFEM_OK) return st;
+    if ((st = dev_alloc(&P.d_lt, static_cast<size_t>(std::max<long long>(S.lt_size, 1)))) != EFEM_OK) return st;
     if ((st = dev_alloc(&P.d_upd, static_cast<size_t>(std::max<long long>(S.upd_size, 1)))) != EFEM_OK) return st;
     if ((st = dev_alloc(&P.d_w, n3)) != EFEM_OK) return st;
     if ((st = dev_alloc(&P.d_y, n3)) != EFEM_OK) return st;
@@ -700,7 +692,8 @@ static efem_status precond_factor(Model& m, int* ok, double* ms_factor)
     }
     if (P.n_inv_tiles > 0) {
         k_inverse<<<P.n_inv_tiles, 32, 0, m.stream>>>(a, P.d_inv);
-        m.launches++;
+        k_transpose_lt<<<P.n_inv_tiles, 256, 0, m.stream>>>(a, P.d_inv);
+        m.launches += 2;
     }
     EFEM_CUDA(cudaGetLastError());
     EFEM_CUDA(cudaEventRecord(e1, m.stream));
@@ -755,6 +748,23 @@ efem_status precond_apply(Model& m, double* d_v)
     }
     Precond& P = *m.precond;
     return apply_with(m, d_v, SolveBufs { P.d_w, P.d_y, P.d_t, P.d_upd });
+}
+
+efem_status precond_enqueue(Model& m, double* d_v, cudaStream_t stream)
+{
+    if (!m.precond || !m.precond->factored || !m.precond->ok) {
+        set_error("preconditioner not factored");
+        return EFEM_ERR_ARG;
+    }
+    Precond& P = *m.precond;
+    if (P.S.n == 0) return EFEM_OK;
+    enqueue_solve(P, args_of(P), SolveBufs { P.d_w, P.d_y, P.d_t, P.d_upd }, d_v, stream);
+    return EFEM_OK;
+}
+
+long long precond_launch_count(const Model& m)
+{
+    return m.precond ? 2 + 4LL * m.precond->nlev : 0;
 }
 
 // ============================================================================

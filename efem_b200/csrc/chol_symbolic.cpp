@@ -295,7 +295,8 @@ void symbolic_analysis(int n, const std::vector<int>& rowptr, const std::vector<
     S.front_off.resize(ns + 1);
     S.dinv_off.resize(ns + 1);
     S.upd_off.resize(ns + 1);
-    S.front_off[0] = S.dinv_off[0] = S.upd_off[0] = 0;
+    S.lt_off.resize(ns + 1);
+    S.front_off[0] = S.dinv_off[0] = S.upd_off[0] = S.lt_off[0] = 0;
     S.nnz_L = 0;
     S.flops = 0;
     for (int k = 0; k < ns; k++) {
@@ -303,12 +304,37 @@ void symbolic_analysis(int n, const std::vector<int>& rowptr, const std::vector<
         S.front_off[k + 1] = S.front_off[k] + r * r;
         S.dinv_off[k + 1] = S.dinv_off[k] + c * c;
         S.upd_off[k + 1] = S.upd_off[k] + 3 * (r - c);
+        S.lt_off[k + 1] = S.lt_off[k] + (r - c) * c;
         S.nnz_L += c * r - c * (c - 1) / 2;
         S.flops += c * c * c / 3.0 + static_cast<double>(r - c) * c * c + static_cast<double>(r - c) * (r - c) * c;
     }
     S.front_size = S.front_off[ns];
     S.dinv_size = S.dinv_off[ns];
     S.upd_size = S.upd_off[ns];
+    S.lt_size = S.lt_off[ns];
+    // children's update-vector entries per parent row, in child order
+    {
+        std::vector<int> cnt(S.rows.size() + 1, 0);
+        for (int k = 0; k < ns; k++) {
+            if (S.parent[k] < 0) continue;
+            const long long base = S.rows_off[S.parent[k]];
+            for (long long j = S.relind_off[k]; j < S.relind_off[k + 1]; j++) cnt[base + S.relind[j] + 1]++;
+        }
+        for (size_t i = 0; i + 1 < cnt.size(); i++) cnt[i + 1] += cnt[i];
+        S.contrib_ptr = cnt;
+        S.contrib_idx.assign(cnt.back(), 0);
+        std::vector<int> fill(S.rows.size(), 0);
+        for (int s = 0; s < ns; s++)  // parents in order, children in list order
+            for (int q = S.child_ptr[s]; q < S.child_ptr[s + 1]; q++) {
+                const int ch = S.child_list[q];
+                const long long base = S.rows_off[s];
+                for (long long j = S.relind_off[ch]; j < S.relind_off[ch + 1]; j++) {
+                    const long long row = base + S.relind[j];
+                    S.contrib_idx[S.contrib_ptr[row] + fill[row]++] =
+                        static_cast<int>(S.upd_off[ch] / 3 + (j - S.relind_off[ch]));
+                }
+            }
+    }
     // original entries (lower triangle) -> front positions
     for (int o = 0; o < n; o++) {
         const int j = iperm[o];

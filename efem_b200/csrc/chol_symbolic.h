@@ -24,8 +24,13 @@ struct Symbolic {
     std::vector<int> relind;           // below rows of a front -> positions in the parent's rows
     std::vector<long long> dinv_off;   // c x c inverse of each diagonal block
     std::vector<long long> upd_off;    // (r - c) x 3 forward-solve update vector
+    std::vector<long long> lt_off;     // row-major copy of each front's L_RJ ((r - c) x c)
+    // for every front row (indexed rows_off[s] + t): the update-vector entries
+    // of the children that land on it, in child order (CSR over rows)
+    std::vector<int> contrib_ptr;
+    std::vector<int> contrib_idx;      // index of a node-triple in the update array (upd_off/3 + j)
     std::vector<int> level_ptr, level_list;  // fronts grouped by level, leaves first
-    long long front_size = 0, dinv_size = 0, upd_size = 0, nnz_L = 0;
+    long long front_size = 0, dinv_size = 0, upd_size = 0, lt_size = 0, nnz_L = 0;
     double flops = 0;
     // original entries: front position of each lower-triangle entry of the CSR
     std::vector<long long> a_pos;

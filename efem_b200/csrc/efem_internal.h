@@ -187,6 +187,7 @@ efem_status ensure_device(Model& m);  // create the stream and upload everything
 // ------------------------------------------------------------------ kernels (residual.cu)
 // r = R(u) on the model's stream; u, r device pointers of length 3*n_free.
 efem_status launch_residual(Model& m, const double* d_u, double* d_r);
+efem_status launch_residual_on(Model& m, const double* d_u, double* d_r, cudaStream_t stream);
 
 // ------------------------------------------------------------------ solver (solver.cu)
 efem_status run_solve(Model& m, double* d_u, efem_solve_info* info);
@@ -198,6 +199,10 @@ void free_solver(Model& m);
 efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor);
 // v <- (L (x) I3)^{-1} v in place on the device (v: 3*n_free interleaved).
 efem_status precond_apply(Model& m, double* d_v);
+// The same H0 application enqueued as plain kernels on `stream` (for capture
+// into a larger graph).
+efem_status precond_enqueue(Model& m, double* d_v, cudaStream_t stream);
+long long precond_launch_count(const Model& m);  // kernels per H0 application
 void free_precond(Model& m);
 void precond_info(const Model& m, efem_model_info* info);
 // Host assembly of L in CSR over free nodes (upper and lower triangle).

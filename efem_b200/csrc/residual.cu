@@ -275,29 +275,34 @@ void dispatch_face(const DevFaces& f, const T* J0, const T* tw, const T* tN, con
 
 efem_status launch_residual(Model& m, const double* d_u, double* d_r)
 {
+    return launch_residual_on(m, d_u, d_r, m.stream);
+}
+
+efem_status launch_residual_on(Model& m, const double* d_u, double* d_r, cudaStream_t stream)
+{
     const size_t n = 3 * static_cast<size_t>(m.n_free);
     if (n == 0) return EFEM_OK;
-    EFEM_CUDA(cudaMemcpyAsync(d_r, m.d_fext, n * sizeof(double), cudaMemcpyDeviceToDevice, m.stream));
+    EFEM_CUDA(cudaMemcpyAsync(d_r, m.d_fext, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
     // r = -f_ext
     extern void launch_scale(double* v, double s, size_t n, cudaStream_t st);
-    launch_scale(d_r, -1.0, n, m.stream);
+    launch_scale(d_r, -1.0, n, stream);
     m.launches++;
     const bool mixed = m.opts.precision == EFEM_MIXED;
     for (auto& b : m.blocks) {
         if (b.n == 0) continue;
         m.launches++;
         if (mixed)
-            dispatch_elem<float>(b, m.d_mats_f, b.vol_f, b.J0inv_f, b.dN_f, b.gw_f, m.n_free, d_u, d_r, m.stream);
+            dispatch_elem<float>(b, m.d_mats_f, b.vol_f, b.J0inv_f, b.dN_f, b.gw_f, m.n_free, d_u, d_r, stream);
         else
-            dispatch_elem<double>(b, m.d_mats, b.vol, b.J0inv, b.dN, b.gw, m.n_free, d_u, d_r, m.stream);
+            dispatch_elem<double>(b, m.d_mats, b.vol, b.J0inv, b.dN, b.gw, m.n_free, d_u, d_r, stream);
     }
     for (auto& f : m.faces) {
         if (f.n == 0) continue;
         m.launches++;
         if (mixed)
-            dispatch_face<float>(f, f.J0inv_f, f.t_w_f, f.t_N_f, f.t_dN_f, m.n_free, d_u, d_r, m.stream);
+            dispatch_face<float>(f, f.J0inv_f, f.t_w_f, f.t_N_f, f.t_dN_f, m.n_free, d_u, d_r, stream);
         else
-            dispatch_face<double>(f, f.J0inv, f.t_w, f.t_N, f.t_dN, m.n_free, d_u, d_r, m.stream);
+            dispatch_face<double>(f, f.J0inv, f.t_w, f.t_N, f.t_dN, m.n_free, d_u, d_r, stream);
     }
     EFEM_CUDA(cudaGetLastError());
     return EFEM_OK;

@@ -5,16 +5,21 @@
 // Vector work is done by grid-stride kernels; dot products and max-norms use a
 // deterministic two-level reduction (per-CTA partials, the last CTA to finish
 // combines them in a fixed order), so results are bitwise repeatable.  The
-// L-BFGS scalars (alpha_j, ys_j, theta) live in device memory and are produced
-// and consumed by kernels without host round trips.  The only host reads are
-// the three line-search scalars (r.d, ||r||_inf, ||x||_inf) after each residual
-// evaluation, which drive the reference's accept / scale decision.
+// L-BFGS state -- history pointer and count, alpha_j, ys_j, theta -- lives in
+// device memory and is produced and consumed by kernels only.
+//
+// One iteration's common path -- add_correction, the two-loop recursion with
+// H0, the start of the line search, its first trial x = xp + d, the residual
+// and the line-search reductions, plus the read-back of five scalars -- is
+// captured once as a CUDA graph and replayed, so an iteration costs one graph
+// launch and one host wait.  The host then makes the reference's
+// accept / scale decision; the rare further trials are launched directly.
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <chrono>
 #include <cmath>
 #include <cstring>
+#include <map>
 
 #include "efem_internal.h"
 
@@ -24,18 +29,18 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kMaxBlocks = 296;  // 2 x 148 SMs
+constexpr int kMaxHist = 64;
 
-// device-resident solver scalars
+// device-resident solver state; the first five doubles are read by the host
 struct Scalars {
-    double dg, rinf, xinf;   // line-search reads (slots 0..2, read by the host)
-    double x2;               // ||x||_2^2
-    double dg0;
+    double dg, rinf, xinf, x2;  // line-search reads (r.d, ||r||_inf, ||x||_inf, ||x||_2^2)
+    double dg0;                 // r.d at the start of the line search
     double theta;
-    double yy;
-    double tmp;
-    double ys[64];
-    double alpha[64];
-    double coef[64];
+    double ys[kMaxHist];
+    double alpha[kMaxHist];
+    double coef[kMaxHist];
+    int ptr, ncorr;             // LBFGSMat::m_ptr, m_ncorr
+    int ptr_next, ncorr_next;
     unsigned int counter[8];
 };
 
@@ -67,7 +72,7 @@ __device__ void block_reduce(double* v, const int* ops)
     if (w == 0) {
 #pragma unroll
         for (int k = 0; k < NV; k++) {
-            double x = lane < kThreads / 32 ? sh[k][lane] : (ops[k] ? 0.0 : 0.0);
+            const double x = lane < kThreads / 32 ? sh[k][lane] : 0.0;
             v[k] = ops[k] ? warp_max(x) : warp_sum(x);
         }
     }
@@ -109,16 +114,24 @@ __device__ bool grid_finish(double* v, const int* ops, double* partials, unsigne
     return threadIdx.x == 0;
 }
 
+#define GRID_STRIDE(i, n) for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (n); i += (size_t)gridDim.x * blockDim.x)
+
 __global__ void k_scale(double* v, double s, size_t n)
 {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) v[i] *= s;
+    GRID_STRIDE(i, n) v[i] *= s;
+}
+
+__global__ void k_state_init(Scalars* S, int m)
+{
+    S->ptr = m;  // makes ptr % m == 0 on the first correction (LBFGSMat.h:68)
+    S->ncorr = 0;
+    S->theta = 1.0;
 }
 
 // x = xp + step d
 __global__ void k_trial(double* __restrict__ x, const double* __restrict__ xp, const double* __restrict__ d, double step, size_t n)
 {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        x[i] = xp[i] + step * d[i];
+    GRID_STRIDE(i, n) x[i] = xp[i] + step * d[i];
 }
 
 // line-search scalars: dg = r.d, rinf = ||r||_inf, xinf = ||x||_inf, x2 = ||x||^2
@@ -127,7 +140,8 @@ __global__ void __launch_bounds__(kThreads) k_ls_reduce(const double* __restrict
 {
     double v[4] = { 0, 0, 0, 0 };
     const int ops[4] = { 0, 1, 1, 0 };
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    GRID_STRIDE(i, n)
+    {
         const double ri = r[i], xi = x[i];
         v[0] += ri * d[i];
         v[1] = fmax(v[1], fabs(ri));
@@ -150,7 +164,8 @@ __global__ void __launch_bounds__(kThreads) k_ls_begin(const double* __restrict_
 {
     double v[1] = { 0 };
     const int ops[1] = { 0 };
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    GRID_STRIDE(i, n)
+    {
         const double ri = r[i];
         v[0] += ri * d[i];
         xp[i] = x[i];
@@ -160,14 +175,19 @@ __global__ void __launch_bounds__(kThreads) k_ls_begin(const double* __restrict_
     if (grid_finish<1>(v, ops, partials, &S->counter[1])) S->dg0 = v[0];
 }
 
-// add_correction: s = x - xp, y = r - rp into history slot loc; ys, theta = yy/ys
+// add_correction (LBFGSMat.h:81-98): s = x - xp, y = r - rp into slot ptr % m;
+// ys, theta = yy/ys; the new pointer and count take effect in k_advance_neg.
 __global__ void __launch_bounds__(kThreads) k_correction(const double* __restrict__ x, const double* __restrict__ xp,
-    const double* __restrict__ r, const double* __restrict__ rp, double* __restrict__ s, double* __restrict__ y, size_t n,
-    int loc, Scalars* S, double* partials)
+    const double* __restrict__ r, const double* __restrict__ rp, double* __restrict__ Sh, double* __restrict__ Yh,
+    size_t n, int m, Scalars* S, double* partials)
 {
+    const int loc = S->ptr % m;
+    double* s = Sh + loc * n;
+    double* y = Yh + loc * n;
     double v[2] = { 0, 0 };
     const int ops[2] = { 0, 0 };
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    GRID_STRIDE(i, n)
+    {
         const double si = x[i] - xp[i], yi = r[i] - rp[i];
         s[i] = si;
         y[i] = yi;
@@ -177,139 +197,133 @@ __global__ void __launch_bounds__(kThreads) k_correction(const double* __restric
     block_reduce<2>(v, ops);
     if (grid_finish<2>(v, ops, partials, &S->counter[2])) {
         S->ys[loc] = v[0];
-        S->yy = v[1];
         S->theta = v[1] / v[0];
+        S->ptr_next = loc + 1;
+        S->ncorr_next = S->ncorr < m ? S->ncorr + 1 : m;
     }
 }
 
-// q = a * v (first use) -- here a = -1 and v = r
-__global__ void k_neg_copy(double* __restrict__ q, const double* __restrict__ r, size_t n)
+// commit the new history pointer / count, and start the two-loop with q = -r
+__global__ void k_advance_neg(double* __restrict__ q, const double* __restrict__ r, size_t n, Scalars* S)
 {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) q[i] = -r[i];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        S->ptr = S->ptr_next;
+        S->ncorr = S->ncorr_next;
+    }
+    GRID_STRIDE(i, n) q[i] = -r[i];
 }
 
-// Two-loop step of the first loop, fused with the previous update:
-//   q -= alpha[prev] * y_prev   (if prev >= 0),   alpha[j] = s_j . q / ys[j]
-__global__ void __launch_bounds__(kThreads) k_loop1(double* __restrict__ q, const double* __restrict__ yprev, int prev,
-    const double* __restrict__ sj, int j, size_t n, Scalars* S, double* partials)
+__global__ void k_neg_copy(double* __restrict__ q, const double* __restrict__ r, size_t n)
 {
-    const double ap = prev >= 0 ? S->alpha[prev] : 0.0;
+    GRID_STRIDE(i, n) q[i] = -r[i];
+}
+
+// first loop, step i (newest history first), fused with step i-1's update:
+//   q -= alpha[j_{i-1}] y_{j_{i-1}};  alpha[j_i] = s_{j_i} . q / ys[j_i]
+// j_i = (ptr - 1 - i) mod m; a step beyond ncorr does nothing
+__global__ void __launch_bounds__(kThreads) k_loop1(double* __restrict__ q, const double* __restrict__ Sh,
+    const double* __restrict__ Yh, int i, int m, size_t n, Scalars* S, double* partials)
+{
+    const int ncorr = S->ncorr, ptr = S->ptr;
+    if (i >= ncorr) return;
+    const int j = ((ptr - 1 - i) % m + m) % m;
+    const int jp = ((ptr - i) % m + m) % m;
+    const double ap = i > 0 ? S->alpha[jp] : 0.0;
+    const double* yp = Yh + jp * n;
+    const double* sj = Sh + j * n;
     double v[1] = { 0 };
     const int ops[1] = { 0 };
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        double qi = q[i];
-        if (prev >= 0) {
-            qi -= ap * yprev[i];
-            q[i] = qi;
+    GRID_STRIDE(t, n)
+    {
+        double qi = q[t];
+        if (i > 0) {
+            qi -= ap * yp[t];
+            q[t] = qi;
         }
-        v[0] += sj[i] * qi;
+        v[0] += sj[t] * qi;
     }
     block_reduce<1>(v, ops);
     if (grid_finish<1>(v, ops, partials, &S->counter[3])) S->alpha[j] = v[0] / S->ys[j];
 }
 
-// last update of the first loop, then H0 = I/theta when there is no factor
-__global__ void k_loop1_tail(double* __restrict__ q, const double* __restrict__ yprev, int prev, int divide_theta, size_t n,
+// last update of the first loop; H0 = I/theta when there is no factor
+__global__ void k_loop1_tail(double* __restrict__ q, const double* __restrict__ Yh, int m, int divide_theta, size_t n,
     const Scalars* S)
 {
-    const double ap = prev >= 0 ? S->alpha[prev] : 0.0;
-    const double it = divide_theta ? 1.0 / S->theta : 1.0;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        double qi = q[i];
-        if (prev >= 0) qi -= ap * yprev[i];
-        if (divide_theta) qi = qi / S->theta;
-        q[i] = qi;
+    const int ncorr = S->ncorr, ptr = S->ptr;
+    const int jl = ((ptr - ncorr) % m + m) % m;  // j of step ncorr - 1 (the oldest)
+    const double al = ncorr > 0 ? S->alpha[jl] : 0.0;
+    const double* yl = Yh + jl * n;
+    const double th = S->theta;
+    GRID_STRIDE(t, n)
+    {
+        double qi = q[t];
+        if (ncorr > 0) qi -= al * yl[t];
+        if (divide_theta) qi = qi / th;
+        q[t] = qi;
     }
-    (void)it;
 }
 
-// Second loop step, fused with the previous update:
-//   q += coef[prev] * s_prev (if prev >= 0),  coef[j] = alpha[j] - y_j . q / ys[j]
-__global__ void __launch_bounds__(kThreads) k_loop2(double* __restrict__ q, const double* __restrict__ sprev, int prev,
-    const double* __restrict__ yj, int j, size_t n, Scalars* S, double* partials)
+// second loop, step i (oldest first), fused with step i-1's update:
+//   q += coef[j_{i-1}] s_{j_{i-1}};  coef[j_i] = alpha[j_i] - y_{j_i} . q / ys[j_i]
+// j_i = (ptr - ncorr + i) mod m
+__global__ void __launch_bounds__(kThreads) k_loop2(double* __restrict__ q, const double* __restrict__ Sh,
+    const double* __restrict__ Yh, int i, int m, size_t n, Scalars* S, double* partials)
 {
-    const double cp = prev >= 0 ? S->coef[prev] : 0.0;
+    const int ncorr = S->ncorr, ptr = S->ptr;
+    if (i >= ncorr) return;
+    const int j = ((ptr - ncorr + i) % m + m) % m;
+    const int jp = ((ptr - ncorr + i - 1) % m + m) % m;
+    const double cp = i > 0 ? S->coef[jp] : 0.0;
+    const double* sp = Sh + jp * n;
+    const double* yj = Yh + j * n;
     double v[1] = { 0 };
     const int ops[1] = { 0 };
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        double qi = q[i];
-        if (prev >= 0) {
-            qi += cp * sprev[i];
-            q[i] = qi;
+    GRID_STRIDE(t, n)
+    {
+        double qi = q[t];
+        if (i > 0) {
+            qi += cp * sp[t];
+            q[t] = qi;
         }
-        v[0] += yj[i] * qi;
+        v[0] += yj[t] * qi;
     }
     block_reduce<1>(v, ops);
     if (grid_finish<1>(v, ops, partials, &S->counter[4])) S->coef[j] = S->alpha[j] - v[0] / S->ys[j];
 }
 
-// d = q + coef[prev] s_prev
-__global__ void k_loop2_tail(double* __restrict__ d, const double* __restrict__ q, const double* __restrict__ sprev, int prev,
+// d = q + coef[j_last] s_{j_last}, j_last the newest slot
+__global__ void k_loop2_tail(double* __restrict__ d, const double* __restrict__ q, const double* __restrict__ Sh, int m,
     size_t n, const Scalars* S)
 {
-    const double cp = prev >= 0 ? S->coef[prev] : 0.0;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        d[i] = prev >= 0 ? q[i] + cp * sprev[i] : q[i];
+    const int ncorr = S->ncorr, ptr = S->ptr;
+    const int jl = ((ptr - 1) % m + m) % m;
+    const double cl = ncorr > 0 ? S->coef[jl] : 0.0;
+    const double* sl = Sh + jl * n;
+    GRID_STRIDE(t, n) d[t] = ncorr > 0 ? q[t] + cl * sl[t] : q[t];
 }
 
 int grid_for(size_t n) { return static_cast<int>(std::min<size_t>(kMaxBlocks, std::max<size_t>(1, (n + kThreads * 4 - 1) / (kThreads * 4)))); }
 
 }  // namespace
 
-// CUDA-event timing of the solve's phases: a pair of events around each
-// residual evaluation / H0 application, harvested after the host syncs the
-// line search already needs.
-struct PhaseTimer {
-    static constexpr int kPairs = 32;
-    cudaEvent_t ev[2 * kPairs] = {};
-    int kind[kPairs] = {};
-    int used = 0;
-    double acc[2] = { 0, 0 };
-    cudaError_t init()
-    {
-        for (auto& e : ev)
-            if (!e) {
-                cudaError_t s = cudaEventCreate(&e);
-                if (s != cudaSuccess) return s;
-            }
-        return cudaSuccess;
-    }
-    void destroy()
-    {
-        for (auto& e : ev)
-            if (e) cudaEventDestroy(e);
-    }
-    int begin(int k, cudaStream_t st)
-    {
-        if (used == kPairs) return -1;  // pool full: this phase goes unmeasured
-        kind[used] = k;
-        cudaEventRecord(ev[2 * used], st);
-        return used++;
-    }
-    void end(int slot, cudaStream_t st)
-    {
-        if (slot >= 0) cudaEventRecord(ev[2 * slot + 1], st);
-    }
-    void harvest()  // call only after the stream has been synchronised
-    {
-        for (int i = 0; i < used; i++) {
-            float ms = 0;
-            if (cudaEventElapsedTime(&ms, ev[2 * i], ev[2 * i + 1]) == cudaSuccess) acc[kind[i]] += ms;
-        }
-        used = 0;
-    }
-};
-
 struct SolverWS {
-    PhaseTimer timer;
     size_t n = 0;
     int m = 0;
     double *r = nullptr, *xp = nullptr, *rp = nullptr, *d = nullptr, *q = nullptr;
     double *S = nullptr, *Y = nullptr;
     double* partials = nullptr;
     Scalars* sc = nullptr;
-    double* h_read = nullptr;  // pinned
-    cudaEvent_t ev[4] = { nullptr, nullptr, nullptr, nullptr };
+    double* h_read = nullptr;  // pinned: the five line-search scalars
+    cudaEvent_t ev[2] = { nullptr, nullptr };
+    // event pairs around the residual and H0, recorded inside the graphs too
+    cudaEvent_t gev[4] = { nullptr, nullptr, nullptr, nullptr };
+    cudaStream_t capture = nullptr;
+    struct Graphs {
+        cudaGraphExec_t first = nullptr;  // line-search start + first trial (iteration 1)
+        cudaGraphExec_t body = nullptr;   // correction + two-loop + H0 + line-search start + first trial
+    };
+    std::map<std::pair<double*, int>, Graphs> graphs;  // per (solution pointer, configuration)
 };
 
 void launch_scale(double* v, double s, size_t n, cudaStream_t st)
@@ -317,10 +331,20 @@ void launch_scale(double* v, double s, size_t n, cudaStream_t st)
     k_scale<<<grid_for(n), kThreads, 0, st>>>(v, s, n);
 }
 
+static void drop_graphs(SolverWS& w)
+{
+    for (auto& kv : w.graphs) {
+        if (kv.second.first) cudaGraphExecDestroy(kv.second.first);
+        if (kv.second.body) cudaGraphExecDestroy(kv.second.body);
+    }
+    w.graphs.clear();
+}
+
 void free_solver(Model& m)
 {
     if (!m.ws) return;
     SolverWS& w = *m.ws;
+    drop_graphs(w);
     dev_free(w.r);
     dev_free(w.xp);
     dev_free(w.rp);
@@ -333,7 +357,9 @@ void free_solver(Model& m)
     if (w.h_read) cudaFreeHost(w.h_read);
     for (auto& e : w.ev)
         if (e) cudaEventDestroy(e);
-    w.timer.destroy();
+    for (auto& e : w.gev)
+        if (e) cudaEventDestroy(e);
+    if (w.capture) cudaStreamDestroy(w.capture);
     delete m.ws;
     m.ws = nullptr;
 }
@@ -343,7 +369,7 @@ static efem_status alloc_ws(Model& m)
     const size_t n = 3 * static_cast<size_t>(m.n_free);
     if (m.ws && m.ws->n == n && m.ws->m == m.opts.m) return EFEM_OK;
     free_solver(m);
-    if (m.opts.m > 64) {
+    if (m.opts.m > kMaxHist) {
         set_error("history length m is limited to 64");
         return EFEM_ERR_ARG;
     }
@@ -361,9 +387,80 @@ static efem_status alloc_ws(Model& m)
     EFEM_CUDA(cudaMemset(w.sc, 0, sizeof(Scalars)));
     EFEM_CUDA(cudaMallocHost(&w.h_read, sizeof(double) * 8));
     for (auto& e : w.ev) EFEM_CUDA(cudaEventCreate(&e));
-    EFEM_CUDA(w.timer.init());
+    for (auto& e : w.gev) EFEM_CUDA(cudaEventCreate(&e));
+    EFEM_CUDA(cudaStreamCreateWithFlags(&w.capture, cudaStreamNonBlocking));
     return EFEM_OK;
 }
+
+namespace {
+
+// one line-search trial with step 1 (after xp = x, rp = r, dg0 = r.d), its
+// residual and reductions, and the scalar read-back
+efem_status enqueue_first_trial(Model& m, SolverWS& w, double* x, cudaStream_t st)
+{
+    const size_t n = w.n;
+    const int G = grid_for(n);
+    k_ls_begin<<<G, kThreads, 0, st>>>(w.r, w.d, x, w.xp, w.rp, n, w.sc, w.partials);
+    k_trial<<<G, kThreads, 0, st>>>(x, w.xp, w.d, 1.0, n);
+    EFEM_CUDA(cudaEventRecordWithFlags(w.gev[0], st, cudaEventRecordExternal));
+    efem_status s = launch_residual_on(m, x, w.r, st);
+    if (s != EFEM_OK) return s;
+    EFEM_CUDA(cudaEventRecordWithFlags(w.gev[1], st, cudaEventRecordExternal));
+    k_ls_reduce<<<G, kThreads, 0, st>>>(w.r, w.d, x, n, w.sc, w.partials);
+    EFEM_CUDA(cudaMemcpyAsync(w.h_read, w.sc, sizeof(double) * 5, cudaMemcpyDeviceToHost, st));
+    return EFEM_OK;
+}
+
+// add_correction + two-loop + H0, leaving the new direction in w.d
+efem_status enqueue_direction(Model& m, SolverWS& w, double* x, bool use_factor, cudaStream_t st)
+{
+    const size_t n = w.n;
+    const int G = grid_for(n), mm = w.m;
+    k_correction<<<G, kThreads, 0, st>>>(x, w.xp, w.r, w.rp, w.S, w.Y, n, mm, w.sc, w.partials);
+    k_advance_neg<<<G, kThreads, 0, st>>>(w.q, w.r, n, w.sc);
+    for (int i = 0; i < mm; i++) k_loop1<<<G, kThreads, 0, st>>>(w.q, w.S, w.Y, i, mm, n, w.sc, w.partials);
+    k_loop1_tail<<<G, kThreads, 0, st>>>(w.q, w.Y, mm, use_factor ? 0 : 1, n, w.sc);
+    if (use_factor) {
+        EFEM_CUDA(cudaEventRecordWithFlags(w.gev[2], st, cudaEventRecordExternal));
+        efem_status s = precond_enqueue(m, w.q, st);
+        if (s != EFEM_OK) return s;
+        EFEM_CUDA(cudaEventRecordWithFlags(w.gev[3], st, cudaEventRecordExternal));
+    }
+    for (int i = 0; i < mm; i++) k_loop2<<<G, kThreads, 0, st>>>(w.q, w.S, w.Y, i, mm, n, w.sc, w.partials);
+    k_loop2_tail<<<G, kThreads, 0, st>>>(w.d, w.q, w.S, mm, n, w.sc);
+    return EFEM_OK;
+}
+
+efem_status capture(Model& m, SolverWS& w, double* x, bool use_factor, bool with_direction, cudaGraphExec_t* out)
+{
+    const long long launches = m.launches;  // capture launches nothing; replays are counted
+    cudaGraph_t g = nullptr;
+    EFEM_CUDA(cudaStreamBeginCapture(w.capture, cudaStreamCaptureModeThreadLocal));
+    efem_status s = EFEM_OK;
+    if (with_direction) s = enqueue_direction(m, w, x, use_factor, w.capture);
+    if (s == EFEM_OK) s = enqueue_first_trial(m, w, x, w.capture);
+    const cudaError_t e = cudaStreamEndCapture(w.capture, &g);
+    m.launches = launches;
+    if (s != EFEM_OK) {
+        if (g) cudaGraphDestroy(g);
+        return s;
+    }
+    if (e != cudaSuccess) {
+        set_error(std::string("graph capture: ") + cudaGetErrorString(e));
+        return EFEM_ERR_CUDA;
+    }
+    EFEM_CUDA(cudaGraphInstantiate(out, g, 0));
+    cudaGraphDestroy(g);
+    return EFEM_OK;
+}
+
+double elapsed_ms(cudaEvent_t a, cudaEvent_t b)
+{
+    float ms = 0.f;
+    return cudaEventElapsedTime(&ms, a, b) == cudaSuccess ? static_cast<double>(ms) : 0.0;
+}
+
+}  // namespace
 
 efem_status run_solve(Model& m, double* x, efem_solve_info* info)
 {
@@ -377,47 +474,46 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
     const double eps = m.opts.residual_criterion;
     std::memset(info, 0, sizeof(*info));
     const long long launches0 = m.launches;
+    const long long per_res = 1 + static_cast<long long>(m.blocks.size() + m.faces.size());
+    double ms_res = 0.0, ms_pc = 0.0;
+    double rinf = 0.0, xinf = 0.0;
+    int k = 1;
+    bool converged = false, ok = false;
     EFEM_CUDA(cudaEventRecord(w.ev[0], st));
-    float ms_res = 0.f;
 
-    w.timer.used = 0;
-    w.timer.acc[0] = w.timer.acc[1] = 0;
-    auto residual = [&](const double* xx) -> efem_status {
+    // direct (non-graph) line-search trial: x = xp + step d (step 0: x as is),
+    // residual, reductions, read-back
+    auto direct_trial = [&](double step) -> efem_status {
+        if (step != 0.0) {
+            k_trial<<<G, kThreads, 0, st>>>(x, w.xp, w.d, step, n);
+            m.launches++;
+        }
+        EFEM_CUDA(cudaEventRecord(w.gev[0], st));
+        efem_status rs = launch_residual_on(m, x, w.r, st);
+        if (rs != EFEM_OK) return rs;
+        EFEM_CUDA(cudaEventRecord(w.gev[1], st));
         info->n_residual_evals++;
-        const int t = w.timer.begin(0, st);
-        efem_status rs = launch_residual(m, xx, w.r);
-        w.timer.end(t, st);
-        return rs;
-    };
-    auto precond = [&](double* v) -> efem_status {
-        info->n_precond_applies++;
-        const int t = w.timer.begin(1, st);
-        efem_status rs = precond_apply(m, v);
-        w.timer.end(t, st);
-        return rs;
-    };
-    auto read_ls = [&]() -> efem_status {
-        m.launches++;
         k_ls_reduce<<<G, kThreads, 0, st>>>(w.r, w.d, x, n, w.sc, w.partials);
-        EFEM_CUDA(cudaMemcpyAsync(w.h_read, w.sc, sizeof(double) * 4, cudaMemcpyDeviceToHost, st));
+        m.launches++;
+        EFEM_CUDA(cudaMemcpyAsync(w.h_read, w.sc, sizeof(double) * 5, cudaMemcpyDeviceToHost, st));
         EFEM_CUDA(cudaStreamSynchronize(st));
-        w.timer.harvest();
+        ms_res += elapsed_ms(w.gev[0], w.gev[1]);
         return EFEM_OK;
     };
 
     // initial residual and early exit (LBFGS.h:110-120); d = 0 so dg = 0 here
     EFEM_CUDA(cudaMemsetAsync(w.d, 0, n * sizeof(double), st));
-    if ((s = residual(x)) != EFEM_OK) return s;
-    if ((s = read_ls()) != EFEM_OK) return s;
-    double rinf = w.h_read[1], xinf = w.h_read[2];
-    int k = 1;
-    bool converged = false, ok = false;
+    k_state_init<<<1, 1, 0, st>>>(w.sc, mm);
+    m.launches++;
+    if ((s = direct_trial(0.0)) != EFEM_OK) return s;
+    rinf = w.h_read[1];
+    xinf = w.h_read[2];
     if (!(std::isfinite(rinf))) goto nan_exit;
     if (rinf <= eps || rinf <= eps * std::sqrt(w.h_read[3])) {
         converged = true;
         goto done;
     }
-    // approximate-Jacobian factor, once (LBFGS.h:122-124)
+    // approximate-Jacobian factor, once per solve (LBFGS.h:122-124)
     if (m.opts.nl_solver == 0) {
         int okf = 0;
         double msf = 0;
@@ -428,26 +524,45 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
         if (!ok) info->flags |= EFEM_SOLVE_PRECOND_FALLBACK;
     }
     // initial direction d = -H0 r
-    m.launches++;
     k_neg_copy<<<G, kThreads, 0, st>>>(w.d, w.r, n);
-    if (ok && (s = precond(w.d)) != EFEM_OK) return s;
+    m.launches++;
+    if (ok) {
+        EFEM_CUDA(cudaEventRecord(w.gev[2], st));
+        if ((s = precond_apply(m, w.d)) != EFEM_OK) return s;
+        EFEM_CUDA(cudaEventRecord(w.gev[3], st));
+        EFEM_CUDA(cudaStreamSynchronize(st));
+        ms_pc += elapsed_ms(w.gev[2], w.gev[3]);
+        info->n_precond_applies++;
+    }
     {
-        int ncorr = 0, ptr = mm;
+        const auto key = std::make_pair(x, (ok ? 1 : 0) | (m.opts.precision << 1));
+        if (!w.graphs.count(key) && w.graphs.size() >= 8) drop_graphs(w);  // many distinct solution pointers
+        SolverWS::Graphs& gr = w.graphs[key];
+        if (!gr.first) {
+            if ((s = capture(m, w, x, ok, false, &gr.first)) != EFEM_OK) return s;
+            if ((s = capture(m, w, x, ok, true, &gr.body)) != EFEM_OK) return s;
+        }
+        const long long per_dir = 5 + 2LL * mm + (ok ? precond_launch_count(m) : 0);
+        bool first = true;
         for (;;) {
-            m.launches++;
-            k_ls_begin<<<G, kThreads, 0, st>>>(w.r, w.d, x, w.xp, w.rp, n, w.sc, w.partials);
-            EFEM_CUDA(cudaMemcpyAsync(w.h_read + 4, &w.sc->dg0, sizeof(double), cudaMemcpyDeviceToHost, st));
-            // residual-projection line search (LineSearchFEA.h:43-67); dg0 is read
-            // together with the first trial's scalars
-            double step = 1.0;
-            for (int it = 0; it < m.opts.max_linesearch; it++) {
-                m.launches++;
-                k_trial<<<G, kThreads, 0, st>>>(x, w.xp, w.d, step, n);
-                if ((s = residual(x)) != EFEM_OK) return s;
-                if ((s = read_ls()) != EFEM_OK) return s;
-                const double dg = w.h_read[0], dg0 = w.h_read[4];
-                if (std::fabs(dg) <= std::fabs(dg0)) break;
+            // common path: one graph launch, one wait
+            EFEM_CUDA(cudaGraphLaunch(first ? gr.first : gr.body, st));
+            EFEM_CUDA(cudaStreamSynchronize(st));
+            m.launches += 3 + per_res + (first ? 0 : per_dir);
+            ms_res += elapsed_ms(w.gev[0], w.gev[1]);
+            if (!first && ok) {
+                ms_pc += elapsed_ms(w.gev[2], w.gev[3]);
+                info->n_precond_applies++;
+            }
+            info->n_residual_evals++;
+            first = false;
+            // residual-projection line search (LineSearchFEA.h:43-67); trial 1 done
+            const double dg0 = w.h_read[4];
+            double dg = w.h_read[0], step = 1.0;
+            for (int it = 1; it < m.opts.max_linesearch && !(std::fabs(dg) <= std::fabs(dg0)); it++) {
                 step *= dg * dg0 > 0 ? 1.5 : 0.5;
+                if ((s = direct_trial(step)) != EFEM_OK) return s;
+                dg = w.h_read[0];
             }
             rinf = w.h_read[1];
             xinf = w.h_read[2];
@@ -460,50 +575,15 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
                 info->flags |= EFEM_SOLVE_MAX_ITERS;
                 break;
             }
-            // add_correction (LBFGSMat.h:81-98)
-            const int loc = ptr % mm;
-            m.launches++;
-            k_correction<<<G, kThreads, 0, st>>>(x, w.xp, w.r, w.rp, w.S + loc * n, w.Y + loc * n, n, loc, w.sc, w.partials);
-            if (ncorr < mm) ncorr++;
-            ptr = loc + 1;
-            // d = -H r, two-loop recursion (LBFGSMat.h:103-131)
-            m.launches++;
-            k_neg_copy<<<G, kThreads, 0, st>>>(w.q, w.r, n);
-            int j = ptr % mm, prev = -1;
-            for (int i = 0; i < ncorr; i++) {
-                j = (j + mm - 1) % mm;
-                m.launches++;
-                k_loop1<<<G, kThreads, 0, st>>>(w.q, prev >= 0 ? w.Y + prev * n : nullptr, prev, w.S + j * n, j, n, w.sc, w.partials);
-                prev = j;
-            }
-            m.launches++;
-            k_loop1_tail<<<G, kThreads, 0, st>>>(w.q, prev >= 0 ? w.Y + prev * n : nullptr, prev, ok ? 0 : 1, n, w.sc);
-            if (ok && (s = precond(w.q)) != EFEM_OK) return s;
-            prev = -1;
-            for (int i = 0; i < ncorr; i++) {
-                m.launches++;
-                k_loop2<<<G, kThreads, 0, st>>>(w.q, prev >= 0 ? w.S + prev * n : nullptr, prev, w.Y + j * n, j, n, w.sc, w.partials);
-                prev = j;
-                j = (j + 1) % mm;
-            }
-            m.launches++;
-            k_loop2_tail<<<G, kThreads, 0, st>>>(w.d, w.q, prev >= 0 ? w.S + prev * n : nullptr, prev, n, w.sc);
-            EFEM_CUDA(cudaGetLastError());
             k++;
         }
     }
 done:
     EFEM_CUDA(cudaEventRecord(w.ev[1], st));
     EFEM_CUDA(cudaEventSynchronize(w.ev[1]));
-    w.timer.harvest();
-    {
-        float ms = 0;
-        cudaEventElapsedTime(&ms, w.ev[0], w.ev[1]);
-        info->ms_total = ms;
-    }
-    info->ms_residual = w.timer.acc[0];
-    info->ms_precond = w.timer.acc[1];
-    (void)ms_res;
+    info->ms_total = elapsed_ms(w.ev[0], w.ev[1]);
+    info->ms_residual = ms_res;
+    info->ms_precond = ms_pc;
     info->niter = k;
     info->u_inf = xinf;
     info->r_inf = rinf;
@@ -518,6 +598,7 @@ nan_exit:
     info->niter = k;
     info->u_inf = xinf;
     info->r_inf = rinf;
+    info->n_kernel_launches = m.launches - launches0;
     set_error("L-BFGS produced a non-finite residual or solution");
     return EFEM_ERR_NAN;
 }
