@@ -79,7 +79,10 @@ struct Precond {
     long long *d_front_off = nullptr, *d_rows_off = nullptr, *d_relind_off = nullptr, *d_dinv_off = nullptr,
               *d_upd_off = nullptr, *d_a_pos = nullptr, *d_a_src = nullptr;
     Tile *d_fy = nullptr, *d_fg = nullptr, *d_bt = nullptr, *d_bx = nullptr, *d_inv = nullptr;
-    int *d_contrib_ptr = nullptr, *d_contrib_idx = nullptr;
+    int *d_contrib_ptr = nullptr, *d_contrib_idx = nullptr, *d_below_front = nullptr;
+    Tile *d_ea = nullptr, *d_oinv = nullptr;  // extend-add column tiles, off-diagonal inverse column groups
+    std::vector<int> ea_off;                  // nlev + 1
+    int n_oinv = 0;
     long long* d_lt_off = nullptr;
     double *d_dinvT = nullptr, *d_lt = nullptr;
     int4* d_syrk = nullptr;
@@ -93,7 +96,8 @@ struct Precond {
 namespace {
 
 struct FrontArgs {
-    const int *first, *ncol, *nrow, *rows, *child_ptr, *child_list, *relind, *level_list, *contrib_ptr, *contrib_idx;
+    const int *first, *ncol, *nrow, *rows, *child_ptr, *child_list, *relind, *level_list, *contrib_ptr, *contrib_idx,
+        *below_front;
     const long long *front_off, *rows_off, *relind_off, *dinv_off, *upd_off, *lt_off;
     double* front;
     double* dinv;   // L_JJ^{-1}, row-major
@@ -124,23 +128,29 @@ __global__ void k_scatter_a(double* __restrict__ front, const long long* __restr
         front[pos[k]] = vals[src[k]];
 }
 
-// children's update blocks into the front (children in list order)
-__global__ void __launch_bounds__(kFT) k_extend_add(FrontArgs a, int level_base)
+// Children's update blocks into the fronts of one level, one warp per front
+// column p (8 per CTA): the contributions landing on column p are added in
+// child order, each one a column j of a child's update block whose rows
+// i >= j go to the parent rows relind[i].  No two warps touch the same entry,
+// so the sums need no atomics and are bitwise repeatable.
+__global__ void __launch_bounds__(kFT) k_extend_add(FrontArgs a, const Tile* __restrict__ tiles)
 {
-    const int s = a.level_list[level_base + blockIdx.x];
+    const Tile tl = tiles[blockIdx.x];
+    const int s = tl.s;
+    const int p = tl.off + (threadIdx.x >> 5), lane = threadIdx.x & 31;
     const int r = a.nrow[s];
-    double* F = a.front + a.front_off[s];
-    for (int q = a.child_ptr[s]; q < a.child_ptr[s + 1]; q++) {
-        const int ch = a.child_list[q];
+    if (p >= r) return;
+    double* Fp = a.front + a.front_off[s] + static_cast<long long>(p) * r;
+    const long long row = a.rows_off[s] + p;
+    for (int q = a.contrib_ptr[row]; q < a.contrib_ptr[row + 1]; q++) {
+        const int idx = a.contrib_idx[q];
+        const int ch = a.below_front[idx];
+        const int j = idx - static_cast<int>(a.upd_off[ch] / 3);
         const int rc = a.nrow[ch], cc = a.ncol[ch], m = rc - cc;
         const int* ri = a.relind + a.relind_off[ch];
-        const double* U = a.front + a.front_off[ch];
-        for (int j = 0; j < m; j++) {
-            const long long dst = static_cast<long long>(ri[j]) * r;
-            const long long src = static_cast<long long>(cc + j) * rc + cc;
-            for (int i = j + threadIdx.x; i < m; i += kFT) F[ri[i] + dst] += U[i + src];
-        }
-        __syncthreads();
+        const double* U = a.front + a.front_off[ch] + static_cast<long long>(cc + j) * rc + cc;
+        for (int i = j + lane; i < m; i += 32) Fp[ri[i]] += U[i];
+        __syncwarp();
     }
 }
 
@@ -251,31 +261,128 @@ __global__ void __launch_bounds__(kFT) k_syrk(FrontArgs a, const int4* __restric
 
 // Inverse of the diagonal block, row-major: X = L_JJ^{-1}.  One warp per 32
 // columns; lane j owns column j and reads only its own earlier entries.
-__global__ void __launch_bounds__(32) k_inverse(FrontArgs a, const Tile* __restrict__ tiles)
+// L_JJ^{-1} in two passes.  Pass 1: the inverse of every 32x32 diagonal tile,
+// one warp per tile, column j of the inverse by forward substitution in
+// shared memory; the tile's upper triangle is written as zeros because pass 2
+// reads whole tiles.
+__global__ void __launch_bounds__(32) k_diag_inv(FrontArgs a, const Tile* __restrict__ tiles)
 {
     const Tile tl = tiles[blockIdx.x];
     const int s = tl.s, j0 = tl.off;
     const int r = a.nrow[s], c = a.ncol[s];
-    const double* L = a.front + a.front_off[s];
+    const int kb = min(kRT, c - j0);
+    const double* F = a.front + a.front_off[s];
+    __shared__ double D[kRT][kRT + 1];
+    __shared__ double X[kRT][kRT + 1];
+    const int j = threadIdx.x;
+    for (int k = 0; k < kb; k++) D[j][k] = j < kb ? F[static_cast<long long>(j0 + k) * r + j0 + j] : 0.0;
+    __syncwarp();
+    for (int i = 0; i < kb; i++) {  // thread j owns column j of X
+        double v = 0.0;
+        if (i == j) {
+            v = 1.0 / D[i][i];
+        } else if (i > j) {
+            double acc = 0.0;
+            for (int k = j; k < i; k++) acc += D[i][k] * X[k][j];
+            v = -acc / D[i][i];
+        }
+        X[i][j] = v;
+    }
+    __syncwarp();
+    if (j >= kb) return;
+    double* Xg = a.dinv + a.dinv_off[s];
+    double* XTg = a.dinvT + a.dinv_off[s];
+    for (int i = 0; i < kb; i++) {
+        Xg[static_cast<long long>(j0 + i) * c + j0 + j] = X[i][j];
+        XTg[static_cast<long long>(j0 + i) * c + j0 + j] = X[j][i];
+    }
+}
+
+// Pass 2: the tiles below the diagonal, for 8 columns [j0, j0+8) per CTA.
+// With J the diagonal tile holding the columns, block row I > J of the
+// inverse is X_IJ = -X_II sum_{K=J}^{I-1} L_IK X_KJ (left-looking, the
+// columns are independent).  The next L_IK / X_KJ tiles are fetched into
+// registers while the current ones are multiplied.
+constexpr int kIC = 8;     // columns per CTA
+constexpr int kIT = 128;   // threads per CTA
+__global__ void __launch_bounds__(kIT) k_offdiag_inv(FrontArgs a, const Tile* __restrict__ tiles)
+{
+    const Tile tl = tiles[blockIdx.x];
+    const int s = tl.s, j0 = tl.off;
+    const int r = a.nrow[s], c = a.ncol[s];
+    const int jb0 = (j0 / kRT) * kRT;
+    if (jb0 + kRT >= c) return;  // no tile below the diagonal one
+    const double* F = a.front + a.front_off[s];
     double* X = a.dinv + a.dinv_off[s];
     double* XT = a.dinvT + a.dinv_off[s];
-    const int j = j0 + threadIdx.x;
-    const bool valid = j < c;
-    for (int i = 0; i < j0; i++)
-        if (valid) {
-            X[static_cast<long long>(i) * c + j] = 0.0;
-            XT[static_cast<long long>(j) * c + i] = 0.0;
+    __shared__ double As[kRT][kRT + 1];
+    __shared__ double Bs[kRT][kIC + 1];
+    const int tid = threadIdx.x, jj = tid & (kIC - 1), ii = tid >> 3;  // rows ii and ii + 16
+    const int ncols = min(kIC, c - j0);
+    double pa[kRT * kRT / kIT], pb[kRT * kIC / kIT];
+    auto fetch = [&](int i0, int ib, int k0) {
+#pragma unroll
+        for (int q = 0; q < kRT * kRT / kIT; q++) {
+            const int idx = tid + q * kIT, kk = idx >> 5, rr = idx & 31;
+            pa[q] = rr < ib ? F[static_cast<long long>(k0 + kk) * r + i0 + rr] : 0.0;
         }
-    for (int i = j0; i < c; i++) {
-        const double* Li = L + i;
-        double acc = 0.0;
-        for (int k = j0; k < i; k++) acc += Li[static_cast<long long>(k) * r] * (valid ? X[static_cast<long long>(k) * c + j] : 0.0);
-        const double lii = Li[static_cast<long long>(i) * r];
-        const double v = (i < j) ? 0.0 : (i == j ? 1.0 / lii : -acc / lii);
-        if (valid) {
-            X[static_cast<long long>(i) * c + j] = v;
-            XT[static_cast<long long>(j) * c + i] = v;
+#pragma unroll
+        for (int q = 0; q < kRT * kIC / kIT; q++) {
+            const int idx = tid + q * kIT, kk = idx >> 3, cc = idx & 7;
+            pb[q] = cc < ncols ? X[static_cast<long long>(k0 + kk) * c + j0 + cc] : 0.0;
         }
+    };
+    for (int i0 = jb0 + kRT; i0 < c; i0 += kRT) {
+        const int ib = min(kRT, c - i0);
+        double acc0 = 0.0, acc1 = 0.0;
+        fetch(i0, ib, jb0);
+        for (int k0 = jb0; k0 < i0; k0 += kRT) {
+#pragma unroll
+            for (int q = 0; q < kRT * kRT / kIT; q++) {
+                const int idx = tid + q * kIT;
+                As[idx & 31][idx >> 5] = pa[q];
+            }
+#pragma unroll
+            for (int q = 0; q < kRT * kIC / kIT; q++) {
+                const int idx = tid + q * kIT;
+                Bs[idx >> 3][idx & 7] = pb[q];
+            }
+            __syncthreads();
+            if (k0 + kRT < i0) fetch(i0, ib, k0 + kRT);
+#pragma unroll 8
+            for (int kk = 0; kk < kRT; kk++) {
+                const double b = Bs[kk][jj];
+                acc0 += As[ii][kk] * b;
+                acc1 += As[ii + 16][kk] * b;
+            }
+            __syncthreads();
+        }
+        // X_IJ = -X_II T, X_II lower triangular with its zeros stored
+        Bs[ii][jj] = acc0;
+        Bs[ii + 16][jj] = acc1;
+        for (int idx = tid; idx < kRT * kRT; idx += kIT) {
+            const int rr = idx >> 5, kk = idx & 31;
+            As[rr][kk] = (rr < ib && kk < ib) ? X[static_cast<long long>(i0 + rr) * c + i0 + kk] : 0.0;
+        }
+        __syncthreads();
+        double x0 = 0.0, x1 = 0.0;
+#pragma unroll 8
+        for (int kk = 0; kk < kRT; kk++) {
+            const double t = Bs[kk][jj];
+            x0 += As[ii][kk] * t;
+            x1 += As[ii + 16][kk] * t;
+        }
+        if (jj < ncols) {
+            if (ii < ib) {
+                X[static_cast<long long>(i0 + ii) * c + j0 + jj] = -x0;
+                XT[static_cast<long long>(j0 + jj) * c + i0 + ii] = -x0;
+            }
+            if (ii + 16 < ib) {
+                X[static_cast<long long>(i0 + ii + 16) * c + j0 + jj] = -x1;
+                XT[static_cast<long long>(j0 + jj) * c + i0 + ii + 16] = -x1;
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -463,7 +570,7 @@ __global__ void __launch_bounds__(256) k_transpose_lt(FrontArgs a, const Tile* _
 FrontArgs args_of(Precond& P)
 {
     return FrontArgs { P.d_first, P.d_ncol, P.d_nrow, P.d_rows, P.d_child_ptr, P.d_child_list, P.d_relind,
-        P.d_level_list, P.d_contrib_ptr, P.d_contrib_idx, P.d_front_off, P.d_rows_off, P.d_relind_off, P.d_dinv_off,
+        P.d_level_list, P.d_contrib_ptr, P.d_contrib_idx, P.d_below_front, P.d_front_off, P.d_rows_off, P.d_relind_off, P.d_dinv_off,
         P.d_upd_off, P.d_lt_off, P.d_front, P.d_dinv, P.d_dinvT, P.d_lt, P.d_fail };
 }
 
@@ -500,12 +607,12 @@ void free_precond(Model& m)
     P.graphs.clear();
     if (P.capture) cudaStreamDestroy(P.capture);
     for (int** p : { &P.d_first, &P.d_ncol, &P.d_nrow, &P.d_rows, &P.d_child_ptr, &P.d_child_list, &P.d_relind,
-             &P.d_level_list, &P.d_perm, &P.d_fail, &P.d_panel_list, &P.d_contrib_ptr, &P.d_contrib_idx })
+             &P.d_level_list, &P.d_perm, &P.d_fail, &P.d_panel_list, &P.d_contrib_ptr, &P.d_contrib_idx, &P.d_below_front })
         dev_free(*p);
     for (long long** p : { &P.d_front_off, &P.d_rows_off, &P.d_relind_off, &P.d_dinv_off, &P.d_upd_off, &P.d_a_pos,
              &P.d_a_src, &P.d_lt_off })
         dev_free(*p);
-    for (Tile** p : { &P.d_fy, &P.d_fg, &P.d_bt, &P.d_bx, &P.d_inv }) dev_free(*p);
+    for (Tile** p : { &P.d_fy, &P.d_fg, &P.d_bt, &P.d_bx, &P.d_inv, &P.d_ea, &P.d_oinv }) dev_free(*p);
     dev_free(P.d_syrk);
     for (double** p : { &P.d_front, &P.d_dinv, &P.d_dinvT, &P.d_lt, &P.d_upd, &P.d_w, &P.d_y, &P.d_t, &P.d_vals })
         dev_free(*p);
@@ -551,7 +658,8 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
     P.nlev = static_cast<int>(S.level_ptr.size()) - 1;
     const int nlev = P.nlev;
     // solve and factor schedules
-    std::vector<Tile> fy, fg, bt, bx, inv;
+    std::vector<Tile> fy, fg, bt, bx, inv, ea, oinv;
+    P.ea_off.assign(1, 0);
     std::vector<int> panel_list;
     std::vector<int4> syrk;
     P.fy_off.assign(1, 0);
@@ -578,12 +686,17 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
                 bx.push_back({ s, o });
             }
             for (int o = 0; o < c; o += kRT) inv.push_back({ s, o });
+            for (int jb = 0; jb + kRT < c; jb += kRT)  // diagonal tiles with rows below them
+                for (int o = jb; o < jb + kRT; o += kIC) oinv.push_back({ s, o });
+            if (S.child_ptr[s + 1] > S.child_ptr[s])
+                for (int o = 0; o < S.nrow[s]; o += kFT / 32) ea.push_back({ s, o });
             for (int o = 0; o < mm; o += kSW) fg.push_back({ s, o });
         }
         P.fy_off.push_back(static_cast<int>(fy.size()));
         P.fg_off.push_back(static_cast<int>(fg.size()));
         P.bt_off.push_back(static_cast<int>(bt.size()));
         P.bx_off.push_back(static_cast<int>(bx.size()));
+        P.ea_off.push_back(static_cast<int>(ea.size()));
         for (int k0 = 0; k0 < maxc; k0 += kNB) {
             Precond::Step st { l, k0, static_cast<int>(panel_list.size()), 0, static_cast<int>(syrk.size()), 0 };
             for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) {
@@ -604,6 +717,7 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
         P.lev_first_step.push_back(static_cast<int>(P.steps.size()));
     }
     P.n_inv_tiles = static_cast<int>(inv.size());
+    P.n_oinv = static_cast<int>(oinv.size());
     const size_t smem_need = sizeof(double) * 3 * static_cast<size_t>(std::max(P.max_c, P.max_m));
     if (smem_need > 200 * 1024) {
         set_error("a front of the approximate-Jacobian factor is too large for the solve kernels ("
@@ -639,6 +753,9 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
     UP(P.d_bt, bt);
     UP(P.d_bx, bx);
     UP(P.d_inv, inv);
+    UP(P.d_oinv, oinv);
+    UP(P.d_ea, ea);
+    UP(P.d_below_front, S.below_front);
     UP(P.d_panel_list, panel_list);
     UP(P.d_syrk, syrk);
 #undef UP
@@ -677,9 +794,11 @@ static efem_status precond_factor(Model& m, int* ok, double* ms_factor)
     m.launches++;
     FrontArgs a = args_of(P);
     for (int l = 0; l < P.nlev; l++) {
-        const int cnt = S.level_ptr[l + 1] - S.level_ptr[l];
-        k_extend_add<<<cnt, kFT, 0, m.stream>>>(a, S.level_ptr[l]);
-        m.launches++;
+        const int cnt = P.ea_off[l + 1] - P.ea_off[l];
+        if (cnt > 0) {
+            k_extend_add<<<cnt, kFT, 0, m.stream>>>(a, P.d_ea + P.ea_off[l]);
+            m.launches++;
+        }
         for (int q = P.lev_first_step[l]; q < P.lev_first_step[l + 1]; q++) {
             const Precond::Step& stp = P.steps[q];
             k_panel<<<stp.panel_cnt, kFT, 0, m.stream>>>(a, P.d_panel_list + stp.panel_off, stp.k0);
@@ -691,9 +810,13 @@ static efem_status precond_factor(Model& m, int* ok, double* ms_factor)
         }
     }
     if (P.n_inv_tiles > 0) {
-        k_inverse<<<P.n_inv_tiles, 32, 0, m.stream>>>(a, P.d_inv);
-        k_transpose_lt<<<P.n_inv_tiles, 256, 0, m.stream>>>(a, P.d_inv);
+        k_diag_inv<<<P.n_inv_tiles, 32, 0, m.stream>>>(a, P.d_inv);
         m.launches += 2;
+        if (P.n_oinv > 0) {
+            k_offdiag_inv<<<P.n_oinv, kIT, 0, m.stream>>>(a, P.d_oinv);
+            m.launches++;
+        }
+        k_transpose_lt<<<P.n_inv_tiles, 256, 0, m.stream>>>(a, P.d_inv);
     }
     EFEM_CUDA(cudaGetLastError());
     EFEM_CUDA(cudaEventRecord(e1, m.stream));

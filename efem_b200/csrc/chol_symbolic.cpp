@@ -322,6 +322,9 @@ void symbolic_analysis(int n, const std::vector<int>& rowptr, const std::vector<
         }
         for (size_t i = 0; i + 1 < cnt.size(); i++) cnt[i + 1] += cnt[i];
         S.contrib_ptr = cnt;
+        S.below_front.assign(static_cast<size_t>(S.upd_size / 3), 0);
+        for (int k = 0; k < ns; k++)
+            for (long long q = S.upd_off[k] / 3; q < S.upd_off[k + 1] / 3; q++) S.below_front[q] = k;
         S.contrib_idx.assign(cnt.back(), 0);
         std::vector<int> fill(S.rows.size(), 0);
         for (int s = 0; s < ns; s++)  // parents in order, children in list order

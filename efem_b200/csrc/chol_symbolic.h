@@ -29,6 +29,7 @@ struct Symbolic {
     // of the children that land on it, in child order (CSR over rows)
     std::vector<int> contrib_ptr;
     std::vector<int> contrib_idx;      // index of a node-triple in the update array (upd_off/3 + j)
+    std::vector<int> below_front;      // for each such index, the front whose update array holds it
     std::vector<int> level_ptr, level_list;  // fronts grouped by level, leaves first
     long long front_size = 0, dinv_size = 0, upd_size = 0, lt_size = 0, nnz_L = 0;
     double flops = 0;
