@@ -49,6 +49,7 @@ constexpr int kTS = 64;   // SYRK tile
 constexpr int kST = 256;  // solve threads: one warp per output row / column
 constexpr int kSW = kST / 32;  // outputs per solve CTA
 constexpr int kRT = 32;   // columns per CTA of the inverse / transpose kernels
+constexpr long long kWholeFront = 8192;  // staged factor entries (c^2 + c m) up to which one CTA solves a whole front
 
 struct Tile {
     int s;    // front
@@ -63,9 +64,12 @@ struct Precond {
     bool ok = false;        // factor is positive definite
     double ms_factor = 0;
     int max_r = 0, max_c = 0, max_m = 0, nlev = 0;
-    // solve schedule: tiles per level for the four solve kernels
-    std::vector<int> fy_off, fg_off, bt_off, bx_off;  // nlev + 1 offsets each
-    std::vector<int> lev_max_c, lev_max_m;
+    // solve schedule: the persistent kernel's items, launch shape
+    int n_items = 0, solve_grid = 1;
+    size_t solve_smem = 0;
+    int4* d_items = nullptr;
+    int *d_tgt = nullptr, *d_parent = nullptr, *d_cnt = nullptr, *d_prow = nullptr;
+    int stage_d = 0, work_d = 0;
     // factor schedule: per (level, step) the fronts with a panel at that step and the SYRK tiles
     struct Step {
         int level, k0, panel_off, panel_cnt, syrk_off, syrk_cnt;
@@ -78,7 +82,7 @@ struct Precond {
         *d_panel_list = nullptr;
     long long *d_front_off = nullptr, *d_rows_off = nullptr, *d_relind_off = nullptr, *d_dinv_off = nullptr,
               *d_upd_off = nullptr, *d_a_pos = nullptr, *d_a_src = nullptr;
-    Tile *d_fy = nullptr, *d_fg = nullptr, *d_bt = nullptr, *d_bx = nullptr, *d_inv = nullptr;
+    Tile* d_inv = nullptr;
     int *d_contrib_ptr = nullptr, *d_contrib_idx = nullptr, *d_below_front = nullptr;
     Tile *d_ea = nullptr, *d_oinv = nullptr;  // extend-add column tiles, off-diagonal inverse column groups
     std::vector<int> ea_off;                  // nlev + 1
@@ -86,7 +90,7 @@ struct Precond {
     long long* d_lt_off = nullptr;
     double *d_dinvT = nullptr, *d_lt = nullptr;
     int4* d_syrk = nullptr;
-    double *d_front = nullptr, *d_dinv = nullptr, *d_upd = nullptr, *d_w = nullptr, *d_y = nullptr, *d_t = nullptr,
+    double *d_front = nullptr, *d_dinv = nullptr, *d_upd = nullptr, *d_y = nullptr, *d_t = nullptr,
            *d_vals = nullptr;
     // graph replay of the solve, per (input vector, work buffers)
     cudaStream_t capture = nullptr;
@@ -106,12 +110,6 @@ struct FrontArgs {
     int* fail;
 };
 
-struct SolveBufs {
-    double* w;    // b, then x (permuted order, 3 per node)
-    double* y;    // forward result
-    double* t;    // backward intermediate
-    double* upd;  // fronts' update vectors
-};
 
 __device__ __forceinline__ double wsum(double v)
 {
@@ -387,42 +385,117 @@ __global__ void __launch_bounds__(kIT) k_offdiag_inv(FrontArgs a, const Tile* __
 }
 
 // ------------------------------------------------------------------ solves
-__global__ void k_gather_rhs(double* __restrict__ w, const double* __restrict__ v, const int* __restrict__ perm, int n)
+//
+// One persistent launch runs the whole solve H0 v (in place on v, 3 values per
+// node).  Its work is a list of items in dependency order -- the forward
+// sweep leaves first, then the backward sweep root first -- and every CTA
+// takes the next item from a ticket counter.  An item waits until the items
+// it depends on have finished (per-front completion counters), so a front
+// starts as soon as its children (forward) or its parent (backward) are done,
+// with no barrier between levels.  An item only waits on items with smaller
+// tickets, which were taken by CTAs already running, so the wait always ends
+// whatever the number of resident CTAs; each wait is still bounded, and a
+// wait that runs out sets the error flag and makes every later wait give up.
+//
+// Before it waits, a CTA stages everything of its item that does not depend
+// on other items -- the factor blocks it multiplies with and the index lists
+// of the assembly -- into shared memory with cp.async, so only the dependent
+// vectors are fetched after the wait.
+//
+// Item kinds (a small front is one item per sweep, one thread per output; a
+// large one is split into tiles of kSW rows or columns, one warp per output):
+//   kFwdFront  y_J = L_JJ^{-1} f_J and g = f_R - L_RJ y_J for a whole front
+//   kFwdY      y rows of one tile             (waits: children's g)
+//   kFwdG      update rows of one tile        (waits: the front's y)
+//   kBwdFront  t_J = y_J - L_RJ^T x_R and x_J = L_JJ^{-T} t_J for a whole front
+//   kBwdT      t columns of one tile          (waits: own y, parent's x)
+//   kBwdX      x rows of one tile             (waits: the front's t)
+// f = b_J (own columns) + the children's update entries, summed in a fixed
+// order; every dot product has a fixed order too, so results are repeatable.
+enum ItemKind { kFwdFront = 0, kFwdY = 1, kFwdG = 2, kBwdFront = 3, kBwdT = 4, kBwdX = 5 };
+
+// device counters, one int array: [cY ns][cGin ns][cT ns][cX ns][ticket][error]
+struct SolveArgs {
+    FrontArgs a;
+    const int* parent;
+    const int* prow;    // per front row (rows_off[s] + t): the node's index in v
+    const int4* items;  // {kind | offset << 3, front, first contribution, end of contributions}
+    const int* tgt;     // targets of the four counter groups
+    int n_items, ns;
+    int stage_d, work_d;  // shared-memory layout: staged doubles, work doubles, then ints
+    double* v;
+    double* y;
+    double* t;
+    double* upd;
+    int* cnt;
+};
+
+constexpr int kSpinLimit = 1 << 22;  // polls of one wait (about half a second)
+
+__device__ __forceinline__ int ld_acquire(const int* p)
 {
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const int o = perm[k];
-        w[3 * k] = v[3 * o];
-        w[3 * k + 1] = v[3 * o + 1];
-        w[3 * k + 2] = v[3 * o + 2];
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// thread 0 only: wait until *c >= target; false on a timeout or an earlier error
+__device__ bool wait_ge(const int* c, int target, int* err)
+{
+    for (int it = 0;; it++) {
+        if (ld_acquire(c) >= target) return true;
+        if (*reinterpret_cast<volatile int*>(err)) return false;
+        if (it >= kSpinLimit) {
+            atomicExch(err, 1);
+            return false;
+        }
+        __nanosleep(64);
     }
 }
 
-__global__ void k_scatter_sol(double* __restrict__ v, const double* __restrict__ w, const int* __restrict__ perm, int n)
+__device__ __forceinline__ void ld3(const double* p, double& a, double& b, double& c)
 {
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const int o = perm[k];
-        v[3 * o] = w[3 * k];
-        v[3 * o + 1] = w[3 * k + 1];
-        v[3 * o + 2] = w[3 * k + 2];
-    }
+    a = __ldcg(p);
+    b = __ldcg(p + 1);
+    c = __ldcg(p + 2);
 }
 
-// Dot product of a contiguous row with a 3-component vector held in shared
-// memory, over k in [k0, k1); the 32 lanes stride the row with four loads in
-// flight each, then the warp reduces.
-__device__ __forceinline__ void warp_dot3(const double* __restrict__ row, const double* __restrict__ v, int k0, int k1,
-    int vbase, int lane, double& s0, double& s1, double& s2)
+// block-cooperative asynchronous copies global -> shared
+__device__ __forceinline__ void stage_d(double* dst, const double* src, int n)
+{
+    for (int i = threadIdx.x; i < n; i += kST) {
+        const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst + i));
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src + i) : "memory");
+    }
+}
+__device__ __forceinline__ void stage_i(int* dst, const int* src, int n)
+{
+    for (int i = threadIdx.x; i < n; i += kST) {
+        const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst + i));
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src + i) : "memory");
+    }
+}
+// columns [j0, j1) of the front's below-diagonal block (column-major), as (j - j0) * m + k
+__device__ __forceinline__ void stage_panel(double* dst, const double* F, int r, int c, int j0, int j1)
+{
+    const int m = r - c, n = (j1 - j0) * m;
+    for (int i = threadIdx.x; i < n; i += kST) {
+        const int j = i / m, k = i - j * m;
+        const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst + i));
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d),
+            "l"(F + static_cast<long long>(j0 + j) * r + c + k) : "memory");
+    }
+}
+__device__ __forceinline__ void stage_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void stage_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Dot product of a row held in shared memory with a 3-component vector also
+// in shared memory, over k in [k0, k1); lanes stride k, then the warp reduces.
+__device__ __forceinline__ void warp_dot3(const double* row, const double* v, int k0, int k1, int vbase, int lane,
+    double& s0, double& s1, double& s2)
 {
     double a0 = 0, a1 = 0, a2 = 0;
-    int k = k0 + lane;
-    for (; k + 96 < k1; k += 128) {
-        const double d0 = row[k], d1 = row[k + 32], d2 = row[k + 64], d3 = row[k + 96];
-        const double* v0 = v + 3 * (k - vbase);
-        a0 += d0 * v0[0] + d1 * v0[96] + d2 * v0[192] + d3 * v0[288];
-        a1 += d0 * v0[1] + d1 * v0[97] + d2 * v0[193] + d3 * v0[289];
-        a2 += d0 * v0[2] + d1 * v0[98] + d2 * v0[194] + d3 * v0[290];
-    }
-    for (; k < k1; k += 32) {
+    for (int k = k0 + lane; k < k1; k += 32) {
         const double d = row[k];
         const double* v0 = v + 3 * (k - vbase);
         a0 += d * v0[0];
@@ -434,123 +507,288 @@ __device__ __forceinline__ void warp_dot3(const double* __restrict__ row, const 
     s2 = wsum(a2);
 }
 
-// f_t = (b_t for own columns) + the children's update entries landing on row t
-__device__ __forceinline__ void assemble_row(const FrontArgs& a, const SolveBufs& b, int s, int t, bool own, int f0,
-    double& f0v, double& f1v, double& f2v)
+// f_t for front rows [t0, t1) into f (3 per row): the right-hand side for own
+// columns (t < c) plus the children's update entries landing on the row, from
+// the staged contribution pointers cp (row t0 first) and indices ci (starting
+// at contribution cbeg) and the staged node indices pr (row t0 first)
+__device__ __forceinline__ void assemble(const SolveArgs& A, int t0, int t1, int c, const int* cp, const int* ci,
+    int cbeg, const int* pr, double* f)
 {
-    double x0 = 0, x1 = 0, x2 = 0;
-    if (own) {
-        x0 = b.w[3 * (f0 + t)];
-        x1 = b.w[3 * (f0 + t) + 1];
-        x2 = b.w[3 * (f0 + t) + 2];
-    }
-    const long long row = a.rows_off[s] + t;
-    for (int q = a.contrib_ptr[row]; q < a.contrib_ptr[row + 1]; q++) {
-        const double* g = b.upd + 3LL * a.contrib_idx[q];
-        x0 += g[0];
-        x1 += g[1];
-        x2 += g[2];
-    }
-    f0v = x0;
-    f1v = x1;
-    f2v = x2;
-}
-
-// y rows [i0, i0+8) of front s: y_i = sum_{k<=i} (L_JJ^{-1})_ik f_k, one warp per row
-__global__ void __launch_bounds__(kST) k_fwd_y(FrontArgs a, SolveBufs b, const Tile* __restrict__ tiles)
-{
-    extern __shared__ double sm[];
-    const Tile tl = tiles[blockIdx.x];
-    const int s = tl.s, i0 = tl.off;
-    const int c = a.ncol[s], f0 = a.first[s];
-    const int kmax = min(c, i0 + kSW);
-    double* f = sm;  // [kmax][3]
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int k = tid; k < kmax; k += kST) assemble_row(a, b, s, k, true, f0, f[3 * k], f[3 * k + 1], f[3 * k + 2]);
-    __syncthreads();
-    const int i = i0 + warp;
-    if (i >= kmax) return;
-    double y0, y1, y2;
-    warp_dot3(a.dinv + a.dinv_off[s] + static_cast<long long>(i) * c, f, 0, i + 1, 0, lane, y0, y1, y2);
-    if (lane == 0) {
-        b.y[3 * (f0 + i)] = y0;
-        b.y[3 * (f0 + i) + 1] = y1;
-        b.y[3 * (f0 + i) + 2] = y2;
+    for (int t = t0 + static_cast<int>(threadIdx.x); t < t1; t += kST) {
+        double x0 = 0, x1 = 0, x2 = 0;
+        if (t < c) ld3(A.v + 3LL * pr[t - t0], x0, x1, x2);
+        for (int q = cp[t - t0]; q < cp[t - t0 + 1]; q++) {
+            double g0, g1, g2;
+            ld3(A.upd + 3LL * ci[q - cbeg], g0, g1, g2);
+            x0 += g0;
+            x1 += g1;
+            x2 += g2;
+        }
+        double* o = f + 3 * (t - t0);
+        o[0] = x0;
+        o[1] = x1;
+        o[2] = x2;
     }
 }
 
-// update rows [k0, k0+8) of front s: g_k = f_{c+k} - (L_RJ)_k . y_J, one warp per row
-__global__ void __launch_bounds__(kST) k_fwd_g(FrontArgs a, SolveBufs b, const Tile* __restrict__ tiles)
+__global__ void __launch_bounds__(kST) k_solve(SolveArgs A)
 {
     extern __shared__ double sm[];
-    const Tile tl = tiles[blockIdx.x];
-    const int s = tl.s, k0 = tl.off;
-    const int r = a.nrow[s], c = a.ncol[s], m = r - c, f0 = a.first[s];
-    double* y = sm;  // [c][3]
+    double* st = sm;                    // staged factor data
+    double* wk = sm + A.stage_d;        // work vectors
+    int* si = reinterpret_cast<int*>(wk + A.work_d);  // staged index lists
+    __shared__ int item_sh, ok_sh;
+    const int ns = A.ns;
+    int* cY = A.cnt;
+    int* cGin = A.cnt + ns;
+    int* cT = A.cnt + 2 * ns;
+    int* cX = A.cnt + 3 * ns;
+    int* ticket = A.cnt + 4 * ns;
+    int* err = ticket + 1;
+    const int* tY = A.tgt;
+    const int* tGin = A.tgt + ns;
+    const int* tT = A.tgt + 2 * ns;
+    const int* tX = A.tgt + 3 * ns;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int k = tid; k < 3 * c; k += kST) y[k] = b.y[3 * f0 + k];
-    __syncthreads();
-    const int k = k0 + warp;
-    if (k >= m) return;
-    double d0, d1, d2;
-    warp_dot3(a.lt + a.lt_off[s] + static_cast<long long>(k) * c, y, 0, c, 0, lane, d0, d1, d2);
-    if (lane == 0) {
-        double f0v, f1v, f2v;
-        assemble_row(a, b, s, c + k, false, f0, f0v, f1v, f2v);
-        double* g = b.upd + a.upd_off[s] + 3 * k;
-        g[0] = f0v - d0;
-        g[1] = f1v - d1;
-        g[2] = f2v - d2;
-    }
-}
-
-// columns [j0, j0+8) of front s: t_j = y_j - (L_RJ)^T_j . x_R, one warp per column
-__global__ void __launch_bounds__(kST) k_bwd_t(FrontArgs a, SolveBufs b, const Tile* __restrict__ tiles)
-{
-    extern __shared__ double sm[];
-    const Tile tl = tiles[blockIdx.x];
-    const int s = tl.s, j0 = tl.off;
-    const int r = a.nrow[s], c = a.ncol[s], m = r - c, f0 = a.first[s];
-    double* xr = sm;  // [m][3]
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int* rows = a.rows + a.rows_off[s] + c;
-    for (int k = tid; k < m; k += kST) {
-        const int g = rows[k];
-        xr[3 * k] = b.w[3 * g];
-        xr[3 * k + 1] = b.w[3 * g + 1];
-        xr[3 * k + 2] = b.w[3 * g + 2];
-    }
-    __syncthreads();
-    const int j = j0 + warp;
-    if (j >= c) return;
-    double s0, s1, s2;
-    warp_dot3(a.front + a.front_off[s] + static_cast<long long>(j) * r + c, xr, 0, m, 0, lane, s0, s1, s2);
-    if (lane == 0) {
-        b.t[3 * (f0 + j)] = b.y[3 * (f0 + j)] - s0;
-        b.t[3 * (f0 + j) + 1] = b.y[3 * (f0 + j) + 1] - s1;
-        b.t[3 * (f0 + j) + 2] = b.y[3 * (f0 + j) + 2] - s2;
-    }
-}
-
-// rows [i0, i0+8) of front s: x_i = sum_{k>=i} (L_JJ^{-1})_ki t_k, one warp per row
-__global__ void __launch_bounds__(kST) k_bwd_x(FrontArgs a, SolveBufs b, const Tile* __restrict__ tiles)
-{
-    extern __shared__ double sm[];
-    const Tile tl = tiles[blockIdx.x];
-    const int s = tl.s, i0 = tl.off;
-    const int c = a.ncol[s], f0 = a.first[s];
-    double* t = sm;  // [c - i0][3]
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int k = tid; k < 3 * (c - i0); k += kST) t[k] = b.t[3 * (f0 + i0) + k];
-    __syncthreads();
-    const int i = i0 + warp;
-    if (i >= c) return;
-    double x0, x1, x2;
-    warp_dot3(a.dinvT + a.dinv_off[s] + static_cast<long long>(i) * c, t, i, c, i0, lane, x0, x1, x2);
-    if (lane == 0) {
-        b.w[3 * (f0 + i)] = x0;
-        b.w[3 * (f0 + i) + 1] = x1;
-        b.w[3 * (f0 + i) + 2] = x2;
+    const FrontArgs& a = A.a;
+    for (;;) {
+        if (tid == 0) item_sh = atomicAdd(ticket, 1);
+        __syncthreads();
+        const int it = item_sh;
+        if (it >= A.n_items) break;
+        const int4 d = A.items[it];
+        const int kind = d.x & 7, off = d.x >> 3, s = d.y, cbeg = d.z, cend = d.w;
+        const int p = A.parent[s];
+        const int r = a.nrow[s], c = a.ncol[s], m = r - c, f0 = a.first[s];
+        const long long ro = a.rows_off[s];
+        const double* F = a.front + a.front_off[s];
+        // stage what does not depend on other items
+        switch (kind) {
+        case kFwdFront:
+            stage_d(st, a.dinvT + a.dinv_off[s], c * c);
+            stage_panel(st + c * c, F, r, c, 0, c);
+            stage_i(si, a.contrib_ptr + ro, r + 1);
+            stage_i(si + r + 1, a.contrib_idx + cbeg, cend - cbeg);
+            stage_i(si + r + 1 + (cend - cbeg), A.prow + ro, c);
+            break;
+        case kFwdY: {
+            const int i1 = min(c, off + kSW);
+            stage_d(st, a.dinv + a.dinv_off[s] + static_cast<long long>(off) * c, (i1 - off) * c);
+            stage_i(si, a.contrib_ptr + ro, i1 + 1);
+            stage_i(si + i1 + 1, a.contrib_idx + cbeg, cend - cbeg);
+            stage_i(si + i1 + 1 + (cend - cbeg), A.prow + ro, i1);
+            break;
+        }
+        case kFwdG: {
+            const int k1 = min(m, off + kSW);
+            stage_d(st, a.lt + a.lt_off[s] + static_cast<long long>(off) * c, (k1 - off) * c);
+            stage_i(si, a.contrib_ptr + ro + c + off, k1 - off + 1);
+            stage_i(si + (k1 - off + 1), a.contrib_idx + cbeg, cend - cbeg);
+            break;
+        }
+        case kBwdFront:
+            stage_d(st, a.dinv + a.dinv_off[s], c * c);
+            stage_d(st + c * c, a.lt + a.lt_off[s], m * c);
+            stage_i(si, A.prow + ro, r);
+            break;
+        case kBwdT:
+            stage_panel(st, F, r, c, off, min(c, off + kSW));
+            stage_i(si, A.prow + ro + c, m);
+            break;
+        default:  // kBwdX
+            stage_d(st, a.dinvT + a.dinv_off[s] + static_cast<long long>(off) * c, (min(c, off + kSW) - off) * c);
+            stage_i(si, A.prow + ro + off, min(c, off + kSW) - off);
+            break;
+        }
+        stage_commit();
+        if (tid == 0) {
+            bool ok;
+            switch (kind) {
+            case kFwdFront:
+            case kFwdY: ok = wait_ge(cGin + s, tGin[s], err); break;
+            case kFwdG: ok = wait_ge(cY + s, tY[s], err); break;
+            case kBwdFront:
+            case kBwdT: ok = wait_ge(cY + s, tY[s], err) && (p < 0 || wait_ge(cX + p, tX[p], err)); break;
+            default: ok = wait_ge(cT + s, tT[s], err); break;
+            }
+            ok_sh = ok;
+        }
+        stage_wait();
+        __syncthreads();
+        if (ok_sh) {
+            switch (kind) {
+            case kFwdFront: {
+                double* f = wk;           // [r][3]
+                double* ys = wk + 3 * r;  // [c][3]
+                const int* cp = si;
+                const int* ci = si + r + 1;
+                const int* pr = ci + (cend - cbeg);
+                assemble(A, 0, r, c, cp, ci, cbeg, pr, f);
+                __syncthreads();
+                for (int i = tid; i < c; i += kST) {  // y_i = sum_{k<=i} XT[k][i] f_k
+                    double y0 = 0, y1 = 0, y2 = 0;
+                    for (int k = 0; k <= i; k++) {
+                        const double x = st[k * c + i];
+                        y0 += x * f[3 * k];
+                        y1 += x * f[3 * k + 1];
+                        y2 += x * f[3 * k + 2];
+                    }
+                    ys[3 * i] = y0;
+                    ys[3 * i + 1] = y1;
+                    ys[3 * i + 2] = y2;
+                    double* yg = A.y + 3LL * (f0 + i);
+                    yg[0] = y0;
+                    yg[1] = y1;
+                    yg[2] = y2;
+                }
+                __syncthreads();
+                const double* P = st + c * c;
+                double* g = A.upd + a.upd_off[s];
+                for (int k = tid; k < m; k += kST) {  // g_k = f_{c+k} - sum_j L[c+k][j] y_j
+                    double g0 = f[3 * (c + k)], g1 = f[3 * (c + k) + 1], g2 = f[3 * (c + k) + 2];
+                    for (int j = 0; j < c; j++) {
+                        const double l = P[j * m + k];
+                        g0 -= l * ys[3 * j];
+                        g1 -= l * ys[3 * j + 1];
+                        g2 -= l * ys[3 * j + 2];
+                    }
+                    g[3 * k] = g0;
+                    g[3 * k + 1] = g1;
+                    g[3 * k + 2] = g2;
+                }
+                break;
+            }
+            case kFwdY: {
+                const int i1 = min(c, off + kSW);
+                const int* cp = si;
+                const int* ci = si + i1 + 1;
+                const int* pr = ci + (cend - cbeg);
+                double* f = wk;  // [i1][3]
+                assemble(A, 0, i1, c, cp, ci, cbeg, pr, f);
+                __syncthreads();
+                const int i = off + warp;
+                if (i < i1) {
+                    double y0, y1, y2;
+                    warp_dot3(st + warp * c, f, 0, i + 1, 0, lane, y0, y1, y2);
+                    if (lane == 0) {
+                        double* yg = A.y + 3LL * (f0 + i);
+                        yg[0] = y0;
+                        yg[1] = y1;
+                        yg[2] = y2;
+                    }
+                }
+                break;
+            }
+            case kFwdG: {
+                const int k1 = min(m, off + kSW);
+                double* ys = wk;           // [c][3]
+                double* fr = wk + 3 * c;   // [kSW][3]
+                for (int k = tid; k < 3 * c; k += kST) ys[k] = __ldcg(A.y + 3LL * f0 + k);
+                assemble(A, c + off, c + k1, c, si, si + (k1 - off + 1), cbeg, nullptr, fr);
+                __syncthreads();
+                const int k = off + warp;
+                if (k < k1) {
+                    double d0, d1, d2;
+                    warp_dot3(st + warp * c, ys, 0, c, 0, lane, d0, d1, d2);
+                    if (lane == 0) {
+                        double* g = A.upd + a.upd_off[s] + 3 * k;
+                        g[0] = fr[3 * warp] - d0;
+                        g[1] = fr[3 * warp + 1] - d1;
+                        g[2] = fr[3 * warp + 2] - d2;
+                    }
+                }
+                break;
+            }
+            case kBwdFront: {
+                double* xr = wk;           // [m][3]
+                double* ts = wk + 3 * m;   // [c][3]
+                const int* pr = si;
+                for (int k = tid; k < m; k += kST) ld3(A.v + 3LL * pr[c + k], xr[3 * k], xr[3 * k + 1], xr[3 * k + 2]);
+                __syncthreads();
+                const double* LT = st + c * c;
+                for (int j = tid; j < c; j += kST) {  // t_j = y_j - sum_k L[c+k][j] x_k
+                    double t0, t1, t2;
+                    ld3(A.y + 3LL * (f0 + j), t0, t1, t2);
+                    for (int k = 0; k < m; k++) {
+                        const double l = LT[k * c + j];
+                        t0 -= l * xr[3 * k];
+                        t1 -= l * xr[3 * k + 1];
+                        t2 -= l * xr[3 * k + 2];
+                    }
+                    ts[3 * j] = t0;
+                    ts[3 * j + 1] = t1;
+                    ts[3 * j + 2] = t2;
+                }
+                __syncthreads();
+                for (int i = tid; i < c; i += kST) {  // x_i = sum_{k>=i} X[k][i] t_k
+                    double x0 = 0, x1 = 0, x2 = 0;
+                    for (int k = i; k < c; k++) {
+                        const double x = st[k * c + i];
+                        x0 += x * ts[3 * k];
+                        x1 += x * ts[3 * k + 1];
+                        x2 += x * ts[3 * k + 2];
+                    }
+                    double* o = A.v + 3LL * pr[i];
+                    o[0] = x0;
+                    o[1] = x1;
+                    o[2] = x2;
+                }
+                break;
+            }
+            case kBwdT: {
+                double* xr = wk;  // [m][3]
+                for (int k = tid; k < m; k += kST) ld3(A.v + 3LL * si[k], xr[3 * k], xr[3 * k + 1], xr[3 * k + 2]);
+                __syncthreads();
+                const int j = off + warp;
+                if (j < c) {
+                    double s0, s1, s2;
+                    warp_dot3(st + warp * m, xr, 0, m, 0, lane, s0, s1, s2);
+                    if (lane == 0) {
+                        double y0, y1, y2;
+                        ld3(A.y + 3LL * (f0 + j), y0, y1, y2);
+                        double* o = A.t + 3LL * (f0 + j);
+                        o[0] = y0 - s0;
+                        o[1] = y1 - s1;
+                        o[2] = y2 - s2;
+                    }
+                }
+                break;
+            }
+            default: {  // kBwdX
+                double* ts = wk;  // [c - off][3]
+                for (int k = tid; k < 3 * (c - off); k += kST) ts[k] = __ldcg(A.t + 3LL * (f0 + off) + k);
+                __syncthreads();
+                const int i = off + warp;
+                if (i < c) {
+                    double x0, x1, x2;
+                    warp_dot3(st + warp * c, ts, i, c, off, lane, x0, x1, x2);
+                    if (lane == 0) {
+                        double* o = A.v + 3LL * si[warp];
+                        o[0] = x0;
+                        o[1] = x1;
+                        o[2] = x2;
+                    }
+                }
+                break;
+            }
+            }
+        }
+        __syncthreads();  // the item's results are written
+        if (tid == 0) {
+            __threadfence();
+            switch (kind) {
+            case kFwdFront:
+                atomicAdd(cY + s, 1);
+                if (p >= 0) atomicAdd(cGin + p, 1);
+                break;
+            case kFwdY: atomicAdd(cY + s, 1); break;
+            case kFwdG:
+                if (p >= 0) atomicAdd(cGin + p, 1);
+                break;
+            case kBwdT: atomicAdd(cT + s, 1); break;
+            default: atomicAdd(cX + s, 1); break;  // kBwdFront, kBwdX
+            }
+        }
     }
 }
 
@@ -570,31 +808,26 @@ __global__ void __launch_bounds__(256) k_transpose_lt(FrontArgs a, const Tile* _
 FrontArgs args_of(Precond& P)
 {
     return FrontArgs { P.d_first, P.d_ncol, P.d_nrow, P.d_rows, P.d_child_ptr, P.d_child_list, P.d_relind,
-        P.d_level_list, P.d_contrib_ptr, P.d_contrib_idx, P.d_below_front, P.d_front_off, P.d_rows_off, P.d_relind_off, P.d_dinv_off,
-        P.d_upd_off, P.d_lt_off, P.d_front, P.d_dinv, P.d_dinvT, P.d_lt, P.d_fail };
+        P.d_level_list, P.d_contrib_ptr, P.d_contrib_idx, P.d_below_front, P.d_front_off, P.d_rows_off,
+        P.d_relind_off, P.d_dinv_off, P.d_upd_off, P.d_lt_off, P.d_front, P.d_dinv, P.d_dinvT, P.d_lt, P.d_fail };
 }
 
-// enqueue one H0 application (gather, levels, scatter) on stream st
+// the work buffers of one solve
+struct SolveBufs {
+    double* y;    // forward result, 3 per node
+    double* t;    // backward intermediate, 3 per node
+    double* upd;  // fronts' update vectors
+    int* cnt;     // completion counters, ticket, error flag (4 ns + 2)
+};
+
+// enqueue one H0 application (counter reset + the persistent solve) on stream st
 void enqueue_solve(const Precond& P, const FrontArgs& a, const SolveBufs& b, double* d_v, cudaStream_t st)
 {
-    const Symbolic& S = P.S;
-    const int n = S.n;
-    const int g = std::min(1184, (n + 255) / 256);
-    k_gather_rhs<<<g, 256, 0, st>>>(b.w, d_v, P.d_perm, n);
-    for (int l = 0; l < P.nlev; l++) {
-        const size_t smc = sizeof(double) * 3 * std::max(P.lev_max_c[l], 1);
-        const int ny = P.fy_off[l + 1] - P.fy_off[l];
-        k_fwd_y<<<ny, kST, smc, st>>>(a, b, P.d_fy + P.fy_off[l]);
-        const int ng = P.fg_off[l + 1] - P.fg_off[l];
-        if (ng > 0) k_fwd_g<<<ng, kST, smc, st>>>(a, b, P.d_fg + P.fg_off[l]);
-    }
-    for (int l = P.nlev - 1; l >= 0; l--) {
-        const int nt = P.bt_off[l + 1] - P.bt_off[l];
-        k_bwd_t<<<nt, kST, sizeof(double) * 3 * std::max(P.lev_max_m[l], 1), st>>>(a, b, P.d_bt + P.bt_off[l]);
-        const int nx = P.bx_off[l + 1] - P.bx_off[l];
-        k_bwd_x<<<nx, kST, sizeof(double) * 3 * std::max(P.lev_max_c[l], 1), st>>>(a, b, P.d_bx + P.bx_off[l]);
-    }
-    k_scatter_sol<<<g, 256, 0, st>>>(d_v, b.w, P.d_perm, n);
+    const int ns = P.S.ns;
+    cudaMemsetAsync(b.cnt, 0, sizeof(int) * (4 * static_cast<size_t>(ns) + 2), st);
+    SolveArgs A { a, P.d_parent, P.d_prow, P.d_items, P.d_tgt, P.n_items, ns, P.stage_d, P.work_d, d_v, b.y, b.t,
+        b.upd, b.cnt };
+    k_solve<<<P.solve_grid, kST, P.solve_smem, st>>>(A);
 }
 
 }  // namespace
@@ -602,19 +835,21 @@ void enqueue_solve(const Precond& P, const FrontArgs& a, const SolveBufs& b, dou
 void free_precond(Model& m)
 {
     if (!m.precond) return;
+    m.epoch++;
     Precond& P = *m.precond;
     for (auto& kv : P.graphs) cudaGraphExecDestroy(kv.second);
     P.graphs.clear();
     if (P.capture) cudaStreamDestroy(P.capture);
     for (int** p : { &P.d_first, &P.d_ncol, &P.d_nrow, &P.d_rows, &P.d_child_ptr, &P.d_child_list, &P.d_relind,
-             &P.d_level_list, &P.d_perm, &P.d_fail, &P.d_panel_list, &P.d_contrib_ptr, &P.d_contrib_idx, &P.d_below_front })
+             &P.d_level_list, &P.d_perm, &P.d_fail, &P.d_panel_list, &P.d_contrib_ptr, &P.d_contrib_idx, &P.d_below_front, &P.d_tgt, &P.d_parent, &P.d_cnt, &P.d_prow })
         dev_free(*p);
     for (long long** p : { &P.d_front_off, &P.d_rows_off, &P.d_relind_off, &P.d_dinv_off, &P.d_upd_off, &P.d_a_pos,
              &P.d_a_src, &P.d_lt_off })
         dev_free(*p);
-    for (Tile** p : { &P.d_fy, &P.d_fg, &P.d_bt, &P.d_bx, &P.d_inv, &P.d_ea, &P.d_oinv }) dev_free(*p);
+    for (Tile** p : { &P.d_inv, &P.d_ea, &P.d_oinv }) dev_free(*p);
+    dev_free(P.d_items);
     dev_free(P.d_syrk);
-    for (double** p : { &P.d_front, &P.d_dinv, &P.d_dinvT, &P.d_lt, &P.d_upd, &P.d_w, &P.d_y, &P.d_t, &P.d_vals })
+    for (double** p : { &P.d_front, &P.d_dinv, &P.d_dinvT, &P.d_lt, &P.d_upd, &P.d_y, &P.d_t, &P.d_vals })
         dev_free(*p);
     delete m.precond;
     m.precond = nullptr;
@@ -658,44 +893,26 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
     P.nlev = static_cast<int>(S.level_ptr.size()) - 1;
     const int nlev = P.nlev;
     // solve and factor schedules
-    std::vector<Tile> fy, fg, bt, bx, inv, ea, oinv;
+    std::vector<Tile> inv, ea, oinv;
     P.ea_off.assign(1, 0);
     std::vector<int> panel_list;
     std::vector<int4> syrk;
-    P.fy_off.assign(1, 0);
-    P.fg_off.assign(1, 0);
-    P.bt_off.assign(1, 0);
-    P.bx_off.assign(1, 0);
-    P.lev_max_c.assign(nlev, 0);
-    P.lev_max_m.assign(nlev, 0);
     P.lev_first_step.assign(1, 0);
     for (int l = 0; l < nlev; l++) {
         int maxc = 0;
         for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) {
             const int s = S.level_list[q];
             const int c = S.ncol[s], mm = S.nrow[s] - c;
-            P.lev_max_c[l] = std::max(P.lev_max_c[l], c);
-            P.lev_max_m[l] = std::max(P.lev_max_m[l], mm);
             P.max_r = std::max(P.max_r, S.nrow[s]);
             P.max_c = std::max(P.max_c, c);
             P.max_m = std::max(P.max_m, mm);
             maxc = std::max(maxc, c);
-            for (int o = 0; o < c; o += kSW) {
-                fy.push_back({ s, o });
-                bt.push_back({ s, o });
-                bx.push_back({ s, o });
-            }
             for (int o = 0; o < c; o += kRT) inv.push_back({ s, o });
             for (int jb = 0; jb + kRT < c; jb += kRT)  // diagonal tiles with rows below them
                 for (int o = jb; o < jb + kRT; o += kIC) oinv.push_back({ s, o });
             if (S.child_ptr[s + 1] > S.child_ptr[s])
                 for (int o = 0; o < S.nrow[s]; o += kFT / 32) ea.push_back({ s, o });
-            for (int o = 0; o < mm; o += kSW) fg.push_back({ s, o });
         }
-        P.fy_off.push_back(static_cast<int>(fy.size()));
-        P.fg_off.push_back(static_cast<int>(fg.size()));
-        P.bt_off.push_back(static_cast<int>(bt.size()));
-        P.bx_off.push_back(static_cast<int>(bx.size()));
         P.ea_off.push_back(static_cast<int>(ea.size()));
         for (int k0 = 0; k0 < maxc; k0 += kNB) {
             Precond::Step st { l, k0, static_cast<int>(panel_list.size()), 0, static_cast<int>(syrk.size()), 0 };
@@ -718,12 +935,100 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
     }
     P.n_inv_tiles = static_cast<int>(inv.size());
     P.n_oinv = static_cast<int>(oinv.size());
-    const size_t smem_need = sizeof(double) * 3 * static_cast<size_t>(std::max(P.max_c, P.max_m));
-    if (smem_need > 200 * 1024) {
-        set_error("a front of the approximate-Jacobian factor is too large for the solve kernels ("
+    // solve items: forward sweep by level (leaves first), backward sweep by
+    // level (root first); within a level the items a later item waits on come
+    // first.  Each item records the range of contributions its rows assemble,
+    // and the shared memory it stages is sized here.
+    std::vector<int4> items;
+    std::vector<int> tgt(4 * static_cast<size_t>(S.ns), 0);
+    std::vector<char> whole(S.ns, 0);
+    size_t stage_d = 1, work_d = 1, ints = 1;
+    auto need = [&](size_t sd, size_t wd, size_t ni) {
+        stage_d = std::max(stage_d, sd);
+        work_d = std::max(work_d, wd);
+        ints = std::max(ints, ni);
+    };
+    auto contrib = [&](int s, int t0, int t1) {  // contribution range of front rows [t0, t1)
+        const long long ro = S.rows_off[s];
+        return std::make_pair(S.contrib_ptr[ro + t0], S.contrib_ptr[ro + t1]);
+    };
+    auto item = [&](int kind, int s, int off, std::pair<int, int> cr) {
+        items.push_back(make_int4(kind | (off << 3), s, cr.first, cr.second));
+    };
+    for (int s = 0; s < S.ns; s++) {
+        const long long c = S.ncol[s], mm = S.nrow[s] - c;
+        whole[s] = c * c + mm * c <= kWholeFront;
+        const int nyt = static_cast<int>((c + kSW - 1) / kSW), ngt = static_cast<int>((mm + kSW - 1) / kSW);
+        tgt[s] = whole[s] ? 1 : nyt;                                          // y of s complete
+        if (S.parent[s] >= 0) tgt[S.ns + S.parent[s]] += whole[s] ? 1 : ngt;  // children's g complete
+        tgt[2 * S.ns + s] = nyt;                                              // t of s complete (tiled fronts)
+        tgt[3 * S.ns + s] = whole[s] ? 1 : nyt;                               // x of s complete
+    }
+    for (int l = 0; l < nlev; l++) {
+        for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) {
+            const int s = S.level_list[q];
+            const int c = S.ncol[s], r = S.nrow[s], mm = r - c;
+            if (whole[s]) {
+                const auto cr = contrib(s, 0, r);
+                item(kFwdFront, s, 0, cr);
+                need(static_cast<size_t>(c) * (c + mm), 3 * static_cast<size_t>(r + c), r + 1 + (cr.second - cr.first) + c);
+            } else {
+                for (int o = 0; o < c; o += kSW) {
+                    const int i1 = std::min(c, o + kSW);
+                    const auto cr = contrib(s, 0, i1);
+                    item(kFwdY, s, o, cr);
+                    need(static_cast<size_t>(i1 - o) * c, 3 * static_cast<size_t>(i1), i1 + 1 + (cr.second - cr.first) + i1);
+                }
+            }
+        }
+        for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) {
+            const int s = S.level_list[q];
+            const int c = S.ncol[s], mm = S.nrow[s] - c;
+            if (whole[s]) continue;
+            for (int o = 0; o < mm; o += kSW) {
+                const int k1 = std::min(mm, o + kSW);
+                const auto cr = contrib(s, c + o, c + k1);
+                item(kFwdG, s, o, cr);
+                need(static_cast<size_t>(k1 - o) * c, 3 * static_cast<size_t>(c) + 3 * kSW, k1 - o + 1 + (cr.second - cr.first));
+            }
+        }
+    }
+    for (int l = nlev - 1; l >= 0; l--) {
+        for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) {
+            const int s = S.level_list[q];
+            const int c = S.ncol[s], r = S.nrow[s], mm = r - c;
+            if (whole[s]) {
+                item(kBwdFront, s, 0, { 0, 0 });
+                need(static_cast<size_t>(c) * (c + mm), 3 * static_cast<size_t>(r), r);
+            } else {
+                for (int o = 0; o < c; o += kSW) {
+                    item(kBwdT, s, o, { 0, 0 });
+                    need(static_cast<size_t>(std::min(c, o + kSW) - o) * mm, 3 * static_cast<size_t>(mm), mm);
+                }
+            }
+        }
+        for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) {
+            const int s = S.level_list[q];
+            const int c = S.ncol[s];
+            if (whole[s]) continue;
+            for (int o = 0; o < c; o += kSW) {
+                item(kBwdX, s, o, { 0, 0 });
+                need(static_cast<size_t>(std::min(c, o + kSW) - o) * c, 3 * static_cast<size_t>(c - o), kSW);
+            }
+        }
+    }
+    P.n_items = static_cast<int>(items.size());
+    P.stage_d = static_cast<int>(stage_d);
+    P.work_d = static_cast<int>(work_d);
+    P.solve_smem = sizeof(double) * (stage_d + work_d) + sizeof(int) * ints;
+    if (P.solve_smem > 200 * 1024) {
+        set_error("a front of the approximate-Jacobian factor is too large for the solve kernel ("
             + std::to_string(P.max_r) + " rows)");
         return EFEM_ERR_UNSUPPORTED;
     }
+    // node index in v of every front row
+    std::vector<int> prow(S.rows.size());
+    for (size_t q = 0; q < S.rows.size(); q++) prow[q] = S.perm[S.rows[q]];
     // device arrays
     efem_status st;
 #define UP(p, v)                                       \
@@ -748,10 +1053,10 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
     UP(P.d_a_pos, S.a_pos);
     UP(P.d_a_src, S.a_src);
     UP(P.d_vals, vals);
-    UP(P.d_fy, fy);
-    UP(P.d_fg, fg);
-    UP(P.d_bt, bt);
-    UP(P.d_bx, bx);
+    UP(P.d_parent, S.parent);
+    UP(P.d_prow, prow);
+    UP(P.d_items, items);
+    UP(P.d_tgt, tgt);
     UP(P.d_inv, inv);
     UP(P.d_oinv, oinv);
     UP(P.d_ea, ea);
@@ -765,12 +1070,16 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
     if ((st = dev_alloc(&P.d_dinvT, static_cast<size_t>(std::max<long long>(S.dinv_size, 1)))) != EFEM_OK) return st;
     if ((st = dev_alloc(&P.d_lt, static_cast<size_t>(std::max<long long>(S.lt_size, 1)))) != EFEM_OK) return st;
     if ((st = dev_alloc(&P.d_upd, static_cast<size_t>(std::max<long long>(S.upd_size, 1)))) != EFEM_OK) return st;
-    if ((st = dev_alloc(&P.d_w, n3)) != EFEM_OK) return st;
     if ((st = dev_alloc(&P.d_y, n3)) != EFEM_OK) return st;
     if ((st = dev_alloc(&P.d_t, n3)) != EFEM_OK) return st;
+    if ((st = dev_alloc(&P.d_cnt, 4 * static_cast<size_t>(S.ns) + 2)) != EFEM_OK) return st;
     if ((st = dev_alloc(&P.d_fail, 1)) != EFEM_OK) return st;
-    for (const void* k : { (const void*)k_fwd_y, (const void*)k_fwd_g, (const void*)k_bwd_t, (const void*)k_bwd_x })
-        EFEM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    // persistent solve: as many CTAs as fit on the device at once
+    EFEM_CUDA(cudaFuncSetAttribute(k_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    int per_sm = 0, sms = 0;
+    EFEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve, kST, P.solve_smem));
+    EFEM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m.device));
+    P.solve_grid = std::max(1, std::min(P.n_items, std::max(per_sm, 1) * sms));
     EFEM_CUDA(cudaStreamCreateWithFlags(&P.capture, cudaStreamNonBlocking));
     P.ready = true;  // analysed; the numeric factor follows
     return precond_factor(m, ok, ms_factor);
@@ -841,7 +1150,7 @@ static efem_status apply_with(Model& m, double* d_v, const SolveBufs& b)
 {
     Precond& P = *m.precond;
     if (P.S.n == 0) return EFEM_OK;
-    const auto key = std::make_pair(d_v, b.w);
+    const auto key = std::make_pair(d_v, b.y);
     auto it = P.graphs.find(key);
     if (it == P.graphs.end()) {
         if (P.graphs.size() >= 8) {  // callers passing many distinct vectors: start over
@@ -859,7 +1168,7 @@ static efem_status apply_with(Model& m, double* d_v, const SolveBufs& b)
         it = P.graphs.emplace(key, ge).first;
     }
     EFEM_CUDA(cudaGraphLaunch(it->second, m.stream));
-    m.launches += 2 + 4LL * P.nlev;
+    m.launches += 1;
     return EFEM_OK;
 }
 
@@ -870,7 +1179,7 @@ efem_status precond_apply(Model& m, double* d_v)
         return EFEM_ERR_ARG;
     }
     Precond& P = *m.precond;
-    return apply_with(m, d_v, SolveBufs { P.d_w, P.d_y, P.d_t, P.d_upd });
+    return apply_with(m, d_v, SolveBufs { P.d_y, P.d_t, P.d_upd, P.d_cnt });
 }
 
 efem_status precond_enqueue(Model& m, double* d_v, cudaStream_t stream)
@@ -881,13 +1190,36 @@ efem_status precond_enqueue(Model& m, double* d_v, cudaStream_t stream)
     }
     Precond& P = *m.precond;
     if (P.S.n == 0) return EFEM_OK;
-    enqueue_solve(P, args_of(P), SolveBufs { P.d_w, P.d_y, P.d_t, P.d_upd }, d_v, stream);
+    enqueue_solve(P, args_of(P), SolveBufs { P.d_y, P.d_t, P.d_upd, P.d_cnt }, d_v, stream);
     return EFEM_OK;
 }
 
 long long precond_launch_count(const Model& m)
 {
-    return m.precond ? 2 + 4LL * m.precond->nlev : 0;
+    return m.precond ? 1 : 0;
+}
+
+const int* precond_error_flag(const Model& m)
+{
+    return m.precond && m.precond->d_cnt ? m.precond->d_cnt + 4LL * m.precond->S.ns + 1 : nullptr;
+}
+
+static efem_status check_solve_flag(const int* d_flag, cudaStream_t st)
+{
+    int flag = 0;
+    EFEM_CUDA(cudaMemcpyAsync(&flag, d_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+    EFEM_CUDA(cudaStreamSynchronize(st));
+    if (flag) {
+        set_error("the triangular solve of the preconditioner gave up waiting for a front");
+        return EFEM_ERR_CUDA;
+    }
+    return EFEM_OK;
+}
+
+efem_status precond_check(Model& m)
+{
+    const int* f = precond_error_flag(m);
+    return f ? check_solve_flag(f, m.stream) : EFEM_OK;
 }
 
 // ============================================================================
@@ -899,19 +1231,20 @@ long long precond_launch_count(const Model& m)
 // device's free memory and must not see foreign allocations), or real-time
 // control loops that forbid the implicit device synchronisation an allocation
 // can cause.  For them efem_precond_apply_noalloc runs the same forward and
-// backward sweeps as efem_precond_apply, but its working vectors (the permuted
-// right-hand side and solution, the forward and backward intermediates, 3 per
-// free node each, and the fronts' update vectors) live in the fixed array
+// backward sweeps as efem_precond_apply, but its working memory (the forward
+// and backward intermediates, 3 per free node each, the fronts' update
+// vectors, and the solve's completion counters) lives in the fixed array
 // below instead of buffers owned by the model.
 //
 // Limits and sharing:
 //   * the array holds kNoAllocDoubles doubles (16 MiB); a model that needs
-//     more (9 * free nodes + its update-vector length) is rejected;
+//     more (6 * free nodes + its update-vector length + 2 * fronts + 1) is
+//     rejected;
 //   * every GPU that loads this library keeps the array until the process
 //     exits;
-//   * all calls share the array and it keeps the last call's contents; every
-//     entry is written before it is read, so nothing has to be cleared, but
-//     calls that overlap on the GPU (other streams, other threads, other
+//   * all calls share the array and it keeps the last call's contents; the
+//     counters are cleared by each call and every other entry is written
+//     before it is read, but calls that overlap on the GPU (other streams, other threads, other
 //     models) race on it and must be serialised by the caller.
 // ============================================================================
 namespace {
@@ -959,7 +1292,8 @@ extern "C" efem_status efem_precond_apply_noalloc(void* model, double* d_v)
     Precond& P = *m.precond;
     const Symbolic& S = P.S;
     const size_t n3 = 3 * static_cast<size_t>(S.n);
-    const size_t need = 3 * n3 + static_cast<size_t>(S.upd_size);
+    const size_t n_cnt = 4 * static_cast<size_t>(S.ns) + 2;
+    const size_t need = 2 * n3 + static_cast<size_t>(S.upd_size) + (n_cnt + 1) / 2;
     if (need > kNoAllocDoubles) {
         set_error("model needs " + std::to_string(need) + " doubles of workspace; the static workspace of "
             "efem_precond_apply_noalloc holds " + std::to_string(kNoAllocDoubles));
@@ -970,9 +1304,12 @@ extern "C" efem_status efem_precond_apply_noalloc(void* model, double* d_v)
     if (st != EFEM_OK) return st;
     EFEM_CUDA(cudaSetDevice(m.device));
     if (S.n == 0) return EFEM_OK;
-    const SolveBufs b { scratch, scratch + n3, scratch + 2 * n3, scratch + 3 * n3 };
+    int* counters = reinterpret_cast<int*>(scratch + 2 * n3 + S.upd_size);
+    const SolveBufs b { scratch, scratch + n3, scratch + 2 * n3, counters };
     enqueue_solve(P, args_of(P), b, d_v, m.stream);
     EFEM_CUDA(cudaGetLastError());
-    EFEM_CUDA(cudaStreamSynchronize(m.stream));
-    return EFEM_OK;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    EFEM_CUDA(cudaStreamIsCapturing(m.stream, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return EFEM_OK;  // recorded into the caller's graph
+    return check_solve_flag(counters + 4LL * S.ns + 1, m.stream);
 }

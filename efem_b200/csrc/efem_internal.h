@@ -134,6 +134,7 @@ struct Model {
     double* d_r = nullptr;
 
     long long launches = 0;           // kernels launched by this model (diagnostics)
+    long long epoch = 0;              // bumped when device arrays that captured graphs point to are rebuilt
     Precond* precond = nullptr;   // owned; freed by free_precond
     SolverWS* ws = nullptr;       // owned; freed by free_solver
 
@@ -203,6 +204,8 @@ efem_status precond_apply(Model& m, double* d_v);
 // into a larger graph).
 efem_status precond_enqueue(Model& m, double* d_v, cudaStream_t stream);
 long long precond_launch_count(const Model& m);  // kernels per H0 application
+const int* precond_error_flag(const Model& m);   // device flag: a solve gave up waiting (nullptr before set-up)
+efem_status precond_check(Model& m);             // wait for the stream and report that flag
 void free_precond(Model& m);
 void precond_info(const Model& m, efem_model_info* info);
 // Host assembly of L in CSR over free nodes (upper and lower triangle).

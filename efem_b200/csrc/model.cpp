@@ -426,6 +426,7 @@ namespace efem {
 // (IntegralElement::initial, src/fe/element/IntegralElement.cpp:3-19).
 efem_status build_blocks(Model& m)
 {
+    m.epoch++;
     const bool reduced = m.opts.integration == 1;
     for (auto& b : m.blocks) {
         dev_free(b.conn);
@@ -914,8 +915,7 @@ efem_status efem_precond_apply(void* model, double* v)
     if (s != EFEM_OK) return s;
     if (!m->opts.device_ptrs)
         EFEM_CUDA(cudaMemcpyAsync(v, dv, sizeof(double) * 3 * m->n_free, cudaMemcpyDeviceToHost, m->stream));
-    EFEM_CUDA(cudaStreamSynchronize(m->stream));
-    return EFEM_OK;
+    return efem::precond_check(*m);
 }
 
 efem_status efem_solve(void* model, double* u_inout, efem_solve_info* info)

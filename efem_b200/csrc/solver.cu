@@ -35,6 +35,7 @@ constexpr int kMaxHist = 64;
 struct Scalars {
     double dg, rinf, xinf, x2;  // line-search reads (r.d, ||r||_inf, ||x||_inf, ||x||_2^2)
     double dg0;                 // r.d at the start of the line search
+    double perr;                // the preconditioner's solve gave up waiting (nonzero)
     double theta;
     double ys[kMaxHist];
     double alpha[kMaxHist];
@@ -136,7 +137,7 @@ __global__ void k_trial(double* __restrict__ x, const double* __restrict__ xp, c
 
 // line-search scalars: dg = r.d, rinf = ||r||_inf, xinf = ||x||_inf, x2 = ||x||^2
 __global__ void __launch_bounds__(kThreads) k_ls_reduce(const double* __restrict__ r, const double* __restrict__ d,
-    const double* __restrict__ x, size_t n, Scalars* S, double* partials)
+    const double* __restrict__ x, size_t n, Scalars* S, double* partials, const int* perr)
 {
     double v[4] = { 0, 0, 0, 0 };
     const int ops[4] = { 0, 1, 1, 0 };
@@ -154,6 +155,7 @@ __global__ void __launch_bounds__(kThreads) k_ls_reduce(const double* __restrict
         S->rinf = v[1];
         S->xinf = v[2];
         S->x2 = v[3];
+        S->perr = perr ? static_cast<double>(*perr) : 0.0;
     }
 }
 
@@ -324,6 +326,7 @@ struct SolverWS {
         cudaGraphExec_t body = nullptr;   // correction + two-loop + H0 + line-search start + first trial
     };
     std::map<std::pair<double*, int>, Graphs> graphs;  // per (solution pointer, configuration)
+    long long epoch = -1;                                // Model::epoch the graphs were captured at
 };
 
 void launch_scale(double* v, double s, size_t n, cudaStream_t st)
@@ -406,8 +409,8 @@ efem_status enqueue_first_trial(Model& m, SolverWS& w, double* x, cudaStream_t s
     efem_status s = launch_residual_on(m, x, w.r, st);
     if (s != EFEM_OK) return s;
     EFEM_CUDA(cudaEventRecordWithFlags(w.gev[1], st, cudaEventRecordExternal));
-    k_ls_reduce<<<G, kThreads, 0, st>>>(w.r, w.d, x, n, w.sc, w.partials);
-    EFEM_CUDA(cudaMemcpyAsync(w.h_read, w.sc, sizeof(double) * 5, cudaMemcpyDeviceToHost, st));
+    k_ls_reduce<<<G, kThreads, 0, st>>>(w.r, w.d, x, n, w.sc, w.partials, precond_error_flag(m));
+    EFEM_CUDA(cudaMemcpyAsync(w.h_read, w.sc, sizeof(double) * 6, cudaMemcpyDeviceToHost, st));
     return EFEM_OK;
 }
 
@@ -493,9 +496,9 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
         if (rs != EFEM_OK) return rs;
         EFEM_CUDA(cudaEventRecord(w.gev[1], st));
         info->n_residual_evals++;
-        k_ls_reduce<<<G, kThreads, 0, st>>>(w.r, w.d, x, n, w.sc, w.partials);
+        k_ls_reduce<<<G, kThreads, 0, st>>>(w.r, w.d, x, n, w.sc, w.partials, precond_error_flag(m));
         m.launches++;
-        EFEM_CUDA(cudaMemcpyAsync(w.h_read, w.sc, sizeof(double) * 5, cudaMemcpyDeviceToHost, st));
+        EFEM_CUDA(cudaMemcpyAsync(w.h_read, w.sc, sizeof(double) * 6, cudaMemcpyDeviceToHost, st));
         EFEM_CUDA(cudaStreamSynchronize(st));
         ms_res += elapsed_ms(w.gev[0], w.gev[1]);
         return EFEM_OK;
@@ -535,6 +538,10 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
         info->n_precond_applies++;
     }
     {
+        if (w.epoch != m.epoch) {  // blocks or factor rebuilt since the graphs were captured
+            drop_graphs(w);
+            w.epoch = m.epoch;
+        }
         const auto key = std::make_pair(x, (ok ? 1 : 0) | (m.opts.precision << 1));
         if (!w.graphs.count(key) && w.graphs.size() >= 8) drop_graphs(w);  // many distinct solution pointers
         SolverWS::Graphs& gr = w.graphs[key];

@@ -171,16 +171,18 @@ efem_status efem_precond_apply(void* model, double* v);
 
 /* H0 v like efem_precond_apply, for callers that cannot allocate device
  * memory at call time (inside a CUDA stream capture, under another
- * framework's caching allocator, in a loop that must not synchronise the
- * device).  No counterpart in the reference.  It calls no cudaMalloc or
- * cudaFree: its working vectors live in a fixed 16 MiB device array that
- * every GPU loading this library keeps until exit.  Requirements: the model's
- * factor exists (efem_solve or efem_precond_apply ran once) and
- * 9 * free nodes + the factor's update-vector length <= 2^21 doubles
- * (EFEM_ERR_ARG otherwise); d_v is a device pointer, overwritten in place.
- * The first call on a device looks up the array's device address (do it
- * before any stream capture).  All calls share the array: calls that overlap
- * on the GPU race and must be serialised by the caller. */
+ * framework's caching allocator).  No counterpart in the reference.  It calls
+ * no cudaMalloc or cudaFree: its working memory lives in a fixed 16 MiB
+ * device array that every GPU loading this library keeps until exit.
+ * Requirements: the model's factor exists (efem_solve or efem_precond_apply
+ * ran once) and 6 * free nodes + the factor's update-vector length
+ * + 2 * fronts + 1 <= 2^21 doubles (EFEM_ERR_ARG otherwise); d_v is a device
+ * pointer, overwritten in place.  Outside a capture the call waits for the
+ * result on the model's stream and reports a solve that gave up waiting
+ * (EFEM_ERR_CUDA); inside a capture it only records the work.  The first
+ * call on a device looks up the array's device address (do it before any
+ * stream capture).  All calls share the array: calls that overlap on the GPU
+ * race and must be serialised by the caller. */
 efem_status efem_precond_apply_noalloc(void* model, double* d_v);
 
 /* Solve R(u) = 0 from u_inout: replaces Integrator::integral
