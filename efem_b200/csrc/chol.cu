@@ -428,6 +428,7 @@ struct SolveArgs {
     double* t;
     double* upd;
     int* cnt;
+    unsigned long long* stamp;  // when set: global timer at the start of the solve
 };
 
 constexpr int kSpinLimit = 1 << 22;  // polls of one wait (about half a second)
@@ -552,7 +553,14 @@ __global__ void __launch_bounds__(kST) k_solve(SolveArgs A)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const FrontArgs& a = A.a;
     for (;;) {
-        if (tid == 0) item_sh = atomicAdd(ticket, 1);
+        if (tid == 0) {
+            item_sh = atomicAdd(ticket, 1);
+            if (item_sh == 0 && A.stamp) {
+                unsigned long long t;
+                asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+                *A.stamp = t;
+            }
+        }
         __syncthreads();
         const int it = item_sh;
         if (it >= A.n_items) break;
@@ -820,13 +828,15 @@ struct SolveBufs {
     int* cnt;     // completion counters, ticket, error flag (4 ns + 2)
 };
 
-// enqueue one H0 application (counter reset + the persistent solve) on stream st
-void enqueue_solve(const Precond& P, const FrontArgs& a, const SolveBufs& b, double* d_v, cudaStream_t st)
+// enqueue one H0 application (counter reset unless the caller cleared them,
+// then the persistent solve) on stream st
+void enqueue_solve(const Precond& P, const FrontArgs& a, const SolveBufs& b, double* d_v, cudaStream_t st,
+    bool clear = true, unsigned long long* stamp = nullptr)
 {
     const int ns = P.S.ns;
-    cudaMemsetAsync(b.cnt, 0, sizeof(int) * (4 * static_cast<size_t>(ns) + 2), st);
+    if (clear) cudaMemsetAsync(b.cnt, 0, sizeof(int) * (4 * static_cast<size_t>(ns) + 2), st);
     SolveArgs A { a, P.d_parent, P.d_prow, P.d_items, P.d_tgt, P.n_items, ns, P.stage_d, P.work_d, d_v, b.y, b.t,
-        b.upd, b.cnt };
+        b.upd, b.cnt, stamp };
     k_solve<<<P.solve_grid, kST, P.solve_smem, st>>>(A);
 }
 
@@ -1182,7 +1192,7 @@ efem_status precond_apply(Model& m, double* d_v)
     return apply_with(m, d_v, SolveBufs { P.d_y, P.d_t, P.d_upd, P.d_cnt });
 }
 
-efem_status precond_enqueue(Model& m, double* d_v, cudaStream_t stream)
+efem_status precond_enqueue(Model& m, double* d_v, cudaStream_t stream, bool clear, unsigned long long* stamp)
 {
     if (!m.precond || !m.precond->factored || !m.precond->ok) {
         set_error("preconditioner not factored");
@@ -1190,8 +1200,14 @@ efem_status precond_enqueue(Model& m, double* d_v, cudaStream_t stream)
     }
     Precond& P = *m.precond;
     if (P.S.n == 0) return EFEM_OK;
-    enqueue_solve(P, args_of(P), SolveBufs { P.d_y, P.d_t, P.d_upd, P.d_cnt }, d_v, stream);
+    enqueue_solve(P, args_of(P), SolveBufs { P.d_y, P.d_t, P.d_upd, P.d_cnt }, d_v, stream, clear, stamp);
     return EFEM_OK;
+}
+
+void precond_counters(const Model& m, int** cnt, int* n)
+{
+    *cnt = m.precond ? m.precond->d_cnt : nullptr;
+    *n = m.precond ? 4 * m.precond->S.ns + 2 : 0;
 }
 
 long long precond_launch_count(const Model& m)

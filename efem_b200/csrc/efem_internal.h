@@ -188,7 +188,9 @@ efem_status ensure_device(Model& m);  // create the stream and upload everything
 // ------------------------------------------------------------------ kernels (residual.cu)
 // r = R(u) on the model's stream; u, r device pointers of length 3*n_free.
 efem_status launch_residual(Model& m, const double* d_u, double* d_r);
-efem_status launch_residual_on(Model& m, const double* d_u, double* d_r, cudaStream_t stream);
+// the same on `stream`; with `stamp`, the GPU's global timer at the start is stored there
+efem_status launch_residual_on(Model& m, const double* d_u, double* d_r, cudaStream_t stream,
+    unsigned long long* stamp = nullptr);
 
 // ------------------------------------------------------------------ solver (solver.cu)
 efem_status run_solve(Model& m, double* d_u, efem_solve_info* info);
@@ -200,9 +202,12 @@ void free_solver(Model& m);
 efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor);
 // v <- (L (x) I3)^{-1} v in place on the device (v: 3*n_free interleaved).
 efem_status precond_apply(Model& m, double* d_v);
-// The same H0 application enqueued as plain kernels on `stream` (for capture
-// into a larger graph).
-efem_status precond_enqueue(Model& m, double* d_v, cudaStream_t stream);
+// The same H0 application enqueued on `stream` (for capture into a larger
+// graph); clear = false when the caller has zeroed precond_counters itself.
+// With `stamp`, the solve's first CTA stores the GPU's global timer there.
+efem_status precond_enqueue(Model& m, double* d_v, cudaStream_t stream, bool clear = true,
+    unsigned long long* stamp = nullptr);
+void precond_counters(const Model& m, int** cnt, int* n);  // the solve's counters, cleared before each H0 v
 long long precond_launch_count(const Model& m);  // kernels per H0 application
 const int* precond_error_flag(const Model& m);   // device flag: a solve gave up waiting (nullptr before set-up)
 efem_status precond_check(Model& m);             // wait for the stream and report that flag

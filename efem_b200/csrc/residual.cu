@@ -278,14 +278,14 @@ efem_status launch_residual(Model& m, const double* d_u, double* d_r)
     return launch_residual_on(m, d_u, d_r, m.stream);
 }
 
-efem_status launch_residual_on(Model& m, const double* d_u, double* d_r, cudaStream_t stream)
+efem_status launch_residual_on(Model& m, const double* d_u, double* d_r, cudaStream_t stream,
+    unsigned long long* stamp)
 {
     const size_t n = 3 * static_cast<size_t>(m.n_free);
     if (n == 0) return EFEM_OK;
-    EFEM_CUDA(cudaMemcpyAsync(d_r, m.d_fext, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
-    // r = -f_ext
-    extern void launch_scale(double* v, double s, size_t n, cudaStream_t st);
-    launch_scale(d_r, -1.0, n, stream);
+    // r = -f_ext (its first thread stores the start time in *stamp when given)
+    extern void launch_neg(double* r, const double* f, size_t n, cudaStream_t st, unsigned long long* stamp);
+    launch_neg(d_r, m.d_fext, n, stream, stamp);
     m.launches++;
     const bool mixed = m.opts.precision == EFEM_MIXED;
     for (auto& b : m.blocks) {

@@ -8,12 +8,33 @@
 // L-BFGS state -- history pointer and count, alpha_j, ys_j, theta -- lives in
 // device memory and is produced and consumed by kernels only.
 //
-// One iteration's common path -- add_correction, the two-loop recursion with
-// H0, the start of the line search, its first trial x = xp + d, the residual
-// and the line-search reductions, plus the read-back of five scalars -- is
-// captured once as a CUDA graph and replayed, so an iteration costs one graph
-// launch and one host wait.  The host then makes the reference's
-// accept / scale decision; the rare further trials are launched directly.
+// The two-loop recursion of LBFGSMat::apply_Hv runs as four passes over the
+// history instead of 2m dependent ones.  With the m x m matrix
+// G[a][b] = s_a . y_b kept up to date (the new pair's row and column are
+// formed in the same pass as s and y themselves), the first loop's
+// alpha_i = rho_i s_i . (q0 - sum_{k newer} alpha_k y_k) needs only the dot
+// products s_i . q0, and the second loop's beta_i only y_i . z0 (z0 = H0 q):
+//   pass 1  s, y of the new pair; G's new row and column; s_i . q0 for all i;
+//           the last CTA runs the alpha recursion (m^2 scalar operations)
+//   pass 2  q = q0 - sum alpha_i y_i                  (then H0 on q -> z0)
+//   pass 3  y_i . z0 for all i; the last CTA runs the beta recursion
+//   pass 4  d = z0 + sum (alpha_i - beta_i) s_i, fused with the start of the
+//           line search (r.d, xp = x, rp = r) and its first trial x = xp + d.
+// This is the same recursion evaluated with the same vectors; only the order
+// of the floating-point sums differs.
+//
+// Iterations run on the device.  After the first one (driven from the host),
+// a CUDA graph holds the loop: a while node over iterations whose body is the
+// four passes with H0, the residual at the first trial and the line-search
+// reductions, then a nested while node over the further trials of the line
+// search, then a one-thread kernel that applies the reference's convergence
+// and iteration-limit tests and sets the loop condition.  The accept / scale
+// rule of the line search is applied by a one-thread kernel as well.  Both
+// loops are bounded: the line search by max_linesearch, the iterations by a
+// per-launch cap, after which the host reads the state and launches the graph
+// again.  Scalars the host reads are written into mapped host memory, and the
+// time spent in the residual and in H0 is summed on the device from the GPU's
+// global timer.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -30,8 +51,9 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kMaxBlocks = 296;  // 2 x 148 SMs
 constexpr int kMaxHist = 64;
+constexpr int kRowBlocks = 64;   // CTAs per history slot in the dot-product passes
 
-// device-resident solver state; the first five doubles are read by the host
+// device-resident solver state
 struct Scalars {
     double dg, rinf, xinf, x2;  // line-search reads (r.d, ||r||_inf, ||x||_inf, ||x||_2^2)
     double dg0;                 // r.d at the start of the line search
@@ -39,11 +61,30 @@ struct Scalars {
     double theta;
     double ys[kMaxHist];
     double alpha[kMaxHist];
-    double coef[kMaxHist];
+    double coef[kMaxHist];      // alpha - beta, per slot
+    double G[kMaxHist][kMaxHist];  // G[a][b] = s_a . y_b
     int ptr, ncorr;             // LBFGSMat::m_ptr, m_ncorr
-    int ptr_next, ncorr_next;
     unsigned int counter[8];
+    // device-driven iterations
+    double eps, step;           // residual criterion; current line-search step
+    int max_iter, max_ls, cap;  // iteration limit (0: none), trials per line search, iterations per launch
+    int k, launch_iters, ls_t, status;
+    unsigned long long n_res, n_extra, n_body;  // residual evaluations, extra trials, device-driven iterations
+    unsigned long long t0_res, t_res, t0_pc, t_pc;  // global-timer stamps and sums (ns)
 };
+
+// host-mapped read-back slots
+enum { kRdDg = 0, kRdRinf, kRdXinf, kRdX2, kRdDg0, kRdPerr, kRdStatus, kRdK, kRdNRes, kRdNExtra, kRdNBody, kRdTRes,
+    kRdTPc, kRdCount };
+// device loop status
+enum { kRunning = 0, kConverged = 1, kMaxIters = 2, kNonFinite = 3, kPrecondFail = 4, kCapReached = 5 };
+
+__device__ __forceinline__ unsigned long long gtimer()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 __device__ __forceinline__ double warp_sum(double v)
 {
@@ -115,12 +156,53 @@ __device__ bool grid_finish(double* v, const int* ops, double* partials, unsigne
     return threadIdx.x == 0;
 }
 
-#define GRID_STRIDE(i, n) for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (n); i += (size_t)gridDim.x * blockDim.x)
-
-__global__ void k_scale(double* v, double s, size_t n)
+// Rows of dot products over a 2D grid: blockIdx.y selects a row (a history
+// slot), blockIdx.x strides the vector.  Each CTA stores NV partials of its
+// row; the last CTA of the whole grid sums every row's partials in CTA order
+// into out[row * NV + k] and returns true (all threads of that CTA).
+template <int NV>
+__device__ bool rows_finish(const double* v, double* partials, unsigned int* counter, double* out)
 {
-    GRID_STRIDE(i, n) v[i] *= s;
+    __shared__ double sh[NV][kThreads / 32];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+        const double x = warp_sum(v[k]);
+        if (lane == 0) sh[k][w] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const size_t base = (static_cast<size_t>(blockIdx.y) * gridDim.x + blockIdx.x) * NV;
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+            double x = 0.0;
+            for (int q = 0; q < kThreads / 32; q++) x += sh[k][q];
+            partials[base + k] = x;
+        }
+        __threadfence();
+        const unsigned int t = atomicAdd(counter, 1u);
+        last = (t == gridDim.x * gridDim.y - 1);
+    }
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    // one warp per (row, value): lanes over the CTAs of the row, then a fixed-order shuffle
+    const int nsum = gridDim.y * NV;
+    for (int q = w; q < nsum; q += kThreads / 32) {
+        const int row = q / NV, k = q - row * NV;
+        double x = 0.0;
+        for (int b = lane; b < static_cast<int>(gridDim.x); b += 32)
+            x += *(volatile double*)&partials[(static_cast<size_t>(row) * gridDim.x + b) * NV + k];
+        x = warp_sum(x);
+        if (lane == 0) out[q] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *counter = 0u;
+    return true;
 }
+
+#define GRID_STRIDE(i, n) for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (n); i += (size_t)gridDim.x * blockDim.x)
 
 __global__ void k_state_init(Scalars* S, int m)
 {
@@ -135,10 +217,12 @@ __global__ void k_trial(double* __restrict__ x, const double* __restrict__ xp, c
     GRID_STRIDE(i, n) x[i] = xp[i] + step * d[i];
 }
 
-// line-search scalars: dg = r.d, rinf = ||r||_inf, xinf = ||x||_inf, x2 = ||x||^2
+// line-search scalars: dg = r.d, rinf = ||r||_inf, xinf = ||x||_inf, x2 = ||x||^2,
+// stored in S and in the host-mapped read-back array
 __global__ void __launch_bounds__(kThreads) k_ls_reduce(const double* __restrict__ r, const double* __restrict__ d,
-    const double* __restrict__ x, size_t n, Scalars* S, double* partials, const int* perr)
+    const double* __restrict__ x, size_t n, Scalars* S, double* partials, const int* perr, double* hread)
 {
+    if (blockIdx.x == 0 && threadIdx.x == 0) S->t_res += gtimer() - S->t0_res;  // the residual just ended
     double v[4] = { 0, 0, 0, 0 };
     const int ops[4] = { 0, 1, 1, 0 };
     GRID_STRIDE(i, n)
@@ -156,63 +240,169 @@ __global__ void __launch_bounds__(kThreads) k_ls_reduce(const double* __restrict
         S->xinf = v[2];
         S->x2 = v[3];
         S->perr = perr ? static_cast<double>(*perr) : 0.0;
+        S->n_res++;
+        hread[kRdDg] = S->dg;
+        hread[kRdRinf] = S->rinf;
+        hread[kRdXinf] = S->xinf;
+        hread[kRdX2] = S->x2;
+        hread[kRdDg0] = S->dg0;
+        hread[kRdPerr] = S->perr;
+        hread[kRdNRes] = static_cast<double>(S->n_res);
+        hread[kRdTRes] = static_cast<double>(S->t_res);
     }
 }
 
-// dg0 = r.d (the line search's initial projection) and xp = x, rp = r
-__global__ void __launch_bounds__(kThreads) k_ls_begin(const double* __restrict__ r, const double* __restrict__ d,
-    const double* __restrict__ x, double* __restrict__ xp, double* __restrict__ rp, size_t n, Scalars* S,
-    double* partials)
+// start of the line search fused with its first trial (step 1):
+// dg0 = r.d, xp = x, rp = r, x = x + d
+__global__ void __launch_bounds__(kThreads) k_ls_begin_trial(const double* __restrict__ r, const double* __restrict__ d,
+    double* __restrict__ x, double* __restrict__ xp, double* __restrict__ rp, size_t n, Scalars* S, double* partials)
 {
     double v[1] = { 0 };
     const int ops[1] = { 0 };
     GRID_STRIDE(i, n)
     {
-        const double ri = r[i];
-        v[0] += ri * d[i];
-        xp[i] = x[i];
+        const double ri = r[i], di = d[i], xi = x[i];
+        v[0] += ri * di;
+        xp[i] = xi;
         rp[i] = ri;
+        x[i] = xi + 1.0 * di;
     }
     block_reduce<1>(v, ops);
     if (grid_finish<1>(v, ops, partials, &S->counter[1])) S->dg0 = v[0];
 }
 
-// add_correction (LBFGSMat.h:81-98): s = x - xp, y = r - rp into slot ptr % m;
-// ys, theta = yy/ys; the new pointer and count take effect in k_advance_neg.
-__global__ void __launch_bounds__(kThreads) k_correction(const double* __restrict__ x, const double* __restrict__ xp,
+// Pass 1 (LBFGSMat::add_correction, LBFGSMat.h:81-98, and the dot products of
+// the first loop).  Grid (kRowBlocks, m + 1): row j < m forms s.Y_j, S_j.y and
+// S_j.q0 (q0 = -r) for history slot j, with the new pair standing in for the
+// slot it replaces; row m writes the new pair and forms s.y and y.y.  The
+// last CTA updates G, ys, theta, the pointer and count, and runs the first
+// loop's recursion (newest pair first).
+__global__ void __launch_bounds__(kThreads) k_pass1(const double* __restrict__ x, const double* __restrict__ xp,
     const double* __restrict__ r, const double* __restrict__ rp, double* __restrict__ Sh, double* __restrict__ Yh,
-    size_t n, int m, Scalars* S, double* partials)
+    size_t n, int m, Scalars* S, double* partials, double* sums)
 {
     const int loc = S->ptr % m;
-    double* s = Sh + loc * n;
-    double* y = Yh + loc * n;
-    double v[2] = { 0, 0 };
-    const int ops[2] = { 0, 0 };
-    GRID_STRIDE(i, n)
-    {
-        const double si = x[i] - xp[i], yi = r[i] - rp[i];
-        s[i] = si;
-        y[i] = yi;
-        v[0] += si * yi;
-        v[1] += yi * yi;
+    const int ncorr = S->ncorr < m ? S->ncorr + 1 : m;  // count after the insertion; slots 0..ncorr-1 hold pairs
+    const int row = blockIdx.y;
+    double v[3] = { 0, 0, 0 };
+    if (row == m) {
+        double* s = Sh + loc * n;
+        double* y = Yh + loc * n;
+        for (size_t i = blockIdx.x * (size_t)kThreads + threadIdx.x; i < n; i += (size_t)gridDim.x * kThreads) {
+            const double si = x[i] - xp[i], yi = r[i] - rp[i];
+            s[i] = si;
+            y[i] = yi;
+            v[0] += si * yi;
+            v[1] += yi * yi;
+        }
+    } else if (row < ncorr) {
+        const double* sj = Sh + row * n;
+        const double* yj = Yh + row * n;
+        const bool self = row == loc;
+        for (size_t i = blockIdx.x * (size_t)kThreads + threadIdx.x; i < n; i += (size_t)gridDim.x * kThreads) {
+            const double si = x[i] - xp[i], yi = r[i] - rp[i];
+            const double sji = self ? si : sj[i], yji = self ? yi : yj[i];
+            v[0] += si * yji;      // s_new . y_j
+            v[1] += sji * yi;      // s_j . y_new
+            v[2] -= sji * r[i];    // s_j . q0
+        }
     }
-    block_reduce<2>(v, ops);
-    if (grid_finish<2>(v, ops, partials, &S->counter[2])) {
-        S->ys[loc] = v[0];
-        S->theta = v[1] / v[0];
-        S->ptr_next = loc + 1;
-        S->ncorr_next = S->ncorr < m ? S->ncorr + 1 : m;
+    if (!rows_finish<3>(v, partials, &S->counter[2], sums)) return;
+    if (threadIdx.x != 0) return;
+    const double ys = sums[3 * m], yy = sums[3 * m + 1];
+    for (int j = 0; j < ncorr; j++) {
+        S->G[loc][j] = sums[3 * j];
+        S->G[j][loc] = sums[3 * j + 1];
+    }
+    S->G[loc][loc] = ys;
+    S->ys[loc] = ys;
+    S->theta = yy / ys;
+    S->ptr = loc + 1;
+    S->ncorr = ncorr;
+    // first loop (LBFGSMat.h:106-113): newest slot first
+    for (int i = 0; i < ncorr; i++) {
+        const int j = ((loc - i) % m + m) % m;
+        double t = sums[3 * j + 2];
+        for (int k = 0; k < i; k++) {
+            const int jk = ((loc - k) % m + m) % m;
+            t -= S->alpha[jk] * S->G[j][jk];
+        }
+        S->alpha[j] = t / S->ys[j];
     }
 }
 
-// commit the new history pointer / count, and start the two-loop with q = -r
-__global__ void k_advance_neg(double* __restrict__ q, const double* __restrict__ r, size_t n, Scalars* S)
+// Pass 2: q = (q0 - sum_j alpha_j y_j) [/ theta when H0 = I / theta]; also
+// clears the preconditioner solve's counters for the H0 application that follows
+__global__ void __launch_bounds__(kThreads) k_pass2(double* __restrict__ q, const double* __restrict__ r,
+    const double* __restrict__ Yh, size_t n, int m, int divide_theta, const Scalars* S, int* clear, int n_clear)
 {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        S->ptr = S->ptr_next;
-        S->ncorr = S->ncorr_next;
+    __shared__ double al[kMaxHist];
+    const int ncorr = S->ncorr;
+    for (int j = threadIdx.x; j < ncorr; j += kThreads) al[j] = S->alpha[j];
+    __syncthreads();
+    const double th = S->theta;
+    GRID_STRIDE(i, n)
+    {
+        double qi = -r[i];
+        for (int j = 0; j < ncorr; j++) qi -= al[j] * Yh[j * n + i];
+        q[i] = divide_theta ? qi / th : qi;
     }
-    GRID_STRIDE(i, n) q[i] = -r[i];
+    if (clear)
+        for (int k = blockIdx.x * kThreads + threadIdx.x; k < n_clear; k += gridDim.x * kThreads) clear[k] = 0;
+}
+
+// Pass 3: y_j . z0 for every slot (grid (kRowBlocks, m)); the last CTA runs
+// the second loop's recursion (LBFGSMat.h:121-128), oldest pair first
+__global__ void __launch_bounds__(kThreads) k_pass3(const double* __restrict__ z, const double* __restrict__ Yh, size_t n,
+    int m, Scalars* S, double* partials, double* sums, int time_pc)
+{
+    const int ncorr = S->ncorr, row = blockIdx.y;
+    if (blockIdx.x == 0 && row == 0 && threadIdx.x == 0 && time_pc) S->t_pc += gtimer() - S->t0_pc;  // H0 just ended
+    double v[1] = { 0 };
+    if (row < ncorr) {
+        const double* yj = Yh + row * n;
+        for (size_t i = blockIdx.x * (size_t)kThreads + threadIdx.x; i < n; i += (size_t)gridDim.x * kThreads)
+            v[0] += yj[i] * z[i];
+    }
+    if (!rows_finish<1>(v, partials, &S->counter[3], sums)) return;
+    if (threadIdx.x != 0) return;
+    const int ptr = S->ptr;
+    for (int o = 0; o < ncorr; o++) {
+        const int j = ((ptr - ncorr + o) % m + m) % m;
+        double t = sums[j];
+        for (int p = 0; p < o; p++) {
+            const int jp = ((ptr - ncorr + p) % m + m) % m;
+            t += S->coef[jp] * S->G[jp][j];
+        }
+        S->coef[j] = S->alpha[j] - t / S->ys[j];
+    }
+}
+
+// Pass 4: d = z0 + sum_j coef_j s_j, then the start of the line search and
+// its first trial as in k_ls_begin_trial
+__global__ void __launch_bounds__(kThreads) k_pass4(double* __restrict__ d, const double* __restrict__ z,
+    const double* __restrict__ Sh, const double* __restrict__ r, double* __restrict__ x, double* __restrict__ xp,
+    double* __restrict__ rp, size_t n, Scalars* S, double* partials)
+{
+    __shared__ double cf[kMaxHist];
+    const int ncorr = S->ncorr;
+    for (int j = threadIdx.x; j < ncorr; j += kThreads) cf[j] = S->coef[j];
+    __syncthreads();
+    double v[1] = { 0 };
+    const int ops[1] = { 0 };
+    GRID_STRIDE(i, n)
+    {
+        double di = z[i];
+        for (int j = 0; j < ncorr; j++) di += cf[j] * Sh[j * n + i];
+        d[i] = di;
+        const double ri = r[i], xi = x[i];
+        v[0] += ri * di;
+        xp[i] = xi;
+        rp[i] = ri;
+        x[i] = xi + 1.0 * di;
+    }
+    block_reduce<1>(v, ops);
+    if (grid_finish<1>(v, ops, partials, &S->counter[1])) S->dg0 = v[0];
 }
 
 __global__ void k_neg_copy(double* __restrict__ q, const double* __restrict__ r, size_t n)
@@ -220,92 +410,90 @@ __global__ void k_neg_copy(double* __restrict__ q, const double* __restrict__ r,
     GRID_STRIDE(i, n) q[i] = -r[i];
 }
 
-// first loop, step i (newest history first), fused with step i-1's update:
-//   q -= alpha[j_{i-1}] y_{j_{i-1}};  alpha[j_i] = s_{j_i} . q / ys[j_i]
-// j_i = (ptr - 1 - i) mod m; a step beyond ncorr does nothing
-__global__ void __launch_bounds__(kThreads) k_loop1(double* __restrict__ q, const double* __restrict__ Sh,
-    const double* __restrict__ Yh, int i, int m, size_t n, Scalars* S, double* partials)
-{
-    const int ncorr = S->ncorr, ptr = S->ptr;
-    if (i >= ncorr) return;
-    const int j = ((ptr - 1 - i) % m + m) % m;
-    const int jp = ((ptr - i) % m + m) % m;
-    const double ap = i > 0 ? S->alpha[jp] : 0.0;
-    const double* yp = Yh + jp * n;
-    const double* sj = Sh + j * n;
-    double v[1] = { 0 };
-    const int ops[1] = { 0 };
-    GRID_STRIDE(t, n)
-    {
-        double qi = q[t];
-        if (i > 0) {
-            qi -= ap * yp[t];
-            q[t] = qi;
-        }
-        v[0] += sj[t] * qi;
-    }
-    block_reduce<1>(v, ops);
-    if (grid_finish<1>(v, ops, partials, &S->counter[3])) S->alpha[j] = v[0] / S->ys[j];
-}
-
-// last update of the first loop; H0 = I/theta when there is no factor
-__global__ void k_loop1_tail(double* __restrict__ q, const double* __restrict__ Yh, int m, int divide_theta, size_t n,
-    const Scalars* S)
-{
-    const int ncorr = S->ncorr, ptr = S->ptr;
-    const int jl = ((ptr - ncorr) % m + m) % m;  // j of step ncorr - 1 (the oldest)
-    const double al = ncorr > 0 ? S->alpha[jl] : 0.0;
-    const double* yl = Yh + jl * n;
-    const double th = S->theta;
-    GRID_STRIDE(t, n)
-    {
-        double qi = q[t];
-        if (ncorr > 0) qi -= al * yl[t];
-        if (divide_theta) qi = qi / th;
-        q[t] = qi;
-    }
-}
-
-// second loop, step i (oldest first), fused with step i-1's update:
-//   q += coef[j_{i-1}] s_{j_{i-1}};  coef[j_i] = alpha[j_i] - y_{j_i} . q / ys[j_i]
-// j_i = (ptr - ncorr + i) mod m
-__global__ void __launch_bounds__(kThreads) k_loop2(double* __restrict__ q, const double* __restrict__ Sh,
-    const double* __restrict__ Yh, int i, int m, size_t n, Scalars* S, double* partials)
-{
-    const int ncorr = S->ncorr, ptr = S->ptr;
-    if (i >= ncorr) return;
-    const int j = ((ptr - ncorr + i) % m + m) % m;
-    const int jp = ((ptr - ncorr + i - 1) % m + m) % m;
-    const double cp = i > 0 ? S->coef[jp] : 0.0;
-    const double* sp = Sh + jp * n;
-    const double* yj = Yh + j * n;
-    double v[1] = { 0 };
-    const int ops[1] = { 0 };
-    GRID_STRIDE(t, n)
-    {
-        double qi = q[t];
-        if (i > 0) {
-            qi += cp * sp[t];
-            q[t] = qi;
-        }
-        v[0] += yj[t] * qi;
-    }
-    block_reduce<1>(v, ops);
-    if (grid_finish<1>(v, ops, partials, &S->counter[4])) S->coef[j] = S->alpha[j] - v[0] / S->ys[j];
-}
-
-// d = q + coef[j_last] s_{j_last}, j_last the newest slot
-__global__ void k_loop2_tail(double* __restrict__ d, const double* __restrict__ q, const double* __restrict__ Sh, int m,
+// x = xp + step d with the step held on the device
+__global__ void k_trial_dev(double* __restrict__ x, const double* __restrict__ xp, const double* __restrict__ d,
     size_t n, const Scalars* S)
 {
-    const int ncorr = S->ncorr, ptr = S->ptr;
-    const int jl = ((ptr - 1) % m + m) % m;
-    const double cl = ncorr > 0 ? S->coef[jl] : 0.0;
-    const double* sl = Sh + jl * n;
-    GRID_STRIDE(t, n) d[t] = ncorr > 0 ? q[t] + cl * sl[t] : q[t];
+    const double step = S->step;
+    GRID_STRIDE(i, n) x[i] = xp[i] + step * d[i];
+}
+
+// Line-search decision after a trial (LineSearchFEA.h:43-67): accept when
+// |r.d| <= |r0.d|; otherwise scale the step by 1.5 (same sign) or 0.5 and try
+// again, at most max_ls trials in all.  Sets the line-search loop condition.
+__global__ void k_ls_decide(Scalars* S, int first, cudaGraphConditionalHandle h)
+{
+    if (threadIdx.x != 0) return;
+    if (first) S->step = 1.0;
+    const int t = first ? 1 : S->ls_t + 1;
+    S->ls_t = t;
+    const double dg = S->dg, dg0 = S->dg0;
+    const bool again = !(fabs(dg) <= fabs(dg0)) && t < S->max_ls;
+    if (again) {
+        S->step *= dg * dg0 > 0 ? 1.5 : 0.5;
+        S->n_extra++;
+    }
+    cudaGraphSetConditional(h, again ? 1u : 0u);
+}
+
+// End of an iteration (LBFGS.h:150-170): stop on a non-finite residual or
+// solution, on convergence (||r||_inf <= eps or <= eps ||x||_inf) or at the
+// iteration limit; otherwise count the iteration and go on, up to `cap`
+// iterations per launch.  Sets the iteration loop condition.
+__global__ void k_iter_decide(Scalars* S, cudaGraphConditionalHandle h, double* hread)
+{
+    if (threadIdx.x != 0) return;
+    const double rinf = S->rinf, xinf = S->xinf;
+    int st = kRunning;
+    S->n_body++;
+    if (S->perr != 0.0)
+        st = kPrecondFail;
+    else if (!isfinite(rinf) || !isfinite(xinf))
+        st = kNonFinite;
+    else if (rinf <= S->eps || rinf <= S->eps * xinf)
+        st = kConverged;
+    else if (S->max_iter != 0 && S->k >= S->max_iter)
+        st = kMaxIters;
+    else {
+        S->k++;
+        if (++S->launch_iters >= S->cap) st = kCapReached;
+    }
+    S->status = st;
+    hread[kRdStatus] = st;
+    hread[kRdK] = S->k;
+    hread[kRdNExtra] = static_cast<double>(S->n_extra);
+    hread[kRdNBody] = static_cast<double>(S->n_body);
+    hread[kRdTPc] = static_cast<double>(S->t_pc);
+    cudaGraphSetConditional(h, st == kRunning ? 1u : 0u);
+}
+
+__global__ void k_loop_start(Scalars* S) { S->launch_iters = 0; }
+
+// options of the device-driven loop, and the iteration number it starts at
+__global__ void k_loop_params(Scalars* S, double eps, int max_iter, int max_ls, int cap, int k)
+{
+    S->eps = eps;
+    S->max_iter = max_iter;
+    S->max_ls = max_ls;
+    S->cap = cap;
+    S->k = k;
+    S->n_extra = 0;
+    S->n_body = 0;
+    S->t_pc = 0;
+}
+
+// counters and timers of one solve
+__global__ void k_solve_init(Scalars* S)
+{
+    S->n_res = 0;
+    S->t_res = 0;
+    S->t_pc = 0;
+    S->n_extra = 0;
+    S->n_body = 0;
 }
 
 int grid_for(size_t n) { return static_cast<int>(std::min<size_t>(kMaxBlocks, std::max<size_t>(1, (n + kThreads * 4 - 1) / (kThreads * 4)))); }
+int row_blocks(size_t n) { return static_cast<int>(std::min<size_t>(kRowBlocks, std::max<size_t>(1, (n + kThreads * 4 - 1) / (kThreads * 4)))); }
 
 }  // namespace
 
@@ -315,30 +503,35 @@ struct SolverWS {
     double *r = nullptr, *xp = nullptr, *rp = nullptr, *d = nullptr, *q = nullptr;
     double *S = nullptr, *Y = nullptr;
     double* partials = nullptr;
+    double* sums = nullptr;
     Scalars* sc = nullptr;
-    double* h_read = nullptr;  // pinned: the five line-search scalars
-    cudaEvent_t ev[2] = { nullptr, nullptr };
-    // event pairs around the residual and H0, recorded inside the graphs too
-    cudaEvent_t gev[4] = { nullptr, nullptr, nullptr, nullptr };
-    cudaStream_t capture = nullptr;
+    double* h_read = nullptr;  // mapped pinned memory: kRdCount scalars written by the device
+    cudaEvent_t ev[4] = { nullptr, nullptr, nullptr, nullptr };  // solve start / end, initial H0 start / end
+    cudaStream_t capture[3] = { nullptr, nullptr, nullptr };      // outer graph, loop body, line-search body
     struct Graphs {
-        cudaGraphExec_t first = nullptr;  // line-search start + first trial (iteration 1)
-        cudaGraphExec_t body = nullptr;   // correction + two-loop + H0 + line-search start + first trial
+        cudaGraphExec_t first = nullptr;  // iteration 1: line-search start + first trial
+        cudaGraphExec_t loop = nullptr;   // iterations 2, 3, ... (device-driven)
     };
     std::map<std::pair<double*, int>, Graphs> graphs;  // per (solution pointer, configuration)
     long long epoch = -1;                                // Model::epoch the graphs were captured at
 };
 
-void launch_scale(double* v, double s, size_t n, cudaStream_t st)
+__global__ void k_neg(double* __restrict__ r, const double* __restrict__ f, size_t n, unsigned long long* stamp)
 {
-    k_scale<<<grid_for(n), kThreads, 0, st>>>(v, s, n);
+    if (stamp && blockIdx.x == 0 && threadIdx.x == 0) *stamp = gtimer();
+    GRID_STRIDE(i, n) r[i] = -f[i];
+}
+
+void launch_neg(double* r, const double* f, size_t n, cudaStream_t st, unsigned long long* stamp)
+{
+    k_neg<<<grid_for(n), kThreads, 0, st>>>(r, f, n, stamp);
 }
 
 static void drop_graphs(SolverWS& w)
 {
     for (auto& kv : w.graphs) {
         if (kv.second.first) cudaGraphExecDestroy(kv.second.first);
-        if (kv.second.body) cudaGraphExecDestroy(kv.second.body);
+        if (kv.second.loop) cudaGraphExecDestroy(kv.second.loop);
     }
     w.graphs.clear();
 }
@@ -356,13 +549,13 @@ void free_solver(Model& m)
     dev_free(w.S);
     dev_free(w.Y);
     dev_free(w.partials);
+    dev_free(w.sums);
     if (w.sc) cudaFree(w.sc);
     if (w.h_read) cudaFreeHost(w.h_read);
     for (auto& e : w.ev)
         if (e) cudaEventDestroy(e);
-    for (auto& e : w.gev)
-        if (e) cudaEventDestroy(e);
-    if (w.capture) cudaStreamDestroy(w.capture);
+    for (auto& c : w.capture)
+        if (c) cudaStreamDestroy(c);
     delete m.ws;
     m.ws = nullptr;
 }
@@ -385,64 +578,165 @@ static efem_status alloc_ws(Model& m)
         if ((s = dev_alloc(p, n)) != EFEM_OK) return s;
     if ((s = dev_alloc(&w.S, n * w.m)) != EFEM_OK) return s;
     if ((s = dev_alloc(&w.Y, n * w.m)) != EFEM_OK) return s;
-    if ((s = dev_alloc(&w.partials, static_cast<size_t>(kMaxBlocks) * 4)) != EFEM_OK) return s;
+    const size_t np = std::max<size_t>(static_cast<size_t>(kMaxBlocks) * 4, static_cast<size_t>(kRowBlocks) * (w.m + 1) * 3);
+    if ((s = dev_alloc(&w.partials, np)) != EFEM_OK) return s;
+    if ((s = dev_alloc(&w.sums, 3 * static_cast<size_t>(w.m + 1))) != EFEM_OK) return s;
     EFEM_CUDA(cudaMalloc(&w.sc, sizeof(Scalars)));
     EFEM_CUDA(cudaMemset(w.sc, 0, sizeof(Scalars)));
-    EFEM_CUDA(cudaMallocHost(&w.h_read, sizeof(double) * 8));
+    EFEM_CUDA(cudaHostAlloc(&w.h_read, sizeof(double) * kRdCount, cudaHostAllocMapped));
+    std::memset(w.h_read, 0, sizeof(double) * kRdCount);
     for (auto& e : w.ev) EFEM_CUDA(cudaEventCreate(&e));
-    for (auto& e : w.gev) EFEM_CUDA(cudaEventCreate(&e));
-    EFEM_CUDA(cudaStreamCreateWithFlags(&w.capture, cudaStreamNonBlocking));
+    for (auto& c : w.capture) EFEM_CUDA(cudaStreamCreateWithFlags(&c, cudaStreamNonBlocking));
     return EFEM_OK;
 }
 
 namespace {
 
-// one line-search trial with step 1 (after xp = x, rp = r, dg0 = r.d), its
-// residual and reductions, and the scalar read-back
-efem_status enqueue_first_trial(Model& m, SolverWS& w, double* x, cudaStream_t st)
+constexpr int kIterCap = 32;  // device-driven iterations per graph launch
+
+double* mapped(double* h)
+{
+    void* d = nullptr;
+    return cudaHostGetDevicePointer(&d, h, 0) == cudaSuccess ? static_cast<double*>(d) : h;
+}
+
+// the residual at the current trial x and the line-search reductions
+efem_status enqueue_trial_tail(Model& m, SolverWS& w, double* x, cudaStream_t st)
 {
     const size_t n = w.n;
-    const int G = grid_for(n);
-    k_ls_begin<<<G, kThreads, 0, st>>>(w.r, w.d, x, w.xp, w.rp, n, w.sc, w.partials);
-    k_trial<<<G, kThreads, 0, st>>>(x, w.xp, w.d, 1.0, n);
-    EFEM_CUDA(cudaEventRecordWithFlags(w.gev[0], st, cudaEventRecordExternal));
-    efem_status s = launch_residual_on(m, x, w.r, st);
+    efem_status s = launch_residual_on(m, x, w.r, st, &w.sc->t0_res);
     if (s != EFEM_OK) return s;
-    EFEM_CUDA(cudaEventRecordWithFlags(w.gev[1], st, cudaEventRecordExternal));
-    k_ls_reduce<<<G, kThreads, 0, st>>>(w.r, w.d, x, n, w.sc, w.partials, precond_error_flag(m));
-    EFEM_CUDA(cudaMemcpyAsync(w.h_read, w.sc, sizeof(double) * 6, cudaMemcpyDeviceToHost, st));
+    k_ls_reduce<<<grid_for(n), kThreads, 0, st>>>(w.r, w.d, x, n, w.sc, w.partials, precond_error_flag(m),
+        mapped(w.h_read));
     return EFEM_OK;
 }
 
-// add_correction + two-loop + H0, leaving the new direction in w.d
-efem_status enqueue_direction(Model& m, SolverWS& w, double* x, bool use_factor, cudaStream_t st)
+// iteration 1: line-search start and first trial along the initial direction
+efem_status enqueue_first(Model& m, SolverWS& w, double* x, cudaStream_t st)
+{
+    k_ls_begin_trial<<<grid_for(w.n), kThreads, 0, st>>>(w.r, w.d, x, w.xp, w.rp, w.n, w.sc, w.partials);
+    return enqueue_trial_tail(m, w, x, st);
+}
+
+// add_correction + two-loop with H0 + line-search start and first trial
+efem_status enqueue_body(Model& m, SolverWS& w, double* x, bool use_factor, cudaStream_t st)
 {
     const size_t n = w.n;
-    const int G = grid_for(n), mm = w.m;
-    k_correction<<<G, kThreads, 0, st>>>(x, w.xp, w.r, w.rp, w.S, w.Y, n, mm, w.sc, w.partials);
-    k_advance_neg<<<G, kThreads, 0, st>>>(w.q, w.r, n, w.sc);
-    for (int i = 0; i < mm; i++) k_loop1<<<G, kThreads, 0, st>>>(w.q, w.S, w.Y, i, mm, n, w.sc, w.partials);
-    k_loop1_tail<<<G, kThreads, 0, st>>>(w.q, w.Y, mm, use_factor ? 0 : 1, n, w.sc);
+    const int mm = w.m;
+    const dim3 g1(row_blocks(n), mm + 1), g3(row_blocks(n), mm);
+    k_pass1<<<g1, kThreads, 0, st>>>(x, w.xp, w.r, w.rp, w.S, w.Y, n, mm, w.sc, w.partials, w.sums);
+    int* clear = nullptr;
+    int n_clear = 0;
+    if (use_factor) precond_counters(m, &clear, &n_clear);
+    k_pass2<<<grid_for(n), kThreads, 0, st>>>(w.q, w.r, w.Y, n, mm, use_factor ? 0 : 1, w.sc, clear, n_clear);
     if (use_factor) {
-        EFEM_CUDA(cudaEventRecordWithFlags(w.gev[2], st, cudaEventRecordExternal));
-        efem_status s = precond_enqueue(m, w.q, st);
+        efem_status s = precond_enqueue(m, w.q, st, false, &w.sc->t0_pc);
         if (s != EFEM_OK) return s;
-        EFEM_CUDA(cudaEventRecordWithFlags(w.gev[3], st, cudaEventRecordExternal));
     }
-    for (int i = 0; i < mm; i++) k_loop2<<<G, kThreads, 0, st>>>(w.q, w.S, w.Y, i, mm, n, w.sc, w.partials);
-    k_loop2_tail<<<G, kThreads, 0, st>>>(w.d, w.q, w.S, mm, n, w.sc);
+    k_pass3<<<g3, kThreads, 0, st>>>(w.q, w.Y, n, mm, w.sc, w.partials, w.sums, use_factor ? 1 : 0);
+    k_pass4<<<grid_for(n), kThreads, 0, st>>>(w.d, w.q, w.S, w.r, x, w.xp, w.rp, n, w.sc, w.partials);
+    return enqueue_trial_tail(m, w, x, st);
+}
+
+efem_status instantiate(cudaGraph_t g, cudaGraphExec_t* out)
+{
+    const cudaError_t e = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        set_error(std::string("graph instantiation: ") + cudaGetErrorString(e));
+        return EFEM_ERR_CUDA;
+    }
     return EFEM_OK;
 }
 
-efem_status capture(Model& m, SolverWS& w, double* x, bool use_factor, bool with_direction, cudaGraphExec_t* out)
+// a while node appended to the work captured so far on `st`; returns its body graph
+efem_status add_while(cudaStream_t st, cudaGraphConditionalHandle h, cudaGraph_t* body)
+{
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    EFEM_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd));
+    cudaGraphNodeParams p = {};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    EFEM_CUDA(cudaGraphAddNode(&node, g, deps, nd, &p));
+    EFEM_CUDA(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+    *body = p.conditional.phGraph_out[0];
+    return EFEM_OK;
+}
+
+// The device-driven iteration loop:
+//   k_loop_start; while (hIter) { body; k_ls_decide(first); while (hLs) { trial; tail; k_ls_decide }; k_iter_decide }
+efem_status capture_loop(Model& m, SolverWS& w, double* x, bool use_factor, cudaGraphExec_t* out)
 {
     const long long launches = m.launches;  // capture launches nothing; replays are counted
+    cudaStream_t s0 = w.capture[0], s1 = w.capture[1], s2 = w.capture[2];
     cudaGraph_t g = nullptr;
-    EFEM_CUDA(cudaStreamBeginCapture(w.capture, cudaStreamCaptureModeThreadLocal));
     efem_status s = EFEM_OK;
-    if (with_direction) s = enqueue_direction(m, w, x, use_factor, w.capture);
-    if (s == EFEM_OK) s = enqueue_first_trial(m, w, x, w.capture);
-    const cudaError_t e = cudaStreamEndCapture(w.capture, &g);
+    EFEM_CUDA(cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal));
+    do {
+        cudaGraph_t outer = nullptr;
+        cudaStreamCaptureStatus cs;
+        if (cudaStreamGetCaptureInfo(s0, &cs, nullptr, &outer, nullptr, nullptr) != cudaSuccess) {
+            s = EFEM_ERR_CUDA;
+            break;
+        }
+        cudaGraphConditionalHandle h_iter, h_ls;
+        if (cudaGraphConditionalHandleCreate(&h_iter, outer, 1, cudaGraphCondAssignDefault) != cudaSuccess) {
+            s = EFEM_ERR_CUDA;
+            break;
+        }
+        k_loop_start<<<1, 1, 0, s0>>>(w.sc);
+        cudaGraph_t body = nullptr, ls_body = nullptr;
+        if ((s = add_while(s0, h_iter, &body)) != EFEM_OK) break;
+        if (cudaGraphConditionalHandleCreate(&h_ls, body, 0, cudaGraphCondAssignDefault) != cudaSuccess) {
+            s = EFEM_ERR_CUDA;
+            break;
+        }
+        if (cudaStreamBeginCaptureToGraph(s1, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            s = EFEM_ERR_CUDA;
+            break;
+        }
+        s = enqueue_body(m, w, x, use_factor, s1);
+        if (s == EFEM_OK) {
+            k_ls_decide<<<1, 32, 0, s1>>>(w.sc, 1, h_ls);
+            s = add_while(s1, h_ls, &ls_body);
+        }
+        if (s == EFEM_OK && cudaStreamBeginCaptureToGraph(s2, ls_body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+            s = EFEM_ERR_CUDA;
+        if (s == EFEM_OK) {
+            k_trial_dev<<<grid_for(w.n), kThreads, 0, s2>>>(x, w.xp, w.d, w.n, w.sc);
+            s = enqueue_trial_tail(m, w, x, s2);
+            k_ls_decide<<<1, 32, 0, s2>>>(w.sc, 0, h_ls);
+            cudaGraph_t tmp = nullptr;
+            if (cudaStreamEndCapture(s2, &tmp) != cudaSuccess && s == EFEM_OK) s = EFEM_ERR_CUDA;
+        }
+        if (s == EFEM_OK) k_iter_decide<<<1, 32, 0, s1>>>(w.sc, h_iter, mapped(w.h_read));
+        cudaGraph_t tmp = nullptr;
+        if (cudaStreamEndCapture(s1, &tmp) != cudaSuccess && s == EFEM_OK) s = EFEM_ERR_CUDA;
+    } while (false);
+    const cudaError_t e = cudaStreamEndCapture(s0, &g);
+    m.launches = launches;
+    if (s != EFEM_OK || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        if (s == EFEM_ERR_CUDA || e != cudaSuccess) set_error(std::string("capture of the iteration loop: ") +
+            cudaGetErrorString(e != cudaSuccess ? e : cudaGetLastError()));
+        return s != EFEM_OK ? s : EFEM_ERR_CUDA;
+    }
+    return instantiate(g, out);
+}
+
+efem_status capture_first(Model& m, SolverWS& w, double* x, cudaGraphExec_t* out)
+{
+    const long long launches = m.launches;
+    cudaGraph_t g = nullptr;
+    EFEM_CUDA(cudaStreamBeginCapture(w.capture[0], cudaStreamCaptureModeThreadLocal));
+    const efem_status s = enqueue_first(m, w, x, w.capture[0]);
+    const cudaError_t e = cudaStreamEndCapture(w.capture[0], &g);
     m.launches = launches;
     if (s != EFEM_OK) {
         if (g) cudaGraphDestroy(g);
@@ -452,9 +746,7 @@ efem_status capture(Model& m, SolverWS& w, double* x, bool use_factor, bool with
         set_error(std::string("graph capture: ") + cudaGetErrorString(e));
         return EFEM_ERR_CUDA;
     }
-    EFEM_CUDA(cudaGraphInstantiate(out, g, 0));
-    cudaGraphDestroy(g);
-    return EFEM_OK;
+    return instantiate(g, out);
 }
 
 double elapsed_ms(cudaEvent_t a, cudaEvent_t b)
@@ -478,29 +770,27 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
     std::memset(info, 0, sizeof(*info));
     const long long launches0 = m.launches;
     const long long per_res = 1 + static_cast<long long>(m.blocks.size() + m.faces.size());
-    double ms_res = 0.0, ms_pc = 0.0;
+    double ms_pc = 0.0;
     double rinf = 0.0, xinf = 0.0;
     int k = 1;
     bool converged = false, ok = false;
+    long long n_body = 0;
+    volatile double* hr = w.h_read;
     EFEM_CUDA(cudaEventRecord(w.ev[0], st));
+    k_solve_init<<<1, 1, 0, st>>>(w.sc);
+    m.launches++;
 
-    // direct (non-graph) line-search trial: x = xp + step d (step 0: x as is),
+    // host-driven line-search trial: x = xp + step d (step 0: x as is),
     // residual, reductions, read-back
     auto direct_trial = [&](double step) -> efem_status {
         if (step != 0.0) {
             k_trial<<<G, kThreads, 0, st>>>(x, w.xp, w.d, step, n);
             m.launches++;
         }
-        EFEM_CUDA(cudaEventRecord(w.gev[0], st));
-        efem_status rs = launch_residual_on(m, x, w.r, st);
+        efem_status rs = enqueue_trial_tail(m, w, x, st);
         if (rs != EFEM_OK) return rs;
-        EFEM_CUDA(cudaEventRecord(w.gev[1], st));
-        info->n_residual_evals++;
-        k_ls_reduce<<<G, kThreads, 0, st>>>(w.r, w.d, x, n, w.sc, w.partials, precond_error_flag(m));
         m.launches++;
-        EFEM_CUDA(cudaMemcpyAsync(w.h_read, w.sc, sizeof(double) * 6, cudaMemcpyDeviceToHost, st));
         EFEM_CUDA(cudaStreamSynchronize(st));
-        ms_res += elapsed_ms(w.gev[0], w.gev[1]);
         return EFEM_OK;
     };
 
@@ -509,10 +799,10 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
     k_state_init<<<1, 1, 0, st>>>(w.sc, mm);
     m.launches++;
     if ((s = direct_trial(0.0)) != EFEM_OK) return s;
-    rinf = w.h_read[1];
-    xinf = w.h_read[2];
+    rinf = hr[kRdRinf];
+    xinf = hr[kRdXinf];
     if (!(std::isfinite(rinf))) goto nan_exit;
-    if (rinf <= eps || rinf <= eps * std::sqrt(w.h_read[3])) {
+    if (rinf <= eps || rinf <= eps * std::sqrt(hr[kRdX2])) {
         converged = true;
         goto done;
     }
@@ -530,11 +820,11 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
     k_neg_copy<<<G, kThreads, 0, st>>>(w.d, w.r, n);
     m.launches++;
     if (ok) {
-        EFEM_CUDA(cudaEventRecord(w.gev[2], st));
+        EFEM_CUDA(cudaEventRecord(w.ev[2], st));
         if ((s = precond_apply(m, w.d)) != EFEM_OK) return s;
-        EFEM_CUDA(cudaEventRecord(w.gev[3], st));
-        EFEM_CUDA(cudaStreamSynchronize(st));
-        ms_pc += elapsed_ms(w.gev[2], w.gev[3]);
+        EFEM_CUDA(cudaEventRecord(w.ev[3], st));
+        if ((s = precond_check(m)) != EFEM_OK) return s;
+        ms_pc += elapsed_ms(w.ev[2], w.ev[3]);
         info->n_precond_applies++;
     }
     {
@@ -546,51 +836,72 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
         if (!w.graphs.count(key) && w.graphs.size() >= 8) drop_graphs(w);  // many distinct solution pointers
         SolverWS::Graphs& gr = w.graphs[key];
         if (!gr.first) {
-            if ((s = capture(m, w, x, ok, false, &gr.first)) != EFEM_OK) return s;
-            if ((s = capture(m, w, x, ok, true, &gr.body)) != EFEM_OK) return s;
+            if ((s = capture_first(m, w, x, &gr.first)) != EFEM_OK) return s;
+            if ((s = capture_loop(m, w, x, ok, &gr.loop)) != EFEM_OK) return s;
         }
-        const long long per_dir = 5 + 2LL * mm + (ok ? precond_launch_count(m) : 0);
-        bool first = true;
+        // iteration 1 from the host
+        EFEM_CUDA(cudaGraphLaunch(gr.first, st));
+        EFEM_CUDA(cudaStreamSynchronize(st));
+        m.launches += per_res + 2;
+        const double dg0 = hr[kRdDg0];
+        double dg = hr[kRdDg], step = 1.0;
+        for (int it = 1; it < m.opts.max_linesearch && !(std::fabs(dg) <= std::fabs(dg0)); it++) {
+            step *= dg * dg0 > 0 ? 1.5 : 0.5;
+            if ((s = direct_trial(step)) != EFEM_OK) return s;
+            dg = hr[kRdDg];
+        }
+        rinf = hr[kRdRinf];
+        xinf = hr[kRdXinf];
+        if (!std::isfinite(rinf) || !std::isfinite(xinf)) goto nan_exit;
+        if (rinf <= eps || rinf <= eps * xinf) {
+            converged = true;
+            goto done;
+        }
+        if (m.opts.max_iterations != 0 && k >= m.opts.max_iterations) {
+            info->flags |= EFEM_SOLVE_MAX_ITERS;
+            goto done;
+        }
+        k++;
+        // iterations 2, 3, ... on the device, kIterCap per graph launch
+        k_loop_params<<<1, 1, 0, st>>>(w.sc, eps, m.opts.max_iterations, std::max(1, m.opts.max_linesearch),
+            kIterCap, k);
+        m.launches++;
+        const long long per_body = 4 + (ok ? precond_launch_count(m) : 0) + per_res + 1 + 2;  // + ls / iteration decisions
+        const long long per_extra = 1 + per_res + 1 + 1;  // trial, residual, reductions, decision
+        long long n_extra = 0;
+        int status = kRunning;
         for (;;) {
-            // common path: one graph launch, one wait
-            EFEM_CUDA(cudaGraphLaunch(first ? gr.first : gr.body, st));
+            EFEM_CUDA(cudaGraphLaunch(gr.loop, st));
             EFEM_CUDA(cudaStreamSynchronize(st));
-            m.launches += 3 + per_res + (first ? 0 : per_dir);
-            ms_res += elapsed_ms(w.gev[0], w.gev[1]);
-            if (!first && ok) {
-                ms_pc += elapsed_ms(w.gev[2], w.gev[3]);
-                info->n_precond_applies++;
-            }
-            info->n_residual_evals++;
-            first = false;
-            // residual-projection line search (LineSearchFEA.h:43-67); trial 1 done
-            const double dg0 = w.h_read[4];
-            double dg = w.h_read[0], step = 1.0;
-            for (int it = 1; it < m.opts.max_linesearch && !(std::fabs(dg) <= std::fabs(dg0)); it++) {
-                step *= dg * dg0 > 0 ? 1.5 : 0.5;
-                if ((s = direct_trial(step)) != EFEM_OK) return s;
-                dg = w.h_read[0];
-            }
-            rinf = w.h_read[1];
-            xinf = w.h_read[2];
-            if (!std::isfinite(rinf) || !std::isfinite(xinf)) goto nan_exit;
-            if (rinf <= eps || rinf <= eps * xinf) {
-                converged = true;
-                break;
-            }
-            if (m.opts.max_iterations != 0 && k >= m.opts.max_iterations) {
-                info->flags |= EFEM_SOLVE_MAX_ITERS;
-                break;
-            }
-            k++;
+            status = static_cast<int>(hr[kRdStatus]);
+            const long long nb = static_cast<long long>(hr[kRdNBody]), ne = static_cast<long long>(hr[kRdNExtra]);
+            m.launches += 1 + (nb - n_body) * per_body + (ne - n_extra) * per_extra;
+            n_body = nb;
+            n_extra = ne;
+            if (status != kCapReached) break;
         }
+        k = static_cast<int>(hr[kRdK]);
+        rinf = hr[kRdRinf];
+        xinf = hr[kRdXinf];
+        if (ok) {
+            info->n_precond_applies += static_cast<int>(n_body);
+            ms_pc += hr[kRdTPc] * 1e-6;
+        }
+        if (status == kPrecondFail) {
+            set_error("the triangular solve of the preconditioner gave up waiting for a front");
+            return EFEM_ERR_CUDA;
+        }
+        if (status == kNonFinite) goto nan_exit;
+        if (status == kConverged) converged = true;
+        if (status == kMaxIters) info->flags |= EFEM_SOLVE_MAX_ITERS;
     }
 done:
     EFEM_CUDA(cudaEventRecord(w.ev[1], st));
     EFEM_CUDA(cudaEventSynchronize(w.ev[1]));
     info->ms_total = elapsed_ms(w.ev[0], w.ev[1]);
-    info->ms_residual = ms_res;
+    info->ms_residual = hr[kRdTRes] * 1e-6;
     info->ms_precond = ms_pc;
+    info->n_residual_evals = static_cast<int>(hr[kRdNRes]);
     info->niter = k;
     info->u_inf = xinf;
     info->r_inf = rinf;
@@ -605,6 +916,7 @@ nan_exit:
     info->niter = k;
     info->u_inf = xinf;
     info->r_inf = rinf;
+    info->n_residual_evals = static_cast<int>(hr[kRdNRes]);
     info->n_kernel_launches = m.launches - launches0;
     set_error("L-BFGS produced a non-finite residual or solution");
     return EFEM_ERR_NAN;
