@@ -47,9 +47,16 @@ constexpr int kFT = 256;  // factor threads
 constexpr int kNB = 32;   // factor panel width
 constexpr int kTS = 64;   // SYRK tile
 constexpr int kST = 256;  // solve threads: one warp per output row / column
-constexpr int kSW = kST / 32;  // outputs per solve CTA
 constexpr int kRT = 32;   // columns per CTA of the inverse / transpose kernels
-constexpr long long kWholeFront = 8192;  // staged factor entries (c^2 + c m) up to which one CTA solves a whole front
+constexpr int kStageBudget = 4096;        // staged doubles per solve tile (rows of a tile x row length)
+constexpr long long kWholeBudget = 4096;  // staged doubles up to which one CTA solves a whole front
+
+// one work item of the persistent triangular solve
+struct SolveItem {
+    int kind, s, r0, r1;  // kind, front, rows [r0, r1) of the tile
+    int cbeg, cend;       // contributions assembled for the front's own rows (or the tile's)
+    int cbeg2, cend2;     // update tiles: contributions of the tile's below-diagonal rows
+};
 
 struct Tile {
     int s;    // front
@@ -67,7 +74,7 @@ struct Precond {
     // solve schedule: the persistent kernel's items, launch shape
     int n_items = 0, solve_grid = 1;
     size_t solve_smem = 0;
-    int4* d_items = nullptr;
+    SolveItem* d_items = nullptr;
     int *d_tgt = nullptr, *d_parent = nullptr, *d_cnt = nullptr, *d_prow = nullptr;
     int stage_d = 0, work_d = 0;
     // factor schedule: per (level, step) the fronts with a panel at that step and the SYRK tiles
@@ -88,7 +95,9 @@ struct Precond {
     std::vector<int> ea_off;                  // nlev + 1
     int n_oinv = 0;
     long long* d_lt_off = nullptr;
-    double *d_dinvT = nullptr, *d_lt = nullptr;
+    double *d_dinvT = nullptr, *d_w = nullptr, *d_wt = nullptr;
+    int4* d_wtiles = nullptr;  // (front, 64-row tile, 64-column tile) of every W
+    int n_wtiles = 0;
     int4* d_syrk = nullptr;
     double *d_front = nullptr, *d_dinv = nullptr, *d_upd = nullptr, *d_y = nullptr, *d_t = nullptr,
            *d_vals = nullptr;
@@ -106,17 +115,11 @@ struct FrontArgs {
     double* front;
     double* dinv;   // L_JJ^{-1}, row-major
     double* dinvT;  // its transpose, row-major
-    double* lt;     // L_RJ, row-major
+    double* w;      // W = L_RJ L_JJ^{-1}, row-major (r - c) x c
+    double* wt;     // W^T, row-major c x (r - c)
     int* fail;
 };
 
-
-__device__ __forceinline__ double wsum(double v)
-{
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
 
 // ------------------------------------------------------------------ factorisation
 __global__ void k_scatter_a(double* __restrict__ front, const long long* __restrict__ pos,
@@ -393,36 +396,40 @@ __global__ void __launch_bounds__(kIT) k_offdiag_inv(FrontArgs a, const Tile* __
 // it depends on have finished (per-front completion counters), so a front
 // starts as soon as its children (forward) or its parent (backward) are done,
 // with no barrier between levels.  An item only waits on items with smaller
-// tickets, which were taken by CTAs already running, so the wait always ends
-// whatever the number of resident CTAs; each wait is still bounded, and a
-// wait that runs out sets the error flag and makes every later wait give up.
+// tickets, which were taken by CTAs already running (a CTA takes its next
+// ticket while it works on the current one, which keeps this true), so the
+// wait always ends whatever the number of resident CTAs; each wait is still
+// bounded, and a wait that runs out sets the error flag and makes every later
+// wait give up.
 //
 // Before it waits, a CTA stages everything of its item that does not depend
-// on other items -- the factor blocks it multiplies with and the index lists
-// of the assembly -- into shared memory with cp.async, so only the dependent
-// vectors are fetched after the wait.
+// on other items -- the factor rows it multiplies with (odd row stride in
+// shared memory, so lanes on different rows hit different banks) and the
+// index lists of the assembly -- with cp.async, so only the dependent vectors
+// are fetched after the wait.
 //
-// Item kinds (a small front is one item per sweep, one thread per output; a
-// large one is split into tiles of kSW rows or columns, one warp per output):
-//   kFwdFront  y_J = L_JJ^{-1} f_J and g = f_R - L_RJ y_J for a whole front
-//   kFwdY      y rows of one tile             (waits: children's g)
-//   kFwdG      update rows of one tile        (waits: the front's y)
-//   kBwdFront  t_J = y_J - L_RJ^T x_R and x_J = L_JJ^{-T} t_J for a whole front
-//   kBwdT      t columns of one tile          (waits: own y, parent's x)
-//   kBwdX      x rows of one tile             (waits: the front's t)
-// f = b_J (own columns) + the children's update entries, summed in a fixed
-// order; every dot product has a fixed order too, so results are repeatable.
-enum ItemKind { kFwdFront = 0, kFwdY = 1, kFwdG = 2, kBwdFront = 3, kBwdT = 4, kBwdX = 5 };
+// Item kinds.  A small front is one item per sweep; a large one is split into
+// tiles of rows sized so that a tile's factor rows fill about kStageBudget
+// doubles.  Every output row is a dot product computed by a group of g lanes
+// (g = 32 for a handful of long rows, down to one thread per row for many
+// short ones).  With W = L_RJ L_JJ^{-1} from the factorisation, each sweep has
+// one dependent step per tree level:
+//   kFwdFront  y_J = L_JJ^{-1} f_J and g = f_R - W f_J for a whole front
+//   kFwdY      y rows of one tile         (waits: children's g)
+//   kFwdG      update rows of one tile    (waits: children's g)
+//   kBwdFront  x_J = L_JJ^{-T} y_J - W^T x_R for a whole front
+//   kBwdX      x rows of one tile         (waits: own y, parent's x)
+enum ItemKind { kFwdFront = 0, kFwdY = 1, kFwdG = 2, kBwdFront = 3, kBwdX = 5 };
 
-// device counters, one int array: [cY ns][cGin ns][cT ns][cX ns][ticket][error]
+// device counters, one int array: [cY ns][cGin ns][unused ns][cX ns][ticket][error]
 struct SolveArgs {
     FrontArgs a;
     const int* parent;
-    const int* prow;    // per front row (rows_off[s] + t): the node's index in v
-    const int4* items;  // {kind | offset << 3, front, first contribution, end of contributions}
-    const int* tgt;     // targets of the four counter groups
+    const int* prow;          // per front row (rows_off[s] + t): the node's index in v
+    const SolveItem* items;
+    const int* tgt;           // targets of the four counter groups
     int n_items, ns;
-    int stage_d, work_d;  // shared-memory layout: staged doubles, work doubles, then ints
+    int stage_d, work_d;      // shared-memory layout: staged doubles, work doubles, then ints
     double* v;
     double* y;
     double* t;
@@ -461,13 +468,10 @@ __device__ __forceinline__ void ld3(const double* p, double& a, double& b, doubl
     c = __ldcg(p + 2);
 }
 
-// block-cooperative asynchronous copies global -> shared
-__device__ __forceinline__ void stage_d(double* dst, const double* src, int n)
+__device__ __forceinline__ void cp8(double* dst, const double* src)
 {
-    for (int i = threadIdx.x; i < n; i += kST) {
-        const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst + i));
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src + i) : "memory");
-    }
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
 }
 __device__ __forceinline__ void stage_i(int* dst, const int* src, int n)
 {
@@ -476,36 +480,63 @@ __device__ __forceinline__ void stage_i(int* dst, const int* src, int n)
         asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src + i) : "memory");
     }
 }
-// columns [j0, j1) of the front's below-diagonal block (column-major), as (j - j0) * m + k
-__device__ __forceinline__ void stage_panel(double* dst, const double* F, int r, int c, int j0, int j1)
+// rows [0, R) of a matrix with leading dimension ld, entries k in [lo(row), hi(row)),
+// into dst with row stride lp; lo / hi: 0 = 0 / L, 1 = 0 / row0 + row + 1 (lower
+// triangle), 2 = row0 + row / L (upper triangle); one warp per row
+__device__ __forceinline__ void stage_rows(double* dst, int lp, const double* src, long long ld, int R, int L, int tri,
+    int row0)
 {
-    const int m = r - c, n = (j1 - j0) * m;
-    for (int i = threadIdx.x; i < n; i += kST) {
-        const int j = i / m, k = i - j * m;
-        const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst + i));
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d),
-            "l"(F + static_cast<long long>(j0 + j) * r + c + k) : "memory");
+    const int lane = threadIdx.x & 31;
+    for (int rr = threadIdx.x >> 5; rr < R; rr += kST / 32) {
+        const int lo = tri == 2 ? row0 + rr : 0;
+        const int hi = tri == 1 ? row0 + rr + 1 : L;
+        const double* sr = src + rr * ld;
+        double* dr = dst + rr * lp;
+        for (int k = lo + lane; k < hi; k += 32) cp8(dr + k, sr + k);
     }
 }
 __device__ __forceinline__ void stage_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void stage_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// Dot product of a row held in shared memory with a 3-component vector also
-// in shared memory, over k in [k0, k1); lanes stride k, then the warp reduces.
-__device__ __forceinline__ void warp_dot3(const double* row, const double* v, int k0, int k1, int vbase, int lane,
-    double& s0, double& s1, double& s2)
+__device__ __forceinline__ int odd(int L) { return L | 1; }
+__device__ __forceinline__ int lanes_per_row(int R)
 {
-    double a0 = 0, a1 = 0, a2 = 0;
-    for (int k = k0 + lane; k < k1; k += 32) {
-        const double d = row[k];
-        const double* v0 = v + 3 * (k - vbase);
-        a0 += d * v0[0];
-        a1 += d * v0[1];
-        a2 += d * v0[2];
+    int g = 32;
+    while (g > 1 && (kST / g) < R) g >>= 1;
+    return g;
+}
+
+// Dot products of staged rows [0, R) (row stride lp) with a 3-component vector
+// v in shared memory (entry k at v[3 (k - vbase)]), over k in [lo, hi) with
+// lo / hi as in stage_rows; g lanes per row, reduced in a fixed order.  out
+// is called with (row, s0, s1, s2) by the first lane of each group.
+template <typename Out>
+__device__ __forceinline__ void rows_dot(const double* M, int lp, const double* v, int vbase, int R, int L, int tri,
+    int row0, Out out)
+{
+    const int g = lanes_per_row(R);
+    const int lig = threadIdx.x & (g - 1), grp = threadIdx.x / g, ngrp = kST / g;
+    for (int base = 0; base < R; base += ngrp) {  // uniform trip count across each warp
+        const int rr = base + grp;
+        const bool valid = rr < R;
+        const int lo = !valid ? 0 : (tri == 2 ? row0 + rr : 0);
+        const int hi = !valid ? 0 : (tri == 1 ? row0 + rr + 1 : L);
+        const double* row = M + rr * lp;
+        double a0 = 0, a1 = 0, a2 = 0;
+        for (int k = lo + lig; k < hi; k += g) {
+            const double d = row[k];
+            const double* vv = v + 3 * (k - vbase);
+            a0 += d * vv[0];
+            a1 += d * vv[1];
+            a2 += d * vv[2];
+        }
+        for (int o = g >> 1; o > 0; o >>= 1) {
+            a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+            a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+            a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+        }
+        if (valid && lig == 0) out(rr, a0, a1, a2);
     }
-    s0 = wsum(a0);
-    s1 = wsum(a1);
-    s2 = wsum(a2);
 }
 
 // f_t for front rows [t0, t1) into f (3 per row): the right-hand side for own
@@ -535,77 +566,82 @@ __device__ __forceinline__ void assemble(const SolveArgs& A, int t0, int t1, int
 __global__ void __launch_bounds__(kST) k_solve(SolveArgs A)
 {
     extern __shared__ double sm[];
-    double* st = sm;                    // staged factor data
-    double* wk = sm + A.stage_d;        // work vectors
+    double* st = sm;                                  // staged factor rows
+    double* wk = sm + A.stage_d;                      // work vectors
     int* si = reinterpret_cast<int*>(wk + A.work_d);  // staged index lists
     __shared__ int item_sh, ok_sh;
     const int ns = A.ns;
     int* cY = A.cnt;
     int* cGin = A.cnt + ns;
-    int* cT = A.cnt + 2 * ns;
     int* cX = A.cnt + 3 * ns;
     int* ticket = A.cnt + 4 * ns;
     int* err = ticket + 1;
     const int* tY = A.tgt;
     const int* tGin = A.tgt + ns;
-    const int* tT = A.tgt + 2 * ns;
     const int* tX = A.tgt + 3 * ns;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x;
     const FrontArgs& a = A.a;
-    for (;;) {
-        if (tid == 0) {
-            item_sh = atomicAdd(ticket, 1);
-            if (item_sh == 0 && A.stamp) {
-                unsigned long long t;
-                asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-                *A.stamp = t;
-            }
+    int next = 0;  // thread 0: the ticket taken ahead
+    if (tid == 0) {
+        next = atomicAdd(ticket, 1);
+        if (next == 0 && A.stamp) {
+            unsigned long long t;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+            *A.stamp = t;
         }
+    }
+    for (;;) {
+        if (tid == 0) item_sh = next;
         __syncthreads();
         const int it = item_sh;
         if (it >= A.n_items) break;
-        const int4 d = A.items[it];
-        const int kind = d.x & 7, off = d.x >> 3, s = d.y, cbeg = d.z, cend = d.w;
+        const SolveItem d = A.items[it];
+        if (tid == 0) next = atomicAdd(ticket, 1);  // in flight while this item runs
+        const int kind = d.kind, s = d.s, r0 = d.r0, r1 = d.r1, R = r1 - r0, cbeg = d.cbeg, cend = d.cend;
         const int p = A.parent[s];
         const int r = a.nrow[s], c = a.ncol[s], m = r - c, f0 = a.first[s];
         const long long ro = a.rows_off[s];
-        const double* F = a.front + a.front_off[s];
+        const double* X = a.dinv + a.dinv_off[s];
+        const double* XT = a.dinvT + a.dinv_off[s];
+        const double* W = a.w + a.lt_off[s];
+        const double* WT = a.wt + a.lt_off[s];
+        const int lc = odd(c), lm = odd(m);
+        const int nci = cend - cbeg, nci2 = d.cend2 - d.cbeg2;
         // stage what does not depend on other items
         switch (kind) {
         case kFwdFront:
-            stage_d(st, a.dinvT + a.dinv_off[s], c * c);
-            stage_panel(st + c * c, F, r, c, 0, c);
+            stage_rows(st, lc, X, c, c, c, 1, 0);           // L_JJ^{-1} rows (lower)
+            stage_rows(st + c * lc, lc, W, c, m, c, 0, 0);  // W rows
             stage_i(si, a.contrib_ptr + ro, r + 1);
-            stage_i(si + r + 1, a.contrib_idx + cbeg, cend - cbeg);
-            stage_i(si + r + 1 + (cend - cbeg), A.prow + ro, c);
+            stage_i(si + r + 1, a.contrib_idx + cbeg, nci);
+            stage_i(si + r + 1 + nci, A.prow + ro, c);
             break;
-        case kFwdY: {
-            const int i1 = min(c, off + kSW);
-            stage_d(st, a.dinv + a.dinv_off[s] + static_cast<long long>(off) * c, (i1 - off) * c);
-            stage_i(si, a.contrib_ptr + ro, i1 + 1);
-            stage_i(si + i1 + 1, a.contrib_idx + cbeg, cend - cbeg);
-            stage_i(si + i1 + 1 + (cend - cbeg), A.prow + ro, i1);
+        case kFwdY:
+            stage_rows(st, lc, X + static_cast<long long>(r0) * c, c, R, c, 1, r0);
+            stage_i(si, a.contrib_ptr + ro, r1 + 1);
+            stage_i(si + r1 + 1, a.contrib_idx + cbeg, nci);
+            stage_i(si + r1 + 1 + nci, A.prow + ro, r1);
             break;
-        }
         case kFwdG: {
-            const int k1 = min(m, off + kSW);
-            stage_d(st, a.lt + a.lt_off[s] + static_cast<long long>(off) * c, (k1 - off) * c);
-            stage_i(si, a.contrib_ptr + ro + c + off, k1 - off + 1);
-            stage_i(si + (k1 - off + 1), a.contrib_idx + cbeg, cend - cbeg);
+            stage_rows(st, lc, W + static_cast<long long>(r0) * c, c, R, c, 0, 0);
+            int* q = si;
+            stage_i(q, a.contrib_ptr + ro, c + 1);
+            stage_i(q + c + 1, a.contrib_idx + cbeg, nci);
+            stage_i(q + c + 1 + nci, A.prow + ro, c);
+            q += 2 * c + 1 + nci;
+            stage_i(q, a.contrib_ptr + ro + c + r0, R + 1);
+            stage_i(q + R + 1, a.contrib_idx + d.cbeg2, nci2);
             break;
         }
         case kBwdFront:
-            stage_d(st, a.dinv + a.dinv_off[s], c * c);
-            stage_d(st + c * c, a.lt + a.lt_off[s], m * c);
+            stage_rows(st, lc, XT, c, c, c, 2, 0);             // L_JJ^{-T} rows (upper)
+            stage_rows(st + c * lc, lm, WT, m, c, m, 0, 0);  // W^T rows
             stage_i(si, A.prow + ro, r);
             break;
-        case kBwdT:
-            stage_panel(st, F, r, c, off, min(c, off + kSW));
-            stage_i(si, A.prow + ro + c, m);
-            break;
         default:  // kBwdX
-            stage_d(st, a.dinvT + a.dinv_off[s] + static_cast<long long>(off) * c, (min(c, off + kSW) - off) * c);
-            stage_i(si, A.prow + ro + off, min(c, off + kSW) - off);
+            stage_rows(st, lc, XT + static_cast<long long>(r0) * c, c, R, c, 2, r0);
+            stage_rows(st + R * lc, lm, WT + static_cast<long long>(r0) * m, m, R, m, 0, 0);
+            stage_i(si, A.prow + ro, r);
             break;
         }
         stage_commit();
@@ -613,11 +649,9 @@ __global__ void __launch_bounds__(kST) k_solve(SolveArgs A)
             bool ok;
             switch (kind) {
             case kFwdFront:
-            case kFwdY: ok = wait_ge(cGin + s, tGin[s], err); break;
-            case kFwdG: ok = wait_ge(cY + s, tY[s], err); break;
-            case kBwdFront:
-            case kBwdT: ok = wait_ge(cY + s, tY[s], err) && (p < 0 || wait_ge(cX + p, tX[p], err)); break;
-            default: ok = wait_ge(cT + s, tT[s], err); break;
+            case kFwdY:
+            case kFwdG: ok = wait_ge(cGin + s, tGin[s], err); break;
+            default: ok = wait_ge(cY + s, tY[s], err) && (p < 0 || wait_ge(cX + p, tX[p], err)); break;
             }
             ok_sh = ok;
         }
@@ -626,157 +660,95 @@ __global__ void __launch_bounds__(kST) k_solve(SolveArgs A)
         if (ok_sh) {
             switch (kind) {
             case kFwdFront: {
-                double* f = wk;           // [r][3]
-                double* ys = wk + 3 * r;  // [c][3]
-                const int* cp = si;
+                double* f = wk;  // [r][3]
                 const int* ci = si + r + 1;
-                const int* pr = ci + (cend - cbeg);
-                assemble(A, 0, r, c, cp, ci, cbeg, pr, f);
+                assemble(A, 0, r, c, si, ci, cbeg, ci + nci, f);
                 __syncthreads();
-                for (int i = tid; i < c; i += kST) {  // y_i = sum_{k<=i} XT[k][i] f_k
-                    double y0 = 0, y1 = 0, y2 = 0;
-                    for (int k = 0; k <= i; k++) {
-                        const double x = st[k * c + i];
-                        y0 += x * f[3 * k];
-                        y1 += x * f[3 * k + 1];
-                        y2 += x * f[3 * k + 2];
-                    }
-                    ys[3 * i] = y0;
-                    ys[3 * i + 1] = y1;
-                    ys[3 * i + 2] = y2;
+                rows_dot(st, lc, f, 0, c, c, 1, 0, [&](int i, double y0, double y1, double y2) {
                     double* yg = A.y + 3LL * (f0 + i);
                     yg[0] = y0;
                     yg[1] = y1;
                     yg[2] = y2;
-                }
-                __syncthreads();
-                const double* P = st + c * c;
+                });
                 double* g = A.upd + a.upd_off[s];
-                for (int k = tid; k < m; k += kST) {  // g_k = f_{c+k} - sum_j L[c+k][j] y_j
-                    double g0 = f[3 * (c + k)], g1 = f[3 * (c + k) + 1], g2 = f[3 * (c + k) + 2];
-                    for (int j = 0; j < c; j++) {
-                        const double l = P[j * m + k];
-                        g0 -= l * ys[3 * j];
-                        g1 -= l * ys[3 * j + 1];
-                        g2 -= l * ys[3 * j + 2];
-                    }
-                    g[3 * k] = g0;
-                    g[3 * k + 1] = g1;
-                    g[3 * k + 2] = g2;
-                }
+                rows_dot(st + c * lc, lc, f, 0, m, c, 0, 0, [&](int k, double d0, double d1, double d2) {
+                    const double* fk = f + 3 * (c + k);
+                    g[3 * k] = fk[0] - d0;
+                    g[3 * k + 1] = fk[1] - d1;
+                    g[3 * k + 2] = fk[2] - d2;
+                });
                 break;
             }
             case kFwdY: {
-                const int i1 = min(c, off + kSW);
-                const int* cp = si;
-                const int* ci = si + i1 + 1;
-                const int* pr = ci + (cend - cbeg);
-                double* f = wk;  // [i1][3]
-                assemble(A, 0, i1, c, cp, ci, cbeg, pr, f);
+                double* f = wk;  // [r1][3]
+                const int* ci = si + r1 + 1;
+                assemble(A, 0, r1, c, si, ci, cbeg, ci + nci, f);
                 __syncthreads();
-                const int i = off + warp;
-                if (i < i1) {
-                    double y0, y1, y2;
-                    warp_dot3(st + warp * c, f, 0, i + 1, 0, lane, y0, y1, y2);
-                    if (lane == 0) {
-                        double* yg = A.y + 3LL * (f0 + i);
-                        yg[0] = y0;
-                        yg[1] = y1;
-                        yg[2] = y2;
-                    }
-                }
+                rows_dot(st, lc, f, 0, R, c, 1, r0, [&](int i, double y0, double y1, double y2) {
+                    double* yg = A.y + 3LL * (f0 + r0 + i);
+                    yg[0] = y0;
+                    yg[1] = y1;
+                    yg[2] = y2;
+                });
                 break;
             }
             case kFwdG: {
-                const int k1 = min(m, off + kSW);
-                double* ys = wk;           // [c][3]
-                double* fr = wk + 3 * c;   // [kSW][3]
-                for (int k = tid; k < 3 * c; k += kST) ys[k] = __ldcg(A.y + 3LL * f0 + k);
-                assemble(A, c + off, c + k1, c, si, si + (k1 - off + 1), cbeg, nullptr, fr);
+                double* fj = wk;          // [c][3]
+                double* fr = wk + 3 * c;  // [R][3]
+                const int* q = si;
+                const int* ci = q + c + 1;
+                assemble(A, 0, c, c, q, ci, cbeg, ci + nci, fj);
+                q += 2 * c + 1 + nci;
+                assemble(A, c + r0, c + r1, c, q, q + R + 1, d.cbeg2, nullptr, fr);
                 __syncthreads();
-                const int k = off + warp;
-                if (k < k1) {
-                    double d0, d1, d2;
-                    warp_dot3(st + warp * c, ys, 0, c, 0, lane, d0, d1, d2);
-                    if (lane == 0) {
-                        double* g = A.upd + a.upd_off[s] + 3 * k;
-                        g[0] = fr[3 * warp] - d0;
-                        g[1] = fr[3 * warp + 1] - d1;
-                        g[2] = fr[3 * warp + 2] - d2;
-                    }
-                }
+                double* g = A.upd + a.upd_off[s] + 3LL * r0;
+                rows_dot(st, lc, fj, 0, R, c, 0, 0, [&](int k, double d0, double d1, double d2) {
+                    g[3 * k] = fr[3 * k] - d0;
+                    g[3 * k + 1] = fr[3 * k + 1] - d1;
+                    g[3 * k + 2] = fr[3 * k + 2] - d2;
+                });
                 break;
             }
             case kBwdFront: {
-                double* xr = wk;           // [m][3]
-                double* ts = wk + 3 * m;   // [c][3]
-                const int* pr = si;
-                for (int k = tid; k < m; k += kST) ld3(A.v + 3LL * pr[c + k], xr[3 * k], xr[3 * k + 1], xr[3 * k + 2]);
+                double* yj = wk;               // [c][3]
+                double* xr = wk + 3 * c;       // [m][3]
+                double* xs = wk + 3 * r;       // [c][3]
+                for (int k = tid; k < 3 * c; k += kST) yj[k] = __ldcg(A.y + 3LL * f0 + k);
+                for (int k = tid; k < m; k += kST) ld3(A.v + 3LL * si[c + k], xr[3 * k], xr[3 * k + 1], xr[3 * k + 2]);
                 __syncthreads();
-                const double* LT = st + c * c;
-                for (int j = tid; j < c; j += kST) {  // t_j = y_j - sum_k L[c+k][j] x_k
-                    double t0, t1, t2;
-                    ld3(A.y + 3LL * (f0 + j), t0, t1, t2);
-                    for (int k = 0; k < m; k++) {
-                        const double l = LT[k * c + j];
-                        t0 -= l * xr[3 * k];
-                        t1 -= l * xr[3 * k + 1];
-                        t2 -= l * xr[3 * k + 2];
-                    }
-                    ts[3 * j] = t0;
-                    ts[3 * j + 1] = t1;
-                    ts[3 * j + 2] = t2;
-                }
+                rows_dot(st, lc, yj, 0, c, c, 2, 0, [&](int i, double x0, double x1, double x2) {
+                    xs[3 * i] = x0;
+                    xs[3 * i + 1] = x1;
+                    xs[3 * i + 2] = x2;
+                });
                 __syncthreads();
-                for (int i = tid; i < c; i += kST) {  // x_i = sum_{k>=i} X[k][i] t_k
-                    double x0 = 0, x1 = 0, x2 = 0;
-                    for (int k = i; k < c; k++) {
-                        const double x = st[k * c + i];
-                        x0 += x * ts[3 * k];
-                        x1 += x * ts[3 * k + 1];
-                        x2 += x * ts[3 * k + 2];
-                    }
-                    double* o = A.v + 3LL * pr[i];
-                    o[0] = x0;
-                    o[1] = x1;
-                    o[2] = x2;
-                }
-                break;
-            }
-            case kBwdT: {
-                double* xr = wk;  // [m][3]
-                for (int k = tid; k < m; k += kST) ld3(A.v + 3LL * si[k], xr[3 * k], xr[3 * k + 1], xr[3 * k + 2]);
-                __syncthreads();
-                const int j = off + warp;
-                if (j < c) {
-                    double s0, s1, s2;
-                    warp_dot3(st + warp * m, xr, 0, m, 0, lane, s0, s1, s2);
-                    if (lane == 0) {
-                        double y0, y1, y2;
-                        ld3(A.y + 3LL * (f0 + j), y0, y1, y2);
-                        double* o = A.t + 3LL * (f0 + j);
-                        o[0] = y0 - s0;
-                        o[1] = y1 - s1;
-                        o[2] = y2 - s2;
-                    }
-                }
+                rows_dot(st + c * lc, lm, xr, 0, c, m, 0, 0, [&](int i, double s0, double s1, double s2) {
+                    double* o = A.v + 3LL * si[i];
+                    o[0] = xs[3 * i] - s0;
+                    o[1] = xs[3 * i + 1] - s1;
+                    o[2] = xs[3 * i + 2] - s2;
+                });
                 break;
             }
             default: {  // kBwdX
-                double* ts = wk;  // [c - off][3]
-                for (int k = tid; k < 3 * (c - off); k += kST) ts[k] = __ldcg(A.t + 3LL * (f0 + off) + k);
+                double* yj = wk;                      // [c - r0][3]
+                double* xr = wk + 3 * (c - r0);       // [m][3]
+                double* xs = xr + 3 * m;              // [R][3]
+                for (int k = tid; k < 3 * (c - r0); k += kST) yj[k] = __ldcg(A.y + 3LL * (f0 + r0) + k);
+                for (int k = tid; k < m; k += kST) ld3(A.v + 3LL * si[c + k], xr[3 * k], xr[3 * k + 1], xr[3 * k + 2]);
                 __syncthreads();
-                const int i = off + warp;
-                if (i < c) {
-                    double x0, x1, x2;
-                    warp_dot3(st + warp * c, ts, i, c, off, lane, x0, x1, x2);
-                    if (lane == 0) {
-                        double* o = A.v + 3LL * si[warp];
-                        o[0] = x0;
-                        o[1] = x1;
-                        o[2] = x2;
-                    }
-                }
+                rows_dot(st, lc, yj, r0, R, c, 2, r0, [&](int i, double x0, double x1, double x2) {
+                    xs[3 * i] = x0;
+                    xs[3 * i + 1] = x1;
+                    xs[3 * i + 2] = x2;
+                });
+                __syncthreads();
+                rows_dot(st + R * lc, lm, xr, 0, R, m, 0, 0, [&](int i, double s0, double s1, double s2) {
+                    double* o = A.v + 3LL * si[r0 + i];
+                    o[0] = xs[3 * i] - s0;
+                    o[1] = xs[3 * i + 1] - s1;
+                    o[2] = xs[3 * i + 2] - s2;
+                });
                 break;
             }
             }
@@ -793,31 +765,71 @@ __global__ void __launch_bounds__(kST) k_solve(SolveArgs A)
             case kFwdG:
                 if (p >= 0) atomicAdd(cGin + p, 1);
                 break;
-            case kBwdT: atomicAdd(cT + s, 1); break;
             default: atomicAdd(cX + s, 1); break;  // kBwdFront, kBwdX
             }
         }
     }
 }
 
-// row-major copy of every front's L_RJ, columns [j0, j0+32) per CTA
-__global__ void __launch_bounds__(256) k_transpose_lt(FrontArgs a, const Tile* __restrict__ tiles)
+// W = L_RJ L_JJ^{-1} for every front, one 64 x 64 tile of W per CTA (4 x 4
+// per thread), L_RJ from the front's panel and L_JJ^{-1} (lower triangular,
+// entries above the diagonal masked) in blocks of 32; written row-major as W
+// and as its transpose.  With W the forward sweep forms a front's update
+// g = f_R - W f_J without waiting for y_J, and the backward sweep forms
+// x_J = L_JJ^{-T} y_J - W^T x_R in one step.
+__global__ void __launch_bounds__(256) k_w(FrontArgs a, const int4* __restrict__ tiles)
 {
-    const Tile tl = tiles[blockIdx.x];
-    const int s = tl.s, j0 = tl.off;
+    const int4 tl = tiles[blockIdx.x];
+    const int s = tl.x, k0 = tl.y * 64, j0 = tl.z * 64;
     const int r = a.nrow[s], c = a.ncol[s], m = r - c;
-    const int j = j0 + (threadIdx.x & 31);
-    if (j >= c) return;
-    const double* F = a.front + a.front_off[s] + static_cast<long long>(j) * r + c;
-    double* LT = a.lt + a.lt_off[s] + j;
-    for (int k = threadIdx.x >> 5; k < m; k += 8) LT[static_cast<long long>(k) * c] = F[k];
+    const double* F = a.front + a.front_off[s];
+    const double* X = a.dinv + a.dinv_off[s];
+    __shared__ double As[32][64 + 1];  // As[i][k] = L_RJ[k0 + k][i0 + i]
+    __shared__ double Bs[32][64 + 1];  // Bs[i][j] = X[i0 + i][j0 + j]
+    const int tid = threadIdx.x, tk = (tid & 15) * 4, tj = (tid >> 4) * 4;
+    double acc[4][4] = {};
+    for (int i0 = (j0 / 32) * 32; i0 < c; i0 += 32) {
+        for (int idx = tid; idx < 32 * 64; idx += 256) {
+            const int i = idx >> 6, kk = idx & 63;
+            const int gi = i0 + i, gk = k0 + kk, gj = j0 + kk;
+            As[i][kk] = (gi < c && gk < m) ? F[static_cast<long long>(gi) * r + c + gk] : 0.0;
+            Bs[i][kk] = (gi < c && gj < c && gi >= gj) ? X[static_cast<long long>(gi) * c + gj] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int i = 0; i < 32; i++) {
+            double av[4], bv[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                av[q] = As[i][tk + q];
+                bv[q] = Bs[i][tj + q];
+            }
+#pragma unroll
+            for (int x = 0; x < 4; x++)
+#pragma unroll
+                for (int y = 0; y < 4; y++) acc[x][y] += av[x] * bv[y];
+        }
+        __syncthreads();
+    }
+    double* W = a.w + a.lt_off[s];
+    double* WT = a.wt + a.lt_off[s];
+#pragma unroll
+    for (int x = 0; x < 4; x++)
+#pragma unroll
+        for (int y = 0; y < 4; y++) {
+            const int gk = k0 + tk + x, gj = j0 + tj + y;
+            if (gk < m && gj < c) {
+                W[static_cast<long long>(gk) * c + gj] = acc[x][y];
+                WT[static_cast<long long>(gj) * m + gk] = acc[x][y];
+            }
+        }
 }
 
 FrontArgs args_of(Precond& P)
 {
     return FrontArgs { P.d_first, P.d_ncol, P.d_nrow, P.d_rows, P.d_child_ptr, P.d_child_list, P.d_relind,
         P.d_level_list, P.d_contrib_ptr, P.d_contrib_idx, P.d_below_front, P.d_front_off, P.d_rows_off,
-        P.d_relind_off, P.d_dinv_off, P.d_upd_off, P.d_lt_off, P.d_front, P.d_dinv, P.d_dinvT, P.d_lt, P.d_fail };
+        P.d_relind_off, P.d_dinv_off, P.d_upd_off, P.d_lt_off, P.d_front, P.d_dinv, P.d_dinvT, P.d_w, P.d_wt, P.d_fail };
 }
 
 // the work buffers of one solve
@@ -859,7 +871,8 @@ void free_precond(Model& m)
     for (Tile** p : { &P.d_inv, &P.d_ea, &P.d_oinv }) dev_free(*p);
     dev_free(P.d_items);
     dev_free(P.d_syrk);
-    for (double** p : { &P.d_front, &P.d_dinv, &P.d_dinvT, &P.d_lt, &P.d_upd, &P.d_y, &P.d_t, &P.d_vals })
+    dev_free(P.d_wtiles);
+    for (double** p : { &P.d_front, &P.d_dinv, &P.d_dinvT, &P.d_w, &P.d_wt, &P.d_upd, &P.d_y, &P.d_t, &P.d_vals })
         dev_free(*p);
     delete m.precond;
     m.precond = nullptr;
@@ -944,12 +957,18 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
         P.lev_first_step.push_back(static_cast<int>(P.steps.size()));
     }
     P.n_inv_tiles = static_cast<int>(inv.size());
+    std::vector<int4> wtiles;
+    for (int s = 0; s < S.ns; s++) {
+        const int c = S.ncol[s], mm = S.nrow[s] - c;
+        for (int tk = 0; tk * 64 < mm; tk++)
+            for (int tj = 0; tj * 64 < c; tj++) wtiles.push_back(make_int4(s, tk, tj, 0));
+    }
+    P.n_wtiles = static_cast<int>(wtiles.size());
     P.n_oinv = static_cast<int>(oinv.size());
     // solve items: forward sweep by level (leaves first), backward sweep by
-    // level (root first); within a level the items a later item waits on come
-    // first.  Each item records the range of contributions its rows assemble,
-    // and the shared memory it stages is sized here.
-    std::vector<int4> items;
+    // level (root first).  Each item records the ranges of contributions its
+    // rows assemble, and the shared memory it stages is sized here.
+    std::vector<SolveItem> items;
     std::vector<int> tgt(4 * static_cast<size_t>(S.ns), 0);
     std::vector<char> whole(S.ns, 0);
     size_t stage_d = 1, work_d = 1, ints = 1;
@@ -958,72 +977,65 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
         work_d = std::max(work_d, wd);
         ints = std::max(ints, ni);
     };
-    auto contrib = [&](int s, int t0, int t1) {  // contribution range of front rows [t0, t1)
-        const long long ro = S.rows_off[s];
-        return std::make_pair(S.contrib_ptr[ro + t0], S.contrib_ptr[ro + t1]);
+    auto odd_h = [](int L) { return L | 1; };
+    auto tile = [&](int per_row) {  // rows per tile when a row stages per_row doubles
+        const int t = (kStageBudget / per_row) / 8 * 8;
+        return std::max(8, std::min(256, t));
     };
-    auto item = [&](int kind, int s, int off, std::pair<int, int> cr) {
-        items.push_back(make_int4(kind | (off << 3), s, cr.first, cr.second));
+    auto ntiles = [&](int n, int per_row) { const int t = tile(per_row); return (n + t - 1) / t; };
+    auto crange = [&](int s, int t0, int t1) {  // contributions of front rows [t0, t1)
+        const long long ro = S.rows_off[s];
+        return t1 > t0 ? std::make_pair(S.contrib_ptr[ro + t0], S.contrib_ptr[ro + t1]) : std::make_pair(0, 0);
     };
     for (int s = 0; s < S.ns; s++) {
-        const long long c = S.ncol[s], mm = S.nrow[s] - c;
-        whole[s] = c * c + mm * c <= kWholeFront;
-        const int nyt = static_cast<int>((c + kSW - 1) / kSW), ngt = static_cast<int>((mm + kSW - 1) / kSW);
-        tgt[s] = whole[s] ? 1 : nyt;                                          // y of s complete
-        if (S.parent[s] >= 0) tgt[S.ns + S.parent[s]] += whole[s] ? 1 : ngt;  // children's g complete
-        tgt[2 * S.ns + s] = nyt;                                              // t of s complete (tiled fronts)
-        tgt[3 * S.ns + s] = whole[s] ? 1 : nyt;                               // x of s complete
+        const int c = S.ncol[s], mm = S.nrow[s] - c, r = S.nrow[s];
+        const int lc = odd_h(c), lm = odd_h(mm);
+        whole[s] = static_cast<long long>(r) * lc <= kWholeBudget && static_cast<long long>(c) * (lc + lm) <= kWholeBudget;
+        tgt[s] = whole[s] ? 1 : ntiles(c, lc);                                              // y of s complete
+        if (S.parent[s] >= 0) tgt[S.ns + S.parent[s]] += whole[s] ? 1 : ntiles(mm, lc);  // children's g complete
+        tgt[3 * S.ns + s] = whole[s] ? 1 : ntiles(c, lc + lm);                              // x of s complete
     }
     for (int l = 0; l < nlev; l++) {
         for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) {
             const int s = S.level_list[q];
-            const int c = S.ncol[s], r = S.nrow[s], mm = r - c;
+            const int c = S.ncol[s], r = S.nrow[s], mm = r - c, lc = odd_h(c);
             if (whole[s]) {
-                const auto cr = contrib(s, 0, r);
-                item(kFwdFront, s, 0, cr);
-                need(static_cast<size_t>(c) * (c + mm), 3 * static_cast<size_t>(r + c), r + 1 + (cr.second - cr.first) + c);
-            } else {
-                for (int o = 0; o < c; o += kSW) {
-                    const int i1 = std::min(c, o + kSW);
-                    const auto cr = contrib(s, 0, i1);
-                    item(kFwdY, s, o, cr);
-                    need(static_cast<size_t>(i1 - o) * c, 3 * static_cast<size_t>(i1), i1 + 1 + (cr.second - cr.first) + i1);
-                }
+                const auto cr = crange(s, 0, r);
+                items.push_back(SolveItem { kFwdFront, s, 0, c, cr.first, cr.second, 0, 0 });
+                need(static_cast<size_t>(r) * lc, 3 * static_cast<size_t>(r), r + 1 + (cr.second - cr.first) + c);
+                continue;
             }
-        }
-        for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) {
-            const int s = S.level_list[q];
-            const int c = S.ncol[s], mm = S.nrow[s] - c;
-            if (whole[s]) continue;
-            for (int o = 0; o < mm; o += kSW) {
-                const int k1 = std::min(mm, o + kSW);
-                const auto cr = contrib(s, c + o, c + k1);
-                item(kFwdG, s, o, cr);
-                need(static_cast<size_t>(k1 - o) * c, 3 * static_cast<size_t>(c) + 3 * kSW, k1 - o + 1 + (cr.second - cr.first));
+            const int ty = tile(lc);
+            for (int o = 0; o < c; o += ty) {
+                const int i1 = std::min(c, o + ty);
+                const auto cr = crange(s, 0, i1);
+                items.push_back(SolveItem { kFwdY, s, o, i1, cr.first, cr.second, 0, 0 });
+                need(static_cast<size_t>(i1 - o) * lc, 3 * static_cast<size_t>(i1), i1 + 1 + (cr.second - cr.first) + i1);
+            }
+            const auto cj = crange(s, 0, c);
+            for (int o = 0; o < mm; o += ty) {
+                const int k1 = std::min(mm, o + ty);
+                const auto cr = crange(s, c + o, c + k1);
+                items.push_back(SolveItem { kFwdG, s, o, k1, cj.first, cj.second, cr.first, cr.second });
+                need(static_cast<size_t>(k1 - o) * lc, 3 * static_cast<size_t>(c + k1 - o),
+                    2 * static_cast<size_t>(c) + 1 + (cj.second - cj.first) + (k1 - o + 1) + (cr.second - cr.first));
             }
         }
     }
     for (int l = nlev - 1; l >= 0; l--) {
         for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) {
             const int s = S.level_list[q];
-            const int c = S.ncol[s], r = S.nrow[s], mm = r - c;
+            const int c = S.ncol[s], r = S.nrow[s], mm = r - c, lc = odd_h(c), lm = odd_h(mm);
             if (whole[s]) {
-                item(kBwdFront, s, 0, { 0, 0 });
-                need(static_cast<size_t>(c) * (c + mm), 3 * static_cast<size_t>(r), r);
-            } else {
-                for (int o = 0; o < c; o += kSW) {
-                    item(kBwdT, s, o, { 0, 0 });
-                    need(static_cast<size_t>(std::min(c, o + kSW) - o) * mm, 3 * static_cast<size_t>(mm), mm);
-                }
+                items.push_back(SolveItem { kBwdFront, s, 0, c, 0, 0, 0, 0 });
+                need(static_cast<size_t>(c) * (lc + lm), 3 * static_cast<size_t>(r + c), r);
+                continue;
             }
-        }
-        for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) {
-            const int s = S.level_list[q];
-            const int c = S.ncol[s];
-            if (whole[s]) continue;
-            for (int o = 0; o < c; o += kSW) {
-                item(kBwdX, s, o, { 0, 0 });
-                need(static_cast<size_t>(std::min(c, o + kSW) - o) * c, 3 * static_cast<size_t>(c - o), kSW);
+            const int tx = tile(lc + lm);
+            for (int o = 0; o < c; o += tx) {
+                const int i1 = std::min(c, o + tx);
+                items.push_back(SolveItem { kBwdX, s, o, i1, 0, 0, 0, 0 });
+                need(static_cast<size_t>(i1 - o) * (lc + lm), 3 * static_cast<size_t>(c - o + mm + i1 - o), r);
             }
         }
     }
@@ -1069,6 +1081,7 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
     UP(P.d_tgt, tgt);
     UP(P.d_inv, inv);
     UP(P.d_oinv, oinv);
+    UP(P.d_wtiles, wtiles);
     UP(P.d_ea, ea);
     UP(P.d_below_front, S.below_front);
     UP(P.d_panel_list, panel_list);
@@ -1078,7 +1091,8 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
     if ((st = dev_alloc(&P.d_front, static_cast<size_t>(S.front_size))) != EFEM_OK) return st;
     if ((st = dev_alloc(&P.d_dinv, static_cast<size_t>(std::max<long long>(S.dinv_size, 1)))) != EFEM_OK) return st;
     if ((st = dev_alloc(&P.d_dinvT, static_cast<size_t>(std::max<long long>(S.dinv_size, 1)))) != EFEM_OK) return st;
-    if ((st = dev_alloc(&P.d_lt, static_cast<size_t>(std::max<long long>(S.lt_size, 1)))) != EFEM_OK) return st;
+    if ((st = dev_alloc(&P.d_w, static_cast<size_t>(std::max<long long>(S.lt_size, 1)))) != EFEM_OK) return st;
+    if ((st = dev_alloc(&P.d_wt, static_cast<size_t>(std::max<long long>(S.lt_size, 1)))) != EFEM_OK) return st;
     if ((st = dev_alloc(&P.d_upd, static_cast<size_t>(std::max<long long>(S.upd_size, 1)))) != EFEM_OK) return st;
     if ((st = dev_alloc(&P.d_y, n3)) != EFEM_OK) return st;
     if ((st = dev_alloc(&P.d_t, n3)) != EFEM_OK) return st;
@@ -1130,12 +1144,15 @@ static efem_status precond_factor(Model& m, int* ok, double* ms_factor)
     }
     if (P.n_inv_tiles > 0) {
         k_diag_inv<<<P.n_inv_tiles, 32, 0, m.stream>>>(a, P.d_inv);
-        m.launches += 2;
+        m.launches++;
         if (P.n_oinv > 0) {
             k_offdiag_inv<<<P.n_oinv, kIT, 0, m.stream>>>(a, P.d_oinv);
             m.launches++;
         }
-        k_transpose_lt<<<P.n_inv_tiles, 256, 0, m.stream>>>(a, P.d_inv);
+        if (P.n_wtiles > 0) {
+            k_w<<<P.n_wtiles, 256, 0, m.stream>>>(a, P.d_wtiles);
+            m.launches++;
+        }
     }
     EFEM_CUDA(cudaGetLastError());
     EFEM_CUDA(cudaEventRecord(e1, m.stream));
