@@ -501,65 +501,173 @@ __device__ __forceinline__ void stage_wait() { asm volatile("cp.async.wait_all;"
 __device__ __forceinline__ int odd(int L) { return L | 1; }
 __device__ __forceinline__ int lanes_per_row(int R)
 {
-    int g = 32;
+    int g = kST;
     while (g > 1 && (kST / g) < R) g >>= 1;
     return g;
 }
 
 // Dot products of staged rows [0, R) (row stride lp) with a 3-component vector
 // v in shared memory (entry k at v[3 (k - vbase)]), over k in [lo, hi) with
-// lo / hi as in stage_rows; g lanes per row, reduced in a fixed order.  out
-// is called with (row, s0, s1, s2) by the first lane of each group.
+// lo / hi as in stage_rows.  Each row gets a group of g threads (g = kST / R
+// rounded to a power of two: a whole CTA for one row, one thread per row for
+// kST rows); a group wider than a warp adds its warps' partial sums through
+// shared memory.  Every sum has a fixed order.  out is called with
+// (row, s0, s1, s2) by the first thread of each group.
 template <typename Out>
 __device__ __forceinline__ void rows_dot(const double* M, int lp, const double* v, int vbase, int R, int L, int tri,
     int row0, Out out)
 {
+    __shared__ double part[kST / 32][3];
     const int g = lanes_per_row(R);
     const int lig = threadIdx.x & (g - 1), grp = threadIdx.x / g, ngrp = kST / g;
-    for (int base = 0; base < R; base += ngrp) {  // uniform trip count across each warp
+    for (int base = 0; base < R; base += ngrp) {  // uniform trip count across the CTA
         const int rr = base + grp;
         const bool valid = rr < R;
         const int lo = !valid ? 0 : (tri == 2 ? row0 + rr : 0);
         const int hi = !valid ? 0 : (tri == 1 ? row0 + rr + 1 : L);
         const double* row = M + rr * lp;
-        double a0 = 0, a1 = 0, a2 = 0;
-        for (int k = lo + lig; k < hi; k += g) {
+        double a0 = 0, a1 = 0, a2 = 0, b0 = 0, b1 = 0, b2 = 0;
+        int k = lo + lig;
+        for (; k + g < hi; k += 2 * g) {
+            const double d = row[k], e = row[k + g];
+            const double* vv = v + 3 * (k - vbase);
+            const double* vw = vv + 3 * g;
+            a0 += d * vv[0];
+            a1 += d * vv[1];
+            a2 += d * vv[2];
+            b0 += e * vw[0];
+            b1 += e * vw[1];
+            b2 += e * vw[2];
+        }
+        if (k < hi) {
             const double d = row[k];
             const double* vv = v + 3 * (k - vbase);
             a0 += d * vv[0];
             a1 += d * vv[1];
             a2 += d * vv[2];
         }
-        for (int o = g >> 1; o > 0; o >>= 1) {
+        a0 += b0;
+        a1 += b1;
+        a2 += b2;
+        const int w = g < 32 ? g : 32;
+        for (int o = w >> 1; o > 0; o >>= 1) {
             a0 += __shfl_xor_sync(0xffffffffu, a0, o);
             a1 += __shfl_xor_sync(0xffffffffu, a1, o);
             a2 += __shfl_xor_sync(0xffffffffu, a2, o);
         }
-        if (valid && lig == 0) out(rr, a0, a1, a2);
+        if (g > 32) {  // several warps per row
+            const int wid = threadIdx.x >> 5;
+            if ((threadIdx.x & 31) == 0) {
+                part[wid][0] = a0;
+                part[wid][1] = a1;
+                part[wid][2] = a2;
+            }
+            __syncthreads();
+            if (valid && lig == 0) {
+                a0 = a1 = a2 = 0.0;
+                for (int q = wid; q < wid + g / 32; q++) {
+                    a0 += part[q][0];
+                    a1 += part[q][1];
+                    a2 += part[q][2];
+                }
+                out(rr, a0, a1, a2);
+            }
+            __syncthreads();
+        } else if (valid && lig == 0) {
+            out(rr, a0, a1, a2);
+        }
     }
 }
 
 // f_t for front rows [t0, t1) into f (3 per row): the right-hand side for own
 // columns (t < c) plus the children's update entries landing on the row, from
 // the staged contribution pointers cp (row t0 first) and indices ci (starting
-// at contribution cbeg) and the staged node indices pr (row t0 first)
+// at contribution cbeg) and the staged node indices pr (row t0 first).  Each
+// thread first issues the loads of up to kBatch rows (right-hand side and the
+// first two contributions of each) and only then adds them, so the rows cost
+// one memory latency instead of one each; further contributions (rows with
+// more than two children behind them) follow in order.
+constexpr int kBatch = 2;
 __device__ __forceinline__ void assemble(const SolveArgs& A, int t0, int t1, int c, const int* cp, const int* ci,
     int cbeg, const int* pr, double* f)
 {
-    for (int t = t0 + static_cast<int>(threadIdx.x); t < t1; t += kST) {
-        double x0 = 0, x1 = 0, x2 = 0;
-        if (t < c) ld3(A.v + 3LL * pr[t - t0], x0, x1, x2);
-        for (int q = cp[t - t0]; q < cp[t - t0 + 1]; q++) {
-            double g0, g1, g2;
-            ld3(A.upd + 3LL * ci[q - cbeg], g0, g1, g2);
-            x0 += g0;
-            x1 += g1;
-            x2 += g2;
+    for (int base = t0; base < t1; base += kST * kBatch) {
+        double b[kBatch][3], g[kBatch][2][3];
+#pragma unroll
+        for (int u = 0; u < kBatch; u++) {
+            const int t = base + static_cast<int>(threadIdx.x) + u * kST;
+            const bool valid = t < t1;
+            const int q0 = valid ? cp[t - t0] : 0, q1 = valid ? cp[t - t0 + 1] : 0;
+            b[u][0] = b[u][1] = b[u][2] = 0.0;
+            if (valid && t < c) ld3(A.v + 3LL * pr[t - t0], b[u][0], b[u][1], b[u][2]);
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                g[u][e][0] = g[u][e][1] = g[u][e][2] = 0.0;
+                if (q0 + e < q1) ld3(A.upd + 3LL * ci[q0 + e - cbeg], g[u][e][0], g[u][e][1], g[u][e][2]);
+            }
         }
-        double* o = f + 3 * (t - t0);
-        o[0] = x0;
-        o[1] = x1;
-        o[2] = x2;
+#pragma unroll
+        for (int u = 0; u < kBatch; u++) {
+            const int t = base + static_cast<int>(threadIdx.x) + u * kST;
+            if (t >= t1) continue;
+            double x0 = b[u][0] + g[u][0][0] + g[u][1][0];
+            double x1 = b[u][1] + g[u][0][1] + g[u][1][1];
+            double x2 = b[u][2] + g[u][0][2] + g[u][1][2];
+            for (int q = cp[t - t0] + 2; q < cp[t - t0 + 1]; q++) {
+                double h0, h1, h2;
+                ld3(A.upd + 3LL * ci[q - cbeg], h0, h1, h2);
+                x0 += h0;
+                x1 += h1;
+                x2 += h2;
+            }
+            double* o = f + 3 * (t - t0);
+            o[0] = x0;
+            o[1] = x1;
+            o[2] = x2;
+        }
+    }
+}
+
+// n doubles from global memory written by other CTAs of this launch into
+// shared memory, loads batched ahead of the stores
+__device__ __forceinline__ void copy_cg(double* dst, const double* src, int n)
+{
+    for (int base = 0; base < n; base += kST * 8) {
+        double v[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            const int i = base + static_cast<int>(threadIdx.x) + u * kST;
+            v[u] = i < n ? __ldcg(src + i) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            const int i = base + static_cast<int>(threadIdx.x) + u * kST;
+            if (i < n) dst[i] = v[u];
+        }
+    }
+}
+
+// x_R: the solution on n front rows whose node indices are pr[0..n), gathered
+// from v (3 per node) into shared memory, loads batched ahead of the stores
+__device__ __forceinline__ void gather3(double* dst, const double* v, const int* pr, int n)
+{
+    for (int base = 0; base < n; base += kST * kBatch) {
+        double x[kBatch][3];
+#pragma unroll
+        for (int u = 0; u < kBatch; u++) {
+            const int k = base + static_cast<int>(threadIdx.x) + u * kST;
+            x[u][0] = x[u][1] = x[u][2] = 0.0;
+            if (k < n) ld3(v + 3LL * pr[k], x[u][0], x[u][1], x[u][2]);
+        }
+#pragma unroll
+        for (int u = 0; u < kBatch; u++) {
+            const int k = base + static_cast<int>(threadIdx.x) + u * kST;
+            if (k < n) {
+                dst[3 * k] = x[u][0];
+                dst[3 * k + 1] = x[u][1];
+                dst[3 * k + 2] = x[u][2];
+            }
+        }
     }
 }
 
@@ -713,8 +821,8 @@ __global__ void __launch_bounds__(kST) k_solve(SolveArgs A)
                 double* yj = wk;               // [c][3]
                 double* xr = wk + 3 * c;       // [m][3]
                 double* xs = wk + 3 * r;       // [c][3]
-                for (int k = tid; k < 3 * c; k += kST) yj[k] = __ldcg(A.y + 3LL * f0 + k);
-                for (int k = tid; k < m; k += kST) ld3(A.v + 3LL * si[c + k], xr[3 * k], xr[3 * k + 1], xr[3 * k + 2]);
+                copy_cg(yj, A.y + 3LL * f0, 3 * c);
+                gather3(xr, A.v, si + c, m);
                 __syncthreads();
                 rows_dot(st, lc, yj, 0, c, c, 2, 0, [&](int i, double x0, double x1, double x2) {
                     xs[3 * i] = x0;
@@ -734,8 +842,8 @@ __global__ void __launch_bounds__(kST) k_solve(SolveArgs A)
                 double* yj = wk;                      // [c - r0][3]
                 double* xr = wk + 3 * (c - r0);       // [m][3]
                 double* xs = xr + 3 * m;              // [R][3]
-                for (int k = tid; k < 3 * (c - r0); k += kST) yj[k] = __ldcg(A.y + 3LL * (f0 + r0) + k);
-                for (int k = tid; k < m; k += kST) ld3(A.v + 3LL * si[c + k], xr[3 * k], xr[3 * k + 1], xr[3 * k + 2]);
+                copy_cg(yj, A.y + 3LL * (f0 + r0), 3 * (c - r0));
+                gather3(xr, A.v, si + c, m);
                 __syncthreads();
                 rows_dot(st, lc, yj, r0, R, c, 2, r0, [&](int i, double x0, double x1, double x2) {
                     xs[3 * i] = x0;
@@ -979,8 +1087,8 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
     };
     auto odd_h = [](int L) { return L | 1; };
     auto tile = [&](int per_row) {  // rows per tile when a row stages per_row doubles
-        const int t = (kStageBudget / per_row) / 8 * 8;
-        return std::max(8, std::min(256, t));
+        const int t = (kStageBudget / per_row) / 4 * 4;
+        return std::max(4, std::min(256, t));
     };
     auto ntiles = [&](int n, int per_row) { const int t = tile(per_row); return (n + t - 1) / t; };
     auto crange = [&](int s, int t0, int t1) {  // contributions of front rows [t0, t1)

@@ -188,9 +188,10 @@ efem_status ensure_device(Model& m);  // create the stream and upload everything
 // ------------------------------------------------------------------ kernels (residual.cu)
 // r = R(u) on the model's stream; u, r device pointers of length 3*n_free.
 efem_status launch_residual(Model& m, const double* d_u, double* d_r);
-// the same on `stream`; with `stamp`, the GPU's global timer at the start is stored there
+// the same on `stream`; with `stamp`, the GPU's global timer at the start is
+// stored there; init_r = false when the caller has already set r = -f_ext
 efem_status launch_residual_on(Model& m, const double* d_u, double* d_r, cudaStream_t stream,
-    unsigned long long* stamp = nullptr);
+    unsigned long long* stamp = nullptr, bool init_r = true);
 
 // ------------------------------------------------------------------ solver (solver.cu)
 efem_status run_solve(Model& m, double* d_u, efem_solve_info* info);

@@ -279,14 +279,16 @@ efem_status launch_residual(Model& m, const double* d_u, double* d_r)
 }
 
 efem_status launch_residual_on(Model& m, const double* d_u, double* d_r, cudaStream_t stream,
-    unsigned long long* stamp)
+    unsigned long long* stamp, bool init_r)
 {
     const size_t n = 3 * static_cast<size_t>(m.n_free);
     if (n == 0) return EFEM_OK;
     // r = -f_ext (its first thread stores the start time in *stamp when given)
     extern void launch_neg(double* r, const double* f, size_t n, cudaStream_t st, unsigned long long* stamp);
-    launch_neg(d_r, m.d_fext, n, stream, stamp);
-    m.launches++;
+    if (init_r) {
+        launch_neg(d_r, m.d_fext, n, stream, stamp);
+        m.launches++;
+    }
     const bool mixed = m.opts.precision == EFEM_MIXED;
     for (auto& b : m.blocks) {
         if (b.n == 0) continue;

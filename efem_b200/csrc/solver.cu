@@ -49,9 +49,9 @@ namespace efem {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kMaxBlocks = 296;  // 2 x 148 SMs
+constexpr int kMaxBlocks = 592;  // 4 x 148 SMs
 constexpr int kMaxHist = 64;
-constexpr int kRowBlocks = 64;   // CTAs per history slot in the dot-product passes
+constexpr int kRowBlocks = 128;  // CTAs per history slot in the dot-product passes
 
 // device-resident solver state
 struct Scalars {
@@ -219,10 +219,19 @@ __global__ void k_trial(double* __restrict__ x, const double* __restrict__ xp, c
 
 // line-search scalars: dg = r.d, rinf = ||r||_inf, xinf = ||x||_inf, x2 = ||x||^2,
 // stored in S and in the host-mapped read-back array
+// With `decide` (inside the device-driven line search) the last CTA also
+// applies the accept / scale rule of LineSearchFEA.h:43-67: accept when
+// |r.d| <= |r0.d|; otherwise scale the step by 1.5 (same sign) or 0.5 and try
+// again, at most max_ls trials in all; it sets the line-search loop condition.
 __global__ void __launch_bounds__(kThreads) k_ls_reduce(const double* __restrict__ r, const double* __restrict__ d,
-    const double* __restrict__ x, size_t n, Scalars* S, double* partials, const int* perr, double* hread)
+    const double* __restrict__ x, size_t n, Scalars* S, double* partials, const int* perr, double* hread,
+    cudaGraphConditionalHandle h, int decide)
 {
-    if (blockIdx.x == 0 && threadIdx.x == 0) S->t_res += gtimer() - S->t0_res;  // the residual just ended
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        S->t_res += gtimer() - S->t0_res;  // the residual just ended
+        // the loop stops unless the last CTA below decides on another trial
+        if (decide) cudaGraphSetConditional(h, 0u);
+    }
     double v[4] = { 0, 0, 0, 0 };
     const int ops[4] = { 0, 1, 1, 0 };
     GRID_STRIDE(i, n)
@@ -249,6 +258,16 @@ __global__ void __launch_bounds__(kThreads) k_ls_reduce(const double* __restrict
         hread[kRdPerr] = S->perr;
         hread[kRdNRes] = static_cast<double>(S->n_res);
         hread[kRdTRes] = static_cast<double>(S->t_res);
+        if (decide) {
+            const int t = ++S->ls_t;
+            const double dg = S->dg, dg0 = S->dg0;
+            const bool again = !(fabs(dg) <= fabs(dg0)) && t < S->max_ls;
+            if (again) {
+                S->step *= dg * dg0 > 0 ? 1.5 : 0.5;
+                S->n_extra++;
+            }
+            cudaGraphSetConditional(h, again ? 1u : 0u);
+        }
     }
 }
 
@@ -308,26 +327,44 @@ __global__ void __launch_bounds__(kThreads) k_pass1(const double* __restrict__ x
         }
     }
     if (!rows_finish<3>(v, partials, &S->counter[2], sums)) return;
-    if (threadIdx.x != 0) return;
+    // last CTA: the small recursion runs on copies in shared memory (m x m G, ys, alpha)
+    extern __shared__ double dyn[];
+    double* sG = dyn;
+    double* sys = dyn + m * m;
+    double* sal = sys + m;
+    const int tid = threadIdx.x;
+    for (int q = tid; q < m * m; q += kThreads) sG[q] = S->G[q / m][q % m];
+    for (int j = tid; j < m; j += kThreads) sys[j] = S->ys[j];
+    __syncthreads();
     const double ys = sums[3 * m], yy = sums[3 * m + 1];
-    for (int j = 0; j < ncorr; j++) {
-        S->G[loc][j] = sums[3 * j];
-        S->G[j][loc] = sums[3 * j + 1];
+    for (int j = tid; j < ncorr; j += kThreads) {
+        sG[loc * m + j] = sums[3 * j];
+        sG[j * m + loc] = sums[3 * j + 1];
     }
-    S->G[loc][loc] = ys;
-    S->ys[loc] = ys;
-    S->theta = yy / ys;
-    S->ptr = loc + 1;
-    S->ncorr = ncorr;
-    // first loop (LBFGSMat.h:106-113): newest slot first
-    for (int i = 0; i < ncorr; i++) {
-        const int j = ((loc - i) % m + m) % m;
-        double t = sums[3 * j + 2];
-        for (int k = 0; k < i; k++) {
-            const int jk = ((loc - k) % m + m) % m;
-            t -= S->alpha[jk] * S->G[j][jk];
+    __syncthreads();
+    if (tid == 0) {
+        sG[loc * m + loc] = ys;
+        sys[loc] = ys;
+        // first loop (LBFGSMat.h:106-113): newest slot first
+        for (int i = 0; i < ncorr; i++) {
+            const int j = ((loc - i) % m + m) % m;
+            double t = sums[3 * j + 2];
+            for (int k = 0; k < i; k++) {
+                const int jk = ((loc - k) % m + m) % m;
+                t -= sal[jk] * sG[j * m + jk];
+            }
+            sal[j] = t / sys[j];
         }
-        S->alpha[j] = t / S->ys[j];
+        S->theta = yy / ys;
+        S->ptr = loc + 1;
+        S->ncorr = ncorr;
+        S->ys[loc] = ys;
+    }
+    __syncthreads();
+    for (int j = tid; j < ncorr; j += kThreads) {
+        S->G[loc][j] = sG[loc * m + j];
+        S->G[j][loc] = sG[j * m + loc];
+        S->alpha[j] = sal[j];
     }
 }
 
@@ -365,24 +402,40 @@ __global__ void __launch_bounds__(kThreads) k_pass3(const double* __restrict__ z
             v[0] += yj[i] * z[i];
     }
     if (!rows_finish<1>(v, partials, &S->counter[3], sums)) return;
-    if (threadIdx.x != 0) return;
-    const int ptr = S->ptr;
-    for (int o = 0; o < ncorr; o++) {
-        const int j = ((ptr - ncorr + o) % m + m) % m;
-        double t = sums[j];
-        for (int p = 0; p < o; p++) {
-            const int jp = ((ptr - ncorr + p) % m + m) % m;
-            t += S->coef[jp] * S->G[jp][j];
-        }
-        S->coef[j] = S->alpha[j] - t / S->ys[j];
+    // last CTA: the recursion on shared-memory copies of G, ys, alpha
+    extern __shared__ double dyn[];
+    double* sG = dyn;
+    double* sys = dyn + m * m;
+    double* sal = sys + m;
+    double* scf = sal + m;
+    const int tid = threadIdx.x;
+    for (int q = tid; q < m * m; q += kThreads) sG[q] = S->G[q / m][q % m];
+    for (int j = tid; j < m; j += kThreads) {
+        sys[j] = S->ys[j];
+        sal[j] = S->alpha[j];
     }
+    __syncthreads();
+    if (tid == 0) {
+        const int ptr = S->ptr;
+        for (int o = 0; o < ncorr; o++) {
+            const int j = ((ptr - ncorr + o) % m + m) % m;
+            double t = sums[j];
+            for (int p = 0; p < o; p++) {
+                const int jp = ((ptr - ncorr + p) % m + m) % m;
+                t += scf[jp] * sG[jp * m + j];
+            }
+            scf[j] = sal[j] - t / sys[j];
+        }
+    }
+    __syncthreads();
+    for (int j = tid; j < ncorr; j += kThreads) S->coef[j] = scf[j];
 }
 
-// Pass 4: d = z0 + sum_j coef_j s_j, then the start of the line search and
-// its first trial as in k_ls_begin_trial
+// Pass 4: d = z0 + sum_j coef_j s_j and the start of the line search
+// (r.d, xp = x, rp = r, step 1, line-search loop condition on)
 __global__ void __launch_bounds__(kThreads) k_pass4(double* __restrict__ d, const double* __restrict__ z,
-    const double* __restrict__ Sh, const double* __restrict__ r, double* __restrict__ x, double* __restrict__ xp,
-    double* __restrict__ rp, size_t n, Scalars* S, double* partials)
+    const double* __restrict__ Sh, const double* __restrict__ r, const double* __restrict__ x, double* __restrict__ xp,
+    double* __restrict__ rp, size_t n, Scalars* S, double* partials, cudaGraphConditionalHandle h_ls)
 {
     __shared__ double cf[kMaxHist];
     const int ncorr = S->ncorr;
@@ -395,14 +448,18 @@ __global__ void __launch_bounds__(kThreads) k_pass4(double* __restrict__ d, cons
         double di = z[i];
         for (int j = 0; j < ncorr; j++) di += cf[j] * Sh[j * n + i];
         d[i] = di;
-        const double ri = r[i], xi = x[i];
+        const double ri = r[i];
         v[0] += ri * di;
-        xp[i] = xi;
+        xp[i] = x[i];
         rp[i] = ri;
-        x[i] = xi + 1.0 * di;
     }
     block_reduce<1>(v, ops);
-    if (grid_finish<1>(v, ops, partials, &S->counter[1])) S->dg0 = v[0];
+    if (grid_finish<1>(v, ops, partials, &S->counter[1])) {
+        S->dg0 = v[0];
+        S->step = 1.0;
+        S->ls_t = 0;
+        cudaGraphSetConditional(h_ls, 1u);  // the line search's first trial always runs
+    }
 }
 
 __global__ void k_neg_copy(double* __restrict__ q, const double* __restrict__ r, size_t n)
@@ -410,30 +467,19 @@ __global__ void k_neg_copy(double* __restrict__ q, const double* __restrict__ r,
     GRID_STRIDE(i, n) q[i] = -r[i];
 }
 
-// x = xp + step d with the step held on the device
+// a trial of the device-driven line search: x = xp + step d with the step
+// held on the device, and r = -f_ext to start the residual at x (its start
+// time is stamped for the residual's timing)
 __global__ void k_trial_dev(double* __restrict__ x, const double* __restrict__ xp, const double* __restrict__ d,
-    size_t n, const Scalars* S)
+    double* __restrict__ r, const double* __restrict__ fext, size_t n, Scalars* S)
 {
+    if (blockIdx.x == 0 && threadIdx.x == 0) S->t0_res = gtimer();
     const double step = S->step;
-    GRID_STRIDE(i, n) x[i] = xp[i] + step * d[i];
-}
-
-// Line-search decision after a trial (LineSearchFEA.h:43-67): accept when
-// |r.d| <= |r0.d|; otherwise scale the step by 1.5 (same sign) or 0.5 and try
-// again, at most max_ls trials in all.  Sets the line-search loop condition.
-__global__ void k_ls_decide(Scalars* S, int first, cudaGraphConditionalHandle h)
-{
-    if (threadIdx.x != 0) return;
-    if (first) S->step = 1.0;
-    const int t = first ? 1 : S->ls_t + 1;
-    S->ls_t = t;
-    const double dg = S->dg, dg0 = S->dg0;
-    const bool again = !(fabs(dg) <= fabs(dg0)) && t < S->max_ls;
-    if (again) {
-        S->step *= dg * dg0 > 0 ? 1.5 : 0.5;
-        S->n_extra++;
+    GRID_STRIDE(i, n)
+    {
+        x[i] = xp[i] + step * d[i];
+        r[i] = -fext[i];
     }
-    cudaGraphSetConditional(h, again ? 1u : 0u);
 }
 
 // End of an iteration (LBFGS.h:150-170): stop on a non-finite residual or
@@ -492,8 +538,9 @@ __global__ void k_solve_init(Scalars* S)
     S->n_body = 0;
 }
 
-int grid_for(size_t n) { return static_cast<int>(std::min<size_t>(kMaxBlocks, std::max<size_t>(1, (n + kThreads * 4 - 1) / (kThreads * 4)))); }
-int row_blocks(size_t n) { return static_cast<int>(std::min<size_t>(kRowBlocks, std::max<size_t>(1, (n + kThreads * 4 - 1) / (kThreads * 4)))); }
+// vector kernels are latency-bound at these sizes: about one element per thread
+int grid_for(size_t n) { return static_cast<int>(std::min<size_t>(kMaxBlocks, std::max<size_t>(1, (n + kThreads - 1) / kThreads))); }
+int row_blocks(size_t n) { return static_cast<int>(std::min<size_t>(kRowBlocks, std::max<size_t>(1, (n + 2 * kThreads - 1) / (2 * kThreads)))); }
 
 }  // namespace
 
@@ -600,14 +647,17 @@ double* mapped(double* h)
     return cudaHostGetDevicePointer(&d, h, 0) == cudaSuccess ? static_cast<double*>(d) : h;
 }
 
-// the residual at the current trial x and the line-search reductions
-efem_status enqueue_trial_tail(Model& m, SolverWS& w, double* x, cudaStream_t st)
+// the residual at the current trial x and the line-search reductions; inside
+// the device-driven line search (h_ls given) r was started by k_trial_dev and
+// the reduction applies the accept / scale rule
+efem_status enqueue_trial_tail(Model& m, SolverWS& w, double* x, cudaStream_t st,
+    const cudaGraphConditionalHandle* h_ls = nullptr)
 {
     const size_t n = w.n;
-    efem_status s = launch_residual_on(m, x, w.r, st, &w.sc->t0_res);
+    efem_status s = launch_residual_on(m, x, w.r, st, &w.sc->t0_res, h_ls == nullptr);
     if (s != EFEM_OK) return s;
     k_ls_reduce<<<grid_for(n), kThreads, 0, st>>>(w.r, w.d, x, n, w.sc, w.partials, precond_error_flag(m),
-        mapped(w.h_read));
+        mapped(w.h_read), h_ls ? *h_ls : cudaGraphConditionalHandle(), h_ls ? 1 : 0);
     return EFEM_OK;
 }
 
@@ -618,13 +668,15 @@ efem_status enqueue_first(Model& m, SolverWS& w, double* x, cudaStream_t st)
     return enqueue_trial_tail(m, w, x, st);
 }
 
-// add_correction + two-loop with H0 + line-search start and first trial
-efem_status enqueue_body(Model& m, SolverWS& w, double* x, bool use_factor, cudaStream_t st)
+// add_correction + two-loop with H0 + line-search start
+efem_status enqueue_body(Model& m, SolverWS& w, double* x, bool use_factor, cudaStream_t st,
+    cudaGraphConditionalHandle h_ls)
 {
     const size_t n = w.n;
     const int mm = w.m;
     const dim3 g1(row_blocks(n), mm + 1), g3(row_blocks(n), mm);
-    k_pass1<<<g1, kThreads, 0, st>>>(x, w.xp, w.r, w.rp, w.S, w.Y, n, mm, w.sc, w.partials, w.sums);
+    const size_t sm1 = sizeof(double) * (mm * mm + 2 * mm), sm3 = sizeof(double) * (mm * mm + 3 * mm);
+    k_pass1<<<g1, kThreads, sm1, st>>>(x, w.xp, w.r, w.rp, w.S, w.Y, n, mm, w.sc, w.partials, w.sums);
     int* clear = nullptr;
     int n_clear = 0;
     if (use_factor) precond_counters(m, &clear, &n_clear);
@@ -633,9 +685,9 @@ efem_status enqueue_body(Model& m, SolverWS& w, double* x, bool use_factor, cuda
         efem_status s = precond_enqueue(m, w.q, st, false, &w.sc->t0_pc);
         if (s != EFEM_OK) return s;
     }
-    k_pass3<<<g3, kThreads, 0, st>>>(w.q, w.Y, n, mm, w.sc, w.partials, w.sums, use_factor ? 1 : 0);
-    k_pass4<<<grid_for(n), kThreads, 0, st>>>(w.d, w.q, w.S, w.r, x, w.xp, w.rp, n, w.sc, w.partials);
-    return enqueue_trial_tail(m, w, x, st);
+    k_pass3<<<g3, kThreads, sm3, st>>>(w.q, w.Y, n, mm, w.sc, w.partials, w.sums, use_factor ? 1 : 0);
+    k_pass4<<<grid_for(n), kThreads, 0, st>>>(w.d, w.q, w.S, w.r, x, w.xp, w.rp, n, w.sc, w.partials, h_ls);
+    return EFEM_OK;
 }
 
 efem_status instantiate(cudaGraph_t g, cudaGraphExec_t* out)
@@ -670,7 +722,8 @@ efem_status add_while(cudaStream_t st, cudaGraphConditionalHandle h, cudaGraph_t
 }
 
 // The device-driven iteration loop:
-//   k_loop_start; while (hIter) { body; k_ls_decide(first); while (hLs) { trial; tail; k_ls_decide }; k_iter_decide }
+//   k_loop_start; while (hIter) { body; while (hLs) { trial; residual; reductions + decision }; k_iter_decide }
+// (pass 4 sets hLs to 1 on every iteration: the first trial always runs)
 efem_status capture_loop(Model& m, SolverWS& w, double* x, bool use_factor, cudaGraphExec_t* out)
 {
     const long long launches = m.launches;  // capture launches nothing; replays are counted
@@ -693,7 +746,7 @@ efem_status capture_loop(Model& m, SolverWS& w, double* x, bool use_factor, cuda
         k_loop_start<<<1, 1, 0, s0>>>(w.sc);
         cudaGraph_t body = nullptr, ls_body = nullptr;
         if ((s = add_while(s0, h_iter, &body)) != EFEM_OK) break;
-        if (cudaGraphConditionalHandleCreate(&h_ls, body, 0, cudaGraphCondAssignDefault) != cudaSuccess) {
+        if (cudaGraphConditionalHandleCreate(&h_ls, body, 1, cudaGraphCondAssignDefault) != cudaSuccess) {
             s = EFEM_ERR_CUDA;
             break;
         }
@@ -701,17 +754,13 @@ efem_status capture_loop(Model& m, SolverWS& w, double* x, bool use_factor, cuda
             s = EFEM_ERR_CUDA;
             break;
         }
-        s = enqueue_body(m, w, x, use_factor, s1);
-        if (s == EFEM_OK) {
-            k_ls_decide<<<1, 32, 0, s1>>>(w.sc, 1, h_ls);
-            s = add_while(s1, h_ls, &ls_body);
-        }
+        s = enqueue_body(m, w, x, use_factor, s1, h_ls);
+        if (s == EFEM_OK) s = add_while(s1, h_ls, &ls_body);
         if (s == EFEM_OK && cudaStreamBeginCaptureToGraph(s2, ls_body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
             s = EFEM_ERR_CUDA;
         if (s == EFEM_OK) {
-            k_trial_dev<<<grid_for(w.n), kThreads, 0, s2>>>(x, w.xp, w.d, w.n, w.sc);
-            s = enqueue_trial_tail(m, w, x, s2);
-            k_ls_decide<<<1, 32, 0, s2>>>(w.sc, 0, h_ls);
+            k_trial_dev<<<grid_for(w.n), kThreads, 0, s2>>>(x, w.xp, w.d, w.r, m.d_fext, w.n, w.sc);
+            s = enqueue_trial_tail(m, w, x, s2, &h_ls);
             cudaGraph_t tmp = nullptr;
             if (cudaStreamEndCapture(s2, &tmp) != cudaSuccess && s == EFEM_OK) s = EFEM_ERR_CUDA;
         }
@@ -866,8 +915,9 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
         k_loop_params<<<1, 1, 0, st>>>(w.sc, eps, m.opts.max_iterations, std::max(1, m.opts.max_linesearch),
             kIterCap, k);
         m.launches++;
-        const long long per_body = 4 + (ok ? precond_launch_count(m) : 0) + per_res + 1 + 2;  // + ls / iteration decisions
-        const long long per_extra = 1 + per_res + 1 + 1;  // trial, residual, reductions, decision
+        // passes, H0, trial (which starts r), residual, reductions, iteration decision
+        const long long per_body = 4 + (ok ? precond_launch_count(m) : 0) + per_res + 2;
+        const long long per_extra = per_res + 1;  // trial, residual, reductions
         long long n_extra = 0;
         int status = kRunning;
         for (;;) {
