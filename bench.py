@@ -158,6 +158,8 @@ def main():
     ap.add_argument("--impl", default="efem_b200", choices=["efem_b200", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--host-loop", action="store_true",
+                    help="drive the L-BFGS iterations from the host (same kernels; for launch-list profiling)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -185,6 +187,7 @@ def main():
     opts = api.default_options()
     opts.precision = api.MIXED if args.precision == "mixed" else api.FP64
     opts.device = local
+    opts.host_loop = 1 if args.host_loop else 0
     t_setup = time.time()
     model = api.Model.from_case(case, opts)
     stream = torch.cuda.current_stream()

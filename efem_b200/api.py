@@ -45,7 +45,8 @@ class Options(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("integration", ctypes.c_int), ("nl_solver", ctypes.c_int),
                 ("m", ctypes.c_int), ("max_iterations", ctypes.c_int), ("max_linesearch", ctypes.c_int),
                 ("residual_criterion", ctypes.c_double), ("dx_criterion", ctypes.c_double),
-                ("device_ptrs", ctypes.c_int), ("deterministic", ctypes.c_int), ("device", ctypes.c_int)]
+                ("device_ptrs", ctypes.c_int), ("deterministic", ctypes.c_int), ("device", ctypes.c_int),
+                ("host_loop", ctypes.c_int)]
 
 
 class SolveInfo(ctypes.Structure):

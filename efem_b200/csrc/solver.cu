@@ -258,6 +258,7 @@ __global__ void __launch_bounds__(kThreads) k_ls_reduce(const double* __restrict
         hread[kRdPerr] = S->perr;
         hread[kRdNRes] = static_cast<double>(S->n_res);
         hread[kRdTRes] = static_cast<double>(S->t_res);
+        hread[kRdTPc] = static_cast<double>(S->t_pc);
         if (decide) {
             const int t = ++S->ls_t;
             const double dg = S->dg, dg0 = S->dg0;
@@ -435,7 +436,7 @@ __global__ void __launch_bounds__(kThreads) k_pass3(const double* __restrict__ z
 // (r.d, xp = x, rp = r, step 1, line-search loop condition on)
 __global__ void __launch_bounds__(kThreads) k_pass4(double* __restrict__ d, const double* __restrict__ z,
     const double* __restrict__ Sh, const double* __restrict__ r, const double* __restrict__ x, double* __restrict__ xp,
-    double* __restrict__ rp, size_t n, Scalars* S, double* partials, cudaGraphConditionalHandle h_ls)
+    double* __restrict__ rp, size_t n, Scalars* S, double* partials, cudaGraphConditionalHandle h_ls, int set_h)
 {
     __shared__ double cf[kMaxHist];
     const int ncorr = S->ncorr;
@@ -458,7 +459,7 @@ __global__ void __launch_bounds__(kThreads) k_pass4(double* __restrict__ d, cons
         S->dg0 = v[0];
         S->step = 1.0;
         S->ls_t = 0;
-        cudaGraphSetConditional(h_ls, 1u);  // the line search's first trial always runs
+        if (set_h) cudaGraphSetConditional(h_ls, 1u);  // the line search's first trial always runs
     }
 }
 
@@ -558,6 +559,7 @@ struct SolverWS {
     struct Graphs {
         cudaGraphExec_t first = nullptr;  // iteration 1: line-search start + first trial
         cudaGraphExec_t loop = nullptr;   // iterations 2, 3, ... (device-driven)
+        cudaGraphExec_t step = nullptr;   // one iteration (host-driven loop)
     };
     std::map<std::pair<double*, int>, Graphs> graphs;  // per (solution pointer, configuration)
     long long epoch = -1;                                // Model::epoch the graphs were captured at
@@ -579,6 +581,7 @@ static void drop_graphs(SolverWS& w)
     for (auto& kv : w.graphs) {
         if (kv.second.first) cudaGraphExecDestroy(kv.second.first);
         if (kv.second.loop) cudaGraphExecDestroy(kv.second.loop);
+        if (kv.second.step) cudaGraphExecDestroy(kv.second.step);
     }
     w.graphs.clear();
 }
@@ -651,10 +654,10 @@ double* mapped(double* h)
 // the device-driven line search (h_ls given) r was started by k_trial_dev and
 // the reduction applies the accept / scale rule
 efem_status enqueue_trial_tail(Model& m, SolverWS& w, double* x, cudaStream_t st,
-    const cudaGraphConditionalHandle* h_ls = nullptr)
+    const cudaGraphConditionalHandle* h_ls = nullptr, bool init_r = true)
 {
     const size_t n = w.n;
-    efem_status s = launch_residual_on(m, x, w.r, st, &w.sc->t0_res, h_ls == nullptr);
+    efem_status s = launch_residual_on(m, x, w.r, st, &w.sc->t0_res, init_r);
     if (s != EFEM_OK) return s;
     k_ls_reduce<<<grid_for(n), kThreads, 0, st>>>(w.r, w.d, x, n, w.sc, w.partials, precond_error_flag(m),
         mapped(w.h_read), h_ls ? *h_ls : cudaGraphConditionalHandle(), h_ls ? 1 : 0);
@@ -670,7 +673,7 @@ efem_status enqueue_first(Model& m, SolverWS& w, double* x, cudaStream_t st)
 
 // add_correction + two-loop with H0 + line-search start
 efem_status enqueue_body(Model& m, SolverWS& w, double* x, bool use_factor, cudaStream_t st,
-    cudaGraphConditionalHandle h_ls)
+    const cudaGraphConditionalHandle* h_ls)
 {
     const size_t n = w.n;
     const int mm = w.m;
@@ -686,7 +689,8 @@ efem_status enqueue_body(Model& m, SolverWS& w, double* x, bool use_factor, cuda
         if (s != EFEM_OK) return s;
     }
     k_pass3<<<g3, kThreads, sm3, st>>>(w.q, w.Y, n, mm, w.sc, w.partials, w.sums, use_factor ? 1 : 0);
-    k_pass4<<<grid_for(n), kThreads, 0, st>>>(w.d, w.q, w.S, w.r, x, w.xp, w.rp, n, w.sc, w.partials, h_ls);
+    k_pass4<<<grid_for(n), kThreads, 0, st>>>(w.d, w.q, w.S, w.r, x, w.xp, w.rp, n, w.sc, w.partials,
+        h_ls ? *h_ls : cudaGraphConditionalHandle(), h_ls ? 1 : 0);
     return EFEM_OK;
 }
 
@@ -754,13 +758,13 @@ efem_status capture_loop(Model& m, SolverWS& w, double* x, bool use_factor, cuda
             s = EFEM_ERR_CUDA;
             break;
         }
-        s = enqueue_body(m, w, x, use_factor, s1, h_ls);
+        s = enqueue_body(m, w, x, use_factor, s1, &h_ls);
         if (s == EFEM_OK) s = add_while(s1, h_ls, &ls_body);
         if (s == EFEM_OK && cudaStreamBeginCaptureToGraph(s2, ls_body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
             s = EFEM_ERR_CUDA;
         if (s == EFEM_OK) {
             k_trial_dev<<<grid_for(w.n), kThreads, 0, s2>>>(x, w.xp, w.d, w.r, m.d_fext, w.n, w.sc);
-            s = enqueue_trial_tail(m, w, x, s2, &h_ls);
+            s = enqueue_trial_tail(m, w, x, s2, &h_ls, false);
             cudaGraph_t tmp = nullptr;
             if (cudaStreamEndCapture(s2, &tmp) != cudaSuccess && s == EFEM_OK) s = EFEM_ERR_CUDA;
         }
@@ -774,6 +778,30 @@ efem_status capture_loop(Model& m, SolverWS& w, double* x, bool use_factor, cuda
         if (g) cudaGraphDestroy(g);
         if (s == EFEM_ERR_CUDA || e != cudaSuccess) set_error(std::string("capture of the iteration loop: ") +
             cudaGetErrorString(e != cudaSuccess ? e : cudaGetLastError()));
+        return s != EFEM_OK ? s : EFEM_ERR_CUDA;
+    }
+    return instantiate(g, out);
+}
+
+// One iteration for the host-driven loop: the passes with H0 and the line
+// search's first trial with its residual and reductions; the host applies the
+// accept / scale rule and the convergence tests.
+efem_status capture_step(Model& m, SolverWS& w, double* x, bool use_factor, cudaGraphExec_t* out)
+{
+    const long long launches = m.launches;
+    cudaStream_t s0 = w.capture[0];
+    cudaGraph_t g = nullptr;
+    EFEM_CUDA(cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal));
+    efem_status s = enqueue_body(m, w, x, use_factor, s0, nullptr);
+    if (s == EFEM_OK) {
+        k_trial_dev<<<grid_for(w.n), kThreads, 0, s0>>>(x, w.xp, w.d, w.r, m.d_fext, w.n, w.sc);
+        s = enqueue_trial_tail(m, w, x, s0, nullptr, false);
+    }
+    const cudaError_t e = cudaStreamEndCapture(s0, &g);
+    m.launches = launches;
+    if (s != EFEM_OK || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        if (s == EFEM_OK) set_error(std::string("graph capture: ") + cudaGetErrorString(e));
         return s != EFEM_OK ? s : EFEM_ERR_CUDA;
     }
     return instantiate(g, out);
@@ -881,12 +909,17 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
             drop_graphs(w);
             w.epoch = m.epoch;
         }
-        const auto key = std::make_pair(x, (ok ? 1 : 0) | (m.opts.precision << 1));
+        const bool host_loop = m.opts.host_loop != 0;
+        const auto key = std::make_pair(x, (ok ? 1 : 0) | (m.opts.precision << 1) | (host_loop ? 4 : 0));
         if (!w.graphs.count(key) && w.graphs.size() >= 8) drop_graphs(w);  // many distinct solution pointers
         SolverWS::Graphs& gr = w.graphs[key];
         if (!gr.first) {
             if ((s = capture_first(m, w, x, &gr.first)) != EFEM_OK) return s;
-            if ((s = capture_loop(m, w, x, ok, &gr.loop)) != EFEM_OK) return s;
+            if (host_loop) {
+                if ((s = capture_step(m, w, x, ok, &gr.step)) != EFEM_OK) return s;
+            } else if ((s = capture_loop(m, w, x, ok, &gr.loop)) != EFEM_OK) {
+                return s;
+            }
         }
         // iteration 1 from the host
         EFEM_CUDA(cudaGraphLaunch(gr.first, st));
@@ -911,6 +944,40 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
             goto done;
         }
         k++;
+        if (host_loop) {  // iterations 2, 3, ... one graph launch each, decisions on the host
+            const long long per_step = 4 + (ok ? precond_launch_count(m) : 0) + per_res + 1;
+            for (;;) {
+                EFEM_CUDA(cudaGraphLaunch(gr.step, st));
+                EFEM_CUDA(cudaStreamSynchronize(st));
+                m.launches += per_step;
+                if (ok) info->n_precond_applies++;
+                if (hr[kRdPerr] != 0.0) {
+                    set_error("the triangular solve of the preconditioner gave up waiting for a front");
+                    return EFEM_ERR_CUDA;
+                }
+                const double dg0h = hr[kRdDg0];
+                double dgh = hr[kRdDg], steph = 1.0;
+                for (int it = 1; it < m.opts.max_linesearch && !(std::fabs(dgh) <= std::fabs(dg0h)); it++) {
+                    steph *= dgh * dg0h > 0 ? 1.5 : 0.5;
+                    if ((s = direct_trial(steph)) != EFEM_OK) return s;
+                    dgh = hr[kRdDg];
+                }
+                rinf = hr[kRdRinf];
+                xinf = hr[kRdXinf];
+                if (!std::isfinite(rinf) || !std::isfinite(xinf)) goto nan_exit;
+                if (rinf <= eps || rinf <= eps * xinf) {
+                    converged = true;
+                    break;
+                }
+                if (m.opts.max_iterations != 0 && k >= m.opts.max_iterations) {
+                    info->flags |= EFEM_SOLVE_MAX_ITERS;
+                    break;
+                }
+                k++;
+            }
+            if (ok) ms_pc += hr[kRdTPc] * 1e-6;
+            goto done;
+        }
         // iterations 2, 3, ... on the device, kIterCap per graph launch
         k_loop_params<<<1, 1, 0, st>>>(w.sc, eps, m.opts.max_iterations, std::max(1, m.opts.max_linesearch),
             kIterCap, k);

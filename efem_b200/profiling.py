@@ -1,10 +1,11 @@
 """Roofline bookkeeping for bench.py.
 
-The solve reports device time per phase, taken with CUDA events on the
-model's stream around every residual evaluation and every H0 application
-(efem_solve_info.ms_residual / ms_precond).  From those and the algorithmic
-byte counts the library reports (efem_model_info), this module picks the
-dominant kernel group of the timed solves and forms
+The solve reports device time per phase, summed on the device from the
+GPU's global timer at the start and end of every residual evaluation and
+every H0 application (efem_solve_info.ms_residual / ms_precond; the first H0
+application of a solve is timed with CUDA events).  From those and the
+algorithmic byte counts the library reports (efem_model_info), this module
+picks the dominant kernel group of the timed solves and forms
 
     achieved = algorithmic bytes per launch / mean launch duration
     frac     = achieved / measured HBM copy bandwidth (MEASURED_PEAKS.json)
@@ -12,9 +13,12 @@ dominant kernel group of the timed solves and forms
 Algorithmic bytes per launch:
   residual   every input read once (connectivity, material index, V_e,
              J0^{-1} per Gauss point, u, f_ext) and r written once
-  H0 apply   the factor's panels (nnz(L) entries) and the inverted diagonal
-             blocks (their lower triangles), each read once in the forward and
-             once in the backward sweep, plus the 3-component work vectors
+  H0 apply   nnz(L) factor entries read in each sweep: the forward sweep
+             reads L_JJ^{-1} (lower triangle) and W = L_RJ L_JJ^{-1}, the
+             backward sweep their transposes; plus five passes over the
+             3-component vectors (right-hand side, y written and read, x
+             gathered and written); the fronts' update vectors (a few per cent
+             of the total) are not counted
 """
 from __future__ import annotations
 
@@ -36,7 +40,8 @@ def hbm_peak():
 
 
 def measured_traffic(kernel_group):
-    """DRAM bytes per launch from a committed ncu summary, if one exists."""
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum of
+    one ncu capture) from profiles/traffic.json, if present."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     try:
         with open(p) as f:
@@ -56,7 +61,7 @@ def roofline_report(model, infos):
     tot_ms = sum(i["ms_total"] for i in infos)
     fac_ms = sum(i["ms_factor"] for i in infos)
     res_bytes = float(info["residual_bytes"])
-    pc_bytes = 2.0 * 8.0 * (info["factor_nnz"] + info["factor_dinv_nnz"]) + 6.0 * 8.0 * n3
+    pc_bytes = 2.0 * 8.0 * info["factor_nnz"] + 5.0 * 8.0 * n3
     groups = {
         "residual": (res_ms, res_calls, res_bytes),
         "precond_apply": (pc_ms, pc_calls, pc_bytes),

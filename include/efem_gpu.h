@@ -91,6 +91,10 @@ typedef struct {
     int device_ptrs;          /* 1: vector arguments are device pointers */
     int deterministic;        /* 1: element scatter by ordered gather (bitwise repeatable) */
     int device;               /* CUDA ordinal; -1 = current device */
+    int host_loop;            /* 1: L-BFGS iterations driven from the host, one graph launch per
+                                 iteration (same kernels; for profilers that do not see kernels
+                                 inside conditional graph nodes); 0: the iteration loop runs on
+                                 the device */
 } efem_options;
 
 enum {

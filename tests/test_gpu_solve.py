@@ -84,3 +84,20 @@ def test_c3d20_reduced_solve_matches_reference(tmp_path):
         u, info = m.solve()
         ref = d["u_solve_reduced"]
         assert np.linalg.norm(u - ref) <= 1e-6 * np.linalg.norm(ref)
+
+
+def test_host_loop_matches_device_loop(tmp_path):
+    """The host-driven iteration loop (host_loop = 1, the mode profilers use)
+    runs the same kernels as the device-driven one and reaches the same
+    solution within the solve's own tolerance."""
+    path = golden_files("cantilever_c3d4_pressure.npz")[0]
+    cfg, d = write_golden_case(path, tmp_path)
+    m = api.Model.from_json(cfg)
+    u_dev, info_dev = m.solve()
+    m.set_options(host_loop=1)
+    u_host, info_host = m.solve()
+    for info in (info_dev, info_host):
+        assert info["flags"] & api.SOLVE_CONVERGED and info["r_inf"] <= 1e-6
+    ref = d["u_solve"]
+    assert np.linalg.norm(u_host - ref) <= 1e-6 * np.linalg.norm(ref)
+    assert np.linalg.norm(u_host - u_dev) <= 1e-6 * np.linalg.norm(ref)
