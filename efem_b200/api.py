@@ -32,7 +32,8 @@ SOLVE_CONVERGED, SOLVE_PRECOND_FALLBACK, SOLVE_DX_CONVERGED, SOLVE_MAX_ITERS = 1
 EXPORTED = ["efem_default_options", "efem_model_create_from_json", "efem_model_create", "efem_model_destroy",
             "efem_get_options", "efem_set_options", "efem_get_model_info", "efem_dof_map", "efem_residual",
             "efem_approx_jacobian_csr", "efem_precond_apply", "efem_precond_apply_noalloc", "efem_solve",
-            "efem_set_stream", "efem_last_error", "efem_version"]
+            "efem_set_stream", "efem_last_error", "efem_version", "efem_hvp", "efem_hvp_transpose",
+            "efem_residual_param_derivative", "efem_adjoint"]
 
 
 class EfemError(RuntimeError):
@@ -46,7 +47,8 @@ class Options(ctypes.Structure):
                 ("m", ctypes.c_int), ("max_iterations", ctypes.c_int), ("max_linesearch", ctypes.c_int),
                 ("residual_criterion", ctypes.c_double), ("dx_criterion", ctypes.c_double),
                 ("device_ptrs", ctypes.c_int), ("deterministic", ctypes.c_int), ("device", ctypes.c_int),
-                ("host_loop", ctypes.c_int)]
+                ("host_loop", ctypes.c_int), ("adjoint_tolerance", ctypes.c_double),
+                ("adjoint_max_iterations", ctypes.c_int)]
 
 
 class SolveInfo(ctypes.Structure):
@@ -60,13 +62,21 @@ class SolveInfo(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class AdjointInfo(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("flags", ctypes.c_int), ("rel_residual", ctypes.c_double),
+                ("ms_total", ctypes.c_double), ("ms_solve", ctypes.c_double), ("ms_params", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class ModelInfo(ctypes.Structure):
     _fields_ = [("n_nodes", ctypes.c_int), ("n_free_nodes", ctypes.c_int), ("n_dof", ctypes.c_int),
                 ("n_elements", ctypes.c_int), ("n_elements_skipped", ctypes.c_int), ("n_faces", ctypes.c_int),
                 ("n_force_nodes", ctypes.c_int), ("n_blocks", ctypes.c_int), ("factor_nnz", ctypes.c_longlong),
                 ("n_supernodes", ctypes.c_int), ("n_levels", ctypes.c_int), ("factor_gflop", ctypes.c_double),
                 ("factor_dinv_nnz", ctypes.c_longlong), ("residual_bytes", ctypes.c_longlong),
-                ("residual_flops", ctypes.c_double)]
+                ("residual_flops", ctypes.c_double), ("n_params", ctypes.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -121,6 +131,10 @@ def lib():
             "efem_last_error": [ctypes.c_char_p, ctypes.c_size_t],
             "efem_set_stream": [vp, vp],
             "efem_precond_apply_noalloc": [vp, vp],
+            "efem_hvp": [vp, vp, vp, vp],
+            "efem_hvp_transpose": [vp, vp, vp, vp],
+            "efem_residual_param_derivative": [vp, vp, ctypes.c_int, vp],
+            "efem_adjoint": [vp, vp, vp, dp, vp, ctypes.POINTER(AdjointInfo)],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -309,6 +323,48 @@ class Model:
         if st not in (OK,):
             raise EfemError(st, last_error())
         return u, info.as_dict()
+
+    # ------------------------------------------------------------------ sensitivities
+    def _vec(self, x):
+        if hasattr(x, "data_ptr"):
+            return x
+        return np.ascontiguousarray(x, dtype=np.float64)
+
+    def _out_like(self, x):
+        if hasattr(x, "data_ptr"):
+            import torch
+            return torch.empty(self.n_dof, dtype=torch.float64, device=x.device)
+        return np.zeros(self.n_dof)
+
+    def hvp(self, u, v, transpose=False):
+        """K(u) v (K(u)^T v with transpose=True), the true tangent at u."""
+        u, v = self._vec(u), self._vec(v)
+        out = self._out_like(u)
+        f = lib().efem_hvp_transpose if transpose else lib().efem_hvp
+        check(f(self.h, _vec_ptr(u), _vec_ptr(v), _vec_ptr(out)))
+        return out
+
+    def param_derivative(self, u, k):
+        """dR/dtheta_k at u (parameter order: efem_residual_param_derivative)."""
+        u = self._vec(u)
+        out = self._out_like(u)
+        check(lib().efem_residual_param_derivative(self.h, _vec_ptr(u), int(k), _vec_ptr(out)))
+        return out
+
+    @property
+    def n_params(self):
+        return self.info()["n_params"]
+
+    def adjoint(self, u, dJdu, want_lambda=False):
+        """dJ/dtheta at the equilibrium u for the objective gradient dJ/du;
+        returns (dJdtheta, lambda or None, info dict)."""
+        u, g = self._vec(u), self._vec(dJdu)
+        out = np.zeros(self.n_params)
+        lam = self._out_like(u) if want_lambda else None
+        info = AdjointInfo()
+        check(lib().efem_adjoint(self.h, _vec_ptr(u), _vec_ptr(g), _ptr(out),
+                                 _vec_ptr(lam) if lam is not None else None, ctypes.byref(info)))
+        return out, lam, info.as_dict()
 
     def approx_jacobian_csr(self):
         nnz = ctypes.c_longlong()

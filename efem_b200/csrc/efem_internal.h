@@ -87,6 +87,7 @@ struct DevFaces {
     double* J0inv = nullptr;      // [n][MAX_FGP][9]
     float* J0inv_f = nullptr;
     double* load = nullptr;       // [n][4]: directed flag, value / vector
+    int* load_idx = nullptr;      // [n]: index of the face's load among the pressure loads
     // face tables for this element kind
     int n_tables = 0;
     int* t_ngp = nullptr;         // [n_tables]
@@ -99,10 +100,12 @@ struct DevFaces {
     // host copies (set-up output; uploaded by ensure_device)
     std::vector<int> h_conn, h_table, h_ngp;
     std::vector<double> h_A0, h_J0inv, h_load, h_w, h_N, h_dN;
+    std::vector<int> h_load_idx;
 };
 
 struct Precond;   // Cholesky preconditioner (chol.cu)
 struct SolverWS;  // L-BFGS workspace (solver.cu)
+struct AdjointWS; // tangent / adjoint workspace (adjoint.cu)
 
 struct Model {
     efem_options opts;
@@ -124,6 +127,7 @@ struct Model {
     std::vector<DevBlock> blocks;
     std::vector<DevFaces> faces;
     int n_faces = 0;
+    int n_pressure_loads = 0;         // follower and directed pressure loads, in input order
 
     MatParams<double>* d_mats = nullptr;
     MatParams<float>* d_mats_f = nullptr;
@@ -137,6 +141,7 @@ struct Model {
     long long epoch = 0;              // bumped when device arrays that captured graphs point to are rebuilt
     Precond* precond = nullptr;   // owned; freed by free_precond
     SolverWS* ws = nullptr;       // owned; freed by free_solver
+    AdjointWS* aws = nullptr;     // owned; freed by free_adjoint
 
     ~Model();
 };
@@ -196,6 +201,16 @@ efem_status launch_residual_on(Model& m, const double* d_u, double* d_r, cudaStr
 // ------------------------------------------------------------------ solver (solver.cu)
 efem_status run_solve(Model& m, double* d_u, efem_solve_info* info);
 void free_solver(Model& m);
+void free_adjoint(Model& m);
+
+// ------------------------------------------------------------------ sensitivities (adjoint.cu)
+int n_params(const Model& m);
+// out = K(u) v (transpose: K(u)^T v); device pointers
+efem_status hvp(Model& m, const double* d_u, const double* d_v, double* d_out, bool transpose);
+efem_status residual_param_derivative(Model& m, const double* d_u, int k, double* d_out);
+efem_status adjoint(Model& m, const double* d_u, const double* d_dJdu, double* dJdtheta, double* d_lambda,
+    efem_adjoint_info* info);
+efem_status adjoint_io(Model& m, double** io);  // an n_dof device buffer for host-pointer calls
 
 // ------------------------------------------------------------------ preconditioner (chol.cu)
 // Build (once) the scalar approximate Jacobian L and its Cholesky factor.

@@ -113,6 +113,7 @@ Model::~Model()
 {
     if (device >= 0) cudaSetDevice(device);
     free_solver(*this);
+    free_adjoint(*this);
     free_precond(*this);
     for (auto& b : blocks) {
         dev_free(b.conn);
@@ -133,6 +134,7 @@ Model::~Model()
         dev_free(f.J0inv);
         dev_free(f.J0inv_f);
         dev_free(f.load);
+        dev_free(f.load_idx);
         dev_free(f.t_ngp);
         dev_free(f.t_w);
         dev_free(f.t_N);
@@ -409,11 +411,13 @@ efem_status build_model(ModelInput& in, Model& m)
             df.h_A0.insert(df.h_A0.end(), F.A0, F.A0 + 3);
             for (int g = 0; g < MAX_FGP; g++) df.h_J0inv.insert(df.h_J0inv.end(), F.J0inv[g], F.J0inv[g] + 9);
             df.h_load.insert(df.h_load.end(), loadvals.begin() + 4 * F.load, loadvals.begin() + 4 * F.load + 4);
+            df.h_load_idx.push_back(F.load);
         }
         df.n_tables = static_cast<int>(table_of_key.size());
         m.faces.push_back(std::move(df));
     }
     m.h_fext = std::move(fext);
+    m.n_pressure_loads = static_cast<int>(loadvals.size() / 4);
     return build_blocks(m);
 }
 
@@ -533,6 +537,7 @@ efem_status ensure_device(Model& m)
         UP(f.J0inv, f.h_J0inv);
         UP(f.J0inv_f, to_f32(f.h_J0inv));
         UP(f.load, f.h_load);
+        UP(f.load_idx, f.h_load_idx);
         UP(f.t_ngp, f.h_ngp);
         UP(f.t_w, f.h_w);
         UP(f.t_N, f.h_N);
@@ -672,6 +677,9 @@ efem_status efem_default_options(efem_options* o)
     o->device_ptrs = 0;
     o->deterministic = 0;
     o->device = -1;
+    o->host_loop = 0;
+    o->adjoint_tolerance = 1e-10;
+    o->adjoint_max_iterations = 2000;
     return EFEM_OK;
 }
 
@@ -839,6 +847,7 @@ efem_status efem_get_model_info(void* model, efem_model_info* info)
     }
     info->residual_bytes = bytes;
     info->residual_flops = flops;
+    info->n_params = efem::n_params(*m);
     efem::precond_info(*m, info);
     return EFEM_OK;
 }
@@ -868,6 +877,75 @@ efem_status efem_residual(void* model, const double* u, double* r)
     if (s != EFEM_OK) return s;
     if (!m->opts.device_ptrs)
         EFEM_CUDA(cudaMemcpyAsync(r, dr, sizeof(double) * 3 * m->n_free, cudaMemcpyDeviceToHost, m->stream));
+    EFEM_CUDA(cudaStreamSynchronize(m->stream));
+    return EFEM_OK;
+}
+
+static efem_status hvp_call(void* model, const double* u, const double* v, double* out, bool transpose)
+{
+    Model* m;
+    efem_status s = guard(model, &m);
+    if (s != EFEM_OK) return s;
+    if (!u || !v || !out) return EFEM_ERR_ARG;
+    if ((s = efem::ensure_device(*m)) != EFEM_OK) return s;
+    double *du, *dv, *io = nullptr;
+    if ((s = efem::adjoint_io(*m, &io)) != EFEM_OK) return s;
+    double* dout = m->opts.device_ptrs ? out : io;
+    if ((s = vec_in(*m, u, &du, m->d_u)) != EFEM_OK) return s;
+    if ((s = vec_in(*m, v, &dv, m->d_r)) != EFEM_OK) return s;
+    if ((s = efem::hvp(*m, du, dv, dout, transpose)) != EFEM_OK) return s;
+    if (!m->opts.device_ptrs)
+        EFEM_CUDA(cudaMemcpyAsync(out, dout, sizeof(double) * 3 * m->n_free, cudaMemcpyDeviceToHost, m->stream));
+    EFEM_CUDA(cudaStreamSynchronize(m->stream));
+    return EFEM_OK;
+}
+
+efem_status efem_hvp(void* model, const double* u, const double* v, double* Kv)
+{
+    return hvp_call(model, u, v, Kv, false);
+}
+
+efem_status efem_hvp_transpose(void* model, const double* u, const double* w, double* KTw)
+{
+    return hvp_call(model, u, w, KTw, true);
+}
+
+efem_status efem_residual_param_derivative(void* model, const double* u, int k, double* dR)
+{
+    Model* m;
+    efem_status s = guard(model, &m);
+    if (s != EFEM_OK) return s;
+    if (!u || !dR) return EFEM_ERR_ARG;
+    if ((s = efem::ensure_device(*m)) != EFEM_OK) return s;
+    double *du, *io = nullptr;
+    if ((s = efem::adjoint_io(*m, &io)) != EFEM_OK) return s;
+    double* dout = m->opts.device_ptrs ? dR : io;
+    if ((s = vec_in(*m, u, &du, m->d_u)) != EFEM_OK) return s;
+    if ((s = efem::residual_param_derivative(*m, du, k, dout)) != EFEM_OK) return s;
+    if (!m->opts.device_ptrs)
+        EFEM_CUDA(cudaMemcpyAsync(dR, dout, sizeof(double) * 3 * m->n_free, cudaMemcpyDeviceToHost, m->stream));
+    EFEM_CUDA(cudaStreamSynchronize(m->stream));
+    return EFEM_OK;
+}
+
+efem_status efem_adjoint(void* model, const double* u, const double* dJdu, double* dJdtheta, double* lambda,
+    efem_adjoint_info* info)
+{
+    Model* m;
+    efem_status s = guard(model, &m);
+    if (s != EFEM_OK) return s;
+    if (!u || !dJdu || !dJdtheta) return EFEM_ERR_ARG;
+    if ((s = efem::ensure_device(*m)) != EFEM_OK) return s;
+    efem_adjoint_info local;
+    if (!info) info = &local;
+    double *du, *dg, *io = nullptr;
+    if ((s = efem::adjoint_io(*m, &io)) != EFEM_OK) return s;
+    if ((s = vec_in(*m, u, &du, m->d_u)) != EFEM_OK) return s;
+    if ((s = vec_in(*m, dJdu, &dg, m->d_r)) != EFEM_OK) return s;
+    double* dl = lambda ? (m->opts.device_ptrs ? lambda : io) : nullptr;
+    if ((s = efem::adjoint(*m, du, dg, dJdtheta, dl, info)) != EFEM_OK) return s;
+    if (lambda && !m->opts.device_ptrs)
+        EFEM_CUDA(cudaMemcpyAsync(lambda, dl, sizeof(double) * 3 * m->n_free, cudaMemcpyDeviceToHost, m->stream));
     EFEM_CUDA(cudaStreamSynchronize(m->stream));
     return EFEM_OK;
 }

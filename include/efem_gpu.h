@@ -95,6 +95,8 @@ typedef struct {
                                  iteration (same kernels; for profilers that do not see kernels
                                  inside conditional graph nodes); 0: the iteration loop runs on
                                  the device */
+    double adjoint_tolerance; /* relative residual of the adjoint solve (default 1e-10) */
+    int adjoint_max_iterations; /* GMRES iteration limit of the adjoint solve (default 2000) */
 } efem_options;
 
 enum {
@@ -112,8 +114,8 @@ typedef struct {
     double u_inf, r_inf;      /* final ||u||_inf and ||r||_inf (Integrator.cpp:37-40) */
     double ms_total;          /* device time of the whole solve (CUDA events on the model's stream) */
     double ms_factor;         /* numeric factorisation of the approximate Jacobian */
-    double ms_residual;       /* all residual evaluations (events around each) */
-    double ms_precond;        /* all H0 applications (events around each) */
+    double ms_residual;       /* all residual evaluations (GPU global timer, summed on the device) */
+    double ms_precond;        /* all H0 applications (GPU global timer; the first one by CUDA events) */
     long long n_kernel_launches;  /* this library's kernels launched by the solve */
     int n_precond_applies;        /* H0 applications (ms_precond covers them) */
 } efem_solve_info;
@@ -129,7 +131,18 @@ typedef struct {
     long long factor_dinv_nnz;            /* entries of the inverted diagonal blocks (lower triangles) */
     long long residual_bytes;             /* algorithmic bytes of one residual evaluation */
     double residual_flops;                /* algorithmic flops of one residual evaluation */
+    int n_params;                         /* sensitivity parameters (efem_adjoint): 5 per material slot
+                                             (C10, C01, C20, C30, D1), then 1 per pressure load */
 } efem_model_info;
+
+typedef struct {
+    int iterations;           /* GMRES iterations of the adjoint solve */
+    int flags;                /* EFEM_SOLVE_CONVERGED: relative residual <= adjoint_tolerance */
+    double rel_residual;      /* ||K(u)^T lambda - dJ/du|| / ||dJ/du|| (GMRES estimate) */
+    double ms_total;          /* wall time of the call */
+    double ms_solve;          /* the adjoint solve */
+    double ms_params;         /* the parameter sensitivities */
+} efem_adjoint_info;
 
 /* --------------------------------------------------------------- lifetime */
 
@@ -192,6 +205,35 @@ efem_status efem_precond_apply_noalloc(void* model, double* d_v);
 /* Solve R(u) = 0 from u_inout: replaces Integrator::integral
  * (src/simulation/Integrator.cpp:22-42) -> LBFGSSolver::solve (LBFGS.h:96-174). */
 efem_status efem_solve(void* model, double* u_inout, efem_solve_info* info);
+
+/* --------------------------------------------------------------- sensitivities
+ * None of these has a counterpart in the reference, which only forms the
+ * approximate Jacobian (src/fe/ElementConstraint.cpp:164-205).  They extend
+ * its residual (SoftObjective::residual, src/simulation/Integrator.cpp:49-55)
+ * with derivatives, for gradient-based design and fitting.  Vectors follow
+ * efem_options.device_ptrs like efem_residual. */
+
+/* Kv = K(u) v, the true tangent dR/du at u applied to v (forward-mode
+ * derivative of the residual, exact to rounding). */
+efem_status efem_hvp(void* model, const double* u, const double* v, double* Kv);
+
+/* KTw = K(u)^T w.  The element part of K is symmetric; the pressure part is
+ * transposed face by face. */
+efem_status efem_hvp_transpose(void* model, const double* u, const double* w, double* KTw);
+
+/* dR = dR/dtheta_k at u for parameter k < efem_model_info.n_params: for
+ * material slot s (the model's material table order) k = 5 s + {0 C10,
+ * 1 C01, 2 C20, 3 C30, 4 D1}; then one scale per pressure load in input
+ * order (a follower load's pressure, a directed load's vector scale). */
+efem_status efem_residual_param_derivative(void* model, const double* u, int k, double* dR);
+
+/* Adjoint sensitivities of J(u(theta)) at an equilibrium u (efem_solve's
+ * result): solves K(u)^T lambda = dJ/du by restarted GMRES preconditioned
+ * with the approximate-Jacobian factor, then dJdtheta[k] = -lambda .
+ * dR/dtheta_k for every parameter (n_params values, host memory).  lambda
+ * (may be NULL) receives the adjoint vector. */
+efem_status efem_adjoint(void* model, const double* u, const double* dJdu, double* dJdtheta, double* lambda,
+    efem_adjoint_info* info);
 
 /* Run the model's device work on the caller's CUDA stream (a cudaStream_t);
  * NULL gives the model its own stream again.  The reference has no streams;
