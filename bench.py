@@ -17,6 +17,11 @@ the warm-up steps.
 shard); value = iterations of all ranks / max-over-ranks time.
 --impl reference: the reference's own CPU solver (compiled from its sources in
 oracle/_ref), timed on the host cores on bounded samples of the same solve.
+
+--workload finger-adjoint: the adjoint gradient time instead (ms per
+gradient): the pneumatic finger, 50 688 C3D10 Yeoh elements with 30 kPa on
+its 8 chamber walls, J = u_z of the tip node, dJ/dtheta for every material
+constant and the pressure, at the converged equilibrium.
 """
 from __future__ import annotations
 
@@ -149,6 +154,72 @@ def run_reference_arm(args):
     print(json.dumps(line))
 
 
+# --------------------------------------------------------------------------- adjoint gradient
+def run_adjoint_bench(args):
+    """Adjoint gradient time on the pneumatic finger (one GPU)."""
+    import torch
+    from efem_b200 import api, meshgen as mg
+    torch.cuda.set_device(0)
+    case, tip = mg.finger_c3d10()
+    opts = api.default_options()
+    t_setup = time.time()
+    model = api.Model.from_case(case, opts)
+    stream = torch.cuda.current_stream()
+    api.check(api.lib().efem_set_stream(model.h, api.ctypes.c_void_p(stream.cuda_stream)))
+    model.set_options(device_ptrs=1)
+    u = torch.zeros(model.n_dof, dtype=torch.float64, device="cuda")
+    _, sinfo = model.solve(u)
+    setup_s = time.time() - t_setup
+    dnode = int(np.nonzero(model.dof_map() == tip)[0][0])
+    g = torch.zeros(model.n_dof, dtype=torch.float64, device="cuda")
+    g[3 * dnode + 2] = 1.0
+    for _ in range(args.warmup):
+        model.adjoint(u, g)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    infos = []
+    with ClockSampler(0) as clocks:
+        for a, b in ev:
+            a.record(stream)
+            grad, _, info = model.adjoint(u, g)
+            b.record(stream)
+            infos.append(info)
+        torch.cuda.synchronize()
+    ms = [a.elapsed_time(b) for a, b in ev]
+    # end to end with host buffers: u and dJ/du copied in, dJ/dtheta out
+    model.set_options(device_ptrs=0)
+    u_h = torch.empty(model.n_dof, dtype=torch.float64).pin_memory()
+    u_h.copy_(u.cpu())
+    g_h = torch.zeros(model.n_dof, dtype=torch.float64).pin_memory()
+    g_h[3 * dnode + 2] = 1.0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    model.adjoint(u_h.numpy(), g_h.numpy())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    info = model.info()
+    line = {"metric": "adjoint gradient time (dJ/dtheta, C3D10 Yeoh finger 50688 el)", "value": float(np.mean(ms)),
+            "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(ms)),
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded structured mesh in the reference's input format)",
+            "config": {"workload": "pneumatic finger 80x15x15 mm, 8 chambers, 50688 C3D10 (Yeoh), 30 kPa on the "
+                                   "chamber walls, J = u_z of the tip node, gradient w.r.t. all material constants "
+                                   "and the pressure at the converged equilibrium", "dof": model.n_dof,
+                       "elements": info["n_elements"], "parameters": info["n_params"],
+                       "adjoint_tolerance": model.options.adjoint_tolerance},
+            "gmres_iterations": float(np.mean([i["iterations"] for i in infos])),
+            "adjoint_solve_ms": float(np.mean([i["ms_solve"] for i in infos])),
+            "parameter_sensitivities_ms": float(np.mean([i["ms_params"] for i in infos])),
+            "equilibrium_solve": {"niter": sinfo["niter"], "ms": sinfo["ms_total"], "r_inf": sinfo["r_inf"]},
+            "setup_s": setup_s,
+            "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 2 * 8 * model.n_dof,
+                    "d2h_bytes_per_step": 8 * info["n_params"]},
+            "clocks": clocks.summary()}
+    print(json.dumps(line))
+    model.close()
+
+
 # --------------------------------------------------------------------------- GPU arm
 def main():
     ap = argparse.ArgumentParser()
@@ -160,9 +231,15 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--host-loop", action="store_true",
                     help="drive the L-BFGS iterations from the host (same kernels; for launch-list profiling)")
+    ap.add_argument("--workload", default="beam", choices=["beam", "finger-adjoint"])
     args = ap.parse_args()
     if args.impl == "reference":
+        if args.workload != "beam":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no adjoint or tangent"}))
+            return
         return run_reference_arm(args)
+    if args.workload == "finger-adjoint":
+        return run_adjoint_bench(args)
 
     import torch
     import torch.distributed as dist
@@ -231,7 +308,7 @@ def main():
 
     # ---- end to end through the C ABI with host buffers (pinned host input / output)
     model.set_options(device_ptrs=0)
-    u_host = np.zeros(model.n_dof)
+    u_host = torch.zeros(model.n_dof, dtype=torch.float64).pin_memory().numpy()
     e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(max(1, args.steps // 2))]
     e2e_iters = 0
     barrier()

@@ -307,6 +307,42 @@ __global__ void __launch_bounds__(kVec) k_axpys(double* __restrict__ y, const do
     }
 }
 
+// one warp per row k < nk: s_k = sum of part[k][0..nb) in order; hacc[k] = s_k
+// (accumulate: hacc[k] += s_k) and coef[k] = -s_k
+__global__ void k_rows_reduce(const double* __restrict__ part, int nk, int nb, double* __restrict__ hacc,
+    double* __restrict__ coef, int accumulate)
+{
+    const int k = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (k >= nk) return;
+    double s = 0.0;
+    for (int b = lane; b < nb; b += 32) s += part[static_cast<size_t>(k) * nb + b];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) {
+        hacc[k] = accumulate ? hacc[k] + s : s;
+        coef[k] = -s;
+    }
+}
+
+// *out = sqrt(sum of part[0..nb))
+__global__ void k_norm_reduce(const double* __restrict__ part, int nb, double* __restrict__ out)
+{
+    double s = 0.0;
+    for (int b = threadIdx.x; b < nb; b += 32) s += part[b];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) *out = ::sqrt(s);
+}
+
+// y = x / *s (0 when *s is 0)
+__global__ void __launch_bounds__(kVec) k_scale_inv(double* __restrict__ y, const double* __restrict__ x,
+    const double* __restrict__ s, size_t n)
+{
+    const double d = *s;
+    const double f = d > 0.0 ? 1.0 / d : 0.0;
+    for (size_t i = blockIdx.x * (size_t)kVec + threadIdx.x; i < n; i += (size_t)gridDim.x * kVec) y[i] = f * x[i];
+}
+
 __global__ void __launch_bounds__(kVec) k_scale_copy(double* __restrict__ y, const double* __restrict__ x, double s, size_t n)
 {
     for (size_t i = blockIdx.x * (size_t)kVec + threadIdx.x; i < n; i += (size_t)gridDim.x * kVec) y[i] = s * x[i];
@@ -322,6 +358,8 @@ struct AdjointWS {
     double *V = nullptr, *Z = nullptr;  // Krylov basis and preconditioned basis, (restart + 1) x n
     double *w = nullptr, *x = nullptr, *b = nullptr, *t = nullptr, *u = nullptr, *io = nullptr;
     double *part = nullptr, *coef = nullptr;
+    double* hcol = nullptr;    // device: the Hessenberg column being formed
+    double* h_hcol = nullptr;  // pinned host copy
     MatParams<Dual>* mats = nullptr;
     double* dscale = nullptr;
     std::vector<double> h_part;
@@ -331,15 +369,17 @@ void free_adjoint(Model& m)
 {
     if (!m.aws) return;
     AdjointWS& w = *m.aws;
-    for (double** p : { &w.V, &w.Z, &w.w, &w.x, &w.b, &w.t, &w.u, &w.io, &w.part, &w.coef, &w.dscale }) dev_free(*p);
+    for (double** p : { &w.V, &w.Z, &w.w, &w.x, &w.b, &w.t, &w.u, &w.io, &w.part, &w.coef, &w.dscale, &w.hcol })
+        dev_free(*p);
     if (w.mats) cudaFree(w.mats);
+    if (w.h_hcol) cudaFreeHost(w.h_hcol);
     delete m.aws;
     m.aws = nullptr;
 }
 
 namespace {
 
-constexpr int kRestart = 40;
+constexpr int kRestart = 100;
 
 efem_status alloc_aws(Model& m)
 {
@@ -358,6 +398,8 @@ efem_status alloc_aws(Model& m)
         if ((s = dev_alloc(p, std::max<size_t>(n, 1))) != EFEM_OK) return s;
     if ((s = dev_alloc(&w.part, static_cast<size_t>(kRestart + 1) * kDotBlocks)) != EFEM_OK) return s;
     if ((s = dev_alloc(&w.coef, static_cast<size_t>(kRestart + 1))) != EFEM_OK) return s;
+    if ((s = dev_alloc(&w.hcol, static_cast<size_t>(kRestart + 2))) != EFEM_OK) return s;
+    EFEM_CUDA(cudaMallocHost(&w.h_hcol, sizeof(double) * (kRestart + 2)));
     if ((s = dev_alloc(&w.dscale, static_cast<size_t>(std::max(m.n_pressure_loads, 1)))) != EFEM_OK) return s;
     EFEM_CUDA(cudaMalloc(&w.mats, sizeof(MatParams<Dual>) * MAX_MATS));
     w.h_part.resize(static_cast<size_t>(kRestart + 1) * kDotBlocks);
@@ -513,7 +555,7 @@ efem_status adjoint_gmres(Model& m, const double* u, double tol, int max_it, int
     *iters = 0;
     *relres = 0.0;
     if (bnorm == 0.0) return EFEM_OK;
-    std::vector<double> H(static_cast<size_t>(R + 1) * R), cs(R), sn(R), g(R + 1), h(R + 1), h2(R + 1), y(R);
+    std::vector<double> H(static_cast<size_t>(R + 1) * R), cs(R), sn(R), g(R + 1), y(R);
     double beta = bnorm;  // residual of x = 0
     EFEM_CUDA(cudaMemcpyAsync(w.t, w.b, sizeof(double) * n, cudaMemcpyDeviceToDevice, m.stream));
     int total = 0;
@@ -528,27 +570,24 @@ efem_status adjoint_gmres(Model& m, const double* u, double tol, int max_it, int
         for (; j < R && total < max_it; j++, total++) {
             double* Zj = w.Z + j * n;
             EFEM_CUDA(cudaMemcpyAsync(Zj, w.V + j * n, sizeof(double) * n, cudaMemcpyDeviceToDevice, m.stream));
-            if ((s = precond_apply(m, Zj)) != EFEM_OK) return s;
+            if ((s = precond_enqueue(m, Zj, m.stream)) != EFEM_OK) return s;
+            m.launches++;
             if ((s = tangent(m, u, Zj, w.w, true)) != EFEM_OK) return s;
-            // two passes of classical Gram-Schmidt
-            if ((s = dots(m, w.V, j + 1, w.w, h.data())) != EFEM_OK) return s;
-            for (int i = 0; i <= j; i++) h2[i] = -h[i];
-            if ((s = axpys(m, w.w, w.V, j + 1, h2.data())) != EFEM_OK) return s;
-            if ((s = dots(m, w.V, j + 1, w.w, h2.data())) != EFEM_OK) return s;
-            for (int i = 0; i <= j; i++) {
-                h[i] += h2[i];
-                h2[i] = -h2[i];
+            // two passes of classical Gram-Schmidt, coefficients kept on the device
+            for (int pass = 0; pass < 2; pass++) {
+                k_dots<<<dim3(kDotBlocks, j + 1), kVec, 0, m.stream>>>(w.V, n, j + 1, w.w, n, w.part);
+                k_rows_reduce<<<(j + 1 + 7) / 8, 256, 0, m.stream>>>(w.part, j + 1, kDotBlocks, w.hcol, w.coef, pass);
+                k_axpys<<<vec_grid(n), kVec, 0, m.stream>>>(w.w, w.V, n, j + 1, w.coef, n);
+                m.launches += 3;
             }
-            if ((s = axpys(m, w.w, w.V, j + 1, h2.data())) != EFEM_OK) return s;
-            double hn = 0.0;
-            if ((s = dots(m, w.w, 1, w.w, &hn)) != EFEM_OK) return s;
-            hn = std::sqrt(hn);
-            for (int i = 0; i <= j; i++) H[static_cast<size_t>(i) * R + j] = h[i];
-            H[static_cast<size_t>(j + 1) * R + j] = hn;
-            if (hn > 0.0) {
-                k_scale_copy<<<vec_grid(n), kVec, 0, m.stream>>>(w.V + (j + 1) * n, w.w, 1.0 / hn, n);
-                m.launches++;
-            }
+            k_dots<<<dim3(kDotBlocks, 1), kVec, 0, m.stream>>>(w.w, n, 1, w.w, n, w.part);
+            k_norm_reduce<<<1, 32, 0, m.stream>>>(w.part, kDotBlocks, w.hcol + j + 1);
+            k_scale_inv<<<vec_grid(n), kVec, 0, m.stream>>>(w.V + (j + 1) * n, w.w, w.hcol + j + 1, n);
+            m.launches += 3;
+            EFEM_CUDA(cudaMemcpyAsync(w.h_hcol, w.hcol, sizeof(double) * (j + 2), cudaMemcpyDeviceToHost, m.stream));
+            EFEM_CUDA(cudaStreamSynchronize(m.stream));
+            for (int i = 0; i <= j + 1; i++) H[static_cast<size_t>(i) * R + j] = w.h_hcol[i];
+            const double hn = w.h_hcol[j + 1];
             // Givens rotations on column j
             for (int i = 0; i < j; i++) {
                 const double a = H[static_cast<size_t>(i) * R + j], c = H[static_cast<size_t>(i + 1) * R + j];
@@ -578,6 +617,7 @@ efem_status adjoint_gmres(Model& m, const double* u, double tol, int max_it, int
             y[i] = t / H[static_cast<size_t>(i) * R + i];
         }
         if ((s = axpys(m, w.x, w.Z, j, y.data())) != EFEM_OK) return s;
+        if ((s = precond_check(m)) != EFEM_OK) return s;
         if (done) break;
         // true residual t = b - K^T x for the restart
         if ((s = tangent(m, u, w.x, w.w, true)) != EFEM_OK) return s;
@@ -650,7 +690,7 @@ efem_status adjoint(Model& m, const double* d_u, const double* d_dJdu, double* d
     if ((s = upload_dual_mats(m, -1, 0)) != EFEM_OK) return s;
     EFEM_CUDA(cudaMemcpyAsync(w.u, d_u, sizeof(double) * n, cudaMemcpyDeviceToDevice, m.stream));
     EFEM_CUDA(cudaMemcpyAsync(w.b, d_dJdu, sizeof(double) * n, cudaMemcpyDeviceToDevice, m.stream));
-    const double tol = m.opts.adjoint_tolerance > 0 ? m.opts.adjoint_tolerance : 1e-10;
+    const double tol = m.opts.adjoint_tolerance > 0 ? m.opts.adjoint_tolerance : 1e-8;
     const int max_it = m.opts.adjoint_max_iterations > 0 ? m.opts.adjoint_max_iterations : 2000;
     int iters = 0;
     double rel = 0.0;

@@ -678,7 +678,7 @@ efem_status efem_default_options(efem_options* o)
     o->deterministic = 0;
     o->device = -1;
     o->host_loop = 0;
-    o->adjoint_tolerance = 1e-10;
+    o->adjoint_tolerance = 1e-8;
     o->adjoint_max_iterations = 2000;
     return EFEM_OK;
 }

@@ -95,7 +95,7 @@ typedef struct {
                                  iteration (same kernels; for profilers that do not see kernels
                                  inside conditional graph nodes); 0: the iteration loop runs on
                                  the device */
-    double adjoint_tolerance; /* relative residual of the adjoint solve (default 1e-10) */
+    double adjoint_tolerance; /* relative residual of the adjoint solve (default 1e-8) */
     int adjoint_max_iterations; /* GMRES iteration limit of the adjoint solve (default 2000) */
 } efem_options;
 

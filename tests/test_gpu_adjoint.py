@@ -109,6 +109,7 @@ def test_adjoint_gradient_matches_finite_differences(etype, mat, load):
     dof = 3 * tip + 2
     g = np.zeros(m.n_dof)
     g[dof] = 1.0
+    m.set_options(adjoint_tolerance=1e-10)
     grad, lam, info = m.adjoint(u, g, want_lambda=True)
     assert info["flags"] & api.SOLVE_CONVERGED, info
     # the adjoint equation holds
