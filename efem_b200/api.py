@@ -33,7 +33,7 @@ EXPORTED = ["efem_default_options", "efem_model_create_from_json", "efem_model_c
             "efem_get_options", "efem_set_options", "efem_get_model_info", "efem_dof_map", "efem_residual",
             "efem_approx_jacobian_csr", "efem_precond_apply", "efem_precond_apply_noalloc", "efem_solve",
             "efem_set_stream", "efem_last_error", "efem_version", "efem_hvp", "efem_hvp_transpose",
-            "efem_residual_param_derivative", "efem_adjoint"]
+            "efem_residual_param_derivative", "efem_adjoint", "efem_strain_energy", "efem_write_vtk"]
 
 
 class EfemError(RuntimeError):
@@ -135,6 +135,8 @@ def lib():
             "efem_hvp_transpose": [vp, vp, vp, vp],
             "efem_residual_param_derivative": [vp, vp, ctypes.c_int, vp],
             "efem_adjoint": [vp, vp, vp, dp, vp, ctypes.POINTER(AdjointInfo)],
+            "efem_strain_energy": [vp, vp, dp],
+            "efem_write_vtk": [vp, vp, ctypes.c_char_p],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -350,6 +352,18 @@ class Model:
         out = self._out_like(u)
         check(lib().efem_residual_param_derivative(self.h, _vec_ptr(u), int(k), _vec_ptr(out)))
         return out
+
+    def write_vtk(self, path, u=None):
+        """Legacy ASCII VTK of the mesh at X + u (u None: reference configuration)."""
+        uu = None if u is None else self._vec(u)
+        check(lib().efem_write_vtk(self.h, _vec_ptr(uu) if uu is not None else None, str(path).encode()))
+
+    def strain_energy(self, u):
+        """Stored strain energy at u, summed in FP64."""
+        u = self._vec(u)
+        e = ctypes.c_double()
+        check(lib().efem_strain_energy(self.h, _vec_ptr(u), ctypes.byref(e)))
+        return e.value
 
     @property
     def n_params(self):

@@ -46,6 +46,7 @@ struct HostLoad {
 struct ModelInput {
     std::vector<double> X;          // (n, 3)
     std::vector<HostBlock> blocks;
+    std::vector<int> cell_ptr, cell_nodes;  // every element in input order (bodies, then file order), for output
     std::vector<HostMaterial> materials;
     std::vector<HostLoad> loads;
     efem_options opts;
@@ -118,6 +119,7 @@ struct Model {
     std::vector<int> dnode_of_node;   // original node -> dnode
     std::vector<double> X;            // original order (n,3)
 
+    std::vector<int> cell_ptr, cell_nodes;     // every input element (output meshes), original node ids
     std::vector<HostMaterial> materials_used;  // index = material slot
     std::vector<double> kappa;                 // elasticity_coeff per slot
 
@@ -211,6 +213,7 @@ efem_status residual_param_derivative(Model& m, const double* d_u, int k, double
 efem_status adjoint(Model& m, const double* d_u, const double* d_dJdu, double* dJdtheta, double* d_lambda,
     efem_adjoint_info* info);
 efem_status adjoint_io(Model& m, double** io);  // an n_dof device buffer for host-pointer calls
+efem_status strain_energy_sum(Model& m, const double* d_u, double* energy);  // energy.cu
 
 // ------------------------------------------------------------------ preconditioner (chol.cu)
 // Build (once) the scalar approximate Jacobian L and its Cholesky factor.

@@ -314,6 +314,13 @@ efem_status read_json_config(const char* path, ModelInput& in)
         body_of_id[bodies[k].id] = static_cast<int>(k);
         in.X.insert(in.X.end(), bodies[k].X.begin(), bodies[k].X.end());
     }
+    // every element in body then file order (the order of the reference's output mesh)
+    in.cell_ptr.assign(1, 0);
+    for (size_t k = 0; k < bodies.size(); k++)
+        for (size_t e = 0; e < bodies[k].elems.size(); e++) {
+            for (int v : bodies[k].elems[e]) in.cell_nodes.push_back(v + offset[k]);
+            in.cell_ptr.push_back(static_cast<int>(in.cell_nodes.size()));
+        }
     // element blocks by node count, in body then file order
     for (int nen : { 4, 8, 10, 20 }) {
         HostBlock hb;

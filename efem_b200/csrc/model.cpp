@@ -9,6 +9,7 @@
 // device buffers are created on the first call that computes.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -158,6 +159,16 @@ efem_status build_model(ModelInput& in, Model& m)
     m.device = -1;
     m.n_nodes = static_cast<int>(in.X.size() / 3);
     m.X = in.X;
+    if (in.cell_ptr.empty()) {  // array input: the blocks in the order given
+        in.cell_ptr.assign(1, 0);
+        for (auto& hb : in.blocks)
+            for (size_t e = 0; e < hb.mat_id.size(); e++) {
+                in.cell_nodes.insert(in.cell_nodes.end(), hb.conn.begin() + e * hb.nen, hb.conn.begin() + (e + 1) * hb.nen);
+                in.cell_ptr.push_back(static_cast<int>(in.cell_nodes.size()));
+            }
+    }
+    m.cell_ptr = in.cell_ptr;
+    m.cell_nodes = in.cell_nodes;
     if (m.n_nodes <= 0) {
         set_error("model has no nodes");
         return EFEM_ERR_MESH;
@@ -948,6 +959,72 @@ efem_status efem_adjoint(void* model, const double* u, const double* dJdu, doubl
         EFEM_CUDA(cudaMemcpyAsync(lambda, dl, sizeof(double) * 3 * m->n_free, cudaMemcpyDeviceToHost, m->stream));
     EFEM_CUDA(cudaStreamSynchronize(m->stream));
     return EFEM_OK;
+}
+
+efem_status efem_write_vtk(void* model, const double* u, const char* path)
+{
+    Model* m;
+    efem_status s = guard(model, &m);
+    if (s != EFEM_OK) return s;
+    if (!path) return EFEM_ERR_ARG;
+    std::vector<double> uh;
+    if (u) {
+        uh.resize(3 * static_cast<size_t>(m->n_free));
+        if (m->opts.device_ptrs) {
+            if ((s = efem::ensure_device(*m)) != EFEM_OK) return s;
+            EFEM_CUDA(cudaMemcpyAsync(uh.data(), u, sizeof(double) * uh.size(), cudaMemcpyDeviceToHost, m->stream));
+            EFEM_CUDA(cudaStreamSynchronize(m->stream));
+        } else {
+            std::copy(u, u + uh.size(), uh.begin());
+        }
+    }
+    std::FILE* f = std::fopen(path, "w");
+    if (!f) {
+        efem::set_error(std::string("cannot write ") + path);
+        return EFEM_ERR_ARG;
+    }
+    // legacy ASCII unstructured grid, the content of Model::saveVTK (src/model/Model.cpp:50-117):
+    // node positions X + dx (fixed nodes stay at X), every element with its VTK cell type
+    std::fprintf(f, "# vtk DataFile Version 3.0\nvtk output\nASCII\nDATASET UNSTRUCTURED_GRID\nPOINTS %d double\n",
+        m->n_nodes);
+    for (int n = 0; n < m->n_nodes; n++) {
+        double p[3] = { m->X[3 * n], m->X[3 * n + 1], m->X[3 * n + 2] };
+        const int d = m->dnode_of_node[n];
+        if (u && d < m->n_free)
+            for (int c = 0; c < 3; c++) p[c] += uh[3 * static_cast<size_t>(d) + c];
+        std::fprintf(f, "%.17g %.17g %.17g\n", p[0], p[1], p[2]);
+    }
+    const int nc = static_cast<int>(m->cell_ptr.size()) - 1;
+    std::fprintf(f, "CELLS %d %d\n", nc, nc + static_cast<int>(m->cell_nodes.size()));
+    for (int e = 0; e < nc; e++) {
+        std::fprintf(f, "%d", m->cell_ptr[e + 1] - m->cell_ptr[e]);
+        for (int k = m->cell_ptr[e]; k < m->cell_ptr[e + 1]; k++) std::fprintf(f, " %d", m->cell_nodes[k]);
+        std::fprintf(f, "\n");
+    }
+    std::fprintf(f, "CELL_TYPES %d\n", nc);
+    for (int e = 0; e < nc; e++) {
+        const int nen = m->cell_ptr[e + 1] - m->cell_ptr[e];
+        // VTK_TETRA, VTK_QUADRATIC_TETRA, VTK_HEXAHEDRON, VTK_QUADRATIC_HEXAHEDRON
+        std::fprintf(f, "%d\n", nen == 4 ? 10 : nen == 10 ? 24 : nen == 8 ? 12 : 25);
+    }
+    const bool ok = std::fclose(f) == 0;
+    if (!ok) {
+        efem::set_error(std::string("cannot write ") + path);
+        return EFEM_ERR_ARG;
+    }
+    return EFEM_OK;
+}
+
+efem_status efem_strain_energy(void* model, const double* u, double* energy)
+{
+    Model* m;
+    efem_status s = guard(model, &m);
+    if (s != EFEM_OK) return s;
+    if (!u || !energy) return EFEM_ERR_ARG;
+    if ((s = efem::ensure_device(*m)) != EFEM_OK) return s;
+    double* du;
+    if ((s = vec_in(*m, u, &du, m->d_u)) != EFEM_OK) return s;
+    return efem::strain_energy_sum(*m, du, energy);
 }
 
 efem_status efem_approx_jacobian_csr(void* model, long long* nnz, int* rowptr, int* colidx, double* vals)

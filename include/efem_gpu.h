@@ -235,6 +235,18 @@ efem_status efem_residual_param_derivative(void* model, const double* u, int k, 
 efem_status efem_adjoint(void* model, const double* u, const double* dJdu, double* dJdtheta, double* lambda,
     efem_adjoint_info* info);
 
+/* Write the mesh as a legacy ASCII VTK unstructured grid: every node at X + u
+ * (u NULL: the reference configuration; fixed nodes stay at X) and every
+ * element with its VTK cell type -- the content of Model::saveVTK
+ * (src/model/Model.cpp:50-117), written without VTK.  u follows
+ * efem_options.device_ptrs. */
+efem_status efem_write_vtk(void* model, const double* u, const char* path);
+
+/* Stored strain energy E(u) = sum_e V_e sum_g w_g W(F_g), summed in FP64 in a
+ * fixed order; dE/du is the element part of R (the laws' energy functions
+ * whose derivative is the reference's P(F)).  No reference counterpart. */
+efem_status efem_strain_energy(void* model, const double* u, double* energy);
+
 /* Run the model's device work on the caller's CUDA stream (a cudaStream_t);
  * NULL gives the model its own stream again.  The reference has no streams;
  * this lets a caller order the library's kernels with its own work. */
