@@ -33,7 +33,8 @@ EXPORTED = ["efem_default_options", "efem_model_create_from_json", "efem_model_c
             "efem_get_options", "efem_set_options", "efem_get_model_info", "efem_dof_map", "efem_residual",
             "efem_approx_jacobian_csr", "efem_precond_apply", "efem_precond_apply_noalloc", "efem_solve",
             "efem_set_stream", "efem_last_error", "efem_version", "efem_hvp", "efem_hvp_transpose",
-            "efem_residual_param_derivative", "efem_adjoint", "efem_strain_energy", "efem_write_vtk"]
+            "efem_residual_param_derivative", "efem_adjoint", "efem_strain_energy", "efem_write_vtk",
+            "efem_batch_solve"]
 
 
 class EfemError(RuntimeError):
@@ -137,6 +138,8 @@ def lib():
             "efem_adjoint": [vp, vp, vp, dp, vp, ctypes.POINTER(AdjointInfo)],
             "efem_strain_energy": [vp, vp, dp],
             "efem_write_vtk": [vp, vp, ctypes.c_char_p],
+            "efem_batch_solve": [ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(vp), ctypes.POINTER(SolveInfo),
+                                 ctypes.c_int],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -401,6 +404,20 @@ class Model:
         """Run on the caller's CUDA stream (an integer cudaStream_t, e.g.
         torch.cuda.current_stream().cuda_stream); None for the model's own."""
         check(lib().efem_set_stream(self.h, ctypes.c_void_p(cuda_stream_handle)))
+
+
+def batch_solve(models, us=None, max_threads=0):
+    """Solve independent models concurrently (efem_batch_solve).  us: initial
+    solutions (zeros by default), numpy arrays or CUDA tensors per each
+    model's device_ptrs option; solved in place.  Returns (us, info dicts)."""
+    n = len(models)
+    if us is None:
+        us = [np.zeros(m.n_dof) for m in models]
+    hs = (ctypes.c_void_p * n)(*[m.h.value for m in models])
+    ptrs = (ctypes.c_void_p * n)(*[_vec_ptr(u).value for u in us])
+    infos = (SolveInfo * n)()
+    check(lib().efem_batch_solve(hs, n, ptrs, infos, int(max_threads)))
+    return us, [infos[i].as_dict() for i in range(n)]
 
 
 class Simulator:

@@ -1295,6 +1295,7 @@ static efem_status apply_with(Model& m, double* d_v, const SolveBufs& b)
         }
         cudaGraph_t g = nullptr;
         cudaGraphExec_t ge = nullptr;
+        std::lock_guard<std::mutex> lock(capture_mutex());
         EFEM_CUDA(cudaStreamBeginCapture(P.capture, cudaStreamCaptureModeThreadLocal));
         enqueue_solve(P, args_of(P), b, d_v, P.capture);
         EFEM_CUDA(cudaStreamEndCapture(P.capture, &g));

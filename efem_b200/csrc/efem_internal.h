@@ -16,6 +16,7 @@
 
 #include <cstdint>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -203,6 +204,10 @@ efem_status launch_residual_on(Model& m, const double* d_u, double* d_r, cudaStr
 // ------------------------------------------------------------------ solver (solver.cu)
 efem_status run_solve(Model& m, double* d_u, efem_solve_info* info);
 void free_solver(Model& m);
+// Held while a CUDA graph is captured and instantiated, so that solves of
+// different models running in parallel host threads never overlap a capture
+// with an allocation or free (which may synchronise the device).
+std::mutex& capture_mutex();
 void free_adjoint(Model& m);
 
 // ------------------------------------------------------------------ sensitivities (adjoint.cu)

@@ -8,6 +8,7 @@
 // forces (:91-167) and pressure faces (:184-827).  Host set-up needs no GPU;
 // device buffers are created on the first call that computes.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -108,6 +109,11 @@ bool face_has_elem_node(const void* c, int i)
 }  // namespace
 
 void set_error(const std::string& msg) { g_error = msg; }
+std::mutex& capture_mutex()
+{
+    static std::mutex mu;
+    return mu;
+}
 const std::string& get_error() { return g_error; }
 
 Model::~Model()
@@ -1096,6 +1102,39 @@ efem_status efem_solve(void* model, double* u_inout, efem_solve_info* info)
         EFEM_CUDA(cudaStreamSynchronize(m->stream));
     }
     return s;
+}
+
+efem_status efem_batch_solve(void** models, int n, double* const* u, efem_solve_info* infos, int max_threads)
+{
+    if (n < 0 || (n > 0 && (!models || !u))) {
+        efem::set_error("null models or solution arrays");
+        return EFEM_ERR_ARG;
+    }
+    if (n == 0) return EFEM_OK;
+    int nt = max_threads > 0 ? max_threads : static_cast<int>(std::thread::hardware_concurrency());
+    nt = std::max(1, std::min(nt, n));
+    std::atomic<int> next(0);
+    std::vector<efem_status> st(n, EFEM_OK);
+    std::vector<std::string> err(n);
+    auto worker = [&]() {
+        for (;;) {
+            const int i = next.fetch_add(1);
+            if (i >= n) return;
+            efem_solve_info local;
+            st[i] = efem_solve(models[i], u[i], infos ? &infos[i] : &local);
+            if (st[i] != EFEM_OK) err[i] = efem::get_error();
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; t++) pool.emplace_back(worker);
+    worker();
+    for (auto& t : pool) t.join();
+    for (int i = 0; i < n; i++)
+        if (st[i] != EFEM_OK) {
+            efem::set_error("model " + std::to_string(i) + ": " + err[i]);
+            return st[i];
+        }
+    return EFEM_OK;
 }
 
 efem_status efem_set_stream(void* model, void* cuda_stream)

@@ -9,7 +9,7 @@
 //
 // Element kernel: one CTA processes EPB elements in three phases.
 //   1. stage: threads (element, node) load conn (SoA, coalesced over elements)
-//      and gather u into shared memory;
+//      and gather u, relative to the element's first node, into shared memory;
 //   2. Gauss point: thread (element, gp) forms H = (u . dN) J0^{-1}, P(I+H) and
 //      S_g = V_e w_g P J0^{-T} (3x3) into shared memory;
 //   3. node: thread (element, node) reduces r_a = sum_g S_g dN_ga and adds it
@@ -56,18 +56,30 @@ __global__ void __launch_bounds__(kBlock) k_elem_residual(ElemArgs<T> a)
     for (int i = tid; i < NGP * NEN * 3; i += kBlock) (&s_dN[0][0][0])[i] = a.dN[i];
     const int e0 = blockIdx.x * EPB;
 
-    // phase 1: stage node displacements
+    // phase 1: stage node displacements relative to the element's first node,
+    // formed in FP64 (H only sees differences, since sum_a dN_a = 0, and FP32
+    // would lose the differences of nearly equal displacements)
     for (int i = tid; i < EPB * NEN; i += kBlock) {
         const int el = i % EPB, nd = i / EPB, e = e0 + el;
         int node = a.n_free;  // out-of-range marker
         T v0 = 0, v1 = 0, v2 = 0;
         if (e < a.n) {
             node = __ldg(a.conn + static_cast<size_t>(nd) * a.n + e);
+            const int n0 = __ldg(a.conn + e);
+            double w0 = 0.0, w1 = 0.0, w2 = 0.0, z0 = 0.0, z1 = 0.0, z2 = 0.0;
             if (node < a.n_free) {
-                v0 = static_cast<T>(__ldg(a.u + 3 * node));
-                v1 = static_cast<T>(__ldg(a.u + 3 * node + 1));
-                v2 = static_cast<T>(__ldg(a.u + 3 * node + 2));
+                w0 = __ldg(a.u + 3 * node);
+                w1 = __ldg(a.u + 3 * node + 1);
+                w2 = __ldg(a.u + 3 * node + 2);
             }
+            if (n0 < a.n_free) {
+                z0 = __ldg(a.u + 3 * n0);
+                z1 = __ldg(a.u + 3 * n0 + 1);
+                z2 = __ldg(a.u + 3 * n0 + 2);
+            }
+            v0 = static_cast<T>(w0 - z0);
+            v1 = static_cast<T>(w1 - z1);
+            v2 = static_cast<T>(w2 - z2);
         }
         s_node[el][nd] = node;
         s_u[el][nd][0] = v0;
@@ -162,13 +174,19 @@ __global__ void __launch_bounds__(kBlock) k_face_residual(FaceArgs<T> a)
     const int ngp = a.t_ngp[t];
     int node[NEN];
     T uu[NEN][3];
+    double u0[3] = { 0.0, 0.0, 0.0 };  // displacements relative to the parent's first node, as in the element kernel
+    {
+        const int n0 = a.conn[f];
+        if (n0 < a.n_free)
+            for (int c = 0; c < 3; c++) u0[c] = a.u[3 * n0 + c];
+    }
 #pragma unroll
     for (int q = 0; q < NEN; q++) {
         node[q] = a.conn[static_cast<size_t>(q) * a.n + f];
         const bool fr = node[q] < a.n_free;
-        uu[q][0] = fr ? static_cast<T>(a.u[3 * node[q]]) : T(0);
-        uu[q][1] = fr ? static_cast<T>(a.u[3 * node[q] + 1]) : T(0);
-        uu[q][2] = fr ? static_cast<T>(a.u[3 * node[q] + 2]) : T(0);
+        uu[q][0] = static_cast<T>((fr ? a.u[3 * node[q]] : 0.0) - u0[0]);
+        uu[q][1] = static_cast<T>((fr ? a.u[3 * node[q] + 1] : 0.0) - u0[1]);
+        uu[q][2] = static_cast<T>((fr ? a.u[3 * node[q] + 2] : 0.0) - u0[2]);
     }
     const T A0[3] = { static_cast<T>(a.A0[3 * f]), static_cast<T>(a.A0[3 * f + 1]), static_cast<T>(a.A0[3 * f + 2]) };
     const bool directed = a.load[4 * f] != 0.0;

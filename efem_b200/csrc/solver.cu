@@ -730,6 +730,7 @@ efem_status add_while(cudaStream_t st, cudaGraphConditionalHandle h, cudaGraph_t
 // (pass 4 sets hLs to 1 on every iteration: the first trial always runs)
 efem_status capture_loop(Model& m, SolverWS& w, double* x, bool use_factor, cudaGraphExec_t* out)
 {
+    std::lock_guard<std::mutex> lock(capture_mutex());
     const long long launches = m.launches;  // capture launches nothing; replays are counted
     cudaStream_t s0 = w.capture[0], s1 = w.capture[1], s2 = w.capture[2];
     cudaGraph_t g = nullptr;
@@ -788,6 +789,7 @@ efem_status capture_loop(Model& m, SolverWS& w, double* x, bool use_factor, cuda
 // accept / scale rule and the convergence tests.
 efem_status capture_step(Model& m, SolverWS& w, double* x, bool use_factor, cudaGraphExec_t* out)
 {
+    std::lock_guard<std::mutex> lock(capture_mutex());
     const long long launches = m.launches;
     cudaStream_t s0 = w.capture[0];
     cudaGraph_t g = nullptr;
@@ -809,6 +811,7 @@ efem_status capture_step(Model& m, SolverWS& w, double* x, bool use_factor, cuda
 
 efem_status capture_first(Model& m, SolverWS& w, double* x, cudaGraphExec_t* out)
 {
+    std::lock_guard<std::mutex> lock(capture_mutex());
     const long long launches = m.launches;
     cudaGraph_t g = nullptr;
     EFEM_CUDA(cudaStreamBeginCapture(w.capture[0], cudaStreamCaptureModeThreadLocal));

@@ -271,6 +271,52 @@ def cantilever_c3d8_force(L=0.2, W=0.04, H=0.04, nx=80, ny=16, nz=16, f=(0.0, 0.
     return Case(m, [mat_mr()], fix, force=[(list(f), tip)])
 
 
+def batch_beams(n=256, seed=20261203, el_min=500, el_max=40000) -> list:
+    """Uneven batch of C3D4 cantilevers: length L ~ U[0.05, 0.20] m, square
+    section side a ~ U[0.010, 0.030] m, element size h ~ U[0.002, 0.005] m
+    adjusted so that the element count (6 tets per grid hex) stays within
+    [el_min, el_max]; Neo-Hookean or Mooney-Rivlin with probability 1/2,
+    C10 log-uniform in [5e4, 5e5] Pa, C01 = U[0, 0.3] C10 (Mooney-Rivlin
+    only), D1 = 1e-6; x = 0 fixed; end-face follower pressure ~ U[1, 20] kPa,
+    capped at half the beam's Euler buckling load (clamped-free,
+    P_cr = pi^2 E I / (4 L^2) with E = 6 (C10 + C01)): the follower pressure
+    on the end face compresses the beam, and a slender soft beam above P_cr
+    has no stable straight equilibrium for any solver to converge to.
+    Returns a list of Cases."""
+    rng = np.random.default_rng(seed)
+    cases = []
+    for _ in range(n):
+        L = rng.uniform(0.05, 0.20)
+        a = rng.uniform(0.010, 0.030)
+        h = rng.uniform(0.002, 0.005)
+        mr = rng.uniform() < 0.5
+        c10 = float(np.exp(rng.uniform(np.log(5e4), np.log(5e5))))
+        c01 = float(rng.uniform(0.0, 0.3) * c10)
+        p = float(rng.uniform(1e3, 2e4))
+        E = 6.0 * (c10 + (c01 if mr else 0.0))
+        p_cr = np.pi ** 2 * E * (a ** 4 / 12.0) / (4.0 * L * L) / (a * a)
+        p = min(p, 0.5 * p_cr)
+
+        def counts(hh):
+            nx, na = max(1, int(round(L / hh))), max(1, int(round(a / hh)))
+            return nx, na, 6 * nx * na * na
+
+        nx, na, ne = counts(h)
+        while ne > el_max:
+            h *= 1.05
+            nx, na, ne = counts(h)
+        while ne < el_min:
+            h /= 1.05
+            nx, na, ne = counts(h)
+        m = hex8_to_tet4(box_hex8(L, a, a, nx, na, na))
+        tol = 1e-9 * L
+        fix = nodes_where(m, lambda X: np.abs(X[:, 0]) < tol)
+        faces = boundary_faces(m, lambda P: bool(np.all(np.abs(P[:, 0] - L) < tol)))
+        mat = mat_mr(C10=c10, C01=c01) if mr else mat_nh(C10=c10)
+        cases.append(Case(m, [mat], fix, pressure=[(p, faces)]))
+    return cases
+
+
 def small_case(etype: str, material: str, load: str, n=(3, 2, 2), size=(0.03, 0.01, 0.01),
                integration="full", seed=0) -> Case:
     """Small parity case: a cantilever block of any element type x material x load."""

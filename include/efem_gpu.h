@@ -247,6 +247,16 @@ efem_status efem_write_vtk(void* model, const double* u, const char* path);
  * whose derivative is the reference's P(F)).  No reference counterpart. */
 efem_status efem_strain_energy(void* model, const double* u, double* energy);
 
+/* Solve n independent models (load cases, material samples, meshes of any
+ * size) concurrently: each model's solve runs on its own CUDA stream from a
+ * pool of max_threads host threads (<= 0: one per hardware thread), so the
+ * models' device-driven iteration graphs overlap on the GPU.  u[i] is model
+ * i's u_inout (host or device per that model's device_ptrs); infos may be
+ * NULL or hold n entries.  Returns the first failing model's status, with
+ * its index in the error message.  The reference solves one problem per
+ * process (Simulator::start, src/simulation/Simulator.cpp:20-41). */
+efem_status efem_batch_solve(void** models, int n, double* const* u, efem_solve_info* infos, int max_threads);
+
 /* Run the model's device work on the caller's CUDA stream (a cudaStream_t);
  * NULL gives the model its own stream again.  The reference has no streams;
  * this lets a caller order the library's kernels with its own work. */
