@@ -65,6 +65,7 @@ constexpr int MAX_MATS = 16;
 
 struct DevBlock {
     int kind = 0, nen = 0, ngp = 0, n = 0;
+    int threads[2] = { 128, 128 };  // element-kernel CTA size per precision (FP64, FP32), from the autotuner
     int* conn = nullptr;          // [nen][n]
     int* mat = nullptr;           // [n]
     double* vol = nullptr;        // [n]
@@ -142,6 +143,7 @@ struct Model {
 
     long long launches = 0;           // kernels launched by this model (diagnostics)
     long long epoch = 0;              // bumped when device arrays that captured graphs point to are rebuilt
+    int tuned_threads = -1;           // opts.elem_threads the element kernels were tuned for (-1: not yet)
     Precond* precond = nullptr;   // owned; freed by free_precond
     SolverWS* ws = nullptr;       // owned; freed by free_solver
     AdjointWS* aws = nullptr;     // owned; freed by free_adjoint
@@ -196,6 +198,7 @@ efem_status ensure_device(Model& m);  // create the stream and upload everything
 // ------------------------------------------------------------------ kernels (residual.cu)
 // r = R(u) on the model's stream; u, r device pointers of length 3*n_free.
 efem_status launch_residual(Model& m, const double* d_u, double* d_r);
+efem_status tune_element_blocks(Model& m);  // autotuner of the element kernels' CTA size
 // the same on `stream`; with `stamp`, the GPU's global timer at the start is
 // stored there; init_r = false when the caller has already set r = -f_ext
 efem_status launch_residual_on(Model& m, const double* d_u, double* d_r, cudaStream_t stream,

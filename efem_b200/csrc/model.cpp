@@ -586,6 +586,12 @@ efem_status ensure_device(Model& m)
     }
 #undef UP
     m.on_device = true;
+    if (m.tuned_threads != m.opts.elem_threads) {
+        // element kernels are tuned before any graph captures them (a retune
+        // invalidates captured graphs through the epoch)
+        if ((s = tune_element_blocks(m)) != EFEM_OK) return s;
+        m.epoch++;
+    }
     return EFEM_OK;
 }
 
@@ -697,6 +703,7 @@ efem_status efem_default_options(efem_options* o)
     o->host_loop = 0;
     o->adjoint_tolerance = 1e-8;
     o->adjoint_max_iterations = 2000;
+    o->elem_threads = 0;
     return EFEM_OK;
 }
 
@@ -865,6 +872,8 @@ efem_status efem_get_model_info(void* model, efem_model_info* info)
     info->residual_bytes = bytes;
     info->residual_flops = flops;
     info->n_params = efem::n_params(*m);
+    info->elem_threads_fp64 = m->blocks.empty() ? 0 : m->blocks[0].threads[0];
+    info->elem_threads_fp32 = m->blocks.empty() ? 0 : m->blocks[0].threads[1];
     efem::precond_info(*m, info);
     return EFEM_OK;
 }

@@ -43,23 +43,29 @@ struct ElemArgs {
     double* __restrict__ r;           // [3*n_free]
 };
 
-template <int NEN, int NGP, typename T>
-__global__ void __launch_bounds__(kBlock) k_elem_residual(ElemArgs<T> a)
+// BLK threads per CTA (64, 128 or 256, picked per element block by the
+// autotuner in tune_element_blocks); EPB = BLK / NGP elements per CTA, at
+// most 128 (shared memory)
+template <int NGP, int BLK>
+constexpr int elems_per_cta() { return (BLK / NGP) < 1 ? 1 : ((BLK / NGP) > 128 ? 128 : BLK / NGP); }
+
+template <int NEN, int NGP, typename T, int BLK>
+__global__ void __launch_bounds__(BLK) k_elem_residual(ElemArgs<T> a)
 {
-    constexpr int EPB = (kBlock / NGP) > 0 ? (kBlock / NGP) : 1;
+    constexpr int EPB = elems_per_cta<NGP, BLK>();
     __shared__ T s_u[EPB][NEN][3];
     __shared__ T s_S[EPB][NGP][9];
     __shared__ T s_dN[NGP][NEN][3];
     __shared__ int s_node[EPB][NEN];
 
     const int tid = threadIdx.x;
-    for (int i = tid; i < NGP * NEN * 3; i += kBlock) (&s_dN[0][0][0])[i] = a.dN[i];
+    for (int i = tid; i < NGP * NEN * 3; i += BLK) (&s_dN[0][0][0])[i] = a.dN[i];
     const int e0 = blockIdx.x * EPB;
 
     // phase 1: stage node displacements relative to the element's first node,
     // formed in FP64 (H only sees differences, since sum_a dN_a = 0, and FP32
     // would lose the differences of nearly equal displacements)
-    for (int i = tid; i < EPB * NEN; i += kBlock) {
+    for (int i = tid; i < EPB * NEN; i += BLK) {
         const int el = i % EPB, nd = i / EPB, e = e0 + el;
         int node = a.n_free;  // out-of-range marker
         T v0 = 0, v1 = 0, v2 = 0;
@@ -127,7 +133,7 @@ __global__ void __launch_bounds__(kBlock) k_elem_residual(ElemArgs<T> a)
     __syncthreads();
 
     // phase 3: one thread per (element, node): r_a = sum_g S_g dN_ga
-    for (int i = tid; i < EPB * NEN; i += kBlock) {
+    for (int i = tid; i < EPB * NEN; i += BLK) {
         const int el = i % EPB, nd = i / EPB, e = e0 + el;
         if (e >= a.n) continue;
         const int node = s_node[el][nd];
@@ -246,24 +252,31 @@ __global__ void __launch_bounds__(kBlock) k_face_residual(FaceArgs<T> a)
     }
 }
 
+template <int NEN, int NGP, typename T, int BLK>
+void launch_elem_blk(const ElemArgs<T>& a, cudaStream_t st)
+{
+    constexpr int EPB = elems_per_cta<NGP, BLK>();
+    k_elem_residual<NEN, NGP, T, BLK><<<(a.n + EPB - 1) / EPB, BLK, 0, st>>>(a);
+}
+
 template <int NEN, int NGP, typename T>
 void launch_elem(const DevBlock& b, const MatParams<T>* mats, const T* vol, const T* J0, const T* dN, const T* gw,
-    int n_free, const double* u, double* r, cudaStream_t st)
+    int n_free, const double* u, double* r, cudaStream_t st, int threads)
 {
-    constexpr int EPB = (kBlock / NGP) > 0 ? (kBlock / NGP) : 1;
     ElemArgs<T> a { b.n, n_free, b.conn, b.mat, vol, J0, dN, gw, mats, u, r };
-    const int grid = (b.n + EPB - 1) / EPB;
-    k_elem_residual<NEN, NGP, T><<<grid, kBlock, 0, st>>>(a);
+    if (threads == 64) launch_elem_blk<NEN, NGP, T, 64>(a, st);
+    else if (threads == 256) launch_elem_blk<NEN, NGP, T, 256>(a, st);
+    else launch_elem_blk<NEN, NGP, T, 128>(a, st);
 }
 
 template <typename T>
 void dispatch_elem(const DevBlock& b, const MatParams<T>* mats, const T* vol, const T* J0, const T* dN, const T* gw,
-    int n_free, const double* u, double* r, cudaStream_t st)
+    int n_free, const double* u, double* r, cudaStream_t st, int threads)
 {
-#define CASE(NEN, NGP)                                                            \
-    if (b.nen == NEN && b.ngp == NGP) {                                           \
-        launch_elem<NEN, NGP, T>(b, mats, vol, J0, dN, gw, n_free, u, r, st);     \
-        return;                                                                   \
+#define CASE(NEN, NGP)                                                                 \
+    if (b.nen == NEN && b.ngp == NGP) {                                                \
+        launch_elem<NEN, NGP, T>(b, mats, vol, J0, dN, gw, n_free, u, r, st, threads); \
+        return;                                                                        \
     }
     CASE(4, 1)
     CASE(10, 4)
@@ -291,6 +304,57 @@ void dispatch_face(const DevFaces& f, const T* J0, const T* tw, const T* tN, con
 
 }  // namespace
 
+// Autotuner of the element kernels' CTA size: for every element block and
+// both precisions, time the 64-, 128- and 256-thread variants (2 warm-up and
+// 5 timed launches each, CUDA events on the model's stream, at u = 0: the
+// kernels' work does not depend on the values) and keep the fastest.
+// opts.elem_threads = 64 / 128 / 256 forces one variant instead.
+efem_status tune_element_blocks(Model& m)
+{
+    const int forced = m.opts.elem_threads;
+    const size_t n = 3 * static_cast<size_t>(std::max(m.n_free, 1));
+    EFEM_CUDA(cudaMemsetAsync(m.d_u, 0, n * sizeof(double), m.stream));
+    cudaEvent_t e0, e1;
+    EFEM_CUDA(cudaEventCreate(&e0));
+    EFEM_CUDA(cudaEventCreate(&e1));
+    for (auto& b : m.blocks) {
+        for (int prec = 0; prec < 2; prec++) {
+            if (forced == 64 || forced == 128 || forced == 256) {
+                b.threads[prec] = forced;
+                continue;
+            }
+            if (b.n == 0) {
+                b.threads[prec] = 128;
+                continue;
+            }
+            float best = 1e30f;
+            for (int t : { 64, 128, 256 }) {
+                for (int rep = 0; rep < 7; rep++) {
+                    if (rep == 2) EFEM_CUDA(cudaEventRecord(e0, m.stream));
+                    if (prec == 1)
+                        dispatch_elem<float>(b, m.d_mats_f, b.vol_f, b.J0inv_f, b.dN_f, b.gw_f, m.n_free, m.d_u, m.d_r,
+                            m.stream, t);
+                    else
+                        dispatch_elem<double>(b, m.d_mats, b.vol, b.J0inv, b.dN, b.gw, m.n_free, m.d_u, m.d_r, m.stream, t);
+                }
+                EFEM_CUDA(cudaEventRecord(e1, m.stream));
+                EFEM_CUDA(cudaEventSynchronize(e1));
+                float ms = 0.f;
+                EFEM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                if (ms < best) {
+                    best = ms;
+                    b.threads[prec] = t;
+                }
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    EFEM_CUDA(cudaGetLastError());
+    m.tuned_threads = forced;
+    return EFEM_OK;
+}
+
 efem_status launch_residual(Model& m, const double* d_u, double* d_r)
 {
     return launch_residual_on(m, d_u, d_r, m.stream);
@@ -312,9 +376,10 @@ efem_status launch_residual_on(Model& m, const double* d_u, double* d_r, cudaStr
         if (b.n == 0) continue;
         m.launches++;
         if (mixed)
-            dispatch_elem<float>(b, m.d_mats_f, b.vol_f, b.J0inv_f, b.dN_f, b.gw_f, m.n_free, d_u, d_r, stream);
+            dispatch_elem<float>(b, m.d_mats_f, b.vol_f, b.J0inv_f, b.dN_f, b.gw_f, m.n_free, d_u, d_r, stream,
+                b.threads[1]);
         else
-            dispatch_elem<double>(b, m.d_mats, b.vol, b.J0inv, b.dN, b.gw, m.n_free, d_u, d_r, stream);
+            dispatch_elem<double>(b, m.d_mats, b.vol, b.J0inv, b.dN, b.gw, m.n_free, d_u, d_r, stream, b.threads[0]);
     }
     for (auto& f : m.faces) {
         if (f.n == 0) continue;

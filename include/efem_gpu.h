@@ -97,6 +97,8 @@ typedef struct {
                                  the device */
     double adjoint_tolerance; /* relative residual of the adjoint solve (default 1e-8) */
     int adjoint_max_iterations; /* GMRES iteration limit of the adjoint solve (default 2000) */
+    int elem_threads;         /* element-kernel CTA size: 0 = chosen per element block by the autotuner
+                                 at set-up (64, 128 or 256 threads, timed); 64 / 128 / 256 = forced */
 } efem_options;
 
 enum {
@@ -133,6 +135,7 @@ typedef struct {
     double residual_flops;                /* algorithmic flops of one residual evaluation */
     int n_params;                         /* sensitivity parameters (efem_adjoint): 5 per material slot
                                              (C10, C01, C20, C30, D1), then 1 per pressure load */
+    int elem_threads_fp64, elem_threads_fp32;  /* the first element block's CTA size (autotuner) */
 } efem_model_info;
 
 typedef struct {

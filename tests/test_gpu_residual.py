@@ -65,3 +65,21 @@ def test_residual_large_mesh_against_oracle():
         o = oracle.Oracle(oracle.read_case(case.write(td)))
         ro = o.residual(u)
     assert np.linalg.norm(r - ro) <= 1e-12 * np.linalg.norm(ro)
+
+
+@pytest.mark.parametrize("path", golden_files()[::7], ids=lambda p: p.split("/")[-1][5:-4])
+def test_element_kernel_variants_agree(path, tmp_path):
+    """The autotuner picks a CTA size per element block; every variant gives
+    the same residual (only the order of the FP64 atomic additions differs)."""
+    cfg, d = write_golden_case(path, tmp_path)
+    m = api.Model.from_json(cfg)
+    u = d["u_solve"]
+    r_auto = m.residual(u)
+    scale = np.linalg.norm(r_auto - m.residual(np.zeros_like(u)))  # |f_int(u)|, the size of what is summed
+    info = m.info()
+    assert info["elem_threads_fp64"] in (64, 128, 256) and info["elem_threads_fp32"] in (64, 128, 256)
+    for t in (64, 128, 256):
+        m.set_options(elem_threads=t)
+        r = m.residual(u)  # the next device call applies the forced size
+        assert m.info()["elem_threads_fp64"] == t
+        assert np.linalg.norm(r - r_auto) <= 1e-13 * scale
