@@ -25,7 +25,10 @@ OK, ERR_ARG, ERR_CONFIG, ERR_MESH, ERR_CUDA, ERR_NAN, ERR_TIMEOUT, ERR_UNSUPPORT
 STATUS_NAMES = {0: "OK", 1: "ERR_ARG", 2: "ERR_CONFIG", 3: "ERR_MESH", 4: "ERR_CUDA", 5: "ERR_NAN",
                 6: "ERR_TIMEOUT", 7: "ERR_UNSUPPORTED", 8: "ERR_NO_DEVICE", 9: "ERR_FACE"}
 NEO_HOOKEAN, MOONEY_RIVLIN, YEOH = 0, 1, 2
-LOAD_FIX, LOAD_FORCE, LOAD_PRESSURE, LOAD_DPRESSURE = 0, 1, 2, 3
+LOAD_FIX, LOAD_FORCE, LOAD_PRESSURE, LOAD_DPRESSURE, LOAD_GRAVITY = 0, 1, 2, 3, 4
+# analysis "gravity" strings (src/io/Config.cpp:45-62) as accelerations
+GRAVITY = {"x": (9.8, 0.0, 0.0), "-x": (-9.8, 0.0, 0.0), "y": (0.0, 9.8, 0.0), "-y": (0.0, -9.8, 0.0),
+           "z": (0.0, 0.0, 9.8), "-z": (0.0, 0.0, -9.8)}
 FP64, MIXED = 0, 1
 SOLVE_CONVERGED, SOLVE_PRECOND_FALLBACK, SOLVE_DX_CONVERGED, SOLVE_MAX_ITERS = 1, 2, 4, 8
 
@@ -34,7 +37,7 @@ EXPORTED = ["efem_default_options", "efem_model_create_from_json", "efem_model_c
             "efem_approx_jacobian_csr", "efem_precond_apply", "efem_precond_apply_noalloc", "efem_solve",
             "efem_set_stream", "efem_last_error", "efem_version", "efem_hvp", "efem_hvp_transpose",
             "efem_residual_param_derivative", "efem_adjoint", "efem_strain_energy", "efem_write_vtk",
-            "efem_batch_solve"]
+            "efem_batch_solve", "efem_external_load"]
 
 
 class EfemError(RuntimeError):
@@ -49,7 +52,8 @@ class Options(ctypes.Structure):
                 ("residual_criterion", ctypes.c_double), ("dx_criterion", ctypes.c_double),
                 ("device_ptrs", ctypes.c_int), ("deterministic", ctypes.c_int), ("device", ctypes.c_int),
                 ("host_loop", ctypes.c_int), ("adjoint_tolerance", ctypes.c_double),
-                ("adjoint_max_iterations", ctypes.c_int), ("elem_threads", ctypes.c_int)]
+                ("adjoint_max_iterations", ctypes.c_int), ("elem_threads", ctypes.c_int),
+                ("consistent_inertia", ctypes.c_int)]
 
 
 class SolveInfo(ctypes.Structure):
@@ -200,7 +204,7 @@ class Model:
         """X (n,3); blocks: list of (conn (ne,nen) 0-based, material ids or None);
         materials: dicts in the reference's JSON form; loads: list of
         ("fix", nodes) / ("force", nodes, [fx,fy,fz]) / ("pressure", faces, p) /
-        ("dpressure", faces, [vx,vy,vz])."""
+        ("dpressure", faces, [vx,vy,vz]) / ("gravity", [gx,gy,gz])."""
         keep = []
         X = np.ascontiguousarray(X, dtype=np.float64)
         keep.append(X)
@@ -236,6 +240,10 @@ class Model:
                 if kind == "force":
                     for c in range(3):
                         lds[i].value[c] = float(ld[2][c])
+            elif kind == "gravity":
+                lds[i].type = LOAD_GRAVITY
+                for c in range(3):
+                    lds[i].value[c] = float(ld[1][c])
             else:
                 faces = ld[1]
                 ptr = np.zeros(len(faces) + 1, dtype=np.int32)
@@ -267,8 +275,13 @@ class Model:
                 loads.append(("dpressure", faces, value))
             else:
                 loads.append(("pressure", faces, value))
+        g = case.analysis.get("gravity")
+        if isinstance(g, str) and g in GRAVITY:
+            loads.append(("gravity", GRAVITY[g]))
         opts = options if options is not None else default_options()
         opts.integration = 1 if case.integration == "reduced" else 0
+        if isinstance(case.analysis.get("consistent_inertia"), bool):
+            opts.consistent_inertia = int(case.analysis["consistent_inertia"])
         return cls.from_arrays(case.mesh.X, [(case.mesh.conn, case.mesh.mat)], case.materials, loads, opts)
 
     def close(self):
@@ -303,6 +316,12 @@ class Model:
     def dof_map(self):
         out = np.zeros(self.n_free, dtype=np.int32)
         check(lib().efem_dof_map(self.h, _ptr(out, ctypes.c_int)))
+        return out
+
+    def external_load(self):
+        """Nodal forces + M g per free DOF (host; no GPU needed)."""
+        out = np.zeros(self.n_dof)
+        check(lib().efem_external_load(self.h, _ptr(out)))
         return out
 
     # ------------------------------------------------------------------ hot path

@@ -135,7 +135,10 @@ struct Model {
 
     MatParams<double>* d_mats = nullptr;
     MatParams<float>* d_mats_f = nullptr;
-    std::vector<double> h_fext;       // [3*n_free]
+    std::vector<double> h_fext;       // [3*n_free]: nodal forces + M g
+    std::vector<double> h_fnodal;     // [3*n_free]: nodal forces alone
+    double gravity[3] = { 0, 0, 0 };  // summed EFEM_LOAD_GRAVITY accelerations
+    bool has_gravity = false;
     bool on_device = false;
     double* d_fext = nullptr;         // [3*n_free]
     double* d_u = nullptr;            // staging for host-pointer calls

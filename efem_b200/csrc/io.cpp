@@ -272,10 +272,19 @@ efem_status read_json_config(const char* path, ModelInput& in)
         if (const Json* s = a->find("residual_criterion"); s && s->is_number()) in.opts.residual_criterion = s->num;
         if (const Json* s = a->find("integration"); s && s->is_string()) in.opts.integration = s->str == "reduced" ? 1 : 0;
         if (const Json* s = a->find("precision"); s && s->is_string()) in.opts.precision = s->str == "mixed" ? EFEM_MIXED : EFEM_FP64;
-        if (const Json* s = a->find("gravity"); s && s->is_string() && s->str != "non") {
-            set_error("gravity loads are not part of this library's hot path");
-            return EFEM_ERR_UNSUPPORTED;
+        // gravity as a load of 9.8 along one signed axis (src/io/Config.cpp:45-65,
+        // src/fe/InertiaConstraint.cpp:64-84); other strings leave it off
+        if (const Json* s = a->find("gravity"); s && s->is_string()) {
+            static const char* axes[6] = { "x", "-x", "y", "-y", "z", "-z" };
+            for (int k = 0; k < 6; k++)
+                if (s->str == axes[k]) {
+                    HostLoad L;
+                    L.type = EFEM_LOAD_GRAVITY;
+                    L.value[k / 2] = (k % 2) ? -9.8 : 9.8;
+                    in.loads.push_back(std::move(L));
+                }
         }
+        if (const Json* s = a->find("consistent_inertia"); s && s->is_bool()) in.opts.consistent_inertia = s->b ? 1 : 0;
     }
 
     // bodies, src/model/Model.cpp:14-37

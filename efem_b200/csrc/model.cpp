@@ -88,6 +88,58 @@ double elasticity_coeff(const HostMaterial& m)
     return 2.94001 * m.C10 + 2.0 / m.D1;
 }
 
+// External load vector: the nodal forces plus, under gravity, M g as the
+// reference's inertia constraint adds it (src/fe/InertiaConstraint.cpp:34-50
+// with the element mass of src/fe/ElementConstraint.cpp:85-137):
+//   consistent  M_ab = rho V_e sum_q w_q N_a(q) N_b(q) over free node pairs,
+//               so row a of M g is rho V_e sum_q w_q N_a(q) sum_{b free} N_b(q) g;
+//   lumped      max(rho V_e, 4e-12) / nen on each free node.
+// The consistent mass always uses the element's full Gauss rule: the reference
+// builds it from the full-integration element it creates
+// (src/fe/Constraint.cpp:9-20), whatever rule the residual uses.
+void external_load(const Model& m, std::vector<double>& f)
+{
+    f = m.h_fnodal;
+    if (!m.has_gravity) return;
+    const double* g = m.gravity;
+    const bool consistent = m.opts.consistent_inertia != 0;
+    for (auto& hb : m.in_blocks) {
+        const int kind = kind_of_nen(hb.nen), nen = hb.nen;
+        double pts[3 * MAX_NGP], w[MAX_NGP], dN[3 * MAX_NEN];
+        std::vector<double> N(static_cast<size_t>(MAX_NGP) * MAX_NEN);
+        const int ngp = gauss_rule(kind, false, pts, w);
+        for (int q = 0; q < ngp; q++) shape_functions(kind, pts + 3 * q, N.data() + static_cast<size_t>(q) * MAX_NEN, dN);
+        double Y[3 * MAX_NEN];
+        int d[MAX_NEN];
+        for (size_t e = 0; e < hb.mat_id.size(); e++) {
+            const int* c = hb.conn.data() + e * nen;
+            for (int a = 0; a < nen; a++) {
+                std::memcpy(Y + 3 * a, m.X.data() + 3 * static_cast<size_t>(c[a]), sizeof(double) * 3);
+                d[a] = m.dnode_of_node[c[a]];
+            }
+            const double V = corner_volume(nen, Y), rho = m.materials_used[hb.mat_id[e]].density;
+            if (consistent) {
+                for (int q = 0; q < ngp; q++) {
+                    const double* Nq = N.data() + static_cast<size_t>(q) * MAX_NEN;
+                    double sfree = 0.0;
+                    for (int b = 0; b < nen; b++)
+                        if (d[b] < m.n_free) sfree += Nq[b];
+                    for (int a = 0; a < nen; a++) {
+                        if (d[a] >= m.n_free) continue;
+                        const double s = w[q] * rho * V * Nq[a] * sfree;
+                        for (int k = 0; k < 3; k++) f[3 * static_cast<size_t>(d[a]) + k] += s * g[k];
+                    }
+                }
+            } else {
+                const double mass = std::max(V * rho, 4e-12) / nen;
+                for (int a = 0; a < nen; a++)
+                    if (d[a] < m.n_free)
+                        for (int k = 0; k < 3; k++) f[3 * static_cast<size_t>(d[a]) + k] += mass * g[k];
+            }
+        }
+    }
+}
+
 struct FaceHost {
     int kind, table_key, load, ngp;
     std::vector<int> enodes;  // parent element's nodes (original ids)
@@ -433,7 +485,15 @@ efem_status build_model(ModelInput& in, Model& m)
         df.n_tables = static_cast<int>(table_of_key.size());
         m.faces.push_back(std::move(df));
     }
-    m.h_fext = std::move(fext);
+    m.h_fnodal = std::move(fext);
+    m.has_gravity = false;
+    for (int k = 0; k < 3; k++) m.gravity[k] = 0.0;
+    for (auto& L : in.loads)
+        if (L.type == EFEM_LOAD_GRAVITY) {
+            m.has_gravity = true;
+            for (int k = 0; k < 3; k++) m.gravity[k] += L.value[k];
+        }
+    external_load(m, m.h_fext);
     m.n_pressure_loads = static_cast<int>(loadvals.size() / 4);
     return build_blocks(m);
 }
@@ -704,6 +764,7 @@ efem_status efem_default_options(efem_options* o)
     o->adjoint_tolerance = 1e-8;
     o->adjoint_max_iterations = 2000;
     o->elem_threads = 0;
+    o->consistent_inertia = 0;
     return EFEM_OK;
 }
 
@@ -777,7 +838,7 @@ efem_status efem_model_create(const efem_mesh_desc* mesh, const efem_material* m
                 if (!(mag > 0)) continue;  // ignored like the reference (ExternalConstraint.cpp:195-197)
                 L.face_ptr.assign(ld.face_ptr, ld.face_ptr + std::max(ld.n, 0) + 1);
                 L.nodes.assign(ld.nodes, ld.nodes + (ld.n > 0 ? ld.face_ptr[ld.n] : 0));
-            } else {
+            } else if (ld.type != EFEM_LOAD_GRAVITY) {
                 efem::set_error("unknown load type");
                 return EFEM_ERR_ARG;
             }
@@ -822,10 +883,18 @@ efem_status efem_set_options(void* model, const efem_options* o)
     }
     const bool reintegrate = o->integration != m->opts.integration;
     const bool new_history = o->m != m->opts.m;
+    const bool new_mass = m->has_gravity && (o->consistent_inertia != 0) != (m->opts.consistent_inertia != 0);
     const int dev = m->device;
     m->opts = *o;
     if (dev >= 0) m->device = dev;  // the device is fixed once buffers exist
     if (m->on_device) cudaSetDevice(m->device);
+    if (new_mass) {
+        // same device buffer, new values: captured graphs keep pointing at it
+        efem::external_load(*m, m->h_fext);
+        if (m->d_fext && m->n_free > 0) {
+            EFEM_CUDA(cudaMemcpy(m->d_fext, m->h_fext.data(), sizeof(double) * m->h_fext.size(), cudaMemcpyHostToDevice));
+        }
+    }
     if (reintegrate) {
         efem::free_precond(*m);
         s = efem::build_blocks(*m);
@@ -885,6 +954,16 @@ efem_status efem_dof_map(void* model, int* node_of_dof)
     if (s != EFEM_OK) return s;
     if (!node_of_dof) return EFEM_ERR_ARG;
     std::copy(m->node_of_dnode.begin(), m->node_of_dnode.begin() + m->n_free, node_of_dof);
+    return EFEM_OK;
+}
+
+efem_status efem_external_load(void* model, double* f)
+{
+    Model* m;
+    efem_status s = guard(model, &m);
+    if (s != EFEM_OK) return s;
+    if (!f) return EFEM_ERR_ARG;
+    std::copy(m->h_fext.begin(), m->h_fext.end(), f);
     return EFEM_OK;
 }
 

@@ -60,14 +60,25 @@ typedef struct {
     const efem_element_block* blocks;
 } efem_mesh_desc;
 
-typedef enum { EFEM_LOAD_FIX = 0, EFEM_LOAD_FORCE = 1, EFEM_LOAD_PRESSURE = 2, EFEM_LOAD_DPRESSURE = 3 } efem_load_type;
+typedef enum {
+    EFEM_LOAD_FIX = 0,
+    EFEM_LOAD_FORCE = 1,
+    EFEM_LOAD_PRESSURE = 2,
+    EFEM_LOAD_DPRESSURE = 3,
+    EFEM_LOAD_GRAVITY = 4
+} efem_load_type;
 
 /* A constraint as the reference's "constraint" JSON entries describe it
  * (src/fe/ExternalConstraint.cpp:13-247).
  *   FIX:       nodes[n]                      (0-based)
  *   FORCE:     nodes[n], value[3]            (each listed occurrence adds value)
  *   PRESSURE:  faces in CSR form, value[0] = follower pressure (> 0)
- *   DPRESSURE: faces in CSR form, value[0..2] = directed pressure vector  */
+ *   DPRESSURE: faces in CSR form, value[0..2] = directed pressure vector
+ *   GRAVITY:   value[0..2] = acceleration (the config's "gravity": "-z" is
+ *              (0, 0, -9.8)); nodes / n unused.  Adds M g to the external
+ *              load, M the consistent or lumped mass from the materials'
+ *              density (efem_options.consistent_inertia), as the reference's
+ *              inertia constraint does (src/fe/InertiaConstraint.cpp:34-84). */
 typedef struct {
     int type;                /* efem_load_type */
     int n;                   /* nodes (FIX, FORCE) or faces (PRESSURE, DPRESSURE) */
@@ -99,6 +110,8 @@ typedef struct {
     int adjoint_max_iterations; /* GMRES iteration limit of the adjoint solve (default 2000) */
     int elem_threads;         /* element-kernel CTA size: 0 = chosen per element block by the autotuner
                                  at set-up (64, 128 or 256 threads, timed); 64 / 128 / 256 = forced */
+    int consistent_inertia;   /* gravity loads: 1 consistent mass, 0 lumped (analysis "consistent_inertia",
+                                 src/io/Config.cpp:63-65) */
 } efem_options;
 
 enum {
@@ -170,6 +183,13 @@ efem_status efem_get_model_info(void* model, efem_model_info* info);
 
 /* node_of_dof[id] = node index of free node id (length n_free_nodes). */
 efem_status efem_dof_map(void* model, int* node_of_dof);
+
+/* f[3 n_free_nodes] (host memory) = the displacement-independent external
+ * load: nodal forces plus, under gravity, M g (the inertia constraint's
+ * -M g term of the residual, src/fe/InertiaConstraint.cpp:34-50, with the
+ * nodal forces of src/fe/ExternalConstraint.cpp:149-167).  Pressure faces
+ * follow the deformation and are not part of it.  Needs no GPU. */
+efem_status efem_external_load(void* model, double* f);
 
 /* --------------------------------------------------------------- hot path */
 

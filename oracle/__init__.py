@@ -27,6 +27,9 @@ LIB_PATH = os.path.join(HERE, "_build", "libefem_oracle.so")
 REF_BIN = os.path.join(HERE, "_ref", "efem_ref")
 
 MAT_TYPES = {"neo_hookean": 0, "mo_riv": 1, "yeoh": 2}
+# analysis.gravity (src/io/Config.cpp:45-62, src/fe/InertiaConstraint.cpp:64-84)
+GRAVITY = {"x": (9.8, 0.0, 0.0), "-x": (-9.8, 0.0, 0.0), "y": (0.0, 9.8, 0.0), "-y": (0.0, -9.8, 0.0),
+           "z": (0.0, 0.0, 9.8), "-z": (0.0, 0.0, -9.8)}
 
 
 # --------------------------------------------------------------------------- reader
@@ -101,13 +104,15 @@ def read_case(cfg_path):
         raise NotImplementedError("the oracle restates single-element-type meshes")
     conn = np.array(conn, dtype=np.int32)
     emat = np.array(emat, dtype=np.int32)
-    mats = []
+    mats, density = [], []
     for mj in cfg.get("material", []):
         t = mj.get("type")
         if t not in MAT_TYPES:
             continue
         mats.append([MAT_TYPES[t], mj.get("id", -1), mj.get("C10", 0.0), mj.get("C01", 0.0),
                      mj.get("C20", 0.0), mj.get("C30", 0.0), mj.get("D1", 0.0)])
+        d = mj.get("density")
+        density.append(float(d) if isinstance(d, (int, float)) and not isinstance(d, bool) else 0.0)
     mats = np.array(mats, dtype=np.float64).reshape(-1, 7)
     fixed = np.zeros(X.shape[0], dtype=np.uint8)
     forces, pressures = [], []
@@ -133,9 +138,13 @@ def read_case(cfg_path):
                 faces.append(face)
             pressures.append((cj.get("value"), faces))
     an = cfg.get("analysis", {})
+    gravity = an.get("gravity")
     return {
         "X": X, "conn": conn, "elem_mat": emat, "mats": mats, "fixed": fixed,
         "forces": forces, "pressures": pressures,
+        "density": np.array(density, dtype=np.float64),
+        "gravity": GRAVITY.get(gravity) if isinstance(gravity, str) else None,
+        "consistent_inertia": an.get("consistent_inertia") is True,
         "reduced": an.get("integration", "full") == "reduced",
         "epsilon": float(an.get("residual_criterion", 1e-6)),
         "max_iterations": int(an.get("max_solver_iters", 0)),
@@ -171,6 +180,7 @@ def lib():
                                  ctypes.POINTER(ctypes.c_ubyte), ctypes.c_int]
         L.orc_add_pressure.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ip, ctypes.c_double, dp]
         L.orc_add_force.argtypes = [ctypes.c_void_p, ctypes.c_int, ip, dp]
+        L.orc_add_gravity.argtypes = [ctypes.c_void_p, dp, ctypes.c_int, dp]
         L.orc_n_dof.argtypes = [ctypes.c_void_p]
         L.orc_n_elem_skipped.argtypes = [ctypes.c_void_p]
         L.orc_residual.argtypes = [ctypes.c_void_p, dp, dp]
@@ -222,6 +232,12 @@ class Oracle:
                     rc = L.orc_add_pressure(self.h, arr.shape[0], nn, _p(arr, ctypes.c_int), float(value or 0.0), None)
                 if rc != 0:
                     raise ValueError(f"oracle: pressure face setup failed ({rc})")
+        if case.get("gravity") is not None:
+            g = np.ascontiguousarray(case["gravity"], dtype=np.float64)
+            rho = np.ascontiguousarray(case["density"], dtype=np.float64)
+            if rho.size == 0:
+                rho = np.zeros(1)
+            L.orc_add_gravity(self.h, _p(g), int(case["consistent_inertia"]), _p(rho))
         self.n_dof = L.orc_n_dof(self.h)
 
     def residual(self, u):

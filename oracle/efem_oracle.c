@@ -287,6 +287,7 @@ struct orc_model {
     int n_force;
     int* force_node;
     double* force_val;
+    double* gvec;     /* gravity load M g per free DOF, or NULL */
     /* incident elements per node (CSR) for the face -> element lookup */
     int* inc_ptr;
     int* inc;
@@ -621,6 +622,51 @@ int orc_add_force(orc_model* m, int n, const int* nodes, const double* f)
     return 0;
 }
 
+/* Gravity (src/fe/InertiaConstraint.cpp:34-84 with the element mass of
+ * src/fe/ElementConstraint.cpp:85-137): the residual gains -M g, with M the
+ * consistent mass (rho V sum_g w_g N_i N_j, free-node pairs only) or the
+ * lumped one (max(rho V, 4e-12) / nen on each free node of the element).
+ * g is the acceleration vector; density[k] belongs to material index k.
+ * The mass is built once, at set-up, from the element's own (full) Gauss
+ * rule: the reference creates only full-integration elements
+ * (src/fe/Constraint.cpp:9-20), so its consistent mass never sees a reduced
+ * rule, and under reduced integration the mass keeps the full one. */
+int orc_add_gravity(orc_model* m, const double* g, int consistent, const double* density)
+{
+    if (!m->gvec) m->gvec = calloc(3 * (size_t)(m->n_free > 0 ? m->n_free : 1), sizeof(double));
+    double pts[3 * MAXG], w[MAXG], N[MAXN], dN[3 * MAXN];
+    const int ngp = gauss(m->nen, 0, pts, w);
+    for (int e = 0; e < m->n_elem; e++) {
+        const int k = m->elem_mat[e];
+        if (k < 0) continue;
+        const int* c = m->conn + m->nen * e;
+        const double V = m->vol[e], rho = density[k];
+        if (consistent) {
+            for (int q = 0; q < ngp; q++) {
+                shape(m->nen, pts + 3 * q, N, dN);
+                double sfree = 0.0;
+                for (int j = 0; j < m->nen; j++)
+                    if (m->id[c[j]] >= 0) sfree += N[j];
+                for (int i = 0; i < m->nen; i++) {
+                    const int id = m->id[c[i]];
+                    if (id < 0) continue;
+                    for (int d = 0; d < 3; d++) m->gvec[3 * id + d] += w[q] * rho * V * N[i] * sfree * g[d];
+                }
+            }
+        } else {
+            double mass = V * rho;
+            if (mass < 4e-12) mass = 4e-12;
+            mass /= m->nen;
+            for (int i = 0; i < m->nen; i++) {
+                const int id = m->id[c[i]];
+                if (id < 0) continue;
+                for (int d = 0; d < 3; d++) m->gvec[3 * id + d] += mass * g[d];
+            }
+        }
+    }
+    return 0;
+}
+
 /* Current nodal positions of element e: X + u for free nodes, X for fixed
  * ones (src/fe/Constraint.cpp:93-101). */
 static void elem_pos(const orc_model* m, int e, const double* u, double* Y)
@@ -707,6 +753,9 @@ void orc_residual(orc_model* m, const double* u, double* r)
                     r[3 * id + k] -= v[k];
         }
     }
+    /* the inertia constraint is appended last (src/fe/Constraint.cpp:87-90) */
+    if (m->gvec)
+        for (int i = 0; i < 3 * m->n_free; i++) r[i] -= m->gvec[i];
 }
 
 /* Scalar approximate Jacobian, ElementConstraint.cpp:164-205:
@@ -1123,6 +1172,7 @@ void orc_destroy(orc_model* m)
     free(m->faces);
     free(m->force_node);
     free(m->force_val);
+    free(m->gvec);
     free(m->inc_ptr);
     free(m->inc);
     free(m);

@@ -44,6 +44,10 @@ orc_model* orc_create(int n_nodes, const double* X, int n_elem, int nen, const i
  * every face with face_nn nodes (3, 4, 6 or 8).  Returns 0 or a negative error. */
 int orc_add_pressure(orc_model* m, int n_faces, int face_nn, const int* faces, double value,
     const double* dvalue);
+/* Gravity as the reference's inertia constraint: the residual gains -M g,
+ * M consistent (1) or lumped (0); g the acceleration, density per material
+ * index (the order of orc_create's mats). */
+int orc_add_gravity(orc_model* m, const double* g, int consistent, const double* density);
 /* Nodal force f on each listed node (repeats accumulate). */
 int orc_add_force(orc_model* m, int n, const int* nodes, const double* f);
 int orc_n_dof(const orc_model* m);

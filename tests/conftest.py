@@ -27,6 +27,8 @@ def case_from_golden(path) -> mg.Case:
     d = np.load(path, allow_pickle=False)
     mesh = mg.Mesh(d["X"], d["conn"].astype(np.int64))
     case = mg.Case(mesh, json.loads(str(d["materials"])), d["fix"])
+    if "analysis" in d:
+        case.analysis.update(json.loads(str(d["analysis"])))
     k = 0
     while f"pressure{k}_faces" in d:
         v = d[f"pressure{k}_value"]

@@ -4,7 +4,8 @@ Run in a container that has the reference tree (the fixtures are committed so
 the tests never need it):
 
     make -C oracle ref
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # everything
+    python tests/golden/make_golden.py gravity    # the gravity fixtures only
 
 Each ``case_<etype>_<mat>_<load>.npz`` holds a complete small input (node
 coordinates, connectivity, fixed nodes, loads, material) together with what the
@@ -39,6 +40,8 @@ LOADS = ["pressure", "dpressure", "force"]
 def case_arrays(case: mg.Case) -> dict:
     out = {"X": case.mesh.X, "conn": case.mesh.conn.astype(np.int32), "fix": np.asarray(case.fix, dtype=np.int32),
            "materials": json.dumps(case.materials)}
+    if case.analysis:
+        out["analysis"] = json.dumps(case.analysis)
     for k, (value, faces) in enumerate(case.pressure):
         out[f"pressure{k}_faces"] = np.asarray(faces, dtype=np.int32)
         out[f"pressure{k}_value"] = np.atleast_1d(np.asarray(value, dtype=np.float64))
@@ -55,7 +58,46 @@ def scalar_L_apply(trip, n_dof, v):
     return out
 
 
+def gravity_cases():
+    """``gravity_<etype>_<consistent|lumped>.npz``: the nodal-force cases with
+    analysis.gravity "-z" and a density on the material, the residual at a
+    seeded u for both integration rules and the converged solve; the C3D8 pair
+    is a dense body under gravity alone (src/fe/InertiaConstraint.cpp:34-84)."""
+    rng = np.random.default_rng(20261204)
+    for et in ETYPES:
+        for consistent in (True, False):
+            if et == "C3D8":
+                case = mg.small_case(et, "mr", "force")
+                case.force = []
+                density = 2.0e5
+            else:
+                case = mg.small_case(et, "nh", "force")
+                density = 1100.0
+            for m in case.materials:
+                m["density"] = density
+            case.analysis.update(gravity="-z", consistent_inertia=consistent)
+            with tempfile.TemporaryDirectory() as td:
+                cfg = case.write(td)
+                meta, _ = oracle.run_ref("info", cfg)
+                n = meta["n_dof"]
+                u = rng.normal(size=n) * 2e-4
+                data = case_arrays(case)
+                data.update(u=u)
+                for integ, red in (("full", False), ("reduced", True)):
+                    _, r = oracle.run_ref("residual", cfg, u, reduced=red)
+                    data[f"r_{integ}"] = r
+                _, r0 = oracle.run_ref("residual", cfg, None)
+                meta, us = oracle.run_ref("solve", cfg)
+                data.update(r_zero=r0, u_solve=us, solve_meta=json.dumps(meta))
+            name = f"gravity_{et}_{'consistent' if consistent else 'lumped'}"
+            np.savez_compressed(os.path.join(HERE, name + ".npz"), **data)
+            print(name, n, meta["niter"])
+
+
 def main():
+    if sys.argv[1:] == ["gravity"]:
+        gravity_cases()
+        return
     rng = np.random.default_rng(20261203)
     for et in ETYPES:
         for mat in MATS:
@@ -113,6 +155,7 @@ def main():
             kappa = json.loads(res.stdout)["elasticity_coeff"]
         np.savez_compressed(os.path.join(HERE, f"piola_{mat}.npz"), F=F, P=P, C=np.array(C), kappa=kappa)
         print("piola", mat, kappa)
+    gravity_cases()
 
 
 if __name__ == "__main__":

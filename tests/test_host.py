@@ -134,3 +134,54 @@ def test_compute_without_gpu_fails_loudly():
     with pytest.raises(api.EfemError) as e:
         m.residual(np.zeros(m.n_dof))
     assert e.value.status == api.ERR_NO_DEVICE
+
+
+@pytest.mark.parametrize("path", golden_files("gravity_*.npz"), ids=lambda p: p.split("/")[-1][8:-4])
+@pytest.mark.parametrize("integration", ["full", "reduced"])
+def test_gravity_external_load_matches_reference(path, integration, tmp_path):
+    """f_ext = nodal forces + M g equals -R(0) of the reference (no pressure
+    faces, so the internal force at u = 0 vanishes); under reduced integration
+    the mass keeps the full rule, as in the reference).  The reference's R(0)
+    carries its stress rounding at F = I (a few 1e-15 N per DOF)."""
+    cfg, d = write_golden_case(path, tmp_path, integration)
+    m = api.Model.from_json(cfg)
+    consistent = json.loads(str(d["analysis"]))["consistent_inertia"]
+    assert m.options.consistent_inertia == int(consistent)
+    ref = -d["r_zero"]
+    assert np.linalg.norm(m.external_load() - ref) <= 1e-11 * np.linalg.norm(ref)
+    from conftest import case_from_golden
+    case = case_from_golden(path)
+    case.integration = integration
+    a = api.Model.from_case(case)
+    assert np.array_equal(a.external_load(), m.external_load())
+
+
+def test_gravity_mass_switch(tmp_path):
+    """Changing consistent_inertia after set-up recomputes M g."""
+    lumped = golden_files("gravity_C3D10_lumped.npz")[0]
+    consistent = golden_files("gravity_C3D10_consistent.npz")[0]
+    cfg, dl = write_golden_case(lumped, tmp_path)
+    dc = np.load(consistent)
+    m = api.Model.from_json(cfg)
+    first = m.external_load()
+    assert np.allclose(first, -dl["r_zero"], rtol=1e-12, atol=1e-13)
+    m.set_options(consistent_inertia=1)
+    assert np.allclose(m.external_load(), -dc["r_zero"], rtol=1e-12, atol=1e-13)
+    assert not np.allclose(m.external_load(), first, rtol=1e-6, atol=0)
+    m.set_options(consistent_inertia=0)
+    assert np.array_equal(m.external_load(), first)
+
+
+def test_gravity_strings(tmp_path):
+    case = mg.small_case("C3D8", "nh", "force")
+    base = api.Model.from_case(case).external_load()
+    for key, g in api.GRAVITY.items():
+        case.analysis = {"gravity": key}
+        m = api.Model.from_json(case.write(str(tmp_path / key.replace("-", "n"))))
+        f = (m.external_load() - base).reshape(-1, 3)
+        axis = int(np.nonzero(g)[0][0])
+        assert np.all(np.sign(f[:, axis]) == np.sign(g[axis]))
+        assert np.all(np.delete(f, axis, axis=1) == 0)
+    case.analysis = {"gravity": "non"}
+    m = api.Model.from_json(case.write(str(tmp_path / "non")))
+    assert np.array_equal(m.external_load(), base)

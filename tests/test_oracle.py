@@ -90,3 +90,52 @@ def test_nonpositive_pressure_is_ignored(tmp_path):
     o_neg = oracle.Oracle(oracle.read_case(case.write(str(tmp_path / "neg"))))
     u = np.full(o_none.n_dof, 1e-4)
     assert np.array_equal(o_neg.residual(u), o_none.residual(u))
+
+
+GRAVITY = golden_files("gravity_*.npz")
+
+
+@pytest.mark.parametrize("path", GRAVITY, ids=lambda p: p.split("/")[-1][8:-4])
+@pytest.mark.parametrize("integration", ["full", "reduced"])
+def test_gravity_residual_matches_reference(path, integration, tmp_path):
+    """R(u) with the inertia constraint's -M g (consistent or lumped M)."""
+    cfg, d = write_golden_case(path, tmp_path, integration)
+    case = oracle.read_case(cfg)
+    assert case["gravity"] == (0.0, 0.0, -9.8)
+    o = oracle.Oracle(case)
+    ref = d[f"r_{integration}"]
+    assert np.linalg.norm(o.residual(d["u"]) - ref) <= 1e-12 * np.linalg.norm(ref)
+    r0 = o.residual(np.zeros(o.n_dof))
+    assert np.linalg.norm(r0 - d["r_zero"]) <= 1e-12 * np.linalg.norm(d["r_zero"])
+
+
+@pytest.mark.parametrize("path", GRAVITY, ids=lambda p: p.split("/")[-1][8:-4])
+def test_gravity_solve_matches_reference(path, tmp_path):
+    cfg, d = write_golden_case(path, tmp_path)
+    o = oracle.Oracle(oracle.read_case(cfg))
+    u, info = o.solve()
+    ref = d["u_solve"]
+    assert info["r_inf"] <= 1e-6
+    assert np.linalg.norm(u - ref) <= 1e-6 * np.linalg.norm(ref)
+    assert abs(info["niter"] - json.loads(str(d["solve_meta"]))["niter"]) <= 2
+
+
+def test_gravity_mass_totals(tmp_path):
+    """Summed over a body with no fixed nodes, M g gives the weight
+    rho g sum_e V_e for either mass (the Gauss weights of each element sum to
+    one).  V_e is the reference's corner-face volume, which warped hexahedra
+    make differ slightly from the box's L W H."""
+    path = golden_files("gravity_C3D8_consistent.npz")[0]
+    cfg, d = write_golden_case(path, tmp_path)
+    case = oracle.read_case(cfg)
+    case["fixed"][:] = 0
+    case["forces"] = []
+    vol = 0.03 * 0.01 * 0.01
+    totals = []
+    for consistent in (True, False):
+        case["consistent_inertia"] = consistent
+        o = oracle.Oracle(case)
+        f = -o.residual(np.zeros(o.n_dof)).reshape(-1, 3).sum(axis=0)
+        assert np.allclose(f, [0.0, 0.0, -9.8 * 2.0e5 * vol], rtol=1e-4, atol=1e-12)
+        totals.append(f)
+    assert np.allclose(totals[0], totals[1], rtol=1e-13, atol=1e-15)
