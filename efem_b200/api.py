@@ -37,7 +37,7 @@ EXPORTED = ["efem_default_options", "efem_model_create_from_json", "efem_model_c
             "efem_approx_jacobian_csr", "efem_precond_apply", "efem_precond_apply_noalloc", "efem_solve",
             "efem_set_stream", "efem_last_error", "efem_version", "efem_hvp", "efem_hvp_transpose",
             "efem_residual_param_derivative", "efem_adjoint", "efem_strain_energy", "efem_write_vtk",
-            "efem_batch_solve", "efem_external_load"]
+            "efem_batch_solve", "efem_external_load", "efem_solve_trace"]
 
 
 class EfemError(RuntimeError):
@@ -53,7 +53,7 @@ class Options(ctypes.Structure):
                 ("device_ptrs", ctypes.c_int), ("deterministic", ctypes.c_int), ("device", ctypes.c_int),
                 ("host_loop", ctypes.c_int), ("adjoint_tolerance", ctypes.c_double),
                 ("adjoint_max_iterations", ctypes.c_int), ("elem_threads", ctypes.c_int),
-                ("consistent_inertia", ctypes.c_int)]
+                ("consistent_inertia", ctypes.c_int), ("trace", ctypes.c_int)]
 
 
 class SolveInfo(ctypes.Structure):
@@ -348,6 +348,19 @@ class Model:
         if st not in (OK,):
             raise EfemError(st, last_error())
         return u, info.as_dict()
+
+    def solve_trace(self):
+        """Convergence trace of the last solve (options.trace > 0): a dict of
+        arrays time_s, r_norm2, r_inf, step, r_evals, one entry per record
+        (record 0: the initial residual; record i: after iteration i)."""
+        n = ctypes.c_int(0)
+        check(lib().efem_solve_trace(self.h, None, 0, ctypes.byref(n)))
+        cap = min(n.value, self.options.trace)
+        out = np.zeros((max(cap, 0), 5))
+        if cap > 0:
+            check(lib().efem_solve_trace(self.h, _ptr(out), cap, ctypes.byref(n)))
+        return {"time_s": out[:, 0], "r_norm2": out[:, 1], "r_inf": out[:, 2], "step": out[:, 3],
+                "r_evals": out[:, 4].astype(np.int64), "n_records": n.value}
 
     # ------------------------------------------------------------------ sensitivities
     def _vec(self, x):

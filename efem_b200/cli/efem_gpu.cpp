@@ -3,7 +3,12 @@
 // same log line after the solve (src/simulation/Integrator.cpp:36-40); with
 // output.save_frame the undeformed and deformed meshes are written as legacy
 // VTK files under <config dir>/results/<date>/<date-time-ms>-{undeformed,deformed}.vtk
-// like Model::saveVTK (src/model/Model.cpp:50-117).
+// like Model::saveVTK (src/model/Model.cpp:50-117).  --benchmark prints the
+// solve's convergence record as LBFGSSolver::printBenchmark does
+// (src/simulation/nlsolver/LBFGS.h:176-189): per record the residual norm
+// scaled to (f_i - f_last) / (f_0 - f_last) and the seconds since the solve
+// started, at most 9000 lines.
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <cstring>
@@ -68,13 +73,16 @@ int main(int argc, char** argv)
 {
     std::string cfg;
     int device = -1;
+    bool benchmark = false;
     for (int i = 1; i < argc; i++) {
         if (!std::strcmp(argv[i], "-f") && i + 1 < argc) {
             cfg = argv[++i];
         } else if (!std::strcmp(argv[i], "--device") && i + 1 < argc) {
             device = std::atoi(argv[++i]);
+        } else if (!std::strcmp(argv[i], "--benchmark")) {
+            benchmark = true;
         } else if (!std::strcmp(argv[i], "-h") || !std::strcmp(argv[i], "--help")) {
-            std::printf("Efficient FEM on the GPU\nUsage: %s -f <config.json> [--device N]\n", argv[0]);
+            std::printf("Efficient FEM on the GPU\nUsage: %s -f <config.json> [--device N] [--benchmark]\n", argv[0]);
             return 0;
         } else {
             std::fprintf(stderr, "unknown argument %s\n", argv[i]);
@@ -104,10 +112,12 @@ int main(int argc, char** argv)
     const std::string workdir = std::filesystem::path(cfg).parent_path().string();
     void* model = nullptr;
     if (efem_model_create_from_json(cfg.c_str(), &model) != EFEM_OK) return fail("reading the config");
-    if (device >= 0) {
+    constexpr int kBenchmarkRows = 9000;
+    if (device >= 0 || benchmark) {
         efem_options o;
         efem_get_options(model, &o);
-        o.device = device;
+        if (device >= 0) o.device = device;
+        if (benchmark) o.trace = kBenchmarkRows;
         efem_set_options(model, &o);
     }
     if (show_log) info("Simulator initialed");
@@ -129,6 +139,25 @@ int main(int argc, char** argv)
         std::snprintf(line, sizeof line, "dx=%.17g, residual=%.17g, niter=%d, r_evalutes=%d, j_evalutes=%d", si.u_inf,
             si.r_inf, si.niter, si.n_residual_evals, si.n_jacobian_evals);
         info(line);
+    }
+    if (benchmark) {
+        int n = 0;
+        efem_solve_trace(model, nullptr, 0, &n);
+        n = std::min(n, kBenchmarkRows);
+        std::vector<double> rec(static_cast<size_t>(n) * 5);
+        if (n > 0) efem_solve_trace(model, rec.data(), n, &n);
+        n = std::min(n, kBenchmarkRows);
+        if (n == 0) {
+            info("no benchmark!");
+        } else {
+            const double last = rec[5 * static_cast<size_t>(n - 1) + 1], span = rec[1] - last;
+            for (int i = 0; i < n; i++) {
+                char line[128];
+                std::snprintf(line, sizeof line, "benchmark[%d]: f=%.17g, time=%.9gs", i,
+                    (rec[5 * static_cast<size_t>(i) + 1] - last) / span, rec[5 * static_cast<size_t>(i)]);
+                info(line);
+            }
+        }
     }
     if (show_log) {
         char line[128];

@@ -209,6 +209,7 @@ efem_status launch_residual_on(Model& m, const double* d_u, double* d_r, cudaStr
 
 // ------------------------------------------------------------------ solver (solver.cu)
 efem_status run_solve(Model& m, double* d_u, efem_solve_info* info);
+efem_status solve_trace(Model& m, double* out, int capacity, int* n_records);
 void free_solver(Model& m);
 // Held while a CUDA graph is captured and instantiated, so that solves of
 // different models running in parallel host threads never overlap a capture

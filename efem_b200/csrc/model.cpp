@@ -765,6 +765,7 @@ efem_status efem_default_options(efem_options* o)
     o->adjoint_max_iterations = 2000;
     o->elem_threads = 0;
     o->consistent_inertia = 0;
+    o->trace = 0;
     return EFEM_OK;
 }
 
@@ -877,7 +878,8 @@ efem_status efem_set_options(void* model, const efem_options* o)
     efem_status s = guard(model, &m);
     if (s != EFEM_OK) return s;
     if (!o || o->m <= 0 || o->max_linesearch <= 0 || o->max_iterations < 0 || o->residual_criterion < 0
-        || (o->precision != EFEM_FP64 && o->precision != EFEM_MIXED) || (o->integration != 0 && o->integration != 1)) {
+        || (o->precision != EFEM_FP64 && o->precision != EFEM_MIXED) || (o->integration != 0 && o->integration != 1)
+        || o->trace < 0) {
         efem::set_error("invalid options (NLSolverParam::check_param rules)");
         return EFEM_ERR_ARG;
     }
@@ -1190,6 +1192,15 @@ efem_status efem_solve(void* model, double* u_inout, efem_solve_info* info)
         EFEM_CUDA(cudaStreamSynchronize(m->stream));
     }
     return s;
+}
+
+efem_status efem_solve_trace(void* model, double* out, int capacity, int* n_records)
+{
+    Model* m;
+    efem_status s = guard(model, &m);
+    if (s != EFEM_OK) return s;
+    if (m->on_device) cudaSetDevice(m->device);
+    return efem::solve_trace(*m, out, capacity, n_records);
 }
 
 efem_status efem_batch_solve(void** models, int n, double* const* u, efem_solve_info* infos, int max_threads)

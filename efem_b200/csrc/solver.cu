@@ -71,11 +71,20 @@ struct Scalars {
     int k, launch_iters, ls_t, status;
     unsigned long long n_res, n_extra, n_body;  // residual evaluations, extra trials, device-driven iterations
     unsigned long long t0_res, t_res, t0_pc, t_pc;  // global-timer stamps and sums (ns)
+    // convergence trace: record i = the state after iteration i's line search
+    // (record 0: the initial residual); kTraceCols doubles per record
+    double* trace;
+    int trace_cap, tr_i, tr_evals;
+    unsigned long long t_start;
 };
+
+// trace record: seconds since the solve started (GPU global timer), ||r||_2,
+// ||r||_inf, the step of the trial, residual evaluations in the iteration
+constexpr int kTraceCols = 5;
 
 // host-mapped read-back slots
 enum { kRdDg = 0, kRdRinf, kRdXinf, kRdX2, kRdDg0, kRdPerr, kRdStatus, kRdK, kRdNRes, kRdNExtra, kRdNBody, kRdTRes,
-    kRdTPc, kRdCount };
+    kRdTPc, kRdTrN, kRdCount };
 // device loop status
 enum { kRunning = 0, kConverged = 1, kMaxIters = 2, kNonFinite = 3, kPrecondFail = 4, kCapReached = 5 };
 
@@ -211,14 +220,18 @@ __global__ void k_state_init(Scalars* S, int m)
     S->theta = 1.0;
 }
 
-// x = xp + step d
-__global__ void k_trial(double* __restrict__ x, const double* __restrict__ xp, const double* __restrict__ d, double step, size_t n)
+// x = xp + step d (a host-driven trial; the step is kept for the trace)
+__global__ void k_trial(double* __restrict__ x, const double* __restrict__ xp, const double* __restrict__ d, double step,
+    size_t n, Scalars* S)
 {
+    if (blockIdx.x == 0 && threadIdx.x == 0) S->step = step;
     GRID_STRIDE(i, n) x[i] = xp[i] + step * d[i];
 }
 
 // line-search scalars: dg = r.d, rinf = ||r||_inf, xinf = ||x||_inf, x2 = ||x||^2,
-// stored in S and in the host-mapped read-back array
+// stored in S and in the host-mapped read-back array; with a trace buffer the
+// trial also (over)writes the current iteration's record, so the record left
+// is the accepted trial's
 // With `decide` (inside the device-driven line search) the last CTA also
 // applies the accept / scale rule of LineSearchFEA.h:43-67: accept when
 // |r.d| <= |r0.d|; otherwise scale the step by 1.5 (same sign) or 0.5 and try
@@ -232,8 +245,8 @@ __global__ void __launch_bounds__(kThreads) k_ls_reduce(const double* __restrict
         // the loop stops unless the last CTA below decides on another trial
         if (decide) cudaGraphSetConditional(h, 0u);
     }
-    double v[4] = { 0, 0, 0, 0 };
-    const int ops[4] = { 0, 1, 1, 0 };
+    double v[5] = { 0, 0, 0, 0, 0 };
+    const int ops[5] = { 0, 1, 1, 0, 0 };
     GRID_STRIDE(i, n)
     {
         const double ri = r[i], xi = x[i];
@@ -241,15 +254,26 @@ __global__ void __launch_bounds__(kThreads) k_ls_reduce(const double* __restrict
         v[1] = fmax(v[1], fabs(ri));
         v[2] = fmax(v[2], fabs(xi));
         v[3] += xi * xi;
+        v[4] += ri * ri;
     }
-    block_reduce<4>(v, ops);
-    if (grid_finish<4>(v, ops, partials, &S->counter[0])) {
+    block_reduce<5>(v, ops);
+    if (grid_finish<5>(v, ops, partials, &S->counter[0])) {
         S->dg = v[0];
         S->rinf = v[1];
         S->xinf = v[2];
         S->x2 = v[3];
         S->perr = perr ? static_cast<double>(*perr) : 0.0;
         S->n_res++;
+        S->tr_evals++;
+        if (S->trace && S->tr_i < S->trace_cap) {
+            double* rec = S->trace + static_cast<size_t>(S->tr_i) * kTraceCols;
+            rec[0] = static_cast<double>(gtimer() - S->t_start) * 1e-9;
+            rec[1] = sqrt(v[4]);
+            rec[2] = v[1];
+            rec[3] = S->step;
+            rec[4] = static_cast<double>(S->tr_evals);
+        }
+        hread[kRdTrN] = static_cast<double>(S->tr_i + 1);
         hread[kRdDg] = S->dg;
         hread[kRdRinf] = S->rinf;
         hread[kRdXinf] = S->xinf;
@@ -288,7 +312,12 @@ __global__ void __launch_bounds__(kThreads) k_ls_begin_trial(const double* __res
         x[i] = xi + 1.0 * di;
     }
     block_reduce<1>(v, ops);
-    if (grid_finish<1>(v, ops, partials, &S->counter[1])) S->dg0 = v[0];
+    if (grid_finish<1>(v, ops, partials, &S->counter[1])) {
+        S->dg0 = v[0];
+        S->step = 1.0;
+        S->tr_i++;  // iteration 1's trace record
+        S->tr_evals = 0;
+    }
 }
 
 // Pass 1 (LBFGSMat::add_correction, LBFGSMat.h:81-98, and the dot products of
@@ -459,6 +488,8 @@ __global__ void __launch_bounds__(kThreads) k_pass4(double* __restrict__ d, cons
         S->dg0 = v[0];
         S->step = 1.0;
         S->ls_t = 0;
+        S->tr_i++;  // the next iteration's trace record
+        S->tr_evals = 0;
         if (set_h) cudaGraphSetConditional(h_ls, 1u);  // the line search's first trial always runs
     }
 }
@@ -529,14 +560,20 @@ __global__ void k_loop_params(Scalars* S, double eps, int max_iter, int max_ls, 
     S->t_pc = 0;
 }
 
-// counters and timers of one solve
-__global__ void k_solve_init(Scalars* S)
+// counters, timers and trace of one solve (the initial residual is trace record 0, step 0)
+__global__ void k_solve_init(Scalars* S, double* trace, int trace_cap)
 {
     S->n_res = 0;
     S->t_res = 0;
     S->t_pc = 0;
     S->n_extra = 0;
     S->n_body = 0;
+    S->trace = trace;
+    S->trace_cap = trace ? trace_cap : 0;
+    S->tr_i = 0;
+    S->tr_evals = 0;
+    S->step = 0.0;
+    S->t_start = gtimer();
 }
 
 // vector kernels are latency-bound at these sizes: about one element per thread
@@ -554,6 +591,9 @@ struct SolverWS {
     double* sums = nullptr;
     Scalars* sc = nullptr;
     double* h_read = nullptr;  // mapped pinned memory: kRdCount scalars written by the device
+    double* trace = nullptr;   // [trace_cap][kTraceCols] convergence trace of the last solve
+    int trace_cap = 0;
+    int trace_n = 0;           // records the last solve produced (may exceed trace_cap)
     cudaEvent_t ev[4] = { nullptr, nullptr, nullptr, nullptr };  // solve start / end, initial H0 start / end
     cudaStream_t capture[3] = { nullptr, nullptr, nullptr };      // outer graph, loop body, line-search body
     struct Graphs {
@@ -600,6 +640,7 @@ void free_solver(Model& m)
     dev_free(w.Y);
     dev_free(w.partials);
     dev_free(w.sums);
+    dev_free(w.trace);
     if (w.sc) cudaFree(w.sc);
     if (w.h_read) cudaFreeHost(w.h_read);
     for (auto& e : w.ev)
@@ -628,7 +669,7 @@ static efem_status alloc_ws(Model& m)
         if ((s = dev_alloc(p, n)) != EFEM_OK) return s;
     if ((s = dev_alloc(&w.S, n * w.m)) != EFEM_OK) return s;
     if ((s = dev_alloc(&w.Y, n * w.m)) != EFEM_OK) return s;
-    const size_t np = std::max<size_t>(static_cast<size_t>(kMaxBlocks) * 4, static_cast<size_t>(kRowBlocks) * (w.m + 1) * 3);
+    const size_t np = std::max<size_t>(static_cast<size_t>(kMaxBlocks) * 5, static_cast<size_t>(kRowBlocks) * (w.m + 1) * 3);
     if ((s = dev_alloc(&w.partials, np)) != EFEM_OK) return s;
     if ((s = dev_alloc(&w.sums, 3 * static_cast<size_t>(w.m + 1))) != EFEM_OK) return s;
     EFEM_CUDA(cudaMalloc(&w.sc, sizeof(Scalars)));
@@ -856,15 +897,25 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
     bool converged = false, ok = false;
     long long n_body = 0;
     volatile double* hr = w.h_read;
+    if (m.opts.trace != w.trace_cap) {  // the buffer is read through Scalars, so graphs need no recapture
+        EFEM_CUDA(cudaStreamSynchronize(st));
+        dev_free(w.trace);
+        w.trace_cap = 0;
+        if (m.opts.trace > 0) {
+            if ((s = dev_alloc(&w.trace, static_cast<size_t>(m.opts.trace) * kTraceCols)) != EFEM_OK) return s;
+            w.trace_cap = m.opts.trace;
+        }
+    }
+    hr[kRdTrN] = 0.0;
     EFEM_CUDA(cudaEventRecord(w.ev[0], st));
-    k_solve_init<<<1, 1, 0, st>>>(w.sc);
+    k_solve_init<<<1, 1, 0, st>>>(w.sc, w.trace, w.trace_cap);
     m.launches++;
 
     // host-driven line-search trial: x = xp + step d (step 0: x as is),
     // residual, reductions, read-back
     auto direct_trial = [&](double step) -> efem_status {
         if (step != 0.0) {
-            k_trial<<<G, kThreads, 0, st>>>(x, w.xp, w.d, step, n);
+            k_trial<<<G, kThreads, 0, st>>>(x, w.xp, w.d, step, n, w.sc);
             m.launches++;
         }
         efem_status rs = enqueue_trial_tail(m, w, x, st);
@@ -1026,6 +1077,7 @@ done:
     info->u_inf = xinf;
     info->r_inf = rinf;
     info->n_kernel_launches = m.launches - launches0;
+    w.trace_n = static_cast<int>(hr[kRdTrN]);
     if (converged) info->flags |= EFEM_SOLVE_CONVERGED;
     if (xinf < m.opts.dx_criterion) info->flags |= EFEM_SOLVE_DX_CONVERGED;
     return EFEM_OK;
@@ -1038,8 +1090,23 @@ nan_exit:
     info->r_inf = rinf;
     info->n_residual_evals = static_cast<int>(hr[kRdNRes]);
     info->n_kernel_launches = m.launches - launches0;
+    w.trace_n = static_cast<int>(hr[kRdTrN]);
     set_error("L-BFGS produced a non-finite residual or solution");
     return EFEM_ERR_NAN;
+}
+
+efem_status solve_trace(Model& m, double* out, int capacity, int* n_records)
+{
+    const int n = m.ws ? m.ws->trace_n : 0;
+    if (n_records) *n_records = n;
+    if (!out || capacity <= 0 || !m.ws || !m.ws->trace) return EFEM_OK;
+    const int k = std::min(std::min(n, capacity), m.ws->trace_cap);
+    if (k > 0) {
+        EFEM_CUDA(cudaMemcpyAsync(out, m.ws->trace, sizeof(double) * kTraceCols * static_cast<size_t>(k),
+            cudaMemcpyDeviceToHost, m.stream));
+        EFEM_CUDA(cudaStreamSynchronize(m.stream));
+    }
+    return EFEM_OK;
 }
 
 }  // namespace efem

@@ -112,6 +112,8 @@ typedef struct {
                                  at set-up (64, 128 or 256 threads, timed); 64 / 128 / 256 = forced */
     int consistent_inertia;   /* gravity loads: 1 consistent mass, 0 lumped (analysis "consistent_inertia",
                                  src/io/Config.cpp:63-65) */
+    int trace;                /* > 0: keep a convergence trace of up to this many records per solve
+                                 (efem_solve_trace); 0: off */
 } efem_options;
 
 enum {
@@ -228,6 +230,16 @@ efem_status efem_precond_apply_noalloc(void* model, double* d_v);
 /* Solve R(u) = 0 from u_inout: replaces Integrator::integral
  * (src/simulation/Integrator.cpp:22-42) -> LBFGSSolver::solve (LBFGS.h:96-174). */
 efem_status efem_solve(void* model, double* u_inout, efem_solve_info* info);
+
+/* The convergence trace of the model's last solve (options.trace > 0), the
+ * reference's benchmark record (src/simulation/nlsolver/LBFGS.h:107-147,
+ * printBenchmark :176-189) kept on the device: record 0 is the initial
+ * residual, record i the state after iteration i's line search.  Each record
+ * is 5 doubles: seconds since the solve started (GPU timer), ||r||_2,
+ * ||r||_inf, the accepted step, residual evaluations in that iteration.
+ * Copies min(records, capacity, options.trace) records to out (host memory;
+ * out may be NULL) and sets *n_records to the number the solve produced. */
+efem_status efem_solve_trace(void* model, double* out, int capacity, int* n_records);
 
 /* --------------------------------------------------------------- sensitivities
  * None of these has a counterpart in the reference, which only forms the

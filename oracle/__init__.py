@@ -181,6 +181,8 @@ def lib():
         L.orc_add_pressure.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ip, ctypes.c_double, dp]
         L.orc_add_force.argtypes = [ctypes.c_void_p, ctypes.c_int, ip, dp]
         L.orc_add_gravity.argtypes = [ctypes.c_void_p, dp, ctypes.c_int, dp]
+        L.orc_set_trace.argtypes = [ctypes.c_void_p, dp, ctypes.c_int]
+        L.orc_trace_count.argtypes = [ctypes.c_void_p]
         L.orc_n_dof.argtypes = [ctypes.c_void_p]
         L.orc_n_elem_skipped.argtypes = [ctypes.c_void_p]
         L.orc_residual.argtypes = [ctypes.c_void_p, dp, dp]
@@ -252,15 +254,23 @@ class Oracle:
         lib().orc_approx_jacobian_dense(self.h, _p(L))
         return L
 
-    def solve(self, u0=None, **over):
+    def solve(self, u0=None, trace=0, **over):
+        """L-BFGS solve; with trace > 0 the info dict also holds "trace", an
+        (records, 5) array (0, ||r||_2, ||r||_inf, step, residual evaluations)."""
         c = dict(self.case)
         c.update(over)
         p = _Params(c["epsilon"], c["max_iterations"], c["max_linesearch"], c.get("m", 6), int(c["use_precond"]))
         u = np.zeros(self.n_dof) if u0 is None else np.array(u0, dtype=np.float64)
         info = _Info()
+        buf = np.zeros((max(trace, 1), 5))
+        lib().orc_set_trace(self.h, _p(buf) if trace > 0 else None, int(trace))
         lib().orc_solve(self.h, ctypes.byref(p), _p(u), ctypes.byref(info))
-        return u, {"niter": info.niter, "r_evals": info.r_evals, "precond_ok": info.precond_ok,
-                   "u_inf": info.u_inf, "r_inf": info.r_inf}
+        out = {"niter": info.niter, "r_evals": info.r_evals, "precond_ok": info.precond_ok,
+               "u_inf": info.u_inf, "r_inf": info.r_inf}
+        if trace > 0:
+            out["trace"] = buf[:min(trace, lib().orc_trace_count(self.h))].copy()
+        lib().orc_set_trace(self.h, None, 0)
+        return u, out
 
     def precond_apply(self, v):
         """H0 v with H0 the inverse approximate Jacobian; None if L is not SPD."""
@@ -289,10 +299,13 @@ def ref_available():
     return os.path.exists(REF_BIN)
 
 
-def run_ref(cmd, cfg, *args, reduced=False, timeout=3600):
-    """Run the reference driver; returns (parsed JSON line, output arrays)."""
+def run_ref(cmd, cfg, *args, reduced=False, trace=False, timeout=3600):
+    """Run the reference driver; returns (parsed JSON line, output arrays).
+    ``trace`` (solve only) adds meta["trace"]: the reference's benchmark
+    record of ||r||_2, initial residual first, then one per line search."""
     with tempfile.TemporaryDirectory() as td:
         out = os.path.join(td, "out.bin")
+        tpath = os.path.join(td, "trace.f64")
         argv = [REF_BIN, cmd, cfg]
         if cmd == "residual":
             u = args[0]
@@ -306,10 +319,14 @@ def run_ref(cmd, cfg, *args, reduced=False, timeout=3600):
         if reduced:
             argv.append("--reduced")
         argv += [str(a) for a in args[1:]] if cmd == "residual" else [str(a) for a in args]
+        if trace:
+            argv += ["--trace", tpath]
         res = subprocess.run(argv, capture_output=True, text=True, timeout=timeout)
         if res.returncode != 0:
             raise RuntimeError(f"efem_ref {cmd} failed: {res.stderr[-500:]}")
         meta = json.loads(res.stdout.strip().splitlines()[-1])
+        if trace:
+            meta["trace"] = np.fromfile(tpath, dtype=np.float64)
         if cmd == "jacobi":
             raw = open(out, "rb").read()
             cnt = np.frombuffer(raw[:8], dtype=np.int64)[0]

@@ -288,6 +288,8 @@ struct orc_model {
     int* force_node;
     double* force_val;
     double* gvec;     /* gravity load M g per free DOF, or NULL */
+    double* trace;    /* caller's buffer for the solve trace, or NULL */
+    int trace_cap, trace_n;
     /* incident elements per node (CSR) for the face -> element lookup */
     int* inc_ptr;
     int* inc;
@@ -1051,6 +1053,32 @@ int orc_precond_apply(orc_model* m, double* v)
     return ok;
 }
 
+/* The solve's convergence record (the reference's benchmark vector,
+ * src/simulation/nlsolver/LBFGS.h:107-147): record 0 after the initial
+ * residual, record i after iteration i's line search; 5 doubles each
+ * (0, ||r||_2, ||r||_inf, step of the last trial, residual evaluations). */
+void orc_set_trace(orc_model* m, double* buf, int cap)
+{
+    m->trace = buf;
+    m->trace_cap = buf ? cap : 0;
+    m->trace_n = 0;
+}
+
+int orc_trace_count(const orc_model* m) { return m->trace_n; }
+
+static void trace_record(orc_model* m, const double* r, int n, double step, int evals)
+{
+    if (m->trace && m->trace_n < m->trace_cap) {
+        double* rec = m->trace + 5 * (size_t)m->trace_n;
+        rec[0] = 0.0;
+        rec[1] = sqrt(dot(r, r, n));
+        rec[2] = inf_norm(r, n);
+        rec[3] = step;
+        rec[4] = evals;
+    }
+    m->trace_n++;
+}
+
 int orc_solve(orc_model* m, const orc_params* p, double* x, orc_info* info)
 {
     int n = 3 * m->n_free, mm = p->m;
@@ -1063,8 +1091,10 @@ int orc_solve(orc_model* m, const orc_params* p, double* x, orc_info* info)
     double theta = 1.0;
     memset(info, 0, sizeof(*info));
 
+    m->trace_n = 0;
     orc_residual(m, x, r);
     evals++;
+    trace_record(m, r, n, 0.0, 1);
     double gnorm = inf_norm(r, n);
     if (gnorm <= p->epsilon || gnorm <= p->epsilon * sqrt(dot(x, x, n))) {
         k = 1;
@@ -1086,17 +1116,21 @@ int orc_solve(orc_model* m, const orc_params* p, double* x, orc_info* info)
         memcpy(xp, x, sizeof(double) * n);
         memcpy(rp, r, sizeof(double) * n);
         /* residual-projection line search */
-        double dg0 = dot(r, d, n), step = 1.0;
+        double dg0 = dot(r, d, n), step = 1.0, tried = 1.0;
+        int trials = 0;
         for (int it = 0; it < p->max_linesearch; it++) {
             for (int i = 0; i < n; i++)
                 x[i] = xp[i] + step * d[i];
             orc_residual(m, x, r);
             evals++;
+            trials++;
+            tried = step;
             double dg = dot(r, d, n);
             if (fabs(dg) <= fabs(dg0))
                 break;
             step *= dg * dg0 > 0 ? 1.5 : 0.5;
         }
+        trace_record(m, r, n, tried, trials);
         gnorm = inf_norm(r, n);
         if (gnorm <= p->epsilon || gnorm <= p->epsilon * inf_norm(x, n))
             break;

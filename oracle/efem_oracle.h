@@ -57,6 +57,11 @@ void orc_residual(orc_model* m, const double* u, double* r);
  * reference's matrix is L (x) I3. */
 void orc_approx_jacobian_dense(orc_model* m, double* L);
 int orc_solve(orc_model* m, const orc_params* p, double* u, orc_info* info);
+/* Record the next solves' convergence trace into buf (cap records of 5
+ * doubles: 0, ||r||_2, ||r||_inf, step, residual evaluations); NULL: off.
+ * orc_trace_count: records the last solve produced (may exceed cap). */
+void orc_set_trace(orc_model* m, double* buf, int cap);
+int orc_trace_count(const orc_model* m);
 /* v <- (L (x) I3)^{-1} v (the preconditioner solve); 0 if L is not SPD. */
 int orc_precond_apply(orc_model* m, double* v);
 /* First Piola-Kirchhoff stress of one material at n column-major 3x3 F. */

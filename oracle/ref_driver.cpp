@@ -9,7 +9,7 @@
 //       Constraint::assignDx + Constraint::getResidual   (src/fe/Constraint.cpp:93-126)
 //   efem_ref jacobi   <cfg.json> <trip_out.bin> [--reduced]
 //       Constraint::getJacobi triplets                    (src/fe/Constraint.cpp:128-138)
-//   efem_ref solve    <cfg.json> <u_out.f64> [--reduced] [--max-iters N]
+//   efem_ref solve    <cfg.json> <u_out.f64> [--reduced] [--max-iters N] [--trace <r2_out.f64>]
 //       LBFGSSolver<SoftObjective>::solve from x = 0      (src/simulation/Integrator.cpp:22-42,
 //                                                          src/simulation/nlsolver/LBFGS.h:96-174)
 //   efem_ref info     <cfg.json> <dofmap_out.i32>
@@ -231,11 +231,14 @@ int main(int argc, char** argv)
         return 1;
     bool reduced = false;
     int max_iters = -1;
+    const char* trace_path = nullptr;
     for (int i = 4; i < argc; i++) {
         if (!strcmp(argv[i], "--reduced"))
             reduced = true;
         if (!strcmp(argv[i], "--max-iters") && i + 1 < argc)
             max_iters = atoi(argv[i + 1]);
+        if (!strcmp(argv[i], "--trace") && i + 1 < argc)
+            trace_path = argv[i + 1];
     }
     std::string cfg = argv[2];
     auto t0 = std::chrono::steady_clock::now();
@@ -302,6 +305,9 @@ int main(int argc, char** argv)
         param.max_iterations = max_iters >= 0 ? max_iters : ac->max_solver_iters;
         param.max_linesearch = ac->max_line_search;
         param.config = p.config;
+        // --trace: the reference's own benchmark record (LBFGS.h:107-147),
+        // ||r||_2 after the initial residual and after every line search
+        param.benchmark = trace_path != nullptr;
         SoftObjective obj;
         obj.constraint = p.constraint;
         obj.dimens = n;
@@ -311,6 +317,8 @@ int main(int argc, char** argv)
         int niter = solver.solve(obj, x);
         auto t3 = std::chrono::steady_clock::now();
         write_raw(argv[3], x.data(), n * sizeof(double));
+        if (trace_path)
+            write_raw(trace_path, solver.m_f_benchmark.data(), solver.m_f_benchmark.size() * sizeof(double));
         double rinf = obj.nl_residual.size() ? obj.nl_residual.lpNorm<Eigen::Infinity>() : 0.0;
         printf("{\"n_dof\": %d, \"niter\": %d, \"r_evals\": %d, \"j_evals\": %d, "
                "\"u_inf\": %.17g, \"r_inf\": %.17g, \"setup_s\": %.6f, \"solve_s\": %.6f}\n",

@@ -6,6 +6,7 @@ the tests never need it):
     make -C oracle ref
     python tests/golden/make_golden.py            # everything
     python tests/golden/make_golden.py gravity    # the gravity fixtures only
+    python tests/golden/make_golden.py trace      # the solve traces only
 
 Each ``case_<etype>_<mat>_<load>.npz`` holds a complete small input (node
 coordinates, connectivity, fixed nodes, loads, material) together with what the
@@ -94,9 +95,30 @@ def gravity_cases():
             print(name, n, meta["niter"])
 
 
+TRACE_CASES = [("C3D4", "nh", "force"), ("C3D8", "mr", "pressure"), ("C3D10", "yeoh", "dpressure"),
+               ("C3D20", "mr", "pressure"), ("C3D8", "nh", "dpressure"), ("C3D10", "nh", "force")]
+
+
+def trace_cases():
+    """``traces.npz``: the reference's benchmark record (||r||_2 after the
+    initial residual and after every line search, LBFGS.h:107-147) of its own
+    solve of six small cases, under the key ``<etype>_<mat>_<load>``."""
+    out = {}
+    for et, mat, load in TRACE_CASES:
+        case = mg.small_case(et, mat, load)
+        with tempfile.TemporaryDirectory() as td:
+            meta, _ = oracle.run_ref("solve", case.write(td), trace=True)
+        out[f"{et}_{mat}_{load}"] = meta["trace"]
+        print("trace", et, mat, load, meta["niter"], len(meta["trace"]))
+    np.savez_compressed(os.path.join(HERE, "traces.npz"), **out)
+
+
 def main():
     if sys.argv[1:] == ["gravity"]:
         gravity_cases()
+        return
+    if sys.argv[1:] == ["trace"]:
+        trace_cases()
         return
     rng = np.random.default_rng(20261203)
     for et in ETYPES:
@@ -156,6 +178,7 @@ def main():
         np.savez_compressed(os.path.join(HERE, f"piola_{mat}.npz"), F=F, P=P, C=np.array(C), kappa=kappa)
         print("piola", mat, kappa)
     gravity_cases()
+    trace_cases()
 
 
 if __name__ == "__main__":

@@ -139,3 +139,23 @@ def test_gravity_mass_totals(tmp_path):
         assert np.allclose(f, [0.0, 0.0, -9.8 * 2.0e5 * vol], rtol=1e-4, atol=1e-12)
         totals.append(f)
     assert np.allclose(totals[0], totals[1], rtol=1e-13, atol=1e-15)
+
+
+@pytest.mark.parametrize("key", list(np.load(golden_files("traces.npz")[0]).files))
+def test_trace_matches_reference(key, tmp_path):
+    """The restatement's convergence record against the reference's benchmark
+    vector (||r||_2 after the initial residual and after each line search).
+    Rounding differences grow along the iteration path, so the early records
+    agree tightly and the whole record to 1e-5 of the initial norm."""
+    from efem_b200 import meshgen as mg
+    ref = np.load(golden_files("traces.npz")[0])[key]
+    et, mat, load = key.split("_")
+    o = oracle.Oracle(oracle.read_case(mg.small_case(et, mat, load).write(str(tmp_path))))
+    _, info = o.solve(trace=1000)
+    t = info["trace"]
+    assert len(t) == info["niter"] + 1 and abs(len(t) - len(ref)) <= 2
+    assert t[0, 3] == 0.0 and np.all(t[1:, 3] != 0.0) and int(t[:, 4].sum()) == info["r_evals"]
+    k = min(len(t), len(ref))
+    rel = np.abs(t[:k, 1] - ref[:k]) / ref[:k]
+    assert rel[:20].max() <= 1e-8 and rel[:50].max() <= 1e-6
+    assert np.abs(t[:k, 1] - ref[:k]).max() <= 1e-5 * ref[0]
