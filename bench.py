@@ -23,6 +23,11 @@ oracle/_ref), timed on the host cores on bounded samples of the same solve.
 solves concurrent (efem_batch_solve), against the plain FP64 path solving the
 same models one after another.
 
+--workload cap: time-to-converge of the closed cylinder cap (C3D20 reduced
+integration, 9088 elements, 10 kPa cavity pressure) in mixed precision next
+to the FP64 path, with the mixed solution's error against FP64 converged to
+1e-10.
+
 --workload finger-adjoint: the adjoint gradient time instead (ms per
 gradient): the pneumatic finger, 50 688 C3D10 Yeoh elements with 30 kPa on
 its 8 chamber walls, J = u_z of the tip node, dJ/dtheta for every material
@@ -225,6 +230,73 @@ def run_adjoint_bench(args):
     model.close()
 
 
+# --------------------------------------------------------------------------- C3D20R cap, mixed vs FP64
+def run_cap_bench(args):
+    """Time-to-converge of the C3D20R cylinder cap, mixed precision vs FP64 (one GPU)."""
+    import torch
+    from efem_b200 import api, meshgen as mg
+    torch.cuda.set_device(0)
+    case = mg.cylinder_cap_c3d20()
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def build(precision, criterion=1e-6):
+        o = api.default_options()
+        o.precision = precision
+        o.residual_criterion = criterion
+        m = api.Model.from_case(case, o)
+        api.check(api.lib().efem_set_stream(m.h, api.ctypes.c_void_p(stream.cuda_stream)))
+        m.set_options(device_ptrs=1)
+        return m, torch.zeros(m.n_dof, dtype=torch.float64, device="cuda")
+
+    def timed(m, u, steps):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        infos = []
+        for k, (a, b) in enumerate(ev):
+            flush.fill_(float(k))
+            u.zero_()
+            a.record(stream)
+            infos.append(m.solve(u)[1])
+            b.record(stream)
+        torch.cuda.synchronize()
+        return float(np.mean([a.elapsed_time(b) for a, b in ev])), infos
+
+    t0 = time.time()
+    m32, u32 = build(api.MIXED)
+    m64, u64 = build(api.FP64)
+    for _ in range(max(1, args.warmup)):
+        timed(m32, u32, 1)
+        timed(m64, u64, 1)
+    setup_s = time.time() - t0
+    with ClockSampler(0) as clocks:
+        ms32, i32 = timed(m32, u32, args.steps)
+        ms64, i64 = timed(m64, u64, args.steps)
+    mref, uref = build(api.FP64, 1e-10)
+    mref.set_options(max_iterations=50000)
+    _, iref = mref.solve(uref)
+    rel = lambda a: float(torch.linalg.norm(a - uref) / torch.linalg.norm(uref))  # noqa: E731
+    r64_at_mixed = float(np.abs(m64.residual(u32.cpu().numpy())).max())
+    info = m32.info()
+    line = {"metric": "time-to-converge, mixed precision (C3D20R cylinder cap, 9088 el)", "value": ms32, "unit": "ms",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms32, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic (seeded structured mesh in the reference's input format)",
+            "config": {"workload": "hollow cylinder ri 20 mm, ro 25 mm, h 30 mm, 5 mm top plate; 64x4x24 shell + "
+                                   "butterfly plate; C3D20 reduced integration; NH C10 114 kPa, D1 1e-6; bottom "
+                                   "fixed; 10 kPa follower pressure on the cavity walls; residual 1e-6",
+                       "elements": info["n_elements"], "dof": m32.n_dof, "faces": info["n_faces"],
+                       "l2": "flushed (256 MB write) before every solve"},
+            "mixed": {"ms": ms32, "niter": float(np.mean([i["niter"] for i in i32])),
+                      "r_inf": i32[-1]["r_inf"], "rel_l2_vs_fp64_1e-10": rel(u32),
+                      "fp64_residual_at_mixed_solution": r64_at_mixed},
+            "fp64": {"ms": ms64, "niter": float(np.mean([i["niter"] for i in i64])),
+                     "r_inf": i64[-1]["r_inf"], "rel_l2_vs_fp64_1e-10": rel(u64)},
+            "fp64_over_mixed_time": ms64 / ms32,
+            "reference_solution": {"niter": iref["niter"], "r_inf": iref["r_inf"]},
+            "setup_s": setup_s, "clocks": clocks.summary()}
+    print(json.dumps(line))
+
+
 # --------------------------------------------------------------------------- batched solves
 def run_batch_bench(args):
     """Mixed-precision batched solves of 256 uneven beams vs the plain FP64 path."""
@@ -322,7 +394,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--host-loop", action="store_true",
                     help="drive the L-BFGS iterations from the host (same kernels; for launch-list profiling)")
-    ap.add_argument("--workload", default="beam", choices=["beam", "finger-adjoint", "batch"])
+    ap.add_argument("--workload", default="beam", choices=["beam", "finger-adjoint", "batch", "cap"])
     args = ap.parse_args()
     if args.impl == "reference":
         if args.workload != "beam":
@@ -333,6 +405,8 @@ def main():
         return run_adjoint_bench(args)
     if args.workload == "batch":
         return run_batch_bench(args)
+    if args.workload == "cap":
+        return run_cap_bench(args)
 
     import torch
     import torch.distributed as dist

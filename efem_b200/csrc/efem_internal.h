@@ -66,6 +66,7 @@ constexpr int MAX_MATS = 16;
 struct DevBlock {
     int kind = 0, nen = 0, ngp = 0, n = 0;
     int threads[2] = { 128, 128 };  // element-kernel CTA size per precision (FP64, FP32), from the autotuner
+    size_t slot0 = 0;             // deterministic scatter: first contribution slot, slot = slot0 + a * n + e
     int* conn = nullptr;          // [nen][n]
     int* mat = nullptr;           // [n]
     double* vol = nullptr;        // [n]
@@ -91,6 +92,7 @@ struct DevFaces {
     float* J0inv_f = nullptr;
     double* load = nullptr;       // [n][4]: directed flag, value / vector
     int* load_idx = nullptr;      // [n]: index of the face's load among the pressure loads
+    size_t slot0 = 0;             // deterministic scatter: first contribution slot, slot = slot0 + q * n + f
     // face tables for this element kind
     int n_tables = 0;
     int* t_ngp = nullptr;         // [n_tables]
@@ -143,6 +145,13 @@ struct Model {
     double* d_fext = nullptr;         // [3*n_free]
     double* d_u = nullptr;            // staging for host-pointer calls
     double* d_r = nullptr;
+    // deterministic scatter (opts.deterministic): nodal contributions of every
+    // (element, node) and (face, node) pair in contrib[3][n_slots]; free node i
+    // sums slots gidx[gptr[i] .. gptr[i+1]) in ascending slot order
+    double* d_contrib = nullptr;
+    int* d_gptr = nullptr;
+    int* d_gidx = nullptr;
+    size_t n_slots = 0;
 
     long long launches = 0;           // kernels launched by this model (diagnostics)
     long long epoch = 0;              // bumped when device arrays that captured graphs point to are rebuilt
@@ -209,6 +218,8 @@ efem_status launch_residual_on(Model& m, const double* d_u, double* d_r, cudaStr
 
 // ------------------------------------------------------------------ solver (solver.cu)
 efem_status run_solve(Model& m, double* d_u, efem_solve_info* info);
+efem_status build_gather(Model& m);
+void free_gather(Model& m);
 efem_status solve_trace(Model& m, double* out, int capacity, int* n_records);
 void free_solver(Model& m);
 // Held while a CUDA graph is captured and instantiated, so that solves of

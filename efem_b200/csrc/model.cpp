@@ -207,6 +207,7 @@ Model::~Model()
     dev_free(d_fext);
     dev_free(d_u);
     dev_free(d_r);
+    free_gather(*this);
     if (stream && own_stream) cudaStreamDestroy(stream);
 }
 
@@ -508,6 +509,7 @@ namespace efem {
 efem_status build_blocks(Model& m)
 {
     m.epoch++;
+    free_gather(m);
     const bool reduced = m.opts.integration == 1;
     for (auto& b : m.blocks) {
         dev_free(b.conn);
@@ -646,6 +648,7 @@ efem_status ensure_device(Model& m)
     }
 #undef UP
     m.on_device = true;
+    if (m.opts.deterministic && !m.d_contrib && (s = build_gather(m)) != EFEM_OK) return s;
     if (m.tuned_threads != m.opts.elem_threads) {
         // element kernels are tuned before any graph captures them (a retune
         // invalidates captured graphs through the epoch)

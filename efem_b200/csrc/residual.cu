@@ -14,11 +14,16 @@
 //      S_g = V_e w_g P J0^{-T} (3x3) into shared memory;
 //   3. node: thread (element, node) reduces r_a = sum_g S_g dN_ga and adds it
 //      to the global residual with FP64 atomics (red.global.add.f64) or, in
-//      deterministic mode, writes it to a per-element buffer that a node-major
-//      gather kernel sums in a fixed order.
+//      deterministic mode (opts.deterministic), stores it in its own slot of a
+//      contribution buffer that k_gather then sums per node in ascending slot
+//      order, so the residual is bitwise repeatable.
 // The arithmetic type T is double (FP64 path) or float (mixed path); the
 // global residual is always accumulated in FP64.
 #include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <vector>
 
 #include "efem_internal.h"
 #include "mechanics.cuh"
@@ -41,6 +46,14 @@ struct ElemArgs {
     const MatParams<T>* __restrict__ mats;
     const double* __restrict__ u;     // [3*n_free]
     double* __restrict__ r;           // [3*n_free]
+    double* __restrict__ contrib;     // deterministic scatter: [3][n_slots], or null for atomics
+    size_t n_slots, slot0;
+};
+
+// where an (element or face, node) pair's nodal force goes
+struct Scatter {
+    double* contrib = nullptr;
+    size_t n_slots = 0, slot0 = 0;
 };
 
 // BLK threads per CTA (64, 128 or 256, picked per element block by the
@@ -147,9 +160,16 @@ __global__ void __launch_bounds__(BLK) k_elem_residual(ElemArgs<T> a)
             r1 += S[3] * d0 + S[4] * d1 + S[5] * d2;
             r2 += S[6] * d0 + S[7] * d1 + S[8] * d2;
         }
-        atomicAdd(a.r + 3 * node, static_cast<double>(r0));
-        atomicAdd(a.r + 3 * node + 1, static_cast<double>(r1));
-        atomicAdd(a.r + 3 * node + 2, static_cast<double>(r2));
+        if (a.contrib) {  // consecutive threads: consecutive elements, consecutive slots
+            const size_t sl = a.slot0 + static_cast<size_t>(nd) * a.n + e;
+            a.contrib[sl] = static_cast<double>(r0);
+            a.contrib[a.n_slots + sl] = static_cast<double>(r1);
+            a.contrib[2 * a.n_slots + sl] = static_cast<double>(r2);
+        } else {
+            atomicAdd(a.r + 3 * node, static_cast<double>(r0));
+            atomicAdd(a.r + 3 * node + 1, static_cast<double>(r1));
+            atomicAdd(a.r + 3 * node + 2, static_cast<double>(r2));
+        }
     }
 }
 
@@ -167,6 +187,8 @@ struct FaceArgs {
     const T* __restrict__ t_dN;       // [t][MAX_FGP][NEN][3]
     const double* __restrict__ u;
     double* __restrict__ r;
+    double* __restrict__ contrib;     // deterministic scatter: [3][n_slots], or null for atomics
+    size_t n_slots, slot0;
 };
 
 // One thread per face: cof(F_g) A0 at every face point, then the nodal forces
@@ -246,10 +268,36 @@ __global__ void __launch_bounds__(kBlock) k_face_residual(FaceArgs<T> a)
             f1 = L[1] * static_cast<double>(v1);
             f2 = L[1] * static_cast<double>(v2);
         }
-        atomicAdd(a.r + 3 * node[q], -f0);
-        atomicAdd(a.r + 3 * node[q] + 1, -f1);
-        atomicAdd(a.r + 3 * node[q] + 2, -f2);
+        if (a.contrib) {
+            const size_t sl = a.slot0 + static_cast<size_t>(q) * a.n + f;
+            a.contrib[sl] = -f0;
+            a.contrib[a.n_slots + sl] = -f1;
+            a.contrib[2 * a.n_slots + sl] = -f2;
+        } else {
+            atomicAdd(a.r + 3 * node[q], -f0);
+            atomicAdd(a.r + 3 * node[q] + 1, -f1);
+            atomicAdd(a.r + 3 * node[q] + 2, -f2);
+        }
     }
+}
+
+// Deterministic scatter, second half: free node i adds its contributions in
+// ascending slot order, r_i += sum_k contrib[gidx[k]], one thread per node
+__global__ void __launch_bounds__(kBlock) k_gather(int n_free, const int* __restrict__ gptr,
+    const int* __restrict__ gidx, const double* __restrict__ contrib, size_t n_slots, double* __restrict__ r)
+{
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    if (i >= n_free) return;
+    double s0 = r[3 * i], s1 = r[3 * i + 1], s2 = r[3 * i + 2];
+    for (int k = gptr[i]; k < gptr[i + 1]; k++) {
+        const size_t sl = static_cast<size_t>(__ldg(gidx + k));
+        s0 += __ldg(contrib + sl);
+        s1 += __ldg(contrib + n_slots + sl);
+        s2 += __ldg(contrib + 2 * n_slots + sl);
+    }
+    r[3 * i] = s0;
+    r[3 * i + 1] = s1;
+    r[3 * i + 2] = s2;
 }
 
 template <int NEN, int NGP, typename T, int BLK>
@@ -261,9 +309,9 @@ void launch_elem_blk(const ElemArgs<T>& a, cudaStream_t st)
 
 template <int NEN, int NGP, typename T>
 void launch_elem(const DevBlock& b, const MatParams<T>* mats, const T* vol, const T* J0, const T* dN, const T* gw,
-    int n_free, const double* u, double* r, cudaStream_t st, int threads)
+    int n_free, const double* u, double* r, cudaStream_t st, int threads, const Scatter& sc)
 {
-    ElemArgs<T> a { b.n, n_free, b.conn, b.mat, vol, J0, dN, gw, mats, u, r };
+    ElemArgs<T> a { b.n, n_free, b.conn, b.mat, vol, J0, dN, gw, mats, u, r, sc.contrib, sc.n_slots, sc.slot0 };
     if (threads == 64) launch_elem_blk<NEN, NGP, T, 64>(a, st);
     else if (threads == 256) launch_elem_blk<NEN, NGP, T, 256>(a, st);
     else launch_elem_blk<NEN, NGP, T, 128>(a, st);
@@ -271,12 +319,12 @@ void launch_elem(const DevBlock& b, const MatParams<T>* mats, const T* vol, cons
 
 template <typename T>
 void dispatch_elem(const DevBlock& b, const MatParams<T>* mats, const T* vol, const T* J0, const T* dN, const T* gw,
-    int n_free, const double* u, double* r, cudaStream_t st, int threads)
+    int n_free, const double* u, double* r, cudaStream_t st, int threads, const Scatter& sc = Scatter())
 {
-#define CASE(NEN, NGP)                                                                 \
-    if (b.nen == NEN && b.ngp == NGP) {                                                \
-        launch_elem<NEN, NGP, T>(b, mats, vol, J0, dN, gw, n_free, u, r, st, threads); \
-        return;                                                                        \
+#define CASE(NEN, NGP)                                                                     \
+    if (b.nen == NEN && b.ngp == NGP) {                                                    \
+        launch_elem<NEN, NGP, T>(b, mats, vol, J0, dN, gw, n_free, u, r, st, threads, sc); \
+        return;                                                                            \
     }
     CASE(4, 1)
     CASE(10, 4)
@@ -290,9 +338,10 @@ void dispatch_elem(const DevBlock& b, const MatParams<T>* mats, const T* vol, co
 
 template <typename T>
 void dispatch_face(const DevFaces& f, const T* J0, const T* tw, const T* tN, const T* tdN, int n_free, const double* u,
-    double* r, cudaStream_t st)
+    double* r, cudaStream_t st, const Scatter& sc)
 {
-    FaceArgs<T> a { f.n, n_free, f.conn, f.table, f.A0, J0, f.load, f.t_ngp, tw, tN, tdN, u, r };
+    FaceArgs<T> a { f.n, n_free, f.conn, f.table, f.A0, J0, f.load, f.t_ngp, tw, tN, tdN, u, r, sc.contrib, sc.n_slots,
+        sc.slot0 };
     const int grid = (f.n + kBlock - 1) / kBlock;
     switch (f.nen) {
     case 4: k_face_residual<4, T><<<grid, kBlock, 0, st>>>(a); break;
@@ -372,24 +421,96 @@ efem_status launch_residual_on(Model& m, const double* d_u, double* d_r, cudaStr
         m.launches++;
     }
     const bool mixed = m.opts.precision == EFEM_MIXED;
+    const bool det = m.opts.deterministic != 0;
+    if (det && !m.d_contrib) {
+        set_error("deterministic scatter requested but its tables are not built");
+        return EFEM_ERR_ARG;
+    }
     for (auto& b : m.blocks) {
         if (b.n == 0) continue;
         m.launches++;
+        Scatter sc;
+        if (det) sc = Scatter { m.d_contrib, m.n_slots, b.slot0 };
         if (mixed)
             dispatch_elem<float>(b, m.d_mats_f, b.vol_f, b.J0inv_f, b.dN_f, b.gw_f, m.n_free, d_u, d_r, stream,
-                b.threads[1]);
+                b.threads[1], sc);
         else
-            dispatch_elem<double>(b, m.d_mats, b.vol, b.J0inv, b.dN, b.gw, m.n_free, d_u, d_r, stream, b.threads[0]);
+            dispatch_elem<double>(b, m.d_mats, b.vol, b.J0inv, b.dN, b.gw, m.n_free, d_u, d_r, stream, b.threads[0], sc);
     }
     for (auto& f : m.faces) {
         if (f.n == 0) continue;
         m.launches++;
+        Scatter sc;
+        if (det) sc = Scatter { m.d_contrib, m.n_slots, f.slot0 };
         if (mixed)
-            dispatch_face<float>(f, f.J0inv_f, f.t_w_f, f.t_N_f, f.t_dN_f, m.n_free, d_u, d_r, stream);
+            dispatch_face<float>(f, f.J0inv_f, f.t_w_f, f.t_N_f, f.t_dN_f, m.n_free, d_u, d_r, stream, sc);
         else
-            dispatch_face<double>(f, f.J0inv, f.t_w, f.t_N, f.t_dN, m.n_free, d_u, d_r, stream);
+            dispatch_face<double>(f, f.J0inv, f.t_w, f.t_N, f.t_dN, m.n_free, d_u, d_r, stream, sc);
+    }
+    if (det) {
+        k_gather<<<(m.n_free + kBlock - 1) / kBlock, kBlock, 0, stream>>>(m.n_free, m.d_gptr, m.d_gidx, m.d_contrib,
+            m.n_slots, d_r);
+        m.launches++;
     }
     EFEM_CUDA(cudaGetLastError());
+    return EFEM_OK;
+}
+
+void free_gather(Model& m)
+{
+    dev_free(m.d_contrib);
+    dev_free(m.d_gptr);
+    dev_free(m.d_gidx);
+    m.n_slots = 0;
+}
+
+// Slots of the deterministic scatter: element block b owns slots
+// [slot0, slot0 + nen n) in node-major order, then each face group likewise;
+// the gather lists of every free node are sorted by slot, so each node's sum
+// has one fixed order whatever the launch configuration.
+efem_status build_gather(Model& m)
+{
+    free_gather(m);
+    size_t slots = 0;
+    for (auto& b : m.blocks) {
+        b.slot0 = slots;
+        slots += static_cast<size_t>(b.nen) * b.n;
+    }
+    for (auto& f : m.faces) {
+        f.slot0 = slots;
+        slots += static_cast<size_t>(f.nen) * f.n;
+    }
+    if (slots >= static_cast<size_t>(INT_MAX)) {
+        set_error("too many element-node pairs for the deterministic scatter");
+        return EFEM_ERR_ARG;
+    }
+    std::vector<int> cnt(static_cast<size_t>(m.n_free) + 1, 0);
+    auto node_of_slot = [&](auto&& visit) {
+        for (auto& b : m.blocks)
+            for (int a = 0; a < b.nen; a++)
+                for (int e = 0; e < b.n; e++)
+                    visit(b.h_conn[static_cast<size_t>(e) * b.nen + a], b.slot0 + static_cast<size_t>(a) * b.n + e);
+        for (auto& f : m.faces)
+            for (int q = 0; q < f.nen; q++)
+                for (int k = 0; k < f.n; k++)
+                    visit(f.h_conn[static_cast<size_t>(q) * f.n + k], f.slot0 + static_cast<size_t>(q) * f.n + k);
+    };
+    node_of_slot([&](int node, size_t) {
+        if (node < m.n_free) cnt[node + 1]++;
+    });
+    for (int i = 0; i < m.n_free; i++) cnt[i + 1] += cnt[i];
+    std::vector<int> idx(static_cast<size_t>(cnt[m.n_free]));
+    std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+    node_of_slot([&](int node, size_t sl) {  // visited in ascending slot order
+        if (node < m.n_free) idx[fill[node]++] = static_cast<int>(sl);
+    });
+    for (int i = 0; i < m.n_free; i++) std::sort(idx.begin() + cnt[i], idx.begin() + cnt[i + 1]);
+    efem_status s;
+    if ((s = dev_alloc(&m.d_contrib, 3 * std::max<size_t>(slots, 1))) != EFEM_OK) return s;
+    if ((s = dev_upload(&m.d_gptr, cnt)) != EFEM_OK) return s;
+    if (idx.empty()) idx.push_back(0);
+    if ((s = dev_upload(&m.d_gidx, idx)) != EFEM_OK) return s;
+    m.n_slots = slots;
     return EFEM_OK;
 }
 

@@ -890,7 +890,7 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
     const double eps = m.opts.residual_criterion;
     std::memset(info, 0, sizeof(*info));
     const long long launches0 = m.launches;
-    const long long per_res = 1 + static_cast<long long>(m.blocks.size() + m.faces.size());
+    const long long per_res = 1 + static_cast<long long>(m.blocks.size() + m.faces.size()) + (m.opts.deterministic ? 1 : 0);
     double ms_pc = 0.0;
     double rinf = 0.0, xinf = 0.0;
     int k = 1;
@@ -964,7 +964,8 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
             w.epoch = m.epoch;
         }
         const bool host_loop = m.opts.host_loop != 0;
-        const auto key = std::make_pair(x, (ok ? 1 : 0) | (m.opts.precision << 1) | (host_loop ? 4 : 0));
+        const auto key = std::make_pair(x, (ok ? 1 : 0) | (m.opts.precision << 1) | (host_loop ? 4 : 0)
+            | (m.opts.deterministic ? 8 : 0));
         if (!w.graphs.count(key) && w.graphs.size() >= 8) drop_graphs(w);  // many distinct solution pointers
         SolverWS::Graphs& gr = w.graphs[key];
         if (!gr.first) {
