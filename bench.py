@@ -275,7 +275,7 @@ def run_cap_bench(args):
     mref.set_options(max_iterations=50000)
     _, iref = mref.solve(uref)
     rel = lambda a: float(torch.linalg.norm(a - uref) / torch.linalg.norm(uref))  # noqa: E731
-    r64_at_mixed = float(np.abs(m64.residual(u32.cpu().numpy())).max())
+    r64_at_mixed = float(m64.residual(u32).abs().max())  # device_ptrs: CUDA tensors in and out
     info = m32.info()
     line = {"metric": "time-to-converge, mixed precision (C3D20R cylinder cap, 9088 el)", "value": ms32, "unit": "ms",
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms32, "higher_is_better": False,

@@ -1446,6 +1446,19 @@ extern "C" efem_status efem_precond_apply_noalloc(void* model, double* d_v)
     if (st != EFEM_OK) return st;
     EFEM_CUDA(cudaSetDevice(m.device));
     if (S.n == 0) return EFEM_OK;
+    cudaStreamCaptureStatus cs0 = cudaStreamCaptureStatusNone;
+    EFEM_CUDA(cudaStreamIsCapturing(m.stream, &cs0));
+    if (cs0 == cudaStreamCaptureStatusNone) {  // d_v must be memory this GPU addresses (not checked while capturing)
+        cudaPointerAttributes a {};
+        const bool ok = cudaPointerGetAttributes(&a, d_v) == cudaSuccess
+            && (a.type == cudaMemoryTypeManaged || (a.type == cudaMemoryTypeDevice && a.device == m.device)
+                || (a.type == cudaMemoryTypeHost && a.devicePointer != nullptr));
+        if (!ok) {
+            cudaGetLastError();
+            set_error("d_v is not device memory of the model's GPU");
+            return EFEM_ERR_ARG;
+        }
+    }
     int* counters = reinterpret_cast<int*>(scratch + 2 * n3 + S.upd_size);
     const SolveBufs b { scratch, scratch + n3, scratch + 2 * n3, counters };
     enqueue_solve(P, args_of(P), b, d_v, m.stream);

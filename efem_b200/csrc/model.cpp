@@ -733,10 +733,35 @@ efem_status guard(void* h, Model** out)
     return EFEM_OK;
 }
 
+// With device_ptrs, a vector argument must be memory this model's GPU can
+// address: a device allocation on the model's device, managed memory, or
+// mapped pinned host memory.  Anything else (pageable host memory, another
+// GPU's buffer) is refused here rather than read by a kernel.
+efem_status dev_vec(const Model& m, const void* p, const char* what)
+{
+    cudaPointerAttributes a {};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        efem::set_error(std::string(what) + ": not a CUDA pointer (device_ptrs is set)");
+        return EFEM_ERR_ARG;
+    }
+    const bool ok = a.type == cudaMemoryTypeManaged || (a.type == cudaMemoryTypeDevice && a.device == m.device)
+        || (a.type == cudaMemoryTypeHost && a.devicePointer != nullptr);
+    if (!ok) {
+        efem::set_error(std::string(what) + (a.type == cudaMemoryTypeDevice
+            ? ": device memory of another GPU (device_ptrs is set)"
+            : ": host memory the GPU cannot address (device_ptrs is set; pass device memory)"));
+        return EFEM_ERR_ARG;
+    }
+    return EFEM_OK;
+}
+
 // copy a vector argument in (device pointer or host pointer) to a device buffer
 efem_status vec_in(Model& m, const double* src, double** dst, double* staging)
 {
     if (m.opts.device_ptrs) {
+        efem_status s = dev_vec(m, src, "input vector");
+        if (s != EFEM_OK) return s;
         *dst = const_cast<double*>(src);
         return EFEM_OK;
     }
@@ -980,6 +1005,7 @@ efem_status efem_residual(void* model, const double* u, double* r)
     if (!u || !r) return EFEM_ERR_ARG;
     s = efem::ensure_device(*m);
     if (s != EFEM_OK) return s;
+    if (m->opts.device_ptrs && (s = dev_vec(*m, r, "r")) != EFEM_OK) return s;
     double *du, *dr = m->opts.device_ptrs ? r : m->d_r;
     s = vec_in(*m, u, &du, m->d_u);
     if (s != EFEM_OK) return s;
@@ -1000,6 +1026,7 @@ static efem_status hvp_call(void* model, const double* u, const double* v, doubl
     if ((s = efem::ensure_device(*m)) != EFEM_OK) return s;
     double *du, *dv, *io = nullptr;
     if ((s = efem::adjoint_io(*m, &io)) != EFEM_OK) return s;
+    if (m->opts.device_ptrs && (s = dev_vec(*m, out, "output vector")) != EFEM_OK) return s;
     double* dout = m->opts.device_ptrs ? out : io;
     if ((s = vec_in(*m, u, &du, m->d_u)) != EFEM_OK) return s;
     if ((s = vec_in(*m, v, &dv, m->d_r)) != EFEM_OK) return s;
@@ -1029,6 +1056,7 @@ efem_status efem_residual_param_derivative(void* model, const double* u, int k, 
     if ((s = efem::ensure_device(*m)) != EFEM_OK) return s;
     double *du, *io = nullptr;
     if ((s = efem::adjoint_io(*m, &io)) != EFEM_OK) return s;
+    if (m->opts.device_ptrs && (s = dev_vec(*m, dR, "dR")) != EFEM_OK) return s;
     double* dout = m->opts.device_ptrs ? dR : io;
     if ((s = vec_in(*m, u, &du, m->d_u)) != EFEM_OK) return s;
     if ((s = efem::residual_param_derivative(*m, du, k, dout)) != EFEM_OK) return s;
@@ -1052,6 +1080,7 @@ efem_status efem_adjoint(void* model, const double* u, const double* dJdu, doubl
     if ((s = efem::adjoint_io(*m, &io)) != EFEM_OK) return s;
     if ((s = vec_in(*m, u, &du, m->d_u)) != EFEM_OK) return s;
     if ((s = vec_in(*m, dJdu, &dg, m->d_r)) != EFEM_OK) return s;
+    if (lambda && m->opts.device_ptrs && (s = dev_vec(*m, lambda, "lambda")) != EFEM_OK) return s;
     double* dl = lambda ? (m->opts.device_ptrs ? lambda : io) : nullptr;
     if ((s = efem::adjoint(*m, du, dg, dJdtheta, dl, info)) != EFEM_OK) return s;
     if (lambda && !m->opts.device_ptrs)
@@ -1071,6 +1100,7 @@ efem_status efem_write_vtk(void* model, const double* u, const char* path)
         uh.resize(3 * static_cast<size_t>(m->n_free));
         if (m->opts.device_ptrs) {
             if ((s = efem::ensure_device(*m)) != EFEM_OK) return s;
+            if ((s = dev_vec(*m, u, "u")) != EFEM_OK) return s;
             EFEM_CUDA(cudaMemcpyAsync(uh.data(), u, sizeof(double) * uh.size(), cudaMemcpyDeviceToHost, m->stream));
             EFEM_CUDA(cudaStreamSynchronize(m->stream));
         } else {
@@ -1161,6 +1191,7 @@ efem_status efem_precond_apply(void* model, double* v)
         return EFEM_ERR_NAN;
     }
     double* dv = v;
+    if (m->opts.device_ptrs && (s = dev_vec(*m, v, "v")) != EFEM_OK) return s;
     if (!m->opts.device_ptrs) {
         dv = m->d_r;
         EFEM_CUDA(cudaMemcpyAsync(dv, v, sizeof(double) * 3 * m->n_free, cudaMemcpyHostToDevice, m->stream));
@@ -1184,6 +1215,7 @@ efem_status efem_solve(void* model, double* u_inout, efem_solve_info* info)
     if (!info) info = &tmp;
     std::memset(info, 0, sizeof(*info));
     double* du = u_inout;
+    if (m->opts.device_ptrs && (s = dev_vec(*m, u_inout, "u")) != EFEM_OK) return s;
     if (!m->opts.device_ptrs) {
         du = m->d_u;
         EFEM_CUDA(cudaMemcpyAsync(du, u_inout, sizeof(double) * 3 * m->n_free, cudaMemcpyHostToDevice, m->stream));

@@ -83,3 +83,21 @@ def test_element_kernel_variants_agree(path, tmp_path):
         r = m.residual(u)  # the next device call applies the forced size
         assert m.info()["elem_threads_fp64"] == t
         assert np.linalg.norm(r - r_auto) <= 1e-13 * scale
+
+
+def test_device_ptrs_refuses_host_memory():
+    """With device_ptrs set, pageable host arrays are refused at the ABI
+    (cudaPointerGetAttributes) before any kernel could read them."""
+    import torch
+    m = api.Model.from_case(mg.small_case("C3D8", "nh", "force"))
+    m.set_options(device_ptrs=1)
+    u_host = np.zeros(m.n_dof)
+    with pytest.raises(api.EfemError, match="host memory"):
+        m.residual(u_host)
+    ut = torch.zeros(m.n_dof, dtype=torch.float64, device="cuda")
+    with pytest.raises(api.EfemError, match="host memory"):
+        m.residual(ut, np.zeros(m.n_dof))
+    with pytest.raises(api.EfemError, match="host memory"):
+        m.solve(u_host)
+    r = m.residual(ut)  # the model stays usable
+    assert torch.isfinite(r).all()
