@@ -51,7 +51,8 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kMaxBlocks = 592;  // 4 x 148 SMs
 constexpr int kMaxHist = 64;
-constexpr int kRowBlocks = 128;  // CTAs per history slot in the dot-product passes
+constexpr int kRowBlocks = 128;  // CTAs per history slot in the dot-product passes (m > kMaxFast)
+constexpr int kMaxFast = 8;      // history lengths with the 1D-grid passes k_pass1_m / k_pass3_m
 
 // device-resident solver state
 struct Scalars {
@@ -398,6 +399,162 @@ __global__ void __launch_bounds__(kThreads) k_pass1(const double* __restrict__ x
     }
 }
 
+// Sums of NV values over a 1D grid in a fixed order: every CTA stores its
+// block sums; the last CTA to finish adds them up, one warp per value (lanes
+// over the CTAs in order, then a fixed shuffle tree), into out[0, NV).
+// Returns true in every thread of the last CTA.
+template <int NV>
+__device__ bool grid_sums(double* v, double* partials, unsigned int* counter, double* out)
+{
+    __shared__ bool last;
+    int ops[NV];
+#pragma unroll
+    for (int k = 0; k < NV; k++) ops[k] = 0;
+    block_reduce<NV>(v, ops);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; k++) partials[blockIdx.x * NV + k] = v[k];
+        __threadfence();
+        last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int k = w; k < NV; k += kThreads / 32) {
+        double x = 0.0;
+        for (int b = lane; b < static_cast<int>(gridDim.x); b += 32) x += *(volatile double*)&partials[b * NV + k];
+        x = warp_sum(x);
+        if (lane == 0) out[k] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *counter = 0u;
+    return true;
+}
+
+// Pass 1 for a history of M <= 8 pairs on a 1D grid: each thread reads x, xp,
+// r, rp once for all slots (the 2D k_pass1 re-reads them per slot) and keeps
+// the 3M + 2 dot products in registers; the last CTA runs the same recursion.
+template <int M>
+__global__ void __launch_bounds__(kThreads) k_pass1_m(const double* __restrict__ x, const double* __restrict__ xp,
+    const double* __restrict__ r, const double* __restrict__ rp, double* __restrict__ Sh, double* __restrict__ Yh,
+    size_t n, Scalars* S, double* partials)
+{
+    constexpr int NV = 3 * M + 2;
+    const int m = M;
+    const int loc = S->ptr % m;
+    const int ncorr = S->ncorr < m ? S->ncorr + 1 : m;
+    double v[NV];
+#pragma unroll
+    for (int k = 0; k < NV; k++) v[k] = 0.0;
+    double* snew = Sh + loc * n;
+    double* ynew = Yh + loc * n;
+    GRID_STRIDE(i, n)
+    {
+        const double si = x[i] - xp[i], ri = r[i], yi = ri - rp[i];
+        snew[i] = si;
+        ynew[i] = yi;
+        v[3 * M] += si * yi;
+        v[3 * M + 1] += yi * yi;
+#pragma unroll
+        for (int j = 0; j < M; j++) {
+            if (j < ncorr) {
+                const bool self = j == loc;
+                const double sj = self ? si : Sh[j * n + i], yj = self ? yi : Yh[j * n + i];
+                v[3 * j] += si * yj;      // s_new . y_j
+                v[3 * j + 1] += sj * yi;  // s_j . y_new
+                v[3 * j + 2] -= sj * ri;  // s_j . q0
+            }
+        }
+    }
+    __shared__ double tot[NV];
+    if (!grid_sums<NV>(v, partials, &S->counter[2], tot)) return;
+    extern __shared__ double dyn[];
+    double* sG = dyn;
+    double* sys = dyn + m * m;
+    double* sal = sys + m;
+    const int tid = threadIdx.x;
+    for (int q = tid; q < m * m; q += kThreads) sG[q] = S->G[q / m][q % m];
+    for (int j = tid; j < m; j += kThreads) sys[j] = S->ys[j];
+    __syncthreads();
+    const double ys = tot[3 * M], yy = tot[3 * M + 1];
+    for (int j = tid; j < ncorr; j += kThreads) {
+        sG[loc * m + j] = tot[3 * j];
+        sG[j * m + loc] = tot[3 * j + 1];
+    }
+    __syncthreads();
+    if (tid == 0) {
+        sG[loc * m + loc] = ys;
+        sys[loc] = ys;
+        for (int i = 0; i < ncorr; i++) {  // first loop (LBFGSMat.h:106-113): newest slot first
+            const int j = ((loc - i) % m + m) % m;
+            double t = tot[3 * j + 2];
+            for (int k = 0; k < i; k++) {
+                const int jk = ((loc - k) % m + m) % m;
+                t -= sal[jk] * sG[j * m + jk];
+            }
+            sal[j] = t / sys[j];
+        }
+        S->theta = yy / ys;
+        S->ptr = loc + 1;
+        S->ncorr = ncorr;
+        S->ys[loc] = ys;
+    }
+    __syncthreads();
+    for (int j = tid; j < ncorr; j += kThreads) {
+        S->G[loc][j] = sG[loc * m + j];
+        S->G[j][loc] = sG[j * m + loc];
+        S->alpha[j] = sal[j];
+    }
+}
+
+// Pass 3 for M <= 8 on a 1D grid: z read once for all slots
+template <int M>
+__global__ void __launch_bounds__(kThreads) k_pass3_m(const double* __restrict__ z, const double* __restrict__ Yh,
+    size_t n, Scalars* S, double* partials, int time_pc)
+{
+    const int m = M, ncorr = S->ncorr;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && time_pc) S->t_pc += gtimer() - S->t0_pc;  // H0 just ended
+    double v[M];
+#pragma unroll
+    for (int k = 0; k < M; k++) v[k] = 0.0;
+    GRID_STRIDE(i, n)
+    {
+        const double zi = z[i];
+#pragma unroll
+        for (int j = 0; j < M; j++)
+            if (j < ncorr) v[j] += Yh[j * n + i] * zi;
+    }
+    __shared__ double tot[M];
+    if (!grid_sums<M>(v, partials, &S->counter[3], tot)) return;
+    extern __shared__ double dyn[];
+    double* sG = dyn;
+    double* sys = dyn + m * m;
+    double* sal = sys + m;
+    double* scf = sal + m;
+    const int tid = threadIdx.x;
+    for (int q = tid; q < m * m; q += kThreads) sG[q] = S->G[q / m][q % m];
+    for (int j = tid; j < m; j += kThreads) {
+        sys[j] = S->ys[j];
+        sal[j] = S->alpha[j];
+    }
+    __syncthreads();
+    if (tid == 0) {  // second loop (LBFGSMat.h:121-128), oldest pair first
+        const int ptr = S->ptr;
+        for (int o = 0; o < ncorr; o++) {
+            const int j = ((ptr - ncorr + o) % m + m) % m;
+            double t = tot[j];
+            for (int p = 0; p < o; p++) {
+                const int jp = ((ptr - ncorr + p) % m + m) % m;
+                t += scf[jp] * sG[jp * m + j];
+            }
+            scf[j] = sal[j] - t / sys[j];
+        }
+    }
+    __syncthreads();
+    for (int j = tid; j < ncorr; j += kThreads) S->coef[j] = scf[j];
+}
+
 // Pass 2: q = (q0 - sum_j alpha_j y_j) [/ theta when H0 = I / theta]; also
 // clears the preconditioner solve's counters for the H0 application that follows
 __global__ void __launch_bounds__(kThreads) k_pass2(double* __restrict__ q, const double* __restrict__ r,
@@ -669,7 +826,8 @@ static efem_status alloc_ws(Model& m)
         if ((s = dev_alloc(p, n)) != EFEM_OK) return s;
     if ((s = dev_alloc(&w.S, n * w.m)) != EFEM_OK) return s;
     if ((s = dev_alloc(&w.Y, n * w.m)) != EFEM_OK) return s;
-    const size_t np = std::max<size_t>(static_cast<size_t>(kMaxBlocks) * 5, static_cast<size_t>(kRowBlocks) * (w.m + 1) * 3);
+    const size_t np = std::max<size_t>(static_cast<size_t>(kMaxBlocks) * (3 * kMaxFast + 2),
+        static_cast<size_t>(kRowBlocks) * (w.m + 1) * 3);
     if ((s = dev_alloc(&w.partials, np)) != EFEM_OK) return s;
     if ((s = dev_alloc(&w.sums, 3 * static_cast<size_t>(w.m + 1))) != EFEM_OK) return s;
     EFEM_CUDA(cudaMalloc(&w.sc, sizeof(Scalars)));
@@ -720,7 +878,13 @@ efem_status enqueue_body(Model& m, SolverWS& w, double* x, bool use_factor, cuda
     const int mm = w.m;
     const dim3 g1(row_blocks(n), mm + 1), g3(row_blocks(n), mm);
     const size_t sm1 = sizeof(double) * (mm * mm + 2 * mm), sm3 = sizeof(double) * (mm * mm + 3 * mm);
-    k_pass1<<<g1, kThreads, sm1, st>>>(x, w.xp, w.r, w.rp, w.S, w.Y, n, mm, w.sc, w.partials, w.sums);
+    const int G = grid_for(n);
+    switch (mm) {
+#define P1(M) case M: k_pass1_m<M><<<G, kThreads, sm1, st>>>(x, w.xp, w.r, w.rp, w.S, w.Y, n, w.sc, w.partials); break;
+        P1(1) P1(2) P1(3) P1(4) P1(5) P1(6) P1(7) P1(8)
+#undef P1
+    default: k_pass1<<<g1, kThreads, sm1, st>>>(x, w.xp, w.r, w.rp, w.S, w.Y, n, mm, w.sc, w.partials, w.sums);
+    }
     int* clear = nullptr;
     int n_clear = 0;
     if (use_factor) precond_counters(m, &clear, &n_clear);
@@ -729,7 +893,12 @@ efem_status enqueue_body(Model& m, SolverWS& w, double* x, bool use_factor, cuda
         efem_status s = precond_enqueue(m, w.q, st, false, &w.sc->t0_pc);
         if (s != EFEM_OK) return s;
     }
-    k_pass3<<<g3, kThreads, sm3, st>>>(w.q, w.Y, n, mm, w.sc, w.partials, w.sums, use_factor ? 1 : 0);
+    switch (mm) {
+#define P3(M) case M: k_pass3_m<M><<<G, kThreads, sm3, st>>>(w.q, w.Y, n, w.sc, w.partials, use_factor ? 1 : 0); break;
+        P3(1) P3(2) P3(3) P3(4) P3(5) P3(6) P3(7) P3(8)
+#undef P3
+    default: k_pass3<<<g3, kThreads, sm3, st>>>(w.q, w.Y, n, mm, w.sc, w.partials, w.sums, use_factor ? 1 : 0);
+    }
     k_pass4<<<grid_for(n), kThreads, 0, st>>>(w.d, w.q, w.S, w.r, x, w.xp, w.rp, n, w.sc, w.partials,
         h_ls ? *h_ls : cudaGraphConditionalHandle(), h_ls ? 1 : 0);
     return EFEM_OK;
