@@ -53,7 +53,8 @@ class Options(ctypes.Structure):
                 ("device_ptrs", ctypes.c_int), ("deterministic", ctypes.c_int), ("device", ctypes.c_int),
                 ("host_loop", ctypes.c_int), ("adjoint_tolerance", ctypes.c_double),
                 ("adjoint_max_iterations", ctypes.c_int), ("elem_threads", ctypes.c_int),
-                ("consistent_inertia", ctypes.c_int), ("trace", ctypes.c_int)]
+                ("consistent_inertia", ctypes.c_int), ("trace", ctypes.c_int),
+                ("solve_subtree_levels", ctypes.c_int)]
 
 
 class SolveInfo(ctypes.Structure):
@@ -82,7 +83,8 @@ class ModelInfo(ctypes.Structure):
                 ("n_supernodes", ctypes.c_int), ("n_levels", ctypes.c_int), ("factor_gflop", ctypes.c_double),
                 ("factor_dinv_nnz", ctypes.c_longlong), ("residual_bytes", ctypes.c_longlong),
                 ("residual_flops", ctypes.c_double), ("n_params", ctypes.c_int),
-                ("elem_threads_fp64", ctypes.c_int), ("elem_threads_fp32", ctypes.c_int)]
+                ("elem_threads_fp64", ctypes.c_int), ("elem_threads_fp32", ctypes.c_int),
+                ("solve_subtree_levels", ctypes.c_int), ("n_solve_subtrees", ctypes.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -62,6 +62,23 @@ struct Tile {
     int s;    // front
     int off;  // first row / column of the tile (multiple of kRT)
 };
+
+// a subtree solved by one CTA (see k_sub_fwd) and its chunks of factor rows
+struct SubTree {
+    int lo, hi;             // fronts [lo, hi] in postorder; hi is the root
+    int j0, ncols;          // the subtree's columns [j0, j0 + ncols) (new numbering)
+    int chunk0, nchunk_f;   // forward chunks
+    int bchunk0, nchunk_b;  // backward chunks
+};
+
+struct SubChunk {
+    int s;      // front
+    int kind;   // 0: rows of L_JJ^{-1}; 1: rows of W; 2: rows of L_JJ^{-T} and of W^T
+    int a, b;   // rows [a, b)
+    int first;  // the front's first chunk of the sweep
+};
+
+constexpr int kSubStage = 4096;  // doubles per stage buffer (two buffers)
 }  // namespace
 
 struct Precond {
@@ -76,6 +93,13 @@ struct Precond {
     size_t solve_smem = 0;
     SolveItem* d_items = nullptr;
     int *d_tgt = nullptr, *d_parent = nullptr, *d_cnt = nullptr, *d_prow = nullptr;
+    // subtree solves below the cut level (sub_levels levels of the tree)
+    int sub_levels = 0, n_subs = 0;
+    int sub_max_r = 0, sub_max_cols = 0, sub_max_depth = 0, sub_max_m = 0, sub_max_c = 0, sub_max_mroot = 0;
+    size_t sub_smem_f = 0, sub_smem_b = 0;
+    SubTree* d_subs = nullptr;
+    SubChunk* d_chunks = nullptr;
+    int *d_depth = nullptr, *d_xidx = nullptr;
     int stage_d = 0, work_d = 0;
     // factor schedule: per (level, step) the fronts with a panel at that step and the SYRK tiles
     struct Step {
@@ -497,6 +521,7 @@ __device__ __forceinline__ void stage_rows(double* dst, int lp, const double* sr
 }
 __device__ __forceinline__ void stage_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void stage_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+__device__ __forceinline__ void stage_wait_but_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
 __device__ __forceinline__ int odd(int L) { return L | 1; }
 __device__ __forceinline__ int lanes_per_row(int R)
@@ -879,6 +904,218 @@ __global__ void __launch_bounds__(kST) k_solve(SolveArgs A)
     }
 }
 
+// ---------------------------------------------------------------- subtree solves
+// Below a cut level the elimination tree has many small fronts, and in the
+// dataflow solve above every one of its levels costs an inter-CTA
+// notification step (a few microseconds) per sweep.  There, each subtree is
+// solved by one CTA from start to end instead: its fronts in postorder
+// (forward) or reverse postorder (backward), the factor rows streamed through
+// a double-buffered cp.async stage in chunks listed at set-up, and what passes
+// between the subtree's fronts kept in shared memory -- the children's
+// updates are added straight into the parent's assembly buffer (one buffer per
+// depth below the subtree root), the solution on ancestor rows is read from
+// the CTA's own copy.  Only the subtree root's update leaves the CTA (for its
+// parent's assembly in k_solve), and the backward sweep reads the solution on
+// the root's below rows once.  The subtree forward sweep runs before k_solve
+// and the backward sweep after it, so the three launches need no counters.
+// Sums keep the dataflow solve's order: b, then the children in list order.
+
+
+struct SubArgs {
+    FrontArgs a;
+    const int* parent;
+    const int* prow;
+    const int* perm;
+    const SubTree* subs;
+    const SubChunk* chunks;
+    const int* depth;  // per front: depth below its subtree root
+    const int* xidx;   // per front row t >= c: >= 0 local column of the row; < 0: -(q + 1), the root's q-th below row
+    int max_r, max_cols, max_depth, max_m, max_c, max_mroot;
+    double* v;
+    double* y;
+    double* upd;
+    unsigned long long* stamp;
+};
+
+__device__ __forceinline__ void sub_stage(const SubArgs& A, const SubChunk& ch, double* dst)
+{
+    const FrontArgs& a = A.a;
+    const int s = ch.s, c = a.ncol[s], m = a.nrow[s] - c, R = ch.b - ch.a;
+    const int lc = odd(c), lm = odd(m);
+    if (ch.kind == 0) {
+        stage_rows(dst, lc, a.dinv + a.dinv_off[s] + static_cast<long long>(ch.a) * c, c, R, c, 1, ch.a);
+    } else if (ch.kind == 1) {
+        stage_rows(dst, lc, a.w + a.lt_off[s] + static_cast<long long>(ch.a) * c, c, R, c, 0, 0);
+    } else {
+        stage_rows(dst, lc, a.dinvT + a.dinv_off[s] + static_cast<long long>(ch.a) * c, c, R, c, 2, ch.a);
+        stage_rows(dst + R * lc, lm, a.wt + a.lt_off[s] + static_cast<long long>(ch.a) * m, m, R, m, 0, 0);
+    }
+    stage_commit();
+}
+
+// Forward sweep of one subtree per CTA: y_J = L_JJ^{-1} f_J for every front
+// and the updates g = f_R - W f_J, added into the parent's buffer or, for the
+// subtree root, written to the update array.
+__global__ void __launch_bounds__(kST) k_sub_fwd(SubArgs A)
+{
+    extern __shared__ double sm[];
+    double* buf[2] = { sm, sm + kSubStage };
+    double* bsub = sm + 2 * kSubStage;          // [ncols][3] right-hand side on the subtree's columns
+    double* acc = bsub + 3 * A.max_cols;        // [max_depth][max_r][3] assembly buffers
+    const SubTree T = A.subs[blockIdx.x];
+    const FrontArgs& a = A.a;
+    if (A.stamp && blockIdx.x == 0 && threadIdx.x == 0) {
+        unsigned long long t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        *A.stamp = t;
+    }
+    const int nch = T.nchunk_f;
+    if (nch > 0) sub_stage(A, A.chunks[T.chunk0], buf[0]);
+    for (int i = threadIdx.x; i < T.ncols; i += kST) {
+        const double* src = A.v + 3LL * A.perm[T.j0 + i];
+        bsub[3 * i] = src[0];
+        bsub[3 * i + 1] = src[1];
+        bsub[3 * i + 2] = src[2];
+    }
+    __syncthreads();
+    for (int i = 0; i < nch; i++) {
+        const SubChunk ch = A.chunks[T.chunk0 + i];
+        if (i + 1 < nch) sub_stage(A, A.chunks[T.chunk0 + i + 1], buf[(i + 1) & 1]);
+        const int s = ch.s, c = a.ncol[s], r = a.nrow[s], lc = odd(c);
+        double* f = acc + static_cast<size_t>(A.depth[s]) * 3 * A.max_r;
+        const bool inner = s != T.hi;  // the parent belongs to the subtree
+        const int p = A.parent[s];
+        if (ch.first) {
+            if (a.child_ptr[s] == a.child_ptr[s + 1]) {  // no children: f = (b_J, 0)
+                const int jc = a.first[s] - T.j0;
+                for (int t = threadIdx.x; t < r; t += kST) {
+                    const bool own = t < c;
+                    f[3 * t] = own ? bsub[3 * (jc + t)] : 0.0;
+                    f[3 * t + 1] = own ? bsub[3 * (jc + t) + 1] : 0.0;
+                    f[3 * t + 2] = own ? bsub[3 * (jc + t) + 2] : 0.0;
+                }
+            }
+            if (inner && a.child_list[a.child_ptr[p]] == s) {  // first child: open the parent's buffer
+                double* fp = acc + static_cast<size_t>(A.depth[p]) * 3 * A.max_r;
+                const int cp = a.ncol[p], rp = a.nrow[p], jp = a.first[p] - T.j0;
+                for (int t = threadIdx.x; t < rp; t += kST) {
+                    const bool own = t < cp;
+                    fp[3 * t] = own ? bsub[3 * (jp + t)] : 0.0;
+                    fp[3 * t + 1] = own ? bsub[3 * (jp + t) + 1] : 0.0;
+                    fp[3 * t + 2] = own ? bsub[3 * (jp + t) + 2] : 0.0;
+                }
+            }
+        }
+        if (i + 1 < nch)
+            stage_wait_but_one();
+        else
+            stage_wait();
+        __syncthreads();
+        const double* cur = buf[i & 1];
+        const int R = ch.b - ch.a;
+        if (ch.kind == 0) {
+            double* yg = A.y + 3LL * (a.first[s] + ch.a);
+            rows_dot(cur, lc, f, 0, R, c, 1, ch.a, [&](int rr, double y0, double y1, double y2) {
+                yg[3 * rr] = y0;
+                yg[3 * rr + 1] = y1;
+                yg[3 * rr + 2] = y2;
+            });
+        } else {
+            double* fp = inner ? acc + static_cast<size_t>(A.depth[p]) * 3 * A.max_r : nullptr;
+            const int* rel = a.relind + a.relind_off[s];
+            double* g = A.upd + a.upd_off[s];
+            rows_dot(cur, lc, f, 0, R, c, 0, 0, [&](int rr, double d0, double d1, double d2) {
+                const int q = ch.a + rr;
+                const double* fq = f + 3 * (c + q);
+                const double g0 = fq[0] - d0, g1 = fq[1] - d1, g2 = fq[2] - d2;
+                if (inner) {
+                    double* o = fp + 3 * rel[q];
+                    o[0] += g0;
+                    o[1] += g1;
+                    o[2] += g2;
+                } else {
+                    g[3 * q] = g0;
+                    g[3 * q + 1] = g1;
+                    g[3 * q + 2] = g2;
+                }
+            });
+        }
+        __syncthreads();  // the buffer is free for the chunk after next; updates are visible
+    }
+}
+
+// Backward sweep of one subtree per CTA, fronts root first:
+// x_J = L_JJ^{-T} y_J - W^T x_R, x_R from the CTA's own copy of the solution.
+__global__ void __launch_bounds__(kST) k_sub_bwd(SubArgs A)
+{
+    extern __shared__ double sm[];
+    double* buf[2] = { sm, sm + kSubStage };
+    double* ysub = sm + 2 * kSubStage;        // [ncols][3]
+    double* xs = ysub + 3 * A.max_cols;       // [ncols][3] solution on the subtree's columns
+    double* xr = xs + 3 * A.max_cols;         // [max_mroot][3] solution on the root's below rows
+    double* xR = xr + 3 * A.max_mroot;        // [max_m][3] x_R of the current front
+    double* tmp = xR + 3 * A.max_m;           // [max_c][3]
+    const SubTree T = A.subs[blockIdx.x];
+    const FrontArgs& a = A.a;
+    const int nch = T.nchunk_b;
+    if (nch > 0) sub_stage(A, A.chunks[T.bchunk0], buf[0]);
+    for (int i = threadIdx.x; i < 3 * T.ncols; i += kST) ysub[i] = __ldcg(A.y + 3LL * T.j0 + i);
+    {
+        const int root = T.hi, cr = a.ncol[root], mr = a.nrow[root] - cr;
+        const int* pr = A.prow + a.rows_off[root] + cr;
+        for (int q = threadIdx.x; q < mr; q += kST) {
+            const double* src = A.v + 3LL * pr[q];
+            xr[3 * q] = __ldcg(src);
+            xr[3 * q + 1] = __ldcg(src + 1);
+            xr[3 * q + 2] = __ldcg(src + 2);
+        }
+    }
+    __syncthreads();
+    for (int i = 0; i < nch; i++) {
+        const SubChunk ch = A.chunks[T.bchunk0 + i];
+        if (i + 1 < nch) sub_stage(A, A.chunks[T.bchunk0 + i + 1], buf[(i + 1) & 1]);
+        const int s = ch.s, c = a.ncol[s], m = a.nrow[s] - c, lc = odd(c), lm = odd(m);
+        const long long ro = a.rows_off[s];
+        const int jc = a.first[s] - T.j0;
+        if (ch.first) {  // x on the front's below rows, from the subtree's columns or the root's below rows
+            const int* xi = A.xidx + ro + c;
+            for (int q = threadIdx.x; q < m; q += kST) {
+                const int li = xi[q];
+                const double* src = li >= 0 ? xs + 3 * li : xr + 3 * (-li - 1);
+                xR[3 * q] = src[0];
+                xR[3 * q + 1] = src[1];
+                xR[3 * q + 2] = src[2];
+            }
+        }
+        if (i + 1 < nch)
+            stage_wait_but_one();
+        else
+            stage_wait();
+        __syncthreads();
+        const double* cur = buf[i & 1];
+        const int R = ch.b - ch.a;
+        rows_dot(cur, lc, ysub + 3 * jc, 0, R, c, 2, ch.a, [&](int rr, double x0, double x1, double x2) {
+            tmp[3 * rr] = x0;
+            tmp[3 * rr + 1] = x1;
+            tmp[3 * rr + 2] = x2;
+        });
+        __syncthreads();
+        const int* pr = A.prow + ro + ch.a;
+        double* xo = xs + 3 * (jc + ch.a);
+        rows_dot(cur + R * lc, lm, xR, 0, R, m, 0, 0, [&](int rr, double s0, double s1, double s2) {
+            const double x0 = tmp[3 * rr] - s0, x1 = tmp[3 * rr + 1] - s1, x2 = tmp[3 * rr + 2] - s2;
+            xo[3 * rr] = x0;
+            xo[3 * rr + 1] = x1;
+            xo[3 * rr + 2] = x2;
+            double* o = A.v + 3LL * pr[rr];
+            o[0] = x0;
+            o[1] = x1;
+            o[2] = x2;
+        });
+        __syncthreads();
+    }
+}
+
 // W = L_RJ L_JJ^{-1} for every front, one 64 x 64 tile of W per CTA (4 x 4
 // per thread), L_RJ from the front's panel and L_JJ^{-1} (lower triangular,
 // entries above the diagonal masked) in blocks of 32; written row-major as W
@@ -955,9 +1192,13 @@ void enqueue_solve(const Precond& P, const FrontArgs& a, const SolveBufs& b, dou
 {
     const int ns = P.S.ns;
     if (clear) cudaMemsetAsync(b.cnt, 0, sizeof(int) * (4 * static_cast<size_t>(ns) + 2), st);
+    const SubArgs B { a, P.d_parent, P.d_prow, P.d_perm, P.d_subs, P.d_chunks, P.d_depth, P.d_xidx, P.sub_max_r,
+        P.sub_max_cols, P.sub_max_depth, P.sub_max_m, P.sub_max_c, P.sub_max_mroot, d_v, b.y, b.upd, stamp };
+    if (P.n_subs > 0) k_sub_fwd<<<P.n_subs, kST, P.sub_smem_f, st>>>(B);
     SolveArgs A { a, P.d_parent, P.d_prow, P.d_items, P.d_tgt, P.n_items, ns, P.stage_d, P.work_d, d_v, b.y, b.t,
-        b.upd, b.cnt, stamp };
-    k_solve<<<P.solve_grid, kST, P.solve_smem, st>>>(A);
+        b.upd, b.cnt, P.n_subs > 0 ? nullptr : stamp };
+    if (P.n_items > 0) k_solve<<<P.solve_grid, kST, P.solve_smem, st>>>(A);
+    if (P.n_subs > 0) k_sub_bwd<<<P.n_subs, kST, P.sub_smem_b, st>>>(B);
 }
 
 }  // namespace
@@ -971,13 +1212,15 @@ void free_precond(Model& m)
     P.graphs.clear();
     if (P.capture) cudaStreamDestroy(P.capture);
     for (int** p : { &P.d_first, &P.d_ncol, &P.d_nrow, &P.d_rows, &P.d_child_ptr, &P.d_child_list, &P.d_relind,
-             &P.d_level_list, &P.d_perm, &P.d_fail, &P.d_panel_list, &P.d_contrib_ptr, &P.d_contrib_idx, &P.d_below_front, &P.d_tgt, &P.d_parent, &P.d_cnt, &P.d_prow })
+             &P.d_level_list, &P.d_perm, &P.d_fail, &P.d_panel_list, &P.d_contrib_ptr, &P.d_contrib_idx, &P.d_below_front, &P.d_tgt, &P.d_parent, &P.d_cnt, &P.d_prow, &P.d_depth, &P.d_xidx })
         dev_free(*p);
     for (long long** p : { &P.d_front_off, &P.d_rows_off, &P.d_relind_off, &P.d_dinv_off, &P.d_upd_off, &P.d_a_pos,
              &P.d_a_src, &P.d_lt_off })
         dev_free(*p);
     for (Tile** p : { &P.d_inv, &P.d_ea, &P.d_oinv }) dev_free(*p);
     dev_free(P.d_items);
+    dev_free(P.d_subs);
+    dev_free(P.d_chunks);
     dev_free(P.d_syrk);
     dev_free(P.d_wtiles);
     for (double** p : { &P.d_front, &P.d_dinv, &P.d_dinvT, &P.d_w, &P.d_wt, &P.d_upd, &P.d_y, &P.d_t, &P.d_vals })
@@ -997,6 +1240,8 @@ void precond_info(const Model& m, efem_model_info* info)
     long long dn = 0;
     for (int s = 0; s < S.ns; s++) dn += static_cast<long long>(S.ncol[s]) * (S.ncol[s] + 1) / 2;
     info->factor_dinv_nnz = dn;
+    info->solve_subtree_levels = m.precond->sub_levels;
+    info->n_solve_subtrees = m.precond->n_subs;
 }
 
 static efem_status precond_factor(Model& m, int* ok, double* ms_factor);
@@ -1073,9 +1318,140 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
     }
     P.n_wtiles = static_cast<int>(wtiles.size());
     P.n_oinv = static_cast<int>(oinv.size());
-    // solve items: forward sweep by level (leaves first), backward sweep by
-    // level (root first).  Each item records the ranges of contributions its
-    // rows assemble, and the shared memory it stages is sized here.
+    auto odd_h = [](int L) { return L | 1; };
+    // Subtree solves: fronts on the lowest K levels are solved per subtree by
+    // one CTA (k_sub_fwd / k_sub_bwd), the levels above by the dataflow
+    // k_solve.  K comes from a latency model of one sweep: a dataflow level
+    // costs one notification step (kLevelStep), a subtree streams its factor
+    // rows at kSubRate bytes/s and spends kSubFront per front; the subtree
+    // kernels add one launch boundary each.  opts.solve_subtree_levels >= 0
+    // asks for a given K instead (lowered until the subtrees fit).
+    constexpr double kLevelStep = 6.5e-6, kSubRate = 50e9, kSubFront = 0.4e-6, kSubLaunch = 2e-6;
+    std::vector<int> lev(S.ns, 0), nsub(S.ns, 1), sdepth(S.ns, 0);
+    for (int l = 0; l < nlev; l++)
+        for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) lev[S.level_list[q]] = l;
+    for (int s = 0; s < S.ns; s++)
+        if (S.parent[s] >= 0) nsub[S.parent[s]] += nsub[s];
+    bool postorder = true;  // every subtree is the index range [s - nsub[s] + 1, s]
+    for (int s = 0; s < S.ns && postorder; s++)
+        for (int k = s - nsub[s] + 1; k < s && postorder; k++) {
+            int u = k;
+            while (u >= 0 && u < s) u = S.parent[u];
+            postorder = u == s;
+        }
+    struct SubPlan {
+        bool ok = true;
+        double t = 0.0;
+        int max_r = 1, max_cols = 1, max_depth = 1, max_m = 1, max_c = 1, max_mroot = 1;
+        size_t smem_f = 0, smem_b = 0;
+        std::vector<int> roots;
+    };
+    auto plan = [&](int K) {
+        SubPlan p;
+        if (K <= 0) return p;
+        for (int s = 0; s < S.ns; s++)
+            if (lev[s] < K && (S.parent[s] < 0 || lev[S.parent[s]] >= K)) p.roots.push_back(s);
+        for (int root : p.roots) {
+            double bytes = 0.0;
+            int cols = 0;
+            for (int k = root; k > root - nsub[root]; k--) {  // parents before children
+                sdepth[k] = k == root ? 0 : sdepth[S.parent[k]] + 1;
+                const int c = S.ncol[k], r = S.nrow[k], mm = r - c;
+                bytes += 8.0 * (0.5 * c * (c + 1.0) + static_cast<double>(mm) * c);
+                cols += c;
+                p.max_r = std::max(p.max_r, r);
+                p.max_m = std::max(p.max_m, mm);
+                p.max_c = std::max(p.max_c, c);
+                p.max_depth = std::max(p.max_depth, sdepth[k] + 1);
+                if (odd_h(c) + odd_h(mm) > kSubStage) p.ok = false;
+            }
+            p.max_cols = std::max(p.max_cols, cols);
+            p.max_mroot = std::max(p.max_mroot, S.nrow[root] - S.ncol[root]);
+            p.t = std::max(p.t, bytes / kSubRate + nsub[root] * kSubFront);
+        }
+        p.smem_f = sizeof(double) * (2 * static_cast<size_t>(kSubStage) + 3 * static_cast<size_t>(p.max_cols)
+            + 3 * static_cast<size_t>(p.max_depth) * p.max_r);
+        p.smem_b = sizeof(double) * (2 * static_cast<size_t>(kSubStage) + 6 * static_cast<size_t>(p.max_cols)
+            + 3 * static_cast<size_t>(p.max_mroot + p.max_m + p.max_c));
+        if (std::max(p.smem_f, p.smem_b) > 200 * 1024) p.ok = false;
+        return p;
+    };
+    int K = 0;
+    if (postorder) {
+        const int want = m.opts.solve_subtree_levels;
+        if (want >= 0) {
+            for (K = std::min(want, nlev); K > 0 && !plan(K).ok; K--) {
+            }
+        } else {
+            double best = nlev * kLevelStep;
+            for (int k = 1; k <= nlev; k++) {
+                const SubPlan p = plan(k);
+                const double t = (nlev - k) * kLevelStep + p.t + kSubLaunch;
+                if (p.ok && t < best) {
+                    best = t;
+                    K = k;
+                }
+            }
+        }
+    }
+    const SubPlan sp = plan(K);  // also leaves sdepth for the chosen subtrees
+    std::vector<char> in_sub(S.ns, 0);
+    for (int s = 0; s < S.ns; s++) in_sub[s] = lev[s] < K;
+    std::vector<SubTree> subs;
+    std::vector<SubChunk> chunks;
+    std::vector<int> xidx(S.rows.size(), 0);
+    for (int root : sp.roots) {
+        SubTree T {};
+        T.lo = root - nsub[root] + 1;
+        T.hi = root;
+        T.j0 = S.first[T.lo];
+        T.ncols = S.first[root] + S.ncol[root] - T.j0;
+        T.chunk0 = static_cast<int>(chunks.size());
+        for (int k = T.lo; k <= T.hi; k++) {
+            const int c = S.ncol[k], mm = S.nrow[k] - c, rx = std::max(1, kSubStage / odd_h(c));
+            for (int a0 = 0; a0 < c; a0 += rx) chunks.push_back(SubChunk { k, 0, a0, std::min(c, a0 + rx), a0 == 0 });
+            for (int a0 = 0; a0 < mm; a0 += rx) chunks.push_back(SubChunk { k, 1, a0, std::min(mm, a0 + rx), 0 });
+        }
+        T.nchunk_f = static_cast<int>(chunks.size()) - T.chunk0;
+        T.bchunk0 = static_cast<int>(chunks.size());
+        for (int k = T.hi; k >= T.lo; k--) {
+            const int c = S.ncol[k], mm = S.nrow[k] - c, rb = std::max(1, kSubStage / (odd_h(c) + odd_h(mm)));
+            for (int a0 = 0; a0 < c; a0 += rb) chunks.push_back(SubChunk { k, 2, a0, std::min(c, a0 + rb), a0 == 0 });
+            // below rows: a column of the subtree, or one of the root's below rows
+            const long long ro = S.rows_off[k];
+            const int* rb0 = S.rows.data() + S.rows_off[root] + S.ncol[root];
+            const int nrb = S.nrow[root] - S.ncol[root];
+            for (int t = c; t < S.nrow[k]; t++) {
+                const int row = S.rows[ro + t];
+                if (row >= T.j0 && row < T.j0 + T.ncols) {
+                    xidx[ro + t] = row - T.j0;
+                } else {
+                    const int q = static_cast<int>(std::lower_bound(rb0, rb0 + nrb, row) - rb0);
+                    if (q >= nrb || rb0[q] != row) {
+                        set_error("internal: a subtree row is neither a subtree column nor a root row");
+                        return EFEM_ERR_CUDA;
+                    }
+                    xidx[ro + t] = -(q + 1);
+                }
+            }
+        }
+        T.nchunk_b = static_cast<int>(chunks.size()) - T.bchunk0;
+        subs.push_back(T);
+    }
+    P.sub_levels = K;
+    P.n_subs = static_cast<int>(subs.size());
+    P.sub_max_r = sp.max_r;
+    P.sub_max_cols = sp.max_cols;
+    P.sub_max_depth = sp.max_depth;
+    P.sub_max_m = sp.max_m;
+    P.sub_max_c = sp.max_c;
+    P.sub_max_mroot = sp.max_mroot;
+    P.sub_smem_f = sp.smem_f;
+    P.sub_smem_b = sp.smem_b;
+    // solve items above the cut: forward sweep by level (leaves first),
+    // backward sweep by level (root first).  Each item records the ranges of
+    // contributions its rows assemble, and the shared memory it stages is
+    // sized here.
     std::vector<SolveItem> items;
     std::vector<int> tgt(4 * static_cast<size_t>(S.ns), 0);
     std::vector<char> whole(S.ns, 0);
@@ -1085,7 +1461,6 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
         work_d = std::max(work_d, wd);
         ints = std::max(ints, ni);
     };
-    auto odd_h = [](int L) { return L | 1; };
     auto tile = [&](int per_row) {  // rows per tile when a row stages per_row doubles
         const int t = (kStageBudget / per_row) / 4 * 4;
         return std::max(4, std::min(256, t));
@@ -1099,11 +1474,12 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
         const int c = S.ncol[s], mm = S.nrow[s] - c, r = S.nrow[s];
         const int lc = odd_h(c), lm = odd_h(mm);
         whole[s] = static_cast<long long>(r) * lc <= kWholeBudget && static_cast<long long>(c) * (lc + lm) <= kWholeBudget;
-        tgt[s] = whole[s] ? 1 : ntiles(c, lc);                                              // y of s complete
-        if (S.parent[s] >= 0) tgt[S.ns + S.parent[s]] += whole[s] ? 1 : ntiles(mm, lc);  // children's g complete
+        tgt[s] = whole[s] ? 1 : ntiles(c, lc);  // y of s complete
+        if (S.parent[s] >= 0 && !in_sub[s])     // children's g complete (subtree roots finish before k_solve)
+            tgt[S.ns + S.parent[s]] += whole[s] ? 1 : ntiles(mm, lc);
         tgt[3 * S.ns + s] = whole[s] ? 1 : ntiles(c, lc + lm);                              // x of s complete
     }
-    for (int l = 0; l < nlev; l++) {
+    for (int l = K; l < nlev; l++) {
         for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) {
             const int s = S.level_list[q];
             const int c = S.ncol[s], r = S.nrow[s], mm = r - c, lc = odd_h(c);
@@ -1130,7 +1506,7 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
             }
         }
     }
-    for (int l = nlev - 1; l >= 0; l--) {
+    for (int l = nlev - 1; l >= K; l--) {
         for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) {
             const int s = S.level_list[q];
             const int c = S.ncol[s], r = S.nrow[s], mm = r - c, lc = odd_h(c), lm = odd_h(mm);
@@ -1187,6 +1563,12 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
     UP(P.d_prow, prow);
     UP(P.d_items, items);
     UP(P.d_tgt, tgt);
+    if (P.n_subs > 0) {
+        UP(P.d_subs, subs);
+        UP(P.d_chunks, chunks);
+        UP(P.d_depth, sdepth);
+        UP(P.d_xidx, xidx);
+    }
     UP(P.d_inv, inv);
     UP(P.d_oinv, oinv);
     UP(P.d_wtiles, wtiles);
@@ -1212,6 +1594,10 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
     EFEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve, kST, P.solve_smem));
     EFEM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m.device));
     P.solve_grid = std::max(1, std::min(P.n_items, std::max(per_sm, 1) * sms));
+    if (P.n_subs > 0) {
+        EFEM_CUDA(cudaFuncSetAttribute(k_sub_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        EFEM_CUDA(cudaFuncSetAttribute(k_sub_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    }
     EFEM_CUDA(cudaStreamCreateWithFlags(&P.capture, cudaStreamNonBlocking));
     P.ready = true;  // analysed; the numeric factor follows
     return precond_factor(m, ok, ms_factor);
@@ -1338,7 +1724,8 @@ void precond_counters(const Model& m, int** cnt, int* n)
 
 long long precond_launch_count(const Model& m)
 {
-    return m.precond ? 1 : 0;
+    if (!m.precond) return 0;
+    return (m.precond->n_items > 0 ? 1 : 0) + (m.precond->n_subs > 0 ? 2 : 0);
 }
 
 const int* precond_error_flag(const Model& m)

@@ -794,6 +794,7 @@ efem_status efem_default_options(efem_options* o)
     o->elem_threads = 0;
     o->consistent_inertia = 0;
     o->trace = 0;
+    o->solve_subtree_levels = -1;
     return EFEM_OK;
 }
 
@@ -914,6 +915,7 @@ efem_status efem_set_options(void* model, const efem_options* o)
     const bool reintegrate = o->integration != m->opts.integration;
     const bool new_history = o->m != m->opts.m;
     const bool new_mass = m->has_gravity && (o->consistent_inertia != 0) != (m->opts.consistent_inertia != 0);
+    const bool new_schedule = o->solve_subtree_levels != m->opts.solve_subtree_levels;
     const int dev = m->device;
     m->opts = *o;
     if (dev >= 0) m->device = dev;  // the device is fixed once buffers exist
@@ -931,6 +933,7 @@ efem_status efem_set_options(void* model, const efem_options* o)
         if (s != EFEM_OK) return s;
     }
     if (new_history) efem::free_solver(*m);
+    if (new_schedule && !reintegrate) efem::free_precond(*m);  // the solve schedule is rebuilt at the next factorisation
     return EFEM_OK;
 }
 

@@ -114,6 +114,9 @@ typedef struct {
                                  src/io/Config.cpp:63-65) */
     int trace;                /* > 0: keep a convergence trace of up to this many records per solve
                                  (efem_solve_trace); 0: off */
+    int solve_subtree_levels; /* H0 triangular solves: fronts on the lowest k levels of the elimination
+                                 tree are solved one subtree per CTA, the levels above by the dataflow
+                                 kernel; -1 = k from the solve's latency model (default), 0 = none */
 } efem_options;
 
 enum {
@@ -151,6 +154,7 @@ typedef struct {
     int n_params;                         /* sensitivity parameters (efem_adjoint): 5 per material slot
                                              (C10, C01, C20, C30, D1), then 1 per pressure load */
     int elem_threads_fp64, elem_threads_fp32;  /* the first element block's CTA size (autotuner) */
+    int solve_subtree_levels, n_solve_subtrees; /* H0 solve schedule: levels solved per subtree, subtrees */
 } efem_model_info;
 
 typedef struct {

@@ -101,3 +101,46 @@ def test_host_loop_matches_device_loop(tmp_path):
     ref = d["u_solve"]
     assert np.linalg.norm(u_host - ref) <= 1e-6 * np.linalg.norm(ref)
     assert np.linalg.norm(u_host - u_dev) <= 1e-6 * np.linalg.norm(ref)
+
+
+@pytest.mark.parametrize("path", CASES[::6] + golden_files("cantilever_c3d4_pressure.npz"),
+                         ids=lambda p: p.split("/")[-1][:-4])
+def test_precond_subtree_schedules_agree(path, tmp_path):
+    """H0 v with every split of the elimination tree between the per-subtree
+    kernels and the dataflow kernel (0 = dataflow only, all levels = subtree
+    kernels only) against the oracle's factor."""
+    cfg, d = write_golden_case(path, tmp_path)
+    o = oracle.Oracle(oracle.read_case(cfg))
+    m = api.Model.from_json(cfg)
+    v = np.random.default_rng(9).standard_normal(m.n_dof)
+    ho = o.precond_apply(v)
+    m.precond_apply(v)
+    nlev = m.info()["n_levels"]
+    for k in sorted({0, 1, 2, nlev // 2, nlev}):
+        m.set_options(solve_subtree_levels=k)
+        hv = m.precond_apply(v)
+        info = m.info()
+        assert info["solve_subtree_levels"] <= k
+        assert np.linalg.norm(hv - ho) <= 1e-10 * np.linalg.norm(ho), (k, info["solve_subtree_levels"])
+
+
+def test_beam_subtree_schedules_agree():
+    """The 20 480-element beam: auto, none and all-but-the-top subtree splits."""
+    from efem_b200 import meshgen as mg
+    m = api.Model.from_case(mg.cantilever_c3d8_force())
+    v = np.random.default_rng(10).standard_normal(m.n_dof)
+    ref = m.precond_apply(v)  # auto
+    auto = m.info()
+    assert auto["solve_subtree_levels"] > 0 and auto["n_solve_subtrees"] > 0
+    nlev = auto["n_levels"]
+    for k in (0, 3, nlev - 2, nlev):
+        m.set_options(solve_subtree_levels=k)
+        hv = m.precond_apply(v)
+        assert np.linalg.norm(hv - ref) <= 1e-11 * np.linalg.norm(ref), (k, m.info()["solve_subtree_levels"])
+    # and the whole solve with the dataflow kernel only
+    m.set_options(solve_subtree_levels=0)
+    u0, i0 = m.solve()
+    m.set_options(solve_subtree_levels=-1)
+    u1, i1 = m.solve()
+    assert i0["flags"] & api.SOLVE_CONVERGED and i1["flags"] & api.SOLVE_CONVERGED
+    assert np.linalg.norm(u1 - u0) <= 1e-4 * np.linalg.norm(u0)
