@@ -1321,12 +1321,14 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
     auto odd_h = [](int L) { return L | 1; };
     // Subtree solves: fronts on the lowest K levels are solved per subtree by
     // one CTA (k_sub_fwd / k_sub_bwd), the levels above by the dataflow
-    // k_solve.  K comes from a latency model of one sweep: a dataflow level
-    // costs one notification step (kLevelStep), a subtree streams its factor
-    // rows at kSubRate bytes/s and spends kSubFront per front; the subtree
-    // kernels add one launch boundary each.  opts.solve_subtree_levels >= 0
-    // asks for a given K instead (lowered until the subtrees fit).
-    constexpr double kLevelStep = 6.5e-6, kSubRate = 50e9, kSubFront = 0.4e-6, kSubLaunch = 2e-6;
+    // k_solve.  opts.solve_subtree_levels = K asks for them (K is lowered
+    // until the subtrees fit in shared memory); the default (-1) is K = 0.
+    // Measured on the 20 480-element C3D8 beam (11 levels), one H0
+    // application inside the solve costs 274 us per iteration with K = 0 and
+    // 290, 322, 361, 450 us with K = 1, 2, 3, 4: a subtree CTA streams its
+    // factor rows one 32 KB chunk ahead, about 20 GB/s, and works through its
+    // fronts one after another, which is slower than the notification steps
+    // of the levels it replaces.
     std::vector<int> lev(S.ns, 0), nsub(S.ns, 1), sdepth(S.ns, 0);
     for (int l = 0; l < nlev; l++)
         for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) lev[S.level_list[q]] = l;
@@ -1341,7 +1343,6 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
         }
     struct SubPlan {
         bool ok = true;
-        double t = 0.0;
         int max_r = 1, max_cols = 1, max_depth = 1, max_m = 1, max_c = 1, max_mroot = 1;
         size_t smem_f = 0, smem_b = 0;
         std::vector<int> roots;
@@ -1352,12 +1353,10 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
         for (int s = 0; s < S.ns; s++)
             if (lev[s] < K && (S.parent[s] < 0 || lev[S.parent[s]] >= K)) p.roots.push_back(s);
         for (int root : p.roots) {
-            double bytes = 0.0;
             int cols = 0;
             for (int k = root; k > root - nsub[root]; k--) {  // parents before children
                 sdepth[k] = k == root ? 0 : sdepth[S.parent[k]] + 1;
                 const int c = S.ncol[k], r = S.nrow[k], mm = r - c;
-                bytes += 8.0 * (0.5 * c * (c + 1.0) + static_cast<double>(mm) * c);
                 cols += c;
                 p.max_r = std::max(p.max_r, r);
                 p.max_m = std::max(p.max_m, mm);
@@ -1367,7 +1366,6 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
             }
             p.max_cols = std::max(p.max_cols, cols);
             p.max_mroot = std::max(p.max_mroot, S.nrow[root] - S.ncol[root]);
-            p.t = std::max(p.t, bytes / kSubRate + nsub[root] * kSubFront);
         }
         p.smem_f = sizeof(double) * (2 * static_cast<size_t>(kSubStage) + 3 * static_cast<size_t>(p.max_cols)
             + 3 * static_cast<size_t>(p.max_depth) * p.max_r);
@@ -1377,23 +1375,9 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
         return p;
     };
     int K = 0;
-    if (postorder) {
-        const int want = m.opts.solve_subtree_levels;
-        if (want >= 0) {
-            for (K = std::min(want, nlev); K > 0 && !plan(K).ok; K--) {
-            }
-        } else {
-            double best = nlev * kLevelStep;
-            for (int k = 1; k <= nlev; k++) {
-                const SubPlan p = plan(k);
-                const double t = (nlev - k) * kLevelStep + p.t + kSubLaunch;
-                if (p.ok && t < best) {
-                    best = t;
-                    K = k;
-                }
-            }
+    if (postorder && m.opts.solve_subtree_levels > 0)
+        for (K = std::min(m.opts.solve_subtree_levels, nlev); K > 0 && !plan(K).ok; K--) {
         }
-    }
     const SubPlan sp = plan(K);  // also leaves sdepth for the chosen subtrees
     std::vector<char> in_sub(S.ns, 0);
     for (int s = 0; s < S.ns; s++) in_sub[s] = lev[s] < K;

@@ -116,7 +116,7 @@ typedef struct {
                                  (efem_solve_trace); 0: off */
     int solve_subtree_levels; /* H0 triangular solves: fronts on the lowest k levels of the elimination
                                  tree are solved one subtree per CTA, the levels above by the dataflow
-                                 kernel; -1 = k from the solve's latency model (default), 0 = none */
+                                 kernel; 0 or -1 (default) = none, the dataflow kernel for every level */
 } efem_options;
 
 enum {

@@ -125,22 +125,22 @@ def test_precond_subtree_schedules_agree(path, tmp_path):
 
 
 def test_beam_subtree_schedules_agree():
-    """The 20 480-element beam: auto, none and all-but-the-top subtree splits."""
+    """The 20 480-element beam: the default (dataflow only) against subtree splits."""
     from efem_b200 import meshgen as mg
     m = api.Model.from_case(mg.cantilever_c3d8_force())
     v = np.random.default_rng(10).standard_normal(m.n_dof)
-    ref = m.precond_apply(v)  # auto
-    auto = m.info()
-    assert auto["solve_subtree_levels"] > 0 and auto["n_solve_subtrees"] > 0
-    nlev = auto["n_levels"]
-    for k in (0, 3, nlev - 2, nlev):
+    ref = m.precond_apply(v)
+    info = m.info()
+    assert info["solve_subtree_levels"] == 0 and info["n_solve_subtrees"] == 0
+    nlev = info["n_levels"]
+    for k in (1, 3, nlev - 2, nlev):
         m.set_options(solve_subtree_levels=k)
         hv = m.precond_apply(v)
         assert np.linalg.norm(hv - ref) <= 1e-11 * np.linalg.norm(ref), (k, m.info()["solve_subtree_levels"])
-    # and the whole solve with the dataflow kernel only
+    # and the whole solve with subtree kernels on the lowest three levels
     m.set_options(solve_subtree_levels=0)
     u0, i0 = m.solve()
-    m.set_options(solve_subtree_levels=-1)
+    m.set_options(solve_subtree_levels=3)
     u1, i1 = m.solve()
     assert i0["flags"] & api.SOLVE_CONVERGED and i1["flags"] & api.SOLVE_CONVERGED
     assert np.linalg.norm(u1 - u0) <= 1e-4 * np.linalg.norm(u0)
