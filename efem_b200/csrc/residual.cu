@@ -66,13 +66,17 @@ template <int NEN, int NGP, typename T, int BLK>
 __global__ void __launch_bounds__(BLK) k_elem_residual(ElemArgs<T> a)
 {
     constexpr int EPB = elems_per_cta<NGP, BLK>();
-    __shared__ T s_u[EPB][NEN][3];
-    __shared__ T s_S[EPB][NGP][9];
-    __shared__ T s_dN[NGP][NEN][3];
-    __shared__ int s_node[EPB][NEN];
+    // per-element rows padded to an odd length, so that threads on
+    // consecutive elements (phases 1 and 3) or Gauss points (phase 2) read
+    // different shared-memory banks
+    constexpr int SU = (NEN * 3) | 1, SS = (NGP * 9) | 1, SD = (NEN * 3) | 1, SN = NEN | 1;
+    __shared__ T s_u[EPB][SU];     // [element][node * 3 + component]
+    __shared__ T s_S[EPB][SS];     // [element][gp * 9 + 3 i + j]
+    __shared__ T s_dN[NGP][SD];    // [gp][node * 3 + k]
+    __shared__ int s_node[EPB][SN];
 
     const int tid = threadIdx.x;
-    for (int i = tid; i < NGP * NEN * 3; i += BLK) (&s_dN[0][0][0])[i] = a.dN[i];
+    for (int i = tid; i < NGP * NEN * 3; i += BLK) s_dN[i / (NEN * 3)][i % (NEN * 3)] = a.dN[i];
     const int e0 = blockIdx.x * EPB;
 
     // phase 1: stage node displacements relative to the element's first node,
@@ -101,9 +105,9 @@ __global__ void __launch_bounds__(BLK) k_elem_residual(ElemArgs<T> a)
             v2 = static_cast<T>(w2 - z2);
         }
         s_node[el][nd] = node;
-        s_u[el][nd][0] = v0;
-        s_u[el][nd][1] = v1;
-        s_u[el][nd][2] = v2;
+        s_u[el][3 * nd] = v0;
+        s_u[el][3 * nd + 1] = v1;
+        s_u[el][3 * nd + 2] = v2;
     }
     __syncthreads();
 
@@ -116,8 +120,8 @@ __global__ void __launch_bounds__(BLK) k_elem_residual(ElemArgs<T> a)
             for (int k = 0; k < 9; k++) A[k] = 0;
 #pragma unroll 4
             for (int q = 0; q < NEN; q++) {
-                const T u0 = s_u[el][q][0], u1 = s_u[el][q][1], u2 = s_u[el][q][2];
-                const T d0 = s_dN[g][q][0], d1 = s_dN[g][q][1], d2 = s_dN[g][q][2];
+                const T u0 = s_u[el][3 * q], u1 = s_u[el][3 * q + 1], u2 = s_u[el][3 * q + 2];
+                const T d0 = s_dN[g][3 * q], d1 = s_dN[g][3 * q + 1], d2 = s_dN[g][3 * q + 2];
                 A[0] += u0 * d0; A[1] += u0 * d1; A[2] += u0 * d2;
                 A[3] += u1 * d0; A[4] += u1 * d1; A[5] += u1 * d2;
                 A[6] += u2 * d0; A[7] += u2 * d1; A[8] += u2 * d2;
@@ -140,7 +144,7 @@ __global__ void __launch_bounds__(BLK) k_elem_residual(ElemArgs<T> a)
             for (int i = 0; i < 3; i++)
 #pragma unroll
                 for (int j = 0; j < 3; j++)
-                    s_S[el][g][3 * i + j] = wv * (P[3 * i] * Ji[3 * j] + P[3 * i + 1] * Ji[3 * j + 1] + P[3 * i + 2] * Ji[3 * j + 2]);
+                    s_S[el][9 * g + 3 * i + j] = wv * (P[3 * i] * Ji[3 * j] + P[3 * i + 1] * Ji[3 * j + 1] + P[3 * i + 2] * Ji[3 * j + 2]);
         }
     }
     __syncthreads();
@@ -154,8 +158,8 @@ __global__ void __launch_bounds__(BLK) k_elem_residual(ElemArgs<T> a)
         T r0 = 0, r1 = 0, r2 = 0;
 #pragma unroll 4
         for (int g = 0; g < NGP; g++) {
-            const T d0 = s_dN[g][nd][0], d1 = s_dN[g][nd][1], d2 = s_dN[g][nd][2];
-            const T* S = s_S[el][g];
+            const T d0 = s_dN[g][3 * nd], d1 = s_dN[g][3 * nd + 1], d2 = s_dN[g][3 * nd + 2];
+            const T* S = &s_S[el][9 * g];
             r0 += S[0] * d0 + S[1] * d1 + S[2] * d2;
             r1 += S[3] * d0 + S[4] * d1 + S[5] * d2;
             r2 += S[6] * d0 + S[7] * d1 + S[8] * d2;
