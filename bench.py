@@ -172,6 +172,7 @@ def run_adjoint_bench(args):
     torch.cuda.set_device(0)
     case, tip = mg.finger_c3d10()
     opts = api.default_options()
+    opts.max_iterations = 20000  # a bound for the equilibrium solve
     t_setup = time.time()
     model = api.Model.from_case(case, opts)
     stream = torch.cuda.current_stream()
@@ -244,6 +245,7 @@ def run_cap_bench(args):
         o = api.default_options()
         o.precision = precision
         o.residual_criterion = criterion
+        o.max_iterations = 20000  # a bound; both precisions converge in a few hundred iterations
         m = api.Model.from_case(case, o)
         api.check(api.lib().efem_set_stream(m.h, api.ctypes.c_void_p(stream.cuda_stream)))
         m.set_options(device_ptrs=1)
@@ -432,6 +434,9 @@ def main():
     opts.precision = api.MIXED if args.precision == "mixed" else api.FP64
     opts.device = local
     opts.host_loop = 1 if args.host_loop else 0
+    # a bound for the timed solves (the FP64 solve converges in about 180
+    # iterations); the FP32 element path stalls above 1e-6 N on this beam
+    opts.max_iterations = 5000
     t_setup = time.time()
     model = api.Model.from_case(case, opts)
     stream = torch.cuda.current_stream()
@@ -507,6 +512,7 @@ def main():
             "time_to_converge_ms": total_ms_max / args.steps,
             "iterations_per_solve": iters / args.steps, "residual_evals_per_solve": sum(i["n_residual_evals"] for i in infos) / args.steps,
             "final_r_inf": infos[-1]["r_inf"], "u_inf": infos[-1]["u_inf"],
+            "converged": all(bool(i["flags"] & api.SOLVE_CONVERGED) for i in infos),
             "factor_ms": float(np.mean([i["ms_factor"] for i in infos])),
             "setup_s": setup_s,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * model.n_dof,

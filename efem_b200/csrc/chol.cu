@@ -103,7 +103,7 @@ struct Precond {
     int stage_d = 0, work_d = 0;
     // factor schedule: per (level, step) the fronts with a panel at that step and the SYRK tiles
     struct Step {
-        int level, k0, panel_off, panel_cnt, syrk_off, syrk_cnt;
+        int level, k0, panel_off, panel_cnt, syrk_off, syrk_cnt, panel_chunks;
     };
     std::vector<Step> steps;
     std::vector<int> lev_first_step;  // index into steps, nlev + 1
@@ -180,11 +180,18 @@ __global__ void __launch_bounds__(kFT) k_extend_add(FrontArgs a, const Tile* __r
 }
 
 // diagonal block and panel of step k0, one CTA per front in the step's list
+// grid (fronts, row chunks): every CTA factors the panel's kb x kb diagonal
+// block (one warp, left-looking: the same operations in the same order as a
+// right-looking sweep, so the factor does not depend on the grid), chunk 0
+// writes it back, and each CTA solves up to kFT of the rows below it, one per
+// thread.
 __global__ void __launch_bounds__(kFT) k_panel(FrontArgs a, const int* __restrict__ list, int k0)
 {
     const int s = list[blockIdx.x];
     const int r = a.nrow[s], c = a.ncol[s];
     const int kb = min(kNB, c - k0);
+    const int row0 = k0 + kb + static_cast<int>(blockIdx.y) * kFT;
+    if (blockIdx.y > 0 && row0 >= r) return;  // uniform over the CTA
     double* F = a.front + a.front_off[s];
     const int tid = threadIdx.x;
     __shared__ double D[kNB][kNB + 1];
@@ -193,32 +200,35 @@ __global__ void __launch_bounds__(kFT) k_panel(FrontArgs a, const int* __restric
         D[i][j] = (i >= j) ? F[(k0 + i) + static_cast<long long>(k0 + j) * r] : 0.0;
     }
     __syncthreads();
-    for (int j = 0; j < kb; j++) {
-        if (tid == 0) {
-            double d = D[j][j];
-            if (!(d > 0.0)) {
-                *a.fail = 1;
-                d = 1.0;
+    if (tid < 32) {
+        const int i = tid;
+        for (int j = 0; j < kb; j++) {
+            if (i == j) {
+                double d = D[j][j];
+                for (int k = 0; k < j; k++) d -= D[j][k] * D[j][k];
+                if (!(d > 0.0)) {
+                    if (blockIdx.y == 0) *a.fail = 1;
+                    d = 1.0;
+                }
+                D[j][j] = sqrt(d);
             }
-            D[j][j] = sqrt(d);
+            __syncwarp();
+            if (i > j && i < kb) {
+                double t = D[i][j];
+                for (int k = 0; k < j; k++) t -= D[i][k] * D[j][k];
+                D[i][j] = t / D[j][j];
+            }
+            __syncwarp();
         }
-        __syncthreads();
-        const double dj = D[j][j];
-        for (int i = j + 1 + tid; i < kb; i += kFT) D[i][j] /= dj;
-        __syncthreads();
-        const int t = kb - j - 1;
-        for (int idx = tid; idx < t * t; idx += kFT) {
-            const int ii = j + 1 + idx % t, kk = j + 1 + idx / t;
-            if (ii >= kk) D[ii][kk] -= D[ii][j] * D[kk][j];
+    }
+    __syncthreads();
+    if (blockIdx.y == 0)
+        for (int idx = tid; idx < kb * kb; idx += kFT) {
+            const int i = idx % kb, j = idx / kb;
+            if (i >= j) F[(k0 + i) + static_cast<long long>(k0 + j) * r] = D[i][j];
         }
-        __syncthreads();
-    }
-    for (int idx = tid; idx < kb * kb; idx += kFT) {
-        const int i = idx % kb, j = idx / kb;
-        if (i >= j) F[(k0 + i) + static_cast<long long>(k0 + j) * r] = D[i][j];
-    }
     // rows below the block: x L^T = f
-    for (int i = k0 + kb + tid; i < r; i += kFT) {
+    for (int i = row0 + tid; i < min(r, row0 + kFT); i += kFT) {
         double x[kNB];
 #pragma unroll
         for (int j = 0; j < kNB; j++) x[j] = j < kb ? F[i + static_cast<long long>(k0 + j) * r] : 0.0;
@@ -1291,7 +1301,7 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
         }
         P.ea_off.push_back(static_cast<int>(ea.size()));
         for (int k0 = 0; k0 < maxc; k0 += kNB) {
-            Precond::Step st { l, k0, static_cast<int>(panel_list.size()), 0, static_cast<int>(syrk.size()), 0 };
+            Precond::Step st { l, k0, static_cast<int>(panel_list.size()), 0, static_cast<int>(syrk.size()), 0, 1 };
             for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) {
                 const int s = S.level_list[q];
                 const int c = S.ncol[s], r = S.nrow[s];
@@ -1299,6 +1309,7 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
                 panel_list.push_back(s);
                 const int kb = std::min(kNB, c - k0);
                 const int m2 = r - k0 - kb;
+                st.panel_chunks = std::max(st.panel_chunks, (m2 + kFT - 1) / kFT);
                 const int nt = (m2 + kTS - 1) / kTS;
                 for (int tj = 0; tj < nt; tj++)
                     for (int ti = tj; ti < nt; ti++) syrk.push_back(make_int4(s, ti, tj, 0));
@@ -1612,7 +1623,7 @@ static efem_status precond_factor(Model& m, int* ok, double* ms_factor)
         }
         for (int q = P.lev_first_step[l]; q < P.lev_first_step[l + 1]; q++) {
             const Precond::Step& stp = P.steps[q];
-            k_panel<<<stp.panel_cnt, kFT, 0, m.stream>>>(a, P.d_panel_list + stp.panel_off, stp.k0);
+            k_panel<<<dim3(stp.panel_cnt, stp.panel_chunks), kFT, 0, m.stream>>>(a, P.d_panel_list + stp.panel_off, stp.k0);
             m.launches++;
             if (stp.syrk_cnt > 0) {
                 k_syrk<<<stp.syrk_cnt, kFT, 0, m.stream>>>(a, P.d_syrk + stp.syrk_off, stp.k0);
