@@ -100,7 +100,7 @@ struct Precond {
     SubTree* d_subs = nullptr;
     SubChunk* d_chunks = nullptr;
     int *d_depth = nullptr, *d_xidx = nullptr;
-    int stage_d = 0, work_d = 0, int_d = 0;
+    int stage_d = 0, work_d = 0;
     // factor schedule: per (level, step) the fronts with a panel at that step and the SYRK tiles
     struct Step {
         int level, k0, panel_off, panel_cnt, syrk_off, syrk_cnt, panel_chunks;
@@ -463,8 +463,7 @@ struct SolveArgs {
     const SolveItem* items;
     const int* tgt;           // targets of the four counter groups
     int n_items, ns;
-    int stage_d, work_d;      // shared-memory layout: two stage buffers of stage_d doubles, work_d doubles,
-    int int_d;                // then two index buffers of int_d ints
+    int stage_d, work_d;      // shared-memory layout: staged doubles, work doubles, then ints
     double* v;
     double* y;
     double* t;
@@ -707,71 +706,13 @@ __device__ __forceinline__ void gather3(double* dst, const double* v, const int*
     }
 }
 
-// Stage what an item reads that does not depend on other items: its factor
-// rows (odd row stride in shared memory, so lanes on different rows hit
-// different banks) and the index lists of its assembly, as one cp.async group.
-__device__ __forceinline__ void stage_item(const SolveArgs& A, const SolveItem& d, double* st, int* si)
-{
-    const FrontArgs& a = A.a;
-    const int kind = d.kind, s = d.s, r0 = d.r0, r1 = d.r1, R = r1 - r0, cbeg = d.cbeg, cend = d.cend;
-    const int r = a.nrow[s], c = a.ncol[s], m = r - c;
-    const long long ro = a.rows_off[s];
-    const double* X = a.dinv + a.dinv_off[s];
-    const double* XT = a.dinvT + a.dinv_off[s];
-    const double* W = a.w + a.lt_off[s];
-    const double* WT = a.wt + a.lt_off[s];
-    const int lc = odd(c), lm = odd(m);
-    const int nci = cend - cbeg, nci2 = d.cend2 - d.cbeg2;
-    switch (kind) {
-    case kFwdFront:
-        stage_rows(st, lc, X, c, c, c, 1, 0);           // L_JJ^{-1} rows (lower)
-        stage_rows(st + c * lc, lc, W, c, m, c, 0, 0);  // W rows
-        stage_i(si, a.contrib_ptr + ro, r + 1);
-        stage_i(si + r + 1, a.contrib_idx + cbeg, nci);
-        stage_i(si + r + 1 + nci, A.prow + ro, c);
-        break;
-    case kFwdY:
-        stage_rows(st, lc, X + static_cast<long long>(r0) * c, c, R, c, 1, r0);
-        stage_i(si, a.contrib_ptr + ro, r1 + 1);
-        stage_i(si + r1 + 1, a.contrib_idx + cbeg, nci);
-        stage_i(si + r1 + 1 + nci, A.prow + ro, r1);
-        break;
-    case kFwdG: {
-        stage_rows(st, lc, W + static_cast<long long>(r0) * c, c, R, c, 0, 0);
-        int* q = si;
-        stage_i(q, a.contrib_ptr + ro, c + 1);
-        stage_i(q + c + 1, a.contrib_idx + cbeg, nci);
-        stage_i(q + c + 1 + nci, A.prow + ro, c);
-        q += 2 * c + 1 + nci;
-        stage_i(q, a.contrib_ptr + ro + c + r0, R + 1);
-        stage_i(q + R + 1, a.contrib_idx + d.cbeg2, nci2);
-        break;
-    }
-    case kBwdFront:
-        stage_rows(st, lc, XT, c, c, c, 2, 0);             // L_JJ^{-T} rows (upper)
-        stage_rows(st + c * lc, lm, WT, m, c, m, 0, 0);  // W^T rows
-        stage_i(si, A.prow + ro, r);
-        break;
-    default:  // kBwdX
-        stage_rows(st, lc, XT + static_cast<long long>(r0) * c, c, R, c, 2, r0);
-        stage_rows(st + R * lc, lm, WT + static_cast<long long>(r0) * m, m, R, m, 0, 0);
-        stage_i(si, A.prow + ro, r);
-        break;
-    }
-    stage_commit();
-}
-
-// Each CTA takes items in ticket order and stages the next item's rows into
-// the second buffer while it waits for, and computes, the current one, so the
-// staging latency is off the dependency chain.
 __global__ void __launch_bounds__(kST) k_solve(SolveArgs A)
 {
     extern __shared__ double sm[];
-    double* stb[2] = { sm, sm + A.stage_d };                  // staged factor rows, two buffers
-    double* wk = sm + 2 * A.stage_d;                          // work vectors
-    int* sib[2] = { reinterpret_cast<int*>(wk + A.work_d),    // staged index lists, two buffers
-        reinterpret_cast<int*>(wk + A.work_d) + A.int_d };
-    __shared__ int cur_sh, nxt_sh, ok_sh;
+    double* st = sm;                                  // staged factor rows
+    double* wk = sm + A.stage_d;                      // work vectors
+    int* si = reinterpret_cast<int*>(wk + A.work_d);  // staged index lists
+    __shared__ int item_sh, ok_sh;
     const int ns = A.ns;
     int* cY = A.cnt;
     int* cGin = A.cnt + ns;
@@ -783,31 +724,70 @@ __global__ void __launch_bounds__(kST) k_solve(SolveArgs A)
     const int* tX = A.tgt + 3 * ns;
     const int tid = threadIdx.x;
     const FrontArgs& a = A.a;
+    int next = 0;  // thread 0: the ticket taken ahead
     if (tid == 0) {
-        const int t0 = atomicAdd(ticket, 1);
-        cur_sh = t0;
-        if (t0 == 0 && A.stamp) {
+        next = atomicAdd(ticket, 1);
+        if (next == 0 && A.stamp) {
             unsigned long long t;
             asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
             *A.stamp = t;
         }
     }
-    __syncthreads();
-    int it = cur_sh, par = 0;
-    if (it < A.n_items) stage_item(A, A.items[it], stb[0], sib[0]);
-    while (it < A.n_items) {
-        if (tid == 0) nxt_sh = atomicAdd(ticket, 1);  // in flight while this item runs
+    for (;;) {
+        if (tid == 0) item_sh = next;
         __syncthreads();
-        const int nx = nxt_sh;
-        if (nx < A.n_items) stage_item(A, A.items[nx], stb[par ^ 1], sib[par ^ 1]);
-        double* st = stb[par];
-        int* si = sib[par];
+        const int it = item_sh;
+        if (it >= A.n_items) break;
         const SolveItem d = A.items[it];
+        if (tid == 0) next = atomicAdd(ticket, 1);  // in flight while this item runs
         const int kind = d.kind, s = d.s, r0 = d.r0, r1 = d.r1, R = r1 - r0, cbeg = d.cbeg, cend = d.cend;
         const int p = A.parent[s];
         const int r = a.nrow[s], c = a.ncol[s], m = r - c, f0 = a.first[s];
+        const long long ro = a.rows_off[s];
+        const double* X = a.dinv + a.dinv_off[s];
+        const double* XT = a.dinvT + a.dinv_off[s];
+        const double* W = a.w + a.lt_off[s];
+        const double* WT = a.wt + a.lt_off[s];
         const int lc = odd(c), lm = odd(m);
-        const int nci = cend - cbeg;
+        const int nci = cend - cbeg, nci2 = d.cend2 - d.cbeg2;
+        // stage what does not depend on other items
+        switch (kind) {
+        case kFwdFront:
+            stage_rows(st, lc, X, c, c, c, 1, 0);           // L_JJ^{-1} rows (lower)
+            stage_rows(st + c * lc, lc, W, c, m, c, 0, 0);  // W rows
+            stage_i(si, a.contrib_ptr + ro, r + 1);
+            stage_i(si + r + 1, a.contrib_idx + cbeg, nci);
+            stage_i(si + r + 1 + nci, A.prow + ro, c);
+            break;
+        case kFwdY:
+            stage_rows(st, lc, X + static_cast<long long>(r0) * c, c, R, c, 1, r0);
+            stage_i(si, a.contrib_ptr + ro, r1 + 1);
+            stage_i(si + r1 + 1, a.contrib_idx + cbeg, nci);
+            stage_i(si + r1 + 1 + nci, A.prow + ro, r1);
+            break;
+        case kFwdG: {
+            stage_rows(st, lc, W + static_cast<long long>(r0) * c, c, R, c, 0, 0);
+            int* q = si;
+            stage_i(q, a.contrib_ptr + ro, c + 1);
+            stage_i(q + c + 1, a.contrib_idx + cbeg, nci);
+            stage_i(q + c + 1 + nci, A.prow + ro, c);
+            q += 2 * c + 1 + nci;
+            stage_i(q, a.contrib_ptr + ro + c + r0, R + 1);
+            stage_i(q + R + 1, a.contrib_idx + d.cbeg2, nci2);
+            break;
+        }
+        case kBwdFront:
+            stage_rows(st, lc, XT, c, c, c, 2, 0);             // L_JJ^{-T} rows (upper)
+            stage_rows(st + c * lc, lm, WT, m, c, m, 0, 0);  // W^T rows
+            stage_i(si, A.prow + ro, r);
+            break;
+        default:  // kBwdX
+            stage_rows(st, lc, XT + static_cast<long long>(r0) * c, c, R, c, 2, r0);
+            stage_rows(st + R * lc, lm, WT + static_cast<long long>(r0) * m, m, R, m, 0, 0);
+            stage_i(si, A.prow + ro, r);
+            break;
+        }
+        stage_commit();
         if (tid == 0) {
             bool ok;
             switch (kind) {
@@ -818,10 +798,7 @@ __global__ void __launch_bounds__(kST) k_solve(SolveArgs A)
             }
             ok_sh = ok;
         }
-        if (nx < A.n_items)
-            stage_wait_but_one();  // the current item's group; the next one's may still be in flight
-        else
-            stage_wait();
+        stage_wait();
         __syncthreads();
         if (ok_sh) {
             switch (kind) {
@@ -934,8 +911,6 @@ __global__ void __launch_bounds__(kST) k_solve(SolveArgs A)
             default: atomicAdd(cX + s, 1); break;  // kBwdFront, kBwdX
             }
         }
-        it = nx;
-        par ^= 1;
     }
 }
 
@@ -1230,7 +1205,7 @@ void enqueue_solve(const Precond& P, const FrontArgs& a, const SolveBufs& b, dou
     const SubArgs B { a, P.d_parent, P.d_prow, P.d_perm, P.d_subs, P.d_chunks, P.d_depth, P.d_xidx, P.sub_max_r,
         P.sub_max_cols, P.sub_max_depth, P.sub_max_m, P.sub_max_c, P.sub_max_mroot, d_v, b.y, b.upd, stamp };
     if (P.n_subs > 0) k_sub_fwd<<<P.n_subs, kST, P.sub_smem_f, st>>>(B);
-    SolveArgs A { a, P.d_parent, P.d_prow, P.d_items, P.d_tgt, P.n_items, ns, P.stage_d, P.work_d, P.int_d, d_v, b.y, b.t,
+    SolveArgs A { a, P.d_parent, P.d_prow, P.d_items, P.d_tgt, P.n_items, ns, P.stage_d, P.work_d, d_v, b.y, b.t,
         b.upd, b.cnt, P.n_subs > 0 ? nullptr : stamp };
     if (P.n_items > 0) k_solve<<<P.solve_grid, kST, P.solve_smem, st>>>(A);
     if (P.n_subs > 0) k_sub_bwd<<<P.n_subs, kST, P.sub_smem_b, st>>>(B);
@@ -1544,15 +1519,9 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
         }
     }
     P.n_items = static_cast<int>(items.size());
-    P.work_d = static_cast<int>(work_d);
-    // two stage buffers (the next item is staged during the current one), the
-    // work vectors, two index buffers; stage_d rounded to even so the second
-    // buffer stays 16-byte aligned, int_d to a multiple of 4
-    stage_d += stage_d & 1;
-    ints = (ints + 3) / 4 * 4;
     P.stage_d = static_cast<int>(stage_d);
-    P.int_d = static_cast<int>(ints);
-    P.solve_smem = sizeof(double) * (2 * stage_d + work_d) + sizeof(int) * 2 * ints;
+    P.work_d = static_cast<int>(work_d);
+    P.solve_smem = sizeof(double) * (stage_d + work_d) + sizeof(int) * ints;
     if (P.solve_smem > 200 * 1024) {
         set_error("a front of the approximate-Jacobian factor is too large for the solve kernel ("
             + std::to_string(P.max_r) + " rows)");
