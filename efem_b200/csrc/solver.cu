@@ -618,11 +618,12 @@ __global__ void __launch_bounds__(kThreads) k_pass3(const double* __restrict__ z
     for (int j = tid; j < ncorr; j += kThreads) S->coef[j] = scf[j];
 }
 
-// Pass 4: d = z0 + sum_j coef_j s_j and the start of the line search
-// (r.d, xp = x, rp = r, step 1, line-search loop condition on)
+// Pass 4: d = z0 + sum_j coef_j s_j, the start of the line search (r.d,
+// xp = x, rp = r, step 1) and its first trial: x = xp + 1 d, r = -f_ext for
+// the residual that follows (whose start time is stamped by the last CTA)
 __global__ void __launch_bounds__(kThreads) k_pass4(double* __restrict__ d, const double* __restrict__ z,
-    const double* __restrict__ Sh, const double* __restrict__ r, const double* __restrict__ x, double* __restrict__ xp,
-    double* __restrict__ rp, size_t n, Scalars* S, double* partials, cudaGraphConditionalHandle h_ls, int set_h)
+    const double* __restrict__ Sh, double* __restrict__ r, double* __restrict__ x, double* __restrict__ xp,
+    double* __restrict__ rp, const double* __restrict__ fext, size_t n, Scalars* S, double* partials)
 {
     __shared__ double cf[kMaxHist];
     const int ncorr = S->ncorr;
@@ -635,10 +636,12 @@ __global__ void __launch_bounds__(kThreads) k_pass4(double* __restrict__ d, cons
         double di = z[i];
         for (int j = 0; j < ncorr; j++) di += cf[j] * Sh[j * n + i];
         d[i] = di;
-        const double ri = r[i];
+        const double ri = r[i], xi = x[i];
         v[0] += ri * di;
-        xp[i] = x[i];
+        xp[i] = xi;
         rp[i] = ri;
+        x[i] = xi + 1.0 * di;
+        r[i] = -fext[i];
     }
     block_reduce<1>(v, ops);
     if (grid_finish<1>(v, ops, partials, &S->counter[1])) {
@@ -647,7 +650,7 @@ __global__ void __launch_bounds__(kThreads) k_pass4(double* __restrict__ d, cons
         S->ls_t = 0;
         S->tr_i++;  // the next iteration's trace record
         S->tr_evals = 0;
-        if (set_h) cudaGraphSetConditional(h_ls, 1u);  // the line search's first trial always runs
+        S->t0_res = gtimer();
     }
 }
 
@@ -850,7 +853,7 @@ double* mapped(double* h)
 }
 
 // the residual at the current trial x and the line-search reductions; inside
-// the device-driven line search (h_ls given) r was started by k_trial_dev and
+// the device-driven line search (h_ls given) r was started by k_pass4 or k_trial_dev and
 // the reduction applies the accept / scale rule
 efem_status enqueue_trial_tail(Model& m, SolverWS& w, double* x, cudaStream_t st,
     const cudaGraphConditionalHandle* h_ls = nullptr, bool init_r = true)
@@ -871,8 +874,7 @@ efem_status enqueue_first(Model& m, SolverWS& w, double* x, cudaStream_t st)
 }
 
 // add_correction + two-loop with H0 + line-search start
-efem_status enqueue_body(Model& m, SolverWS& w, double* x, bool use_factor, cudaStream_t st,
-    const cudaGraphConditionalHandle* h_ls)
+efem_status enqueue_body(Model& m, SolverWS& w, double* x, bool use_factor, cudaStream_t st)
 {
     const size_t n = w.n;
     const int mm = w.m;
@@ -899,8 +901,7 @@ efem_status enqueue_body(Model& m, SolverWS& w, double* x, bool use_factor, cuda
 #undef P3
     default: k_pass3<<<g3, kThreads, sm3, st>>>(w.q, w.Y, n, mm, w.sc, w.partials, w.sums, use_factor ? 1 : 0);
     }
-    k_pass4<<<grid_for(n), kThreads, 0, st>>>(w.d, w.q, w.S, w.r, x, w.xp, w.rp, n, w.sc, w.partials,
-        h_ls ? *h_ls : cudaGraphConditionalHandle(), h_ls ? 1 : 0);
+    k_pass4<<<grid_for(n), kThreads, 0, st>>>(w.d, w.q, w.S, w.r, x, w.xp, w.rp, m.d_fext, n, w.sc, w.partials);
     return EFEM_OK;
 }
 
@@ -936,8 +937,9 @@ efem_status add_while(cudaStream_t st, cudaGraphConditionalHandle h, cudaGraph_t
 }
 
 // The device-driven iteration loop:
-//   k_loop_start; while (hIter) { body; while (hLs) { trial; residual; reductions + decision }; k_iter_decide }
-// (pass 4 sets hLs to 1 on every iteration: the first trial always runs)
+//   k_loop_start;
+//   while (hIter) { passes + H0 + first trial; residual; reductions + decision (sets hLs);
+//                   while (hLs) { trial; residual; reductions + decision }; k_iter_decide }
 efem_status capture_loop(Model& m, SolverWS& w, double* x, bool use_factor, cudaGraphExec_t* out)
 {
     std::lock_guard<std::mutex> lock(capture_mutex());
@@ -969,7 +971,10 @@ efem_status capture_loop(Model& m, SolverWS& w, double* x, bool use_factor, cuda
             s = EFEM_ERR_CUDA;
             break;
         }
-        s = enqueue_body(m, w, x, use_factor, s1, &h_ls);
+        // passes, H0 and the first trial (pass 4), its residual and the line
+        // search's decision, which sets hLs; then the further trials
+        s = enqueue_body(m, w, x, use_factor, s1);
+        if (s == EFEM_OK) s = enqueue_trial_tail(m, w, x, s1, &h_ls, false);
         if (s == EFEM_OK) s = add_while(s1, h_ls, &ls_body);
         if (s == EFEM_OK && cudaStreamBeginCaptureToGraph(s2, ls_body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
             s = EFEM_ERR_CUDA;
@@ -1004,11 +1009,8 @@ efem_status capture_step(Model& m, SolverWS& w, double* x, bool use_factor, cuda
     cudaStream_t s0 = w.capture[0];
     cudaGraph_t g = nullptr;
     EFEM_CUDA(cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal));
-    efem_status s = enqueue_body(m, w, x, use_factor, s0, nullptr);
-    if (s == EFEM_OK) {
-        k_trial_dev<<<grid_for(w.n), kThreads, 0, s0>>>(x, w.xp, w.d, w.r, m.d_fext, w.n, w.sc);
-        s = enqueue_trial_tail(m, w, x, s0, nullptr, false);
-    }
+    efem_status s = enqueue_body(m, w, x, use_factor, s0);
+    if (s == EFEM_OK) s = enqueue_trial_tail(m, w, x, s0, nullptr, false);  // pass 4 started the first trial
     const cudaError_t e = cudaStreamEndCapture(s0, &g);
     m.launches = launches;
     if (s != EFEM_OK || e != cudaSuccess) {
@@ -1169,7 +1171,7 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
         }
         k++;
         if (host_loop) {  // iterations 2, 3, ... one graph launch each, decisions on the host
-            const long long per_step = 4 + (ok ? precond_launch_count(m) : 0) + per_res + 1;
+            const long long per_step = 4 + (ok ? precond_launch_count(m) : 0) + (per_res - 1) + 1;
             for (;;) {
                 EFEM_CUDA(cudaGraphLaunch(gr.step, st));
                 EFEM_CUDA(cudaStreamSynchronize(st));
@@ -1207,7 +1209,8 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
             kIterCap, k);
         m.launches++;
         // passes, H0, trial (which starts r), residual, reductions, iteration decision
-        const long long per_body = 4 + (ok ? precond_launch_count(m) : 0) + per_res + 2;
+        // passes (pass 4 starts the first trial), H0, residual, reductions, iteration decision
+        const long long per_body = 4 + (ok ? precond_launch_count(m) : 0) + (per_res - 1) + 2;
         const long long per_extra = per_res + 1;  // trial, residual, reductions
         long long n_extra = 0;
         int status = kRunning;
