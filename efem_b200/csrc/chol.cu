@@ -179,12 +179,12 @@ __global__ void __launch_bounds__(kFT) k_extend_add(FrontArgs a, const Tile* __r
     }
 }
 
-// diagonal block and panel of step k0, one CTA per front in the step's list
-// grid (fronts, row chunks): every CTA factors the panel's kb x kb diagonal
-// block (one warp, left-looking: the same operations in the same order as a
-// right-looking sweep, so the factor does not depend on the grid), chunk 0
-// writes it back, and each CTA solves up to kFT of the rows below it, one per
-// thread.
+// Diagonal block and panel of step k0 for the fronts in the step's list.
+// Grid (fronts, row chunks): every CTA factors the panel's kb x kb diagonal
+// block (one warp, left-looking, with the reciprocals of the pivots so that
+// no division sits on a dependent chain; every CTA computes the same block,
+// so the factor does not depend on the grid), chunk 0 writes it back, and
+// each CTA solves up to kFT of the rows below it, one per thread.
 __global__ void __launch_bounds__(kFT) k_panel(FrontArgs a, const int* __restrict__ list, int k0)
 {
     const int s = list[blockIdx.x];
@@ -195,6 +195,7 @@ __global__ void __launch_bounds__(kFT) k_panel(FrontArgs a, const int* __restric
     double* F = a.front + a.front_off[s];
     const int tid = threadIdx.x;
     __shared__ double D[kNB][kNB + 1];
+    __shared__ double Dinv[kNB];  // 1 / L_jj: the divisions leave the dependent chains
     for (int idx = tid; idx < kb * kb; idx += kFT) {
         const int i = idx % kb, j = idx / kb;
         D[i][j] = (i >= j) ? F[(k0 + i) + static_cast<long long>(k0 + j) * r] : 0.0;
@@ -210,13 +211,15 @@ __global__ void __launch_bounds__(kFT) k_panel(FrontArgs a, const int* __restric
                     if (blockIdx.y == 0) *a.fail = 1;
                     d = 1.0;
                 }
-                D[j][j] = sqrt(d);
+                const double sd = sqrt(d);
+                D[j][j] = sd;
+                Dinv[j] = 1.0 / sd;
             }
             __syncwarp();
             if (i > j && i < kb) {
                 double t = D[i][j];
                 for (int k = 0; k < j; k++) t -= D[i][k] * D[j][k];
-                D[i][j] = t / D[j][j];
+                D[i][j] = t * Dinv[j];
             }
             __syncwarp();
         }
@@ -239,7 +242,7 @@ __global__ void __launch_bounds__(kFT) k_panel(FrontArgs a, const int* __restric
 #pragma unroll
                 for (int k = 0; k < kNB; k++)
                     if (k < j) sum -= x[k] * D[j][k];
-                x[j] = sum / D[j][j];
+                x[j] = sum * Dinv[j];
             }
         }
 #pragma unroll
