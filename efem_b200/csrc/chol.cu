@@ -125,6 +125,9 @@ struct Precond {
     int4* d_syrk = nullptr;
     double *d_front = nullptr, *d_dinv = nullptr, *d_upd = nullptr, *d_y = nullptr, *d_t = nullptr,
            *d_vals = nullptr;
+    // graph replay of the numeric factorisation (the same launches every solve)
+    cudaGraphExec_t factor_exec = nullptr;
+    long long factor_launches = 0;
     // graph replay of the solve, per (input vector, work buffers)
     cudaStream_t capture = nullptr;
     std::map<std::pair<double*, double*>, cudaGraphExec_t> graphs;
@@ -1223,6 +1226,7 @@ void free_precond(Model& m)
     Precond& P = *m.precond;
     for (auto& kv : P.graphs) cudaGraphExecDestroy(kv.second);
     P.graphs.clear();
+    if (P.factor_exec) cudaGraphExecDestroy(P.factor_exec);
     if (P.capture) cudaStreamDestroy(P.capture);
     for (int** p : { &P.d_first, &P.d_ncol, &P.d_nrow, &P.d_rows, &P.d_child_ptr, &P.d_child_list, &P.d_relind,
              &P.d_level_list, &P.d_perm, &P.d_fail, &P.d_panel_list, &P.d_contrib_ptr, &P.d_contrib_idx, &P.d_below_front, &P.d_tgt, &P.d_parent, &P.d_cnt, &P.d_prow, &P.d_depth, &P.d_xidx })
@@ -1603,49 +1607,80 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
 
 // Numeric factorisation (every solve, like LBFGSSolver::updateApproxJacobi):
 // scatter L into the fronts, factor level by level, invert the diagonal blocks.
-static efem_status precond_factor(Model& m, int* ok, double* ms_factor)
+// the launches of one numeric factorisation, in order, on stream st; returns
+// the number of kernels
+static long long enqueue_factor(Precond& P, cudaStream_t st)
 {
-    Precond& P = *m.precond;
     const Symbolic& S = P.S;
-    cudaEvent_t e0, e1;
-    EFEM_CUDA(cudaEventCreate(&e0));
-    EFEM_CUDA(cudaEventCreate(&e1));
-    EFEM_CUDA(cudaEventRecord(e0, m.stream));
-    EFEM_CUDA(cudaMemsetAsync(P.d_front, 0, sizeof(double) * S.front_size, m.stream));
-    EFEM_CUDA(cudaMemsetAsync(P.d_fail, 0, sizeof(int), m.stream));
+    long long n = 0;
+    cudaMemsetAsync(P.d_front, 0, sizeof(double) * S.front_size, st);
+    cudaMemsetAsync(P.d_fail, 0, sizeof(int), st);
     const long long na = static_cast<long long>(S.a_pos.size());
-    k_scatter_a<<<static_cast<int>(std::min<long long>(1184, (na + 255) / 256 + 1)), 256, 0, m.stream>>>(
+    k_scatter_a<<<static_cast<int>(std::min<long long>(1184, (na + 255) / 256 + 1)), 256, 0, st>>>(
         P.d_front, P.d_a_pos, P.d_a_src, P.d_vals, na);
-    m.launches++;
+    n++;
     FrontArgs a = args_of(P);
     for (int l = 0; l < P.nlev; l++) {
         const int cnt = P.ea_off[l + 1] - P.ea_off[l];
         if (cnt > 0) {
-            k_extend_add<<<cnt, kFT, 0, m.stream>>>(a, P.d_ea + P.ea_off[l]);
-            m.launches++;
+            k_extend_add<<<cnt, kFT, 0, st>>>(a, P.d_ea + P.ea_off[l]);
+            n++;
         }
         for (int q = P.lev_first_step[l]; q < P.lev_first_step[l + 1]; q++) {
             const Precond::Step& stp = P.steps[q];
-            k_panel<<<dim3(stp.panel_cnt, stp.panel_chunks), kFT, 0, m.stream>>>(a, P.d_panel_list + stp.panel_off, stp.k0);
-            m.launches++;
+            k_panel<<<dim3(stp.panel_cnt, stp.panel_chunks), kFT, 0, st>>>(a, P.d_panel_list + stp.panel_off, stp.k0);
+            n++;
             if (stp.syrk_cnt > 0) {
-                k_syrk<<<stp.syrk_cnt, kFT, 0, m.stream>>>(a, P.d_syrk + stp.syrk_off, stp.k0);
-                m.launches++;
+                k_syrk<<<stp.syrk_cnt, kFT, 0, st>>>(a, P.d_syrk + stp.syrk_off, stp.k0);
+                n++;
             }
         }
     }
     if (P.n_inv_tiles > 0) {
-        k_diag_inv<<<P.n_inv_tiles, 32, 0, m.stream>>>(a, P.d_inv);
-        m.launches++;
+        k_diag_inv<<<P.n_inv_tiles, 32, 0, st>>>(a, P.d_inv);
+        n++;
         if (P.n_oinv > 0) {
-            k_offdiag_inv<<<P.n_oinv, kIT, 0, m.stream>>>(a, P.d_oinv);
-            m.launches++;
+            k_offdiag_inv<<<P.n_oinv, kIT, 0, st>>>(a, P.d_oinv);
+            n++;
         }
         if (P.n_wtiles > 0) {
-            k_w<<<P.n_wtiles, 256, 0, m.stream>>>(a, P.d_wtiles);
-            m.launches++;
+            k_w<<<P.n_wtiles, 256, 0, st>>>(a, P.d_wtiles);
+            n++;
         }
     }
+    return n;
+}
+
+// The factorisation's few hundred dependent launches are captured once into a
+// CUDA graph and replayed every solve (shorter gaps between the launches).
+static efem_status precond_factor(Model& m, int* ok, double* ms_factor)
+{
+    Precond& P = *m.precond;
+    if (!P.factor_exec) {
+        std::lock_guard<std::mutex> lock(capture_mutex());
+        cudaGraph_t g = nullptr;
+        EFEM_CUDA(cudaStreamBeginCapture(P.capture, cudaStreamCaptureModeThreadLocal));
+        P.factor_launches = enqueue_factor(P, P.capture);
+        const cudaError_t e = cudaStreamEndCapture(P.capture, &g);
+        if (e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            set_error(std::string("capture of the factorisation: ") + cudaGetErrorString(e));
+            return EFEM_ERR_CUDA;
+        }
+        const cudaError_t ei = cudaGraphInstantiate(&P.factor_exec, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) {
+            P.factor_exec = nullptr;
+            set_error(std::string("factorisation graph: ") + cudaGetErrorString(ei));
+            return EFEM_ERR_CUDA;
+        }
+    }
+    cudaEvent_t e0, e1;
+    EFEM_CUDA(cudaEventCreate(&e0));
+    EFEM_CUDA(cudaEventCreate(&e1));
+    EFEM_CUDA(cudaEventRecord(e0, m.stream));
+    EFEM_CUDA(cudaGraphLaunch(P.factor_exec, m.stream));
+    m.launches += P.factor_launches;
     EFEM_CUDA(cudaGetLastError());
     EFEM_CUDA(cudaEventRecord(e1, m.stream));
     int fail = 0;
