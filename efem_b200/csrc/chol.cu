@@ -714,6 +714,7 @@ __device__ __forceinline__ void gather3(double* dst, const double* v, const int*
 
 __global__ void __launch_bounds__(kST) k_solve(SolveArgs A)
 {
+    griddep_wait();
     extern __shared__ double sm[];
     double* st = sm;                                  // staged factor rows
     double* wk = sm + A.stage_d;                      // work vectors
@@ -743,7 +744,10 @@ __global__ void __launch_bounds__(kST) k_solve(SolveArgs A)
         if (tid == 0) item_sh = next;
         __syncthreads();
         const int it = item_sh;
-        if (it >= A.n_items) break;
+        if (it >= A.n_items) {
+            griddep_launch();  // no more items for this CTA
+            break;
+        }
         const SolveItem d = A.items[it];
         if (tid == 0) next = atomicAdd(ticket, 1);  // in flight while this item runs
         const int kind = d.kind, s = d.s, r0 = d.r0, r1 = d.r1, R = r1 - r0, cbeg = d.cbeg, cend = d.cend;
@@ -1213,7 +1217,7 @@ void enqueue_solve(const Precond& P, const FrontArgs& a, const SolveBufs& b, dou
     if (P.n_subs > 0) k_sub_fwd<<<P.n_subs, kST, P.sub_smem_f, st>>>(B);
     SolveArgs A { a, P.d_parent, P.d_prow, P.d_items, P.d_tgt, P.n_items, ns, P.stage_d, P.work_d, d_v, b.y, b.t,
         b.upd, b.cnt, P.n_subs > 0 ? nullptr : stamp };
-    if (P.n_items > 0) k_solve<<<P.solve_grid, kST, P.solve_smem, st>>>(A);
+    if (P.n_items > 0) launch_k(k_solve, P.solve_grid, kST, P.solve_smem, st, A);
     if (P.n_subs > 0) k_sub_bwd<<<P.n_subs, kST, P.sub_smem_b, st>>>(B);
 }
 

@@ -18,6 +18,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/efem_gpu.h"
@@ -166,6 +167,40 @@ struct Model {
 // ------------------------------------------------------------------ errors
 void set_error(const std::string& msg);
 const std::string& get_error();
+
+// Programmatic dependent launch inside the solver's graph captures: while
+// t_pdl is set, kernels launched through launch_k may be scheduled while the
+// kernel before them in the stream is still finishing (their CTAs become
+// resident and wait), which takes the launch gap off the iteration's chain.
+// Every kernel launched this way calls griddep_wait() before it touches
+// memory; kernels call griddep_launch() once their main work is issued.
+// Outside such captures launch_k is a plain launch.
+extern thread_local bool t_pdl;
+
+#ifdef __CUDACC__
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <typename... P, typename... A>
+inline void launch_k(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, A&&... args)
+{
+    if (!t_pdl) {
+        kernel<<<grid, block, smem, st>>>(std::forward<A>(args)...);
+        return;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
+}
+#endif
 
 #define EFEM_CUDA(call)                                                                          \
     do {                                                                                         \

@@ -65,6 +65,7 @@ constexpr int elems_per_cta() { return (BLK / NGP) < 1 ? 1 : ((BLK / NGP) > 128 
 template <int NEN, int NGP, typename T, int BLK>
 __global__ void __launch_bounds__(BLK) k_elem_residual(ElemArgs<T> a)
 {
+    griddep_wait();
     constexpr int EPB = elems_per_cta<NGP, BLK>();
     // per-element rows padded to an odd length, so that threads on
     // consecutive elements (phases 1 and 3) or Gauss points (phase 2) read
@@ -175,6 +176,7 @@ __global__ void __launch_bounds__(BLK) k_elem_residual(ElemArgs<T> a)
             atomicAdd(a.r + 3 * node + 2, static_cast<double>(r2));
         }
     }
+    griddep_launch();
 }
 
 template <typename T>
@@ -200,6 +202,7 @@ struct FaceArgs {
 template <int NEN, typename T>
 __global__ void __launch_bounds__(kBlock) k_face_residual(FaceArgs<T> a)
 {
+    griddep_wait();
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= a.n) return;
     const int t = a.table[f];
@@ -290,6 +293,7 @@ __global__ void __launch_bounds__(kBlock) k_face_residual(FaceArgs<T> a)
 __global__ void __launch_bounds__(kBlock) k_gather(int n_free, const int* __restrict__ gptr,
     const int* __restrict__ gidx, const double* __restrict__ contrib, size_t n_slots, double* __restrict__ r)
 {
+    griddep_wait();
     const int i = blockIdx.x * kBlock + threadIdx.x;
     if (i >= n_free) return;
     double s0 = r[3 * i], s1 = r[3 * i + 1], s2 = r[3 * i + 2];
@@ -308,7 +312,7 @@ template <int NEN, int NGP, typename T, int BLK>
 void launch_elem_blk(const ElemArgs<T>& a, cudaStream_t st)
 {
     constexpr int EPB = elems_per_cta<NGP, BLK>();
-    k_elem_residual<NEN, NGP, T, BLK><<<(a.n + EPB - 1) / EPB, BLK, 0, st>>>(a);
+    launch_k(k_elem_residual<NEN, NGP, T, BLK>, (a.n + EPB - 1) / EPB, BLK, 0, st, a);
 }
 
 template <int NEN, int NGP, typename T>
@@ -348,10 +352,10 @@ void dispatch_face(const DevFaces& f, const T* J0, const T* tw, const T* tN, con
         sc.slot0 };
     const int grid = (f.n + kBlock - 1) / kBlock;
     switch (f.nen) {
-    case 4: k_face_residual<4, T><<<grid, kBlock, 0, st>>>(a); break;
-    case 8: k_face_residual<8, T><<<grid, kBlock, 0, st>>>(a); break;
-    case 10: k_face_residual<10, T><<<grid, kBlock, 0, st>>>(a); break;
-    case 20: k_face_residual<20, T><<<grid, kBlock, 0, st>>>(a); break;
+    case 4: launch_k(k_face_residual<4, T>, grid, kBlock, 0, st, a); break;
+    case 8: launch_k(k_face_residual<8, T>, grid, kBlock, 0, st, a); break;
+    case 10: launch_k(k_face_residual<10, T>, grid, kBlock, 0, st, a); break;
+    case 20: launch_k(k_face_residual<20, T>, grid, kBlock, 0, st, a); break;
     }
 }
 
@@ -452,8 +456,8 @@ efem_status launch_residual_on(Model& m, const double* d_u, double* d_r, cudaStr
             dispatch_face<double>(f, f.J0inv, f.t_w, f.t_N, f.t_dN, m.n_free, d_u, d_r, stream, sc);
     }
     if (det) {
-        k_gather<<<(m.n_free + kBlock - 1) / kBlock, kBlock, 0, stream>>>(m.n_free, m.d_gptr, m.d_gidx, m.d_contrib,
-            m.n_slots, d_r);
+        launch_k(k_gather, (m.n_free + kBlock - 1) / kBlock, kBlock, 0, stream, m.n_free, m.d_gptr, m.d_gidx,
+            m.d_contrib, m.n_slots, d_r);
         m.launches++;
     }
     EFEM_CUDA(cudaGetLastError());

@@ -46,6 +46,8 @@
 
 namespace efem {
 
+thread_local bool t_pdl = false;
+
 namespace {
 
 constexpr int kThreads = 256;
@@ -241,6 +243,7 @@ __global__ void __launch_bounds__(kThreads) k_ls_reduce(const double* __restrict
     const double* __restrict__ x, size_t n, Scalars* S, double* partials, const int* perr, double* hread,
     cudaGraphConditionalHandle h, int decide)
 {
+    griddep_wait();
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         S->t_res += gtimer() - S->t0_res;  // the residual just ended
         // the loop stops unless the last CTA below decides on another trial
@@ -257,6 +260,7 @@ __global__ void __launch_bounds__(kThreads) k_ls_reduce(const double* __restrict
         v[3] += xi * xi;
         v[4] += ri * ri;
     }
+    griddep_launch();
     block_reduce<5>(v, ops);
     if (grid_finish<5>(v, ops, partials, &S->counter[0])) {
         S->dg = v[0];
@@ -331,6 +335,7 @@ __global__ void __launch_bounds__(kThreads) k_pass1(const double* __restrict__ x
     const double* __restrict__ r, const double* __restrict__ rp, double* __restrict__ Sh, double* __restrict__ Yh,
     size_t n, int m, Scalars* S, double* partials, double* sums)
 {
+    griddep_wait();
     const int loc = S->ptr % m;
     const int ncorr = S->ncorr < m ? S->ncorr + 1 : m;  // count after the insertion; slots 0..ncorr-1 hold pairs
     const int row = blockIdx.y;
@@ -440,6 +445,7 @@ __global__ void __launch_bounds__(kThreads) k_pass1_m(const double* __restrict__
     const double* __restrict__ r, const double* __restrict__ rp, double* __restrict__ Sh, double* __restrict__ Yh,
     size_t n, Scalars* S, double* partials)
 {
+    griddep_wait();
     constexpr int NV = 3 * M + 2;
     const int m = M;
     const int loc = S->ptr % m;
@@ -467,6 +473,7 @@ __global__ void __launch_bounds__(kThreads) k_pass1_m(const double* __restrict__
             }
         }
     }
+    griddep_launch();
     __shared__ double tot[NV];
     if (!grid_sums<NV>(v, partials, &S->counter[2], tot)) return;
     extern __shared__ double dyn[];
@@ -513,6 +520,7 @@ template <int M>
 __global__ void __launch_bounds__(kThreads) k_pass3_m(const double* __restrict__ z, const double* __restrict__ Yh,
     size_t n, Scalars* S, double* partials, int time_pc)
 {
+    griddep_wait();
     const int m = M, ncorr = S->ncorr;
     if (blockIdx.x == 0 && threadIdx.x == 0 && time_pc) S->t_pc += gtimer() - S->t0_pc;  // H0 just ended
     double v[M];
@@ -525,6 +533,7 @@ __global__ void __launch_bounds__(kThreads) k_pass3_m(const double* __restrict__
         for (int j = 0; j < M; j++)
             if (j < ncorr) v[j] += Yh[j * n + i] * zi;
     }
+    griddep_launch();
     __shared__ double tot[M];
     if (!grid_sums<M>(v, partials, &S->counter[3], tot)) return;
     extern __shared__ double dyn[];
@@ -560,6 +569,7 @@ __global__ void __launch_bounds__(kThreads) k_pass3_m(const double* __restrict__
 __global__ void __launch_bounds__(kThreads) k_pass2(double* __restrict__ q, const double* __restrict__ r,
     const double* __restrict__ Yh, size_t n, int m, int divide_theta, const Scalars* S, int* clear, int n_clear)
 {
+    griddep_wait();
     __shared__ double al[kMaxHist];
     const int ncorr = S->ncorr;
     for (int j = threadIdx.x; j < ncorr; j += kThreads) al[j] = S->alpha[j];
@@ -571,6 +581,7 @@ __global__ void __launch_bounds__(kThreads) k_pass2(double* __restrict__ q, cons
         for (int j = 0; j < ncorr; j++) qi -= al[j] * Yh[j * n + i];
         q[i] = divide_theta ? qi / th : qi;
     }
+    griddep_launch();
     if (clear)
         for (int k = blockIdx.x * kThreads + threadIdx.x; k < n_clear; k += gridDim.x * kThreads) clear[k] = 0;
 }
@@ -580,6 +591,7 @@ __global__ void __launch_bounds__(kThreads) k_pass2(double* __restrict__ q, cons
 __global__ void __launch_bounds__(kThreads) k_pass3(const double* __restrict__ z, const double* __restrict__ Yh, size_t n,
     int m, Scalars* S, double* partials, double* sums, int time_pc)
 {
+    griddep_wait();
     const int ncorr = S->ncorr, row = blockIdx.y;
     if (blockIdx.x == 0 && row == 0 && threadIdx.x == 0 && time_pc) S->t_pc += gtimer() - S->t0_pc;  // H0 just ended
     double v[1] = { 0 };
@@ -625,6 +637,7 @@ __global__ void __launch_bounds__(kThreads) k_pass4(double* __restrict__ d, cons
     const double* __restrict__ Sh, double* __restrict__ r, double* __restrict__ x, double* __restrict__ xp,
     double* __restrict__ rp, const double* __restrict__ fext, size_t n, Scalars* S, double* partials)
 {
+    griddep_wait();
     __shared__ double cf[kMaxHist];
     const int ncorr = S->ncorr;
     for (int j = threadIdx.x; j < ncorr; j += kThreads) cf[j] = S->coef[j];
@@ -643,6 +656,7 @@ __global__ void __launch_bounds__(kThreads) k_pass4(double* __restrict__ d, cons
         x[i] = xi + 1.0 * di;
         r[i] = -fext[i];
     }
+    griddep_launch();
     block_reduce<1>(v, ops);
     if (grid_finish<1>(v, ops, partials, &S->counter[1])) {
         S->dg0 = v[0];
@@ -665,6 +679,7 @@ __global__ void k_neg_copy(double* __restrict__ q, const double* __restrict__ r,
 __global__ void k_trial_dev(double* __restrict__ x, const double* __restrict__ xp, const double* __restrict__ d,
     double* __restrict__ r, const double* __restrict__ fext, size_t n, Scalars* S)
 {
+    griddep_wait();
     if (blockIdx.x == 0 && threadIdx.x == 0) S->t0_res = gtimer();
     const double step = S->step;
     GRID_STRIDE(i, n)
@@ -680,6 +695,7 @@ __global__ void k_trial_dev(double* __restrict__ x, const double* __restrict__ x
 // iterations per launch.  Sets the iteration loop condition.
 __global__ void k_iter_decide(Scalars* S, cudaGraphConditionalHandle h, double* hread)
 {
+    griddep_wait();
     if (threadIdx.x != 0) return;
     const double rinf = S->rinf, xinf = S->xinf;
     int st = kRunning;
@@ -745,6 +761,7 @@ int row_blocks(size_t n) { return static_cast<int>(std::min<size_t>(kRowBlocks, 
 struct SolverWS {
     size_t n = 0;
     int m = 0;
+    bool pdl = true;  // programmatic dependent launch in the captured iteration graphs (off if a capture refused it)
     double *r = nullptr, *xp = nullptr, *rp = nullptr, *d = nullptr, *q = nullptr;
     double *S = nullptr, *Y = nullptr;
     double* partials = nullptr;
@@ -861,7 +878,7 @@ efem_status enqueue_trial_tail(Model& m, SolverWS& w, double* x, cudaStream_t st
     const size_t n = w.n;
     efem_status s = launch_residual_on(m, x, w.r, st, &w.sc->t0_res, init_r);
     if (s != EFEM_OK) return s;
-    k_ls_reduce<<<grid_for(n), kThreads, 0, st>>>(w.r, w.d, x, n, w.sc, w.partials, precond_error_flag(m),
+    launch_k(k_ls_reduce, grid_for(n), kThreads, 0, st, w.r, w.d, x, n, w.sc, w.partials, precond_error_flag(m),
         mapped(w.h_read), h_ls ? *h_ls : cudaGraphConditionalHandle(), h_ls ? 1 : 0);
     return EFEM_OK;
 }
@@ -890,18 +907,18 @@ efem_status enqueue_body(Model& m, SolverWS& w, double* x, bool use_factor, cuda
     int* clear = nullptr;
     int n_clear = 0;
     if (use_factor) precond_counters(m, &clear, &n_clear);
-    k_pass2<<<grid_for(n), kThreads, 0, st>>>(w.q, w.r, w.Y, n, mm, use_factor ? 0 : 1, w.sc, clear, n_clear);
+    launch_k(k_pass2, grid_for(n), kThreads, 0, st, w.q, w.r, w.Y, n, mm, use_factor ? 0 : 1, w.sc, clear, n_clear);
     if (use_factor) {
         efem_status s = precond_enqueue(m, w.q, st, false, &w.sc->t0_pc);
         if (s != EFEM_OK) return s;
     }
     switch (mm) {
-#define P3(M) case M: k_pass3_m<M><<<G, kThreads, sm3, st>>>(w.q, w.Y, n, w.sc, w.partials, use_factor ? 1 : 0); break;
+#define P3(M) case M: launch_k(k_pass3_m<M>, G, kThreads, sm3, st, w.q, w.Y, n, w.sc, w.partials, use_factor ? 1 : 0); break;
         P3(1) P3(2) P3(3) P3(4) P3(5) P3(6) P3(7) P3(8)
 #undef P3
-    default: k_pass3<<<g3, kThreads, sm3, st>>>(w.q, w.Y, n, mm, w.sc, w.partials, w.sums, use_factor ? 1 : 0);
+    default: launch_k(k_pass3, g3, kThreads, sm3, st, w.q, w.Y, n, mm, w.sc, w.partials, w.sums, use_factor ? 1 : 0);
     }
-    k_pass4<<<grid_for(n), kThreads, 0, st>>>(w.d, w.q, w.S, w.r, x, w.xp, w.rp, m.d_fext, n, w.sc, w.partials);
+    launch_k(k_pass4, grid_for(n), kThreads, 0, st, w.d, w.q, w.S, w.r, x, w.xp, w.rp, m.d_fext, n, w.sc, w.partials);
     return EFEM_OK;
 }
 
@@ -940,9 +957,16 @@ efem_status add_while(cudaStream_t st, cudaGraphConditionalHandle h, cudaGraph_t
 //   k_loop_start;
 //   while (hIter) { passes + H0 + first trial; residual; reductions + decision (sets hLs);
 //                   while (hLs) { trial; residual; reductions + decision }; k_iter_decide }
+// launch_k uses programmatic dependent launch while one of these is alive
+struct PdlScope {
+    explicit PdlScope(bool on) { t_pdl = on; }
+    ~PdlScope() { t_pdl = false; }
+};
+
 efem_status capture_loop(Model& m, SolverWS& w, double* x, bool use_factor, cudaGraphExec_t* out)
 {
     std::lock_guard<std::mutex> lock(capture_mutex());
+    PdlScope pdl(w.pdl);  // the first kernel of each body graph is a plain launch
     const long long launches = m.launches;  // capture launches nothing; replays are counted
     cudaStream_t s0 = w.capture[0], s1 = w.capture[1], s2 = w.capture[2];
     cudaGraph_t g = nullptr;
@@ -1005,6 +1029,7 @@ efem_status capture_loop(Model& m, SolverWS& w, double* x, bool use_factor, cuda
 efem_status capture_step(Model& m, SolverWS& w, double* x, bool use_factor, cudaGraphExec_t* out)
 {
     std::lock_guard<std::mutex> lock(capture_mutex());
+    PdlScope pdl(w.pdl);
     const long long launches = m.launches;
     cudaStream_t s0 = w.capture[0];
     cudaGraph_t g = nullptr;
@@ -1141,11 +1166,13 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
         SolverWS::Graphs& gr = w.graphs[key];
         if (!gr.first) {
             if ((s = capture_first(m, w, x, &gr.first)) != EFEM_OK) return s;
-            if (host_loop) {
-                if ((s = capture_step(m, w, x, ok, &gr.step)) != EFEM_OK) return s;
-            } else if ((s = capture_loop(m, w, x, ok, &gr.loop)) != EFEM_OK) {
-                return s;
+            for (int attempt = 0; attempt < 2; attempt++) {
+                s = host_loop ? capture_step(m, w, x, ok, &gr.step) : capture_loop(m, w, x, ok, &gr.loop);
+                if (s == EFEM_OK || !w.pdl) break;
+                cudaGetLastError();
+                w.pdl = false;  // capture again with plain launches
             }
+            if (s != EFEM_OK) return s;
         }
         // iteration 1 from the host
         EFEM_CUDA(cudaGraphLaunch(gr.first, st));
