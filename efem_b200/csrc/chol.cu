@@ -12,8 +12,10 @@
 //                 the precomputed relative indices, children in a fixed order
 //                 (the factor is bitwise repeatable);
 //   per 32-column panel step of the level's fronts:
-//   k_panel       one CTA per front: Cholesky of the 32x32 diagonal block in
-//                 shared memory, then the panel TRSM, row-parallel;
+//   k_panel       per front and chunk of rows: Cholesky of the 32x32
+//                 diagonal block in shared memory (one warp), then the
+//                 panel TRSM on the chunk's rows; k_panel_store then writes
+//                 the factored diagonal blocks into the fronts;
 //   k_syrk        one CTA per 64x64 tile of every front's trailing lower
 //                 triangle: register-blocked rank-32 update.
 //   k_inverse     one warp per 32 columns of each diagonal block: L_JJ^{-1},
@@ -123,6 +125,8 @@ struct Precond {
     int4* d_wtiles = nullptr;  // (front, 64-row tile, 64-column tile) of every W
     int n_wtiles = 0;
     int4* d_syrk = nullptr;
+    double* d_diag_tmp = nullptr;  // factored diagonal blocks of one panel step, [fronts in step][kNB][kNB]
+    int max_panel_cnt = 0;
     double *d_front = nullptr, *d_dinv = nullptr, *d_upd = nullptr, *d_y = nullptr, *d_t = nullptr,
            *d_vals = nullptr;
     // graph replay of the numeric factorisation (the same launches every solve)
@@ -186,9 +190,13 @@ __global__ void __launch_bounds__(kFT) k_extend_add(FrontArgs a, const Tile* __r
 // Grid (fronts, row chunks): every CTA factors the panel's kb x kb diagonal
 // block (one warp, left-looking, with the reciprocals of the pivots so that
 // no division sits on a dependent chain; every CTA computes the same block,
-// so the factor does not depend on the grid), chunk 0 writes it back, and
-// each CTA solves up to kFT of the rows below it, one per thread.
-__global__ void __launch_bounds__(kFT) k_panel(FrontArgs a, const int* __restrict__ list, int k0)
+// so the factor does not depend on the grid) and solves up to kFT of the rows
+// below it, one per thread.  Chunk 0 leaves the factored block in tmp, and
+// k_panel_store copies it into the front afterwards: written in place, it
+// could reach a chunk CTA of a later wave before that CTA has read the
+// unfactored block.
+__global__ void __launch_bounds__(kFT) k_panel(FrontArgs a, const int* __restrict__ list, int k0,
+    double* __restrict__ tmp)
 {
     const int s = list[blockIdx.x];
     const int r = a.nrow[s], c = a.ncol[s];
@@ -231,7 +239,7 @@ __global__ void __launch_bounds__(kFT) k_panel(FrontArgs a, const int* __restric
     if (blockIdx.y == 0)
         for (int idx = tid; idx < kb * kb; idx += kFT) {
             const int i = idx % kb, j = idx / kb;
-            if (i >= j) F[(k0 + i) + static_cast<long long>(k0 + j) * r] = D[i][j];
+            if (i >= j) tmp[static_cast<size_t>(blockIdx.x) * kNB * kNB + idx] = D[i][j];
         }
     // rows below the block: x L^T = f
     for (int i = row0 + tid; i < min(r, row0 + kFT); i += kFT) {
@@ -251,6 +259,20 @@ __global__ void __launch_bounds__(kFT) k_panel(FrontArgs a, const int* __restric
 #pragma unroll
         for (int j = 0; j < kNB; j++)
             if (j < kb) F[i + static_cast<long long>(k0 + j) * r] = x[j];
+    }
+}
+
+// the factored diagonal blocks of a panel step, from k_panel's tmp into the fronts
+__global__ void __launch_bounds__(kFT) k_panel_store(FrontArgs a, const int* __restrict__ list, int k0,
+    const double* __restrict__ tmp)
+{
+    const int s = list[blockIdx.x];
+    const int r = a.nrow[s], c = a.ncol[s];
+    const int kb = min(kNB, c - k0);
+    double* F = a.front + a.front_off[s];
+    for (int idx = threadIdx.x; idx < kb * kb; idx += kFT) {
+        const int i = idx % kb, j = idx / kb;
+        if (i >= j) F[(k0 + i) + static_cast<long long>(k0 + j) * r] = tmp[static_cast<size_t>(blockIdx.x) * kNB * kNB + idx];
     }
 }
 
@@ -1244,7 +1266,8 @@ void free_precond(Model& m)
     dev_free(P.d_chunks);
     dev_free(P.d_syrk);
     dev_free(P.d_wtiles);
-    for (double** p : { &P.d_front, &P.d_dinv, &P.d_dinvT, &P.d_w, &P.d_wt, &P.d_upd, &P.d_y, &P.d_t, &P.d_vals })
+    for (double** p : { &P.d_front, &P.d_dinv, &P.d_dinvT, &P.d_w, &P.d_wt, &P.d_upd, &P.d_y, &P.d_t, &P.d_vals,
+             &P.d_diag_tmp })
         dev_free(*p);
     delete m.precond;
     m.precond = nullptr;
@@ -1327,6 +1350,7 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
             }
             st.panel_cnt = static_cast<int>(panel_list.size()) - st.panel_off;
             st.syrk_cnt = static_cast<int>(syrk.size()) - st.syrk_off;
+            P.max_panel_cnt = std::max(P.max_panel_cnt, st.panel_cnt);
             P.steps.push_back(st);
         }
         P.lev_first_step.push_back(static_cast<int>(P.steps.size()));
@@ -1594,6 +1618,8 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
     if ((st = dev_alloc(&P.d_t, n3)) != EFEM_OK) return st;
     if ((st = dev_alloc(&P.d_cnt, 4 * static_cast<size_t>(S.ns) + 2)) != EFEM_OK) return st;
     if ((st = dev_alloc(&P.d_fail, 1)) != EFEM_OK) return st;
+    if ((st = dev_alloc(&P.d_diag_tmp, static_cast<size_t>(std::max(P.max_panel_cnt, 1)) * kNB * kNB)) != EFEM_OK)
+        return st;
     // persistent solve: as many CTAs as fit on the device at once
     EFEM_CUDA(cudaFuncSetAttribute(k_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     int per_sm = 0, sms = 0;
@@ -1632,8 +1658,10 @@ static long long enqueue_factor(Precond& P, cudaStream_t st)
         }
         for (int q = P.lev_first_step[l]; q < P.lev_first_step[l + 1]; q++) {
             const Precond::Step& stp = P.steps[q];
-            k_panel<<<dim3(stp.panel_cnt, stp.panel_chunks), kFT, 0, st>>>(a, P.d_panel_list + stp.panel_off, stp.k0);
-            n++;
+            k_panel<<<dim3(stp.panel_cnt, stp.panel_chunks), kFT, 0, st>>>(a, P.d_panel_list + stp.panel_off, stp.k0,
+                P.d_diag_tmp);
+            k_panel_store<<<stp.panel_cnt, kFT, 0, st>>>(a, P.d_panel_list + stp.panel_off, stp.k0, P.d_diag_tmp);
+            n += 2;
             if (stp.syrk_cnt > 0) {
                 k_syrk<<<stp.syrk_cnt, kFT, 0, st>>>(a, P.d_syrk + stp.syrk_off, stp.k0);
                 n++;
