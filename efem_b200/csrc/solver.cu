@@ -405,8 +405,9 @@ __global__ void __launch_bounds__(kThreads) k_pass1(const double* __restrict__ x
 }
 
 // Sums of NV values over a 1D grid in a fixed order: every CTA stores its
-// block sums; the last CTA to finish adds them up, one warp per value (lanes
-// over the CTAs in order, then a fixed shuffle tree), into out[0, NV).
+// block sums; the last CTA to finish adds them up -- each thread the CTAs
+// b = t, t + kThreads, ... for all NV values at once (independent loads, a
+// couple of round trips), then a block reduction -- into out[0, NV).
 // Returns true in every thread of the last CTA.
 template <int NV>
 __device__ bool grid_sums(double* v, double* partials, unsigned int* counter, double* out)
@@ -425,15 +426,24 @@ __device__ bool grid_sums(double* v, double* partials, unsigned int* counter, do
     __syncthreads();
     if (!last) return false;
     __threadfence();
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int k = w; k < NV; k += kThreads / 32) {
-        double x = 0.0;
-        for (int b = lane; b < static_cast<int>(gridDim.x); b += 32) x += *(volatile double*)&partials[b * NV + k];
-        x = warp_sum(x);
-        if (lane == 0) out[k] = x;
+    double acc[NV];
+#pragma unroll
+    for (int k = 0; k < NV; k++) acc[k] = 0.0;
+    for (int b = threadIdx.x; b < static_cast<int>(gridDim.x); b += kThreads) {
+        const volatile double* pb = partials + static_cast<size_t>(b) * NV;
+        double p[NV];
+#pragma unroll
+        for (int k = 0; k < NV; k++) p[k] = pb[k];
+#pragma unroll
+        for (int k = 0; k < NV; k++) acc[k] += p[k];
+    }
+    block_reduce<NV>(acc, ops);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; k++) out[k] = acc[k];
+        *counter = 0u;
     }
     __syncthreads();
-    if (threadIdx.x == 0) *counter = 0u;
     return true;
 }
 
