@@ -513,6 +513,7 @@ def main():
             "iterations_per_solve": iters / args.steps, "residual_evals_per_solve": sum(i["n_residual_evals"] for i in infos) / args.steps,
             "final_r_inf": infos[-1]["r_inf"], "u_inf": infos[-1]["u_inf"],
             "converged": all(bool(i["flags"] & api.SOLVE_CONVERGED) for i in infos),
+            "programmatic_dependent_launch": all(bool(i["flags"] & api.SOLVE_PDL) for i in infos),
             "factor_ms": float(np.mean([i["ms_factor"] for i in infos])),
             "setup_s": setup_s,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * model.n_dof,

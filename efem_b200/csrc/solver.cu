@@ -1184,6 +1184,7 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
             }
             if (s != EFEM_OK) return s;
         }
+        if (w.pdl) info->flags |= EFEM_SOLVE_PDL;
         // iteration 1 from the host
         EFEM_CUDA(cudaGraphLaunch(gr.first, st));
         EFEM_CUDA(cudaStreamSynchronize(st));

@@ -123,7 +123,9 @@ enum {
     EFEM_SOLVE_CONVERGED = 1,      /* residual test passed */
     EFEM_SOLVE_PRECOND_FALLBACK = 2,/* factorisation failed; H0 = I/theta used (LBFGS.h:76-79) */
     EFEM_SOLVE_DX_CONVERGED = 4,   /* ||u||_inf < dx_criterion (the reference's return flag) */
-    EFEM_SOLVE_MAX_ITERS = 8
+    EFEM_SOLVE_MAX_ITERS = 8,
+    EFEM_SOLVE_PDL = 16            /* the captured iterations chain their kernels with programmatic
+                                      dependent launch (a capture that refuses it falls back to plain launches) */
 };
 
 typedef struct {
