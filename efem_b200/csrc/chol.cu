@@ -52,7 +52,6 @@ constexpr int kST = 256;  // solve threads: one warp per output row / column
 constexpr int kRT = 32;   // columns per CTA of the inverse / transpose kernels
 constexpr int kStageBudget = 4096;        // staged doubles per solve tile (rows of a tile x row length)
 constexpr long long kWholeBudget = 4096;  // staged doubles up to which one CTA solves a whole front
-constexpr int kZMinCols = 64;             // root fronts from this many columns are solved from Z = X^T X
 
 // one work item of the persistent triangular solve
 struct SolveItem {
@@ -124,11 +123,6 @@ struct Precond {
     long long* d_lt_off = nullptr;
     double *d_dinvT = nullptr, *d_w = nullptr, *d_wt = nullptr;
     int4* d_wtiles = nullptr;  // (front, 64-row tile, 64-column tile) of every W
-    // Z = L_JJ^{-T} L_JJ^{-1} of large root fronts (their two sweeps in one step)
-    double* d_z = nullptr;
-    long long* d_z_off = nullptr;
-    int4* d_ztiles = nullptr;
-    int n_ztiles = 0;
     int n_wtiles = 0;
     int4* d_syrk = nullptr;
     double* d_diag_tmp = nullptr;  // factored diagonal blocks of one panel step, [fronts in step][kNB][kNB]
@@ -155,8 +149,6 @@ struct FrontArgs {
     double* w;      // W = L_RJ L_JJ^{-1}, row-major (r - c) x c
     double* wt;     // W^T, row-major c x (r - c)
     int* fail;
-    double* z;               // Z = L_JJ^{-T} L_JJ^{-1} of a root front (full c x c, row-major)
-    const long long* z_off;  // per front: offset of its Z, -1 if it has none
 };
 
 
@@ -489,13 +481,7 @@ __global__ void __launch_bounds__(kIT) k_offdiag_inv(FrontArgs a, const Tile* __
 //   kFwdG      update rows of one tile    (waits: children's g)
 //   kBwdFront  x_J = L_JJ^{-T} y_J - W^T x_R for a whole front
 //   kBwdX      x rows of one tile         (waits: own y, parent's x)
-//   kRootX     x rows of a root front from Z = L_JJ^{-T} L_JJ^{-1}: the
-//              root's forward and backward steps in one (waits: children's
-//              g and the root's kSaveB); x overwrites v on the root's columns
-//   kSaveB     the right-hand side on a root's columns, copied aside (into
-//              the t buffer) before any kRootX tile can overwrite it; the
-//              first items of the solve
-enum ItemKind { kFwdFront = 0, kFwdY = 1, kFwdG = 2, kBwdFront = 3, kRootX = 4, kBwdX = 5, kSaveB = 6 };
+enum ItemKind { kFwdFront = 0, kFwdY = 1, kFwdG = 2, kBwdFront = 3, kBwdX = 5 };
 
 // device counters, one int array: [cY ns][cGin ns][unused ns][cX ns][ticket][error]
 struct SolveArgs {
@@ -666,7 +652,7 @@ __device__ __forceinline__ void rows_dot(const double* M, int lp, const double* 
 // more than two children behind them) follow in order.
 constexpr int kBatch = 2;
 __device__ __forceinline__ void assemble(const SolveArgs& A, int t0, int t1, int c, const int* cp, const int* ci,
-    int cbeg, const int* pr, double* f, const double* bdirect = nullptr)
+    int cbeg, const int* pr, double* f)
 {
     for (int base = t0; base < t1; base += kST * kBatch) {
         double b[kBatch][3], g[kBatch][2][3];
@@ -676,7 +662,7 @@ __device__ __forceinline__ void assemble(const SolveArgs& A, int t0, int t1, int
             const bool valid = t < t1;
             const int q0 = valid ? cp[t - t0] : 0, q1 = valid ? cp[t - t0 + 1] : 0;
             b[u][0] = b[u][1] = b[u][2] = 0.0;
-            if (valid && t < c) ld3(bdirect ? bdirect + 3LL * t : A.v + 3LL * pr[t - t0], b[u][0], b[u][1], b[u][2]);
+            if (valid && t < c) ld3(A.v + 3LL * pr[t - t0], b[u][0], b[u][1], b[u][2]);
 #pragma unroll
             for (int e = 0; e < 2; e++) {
                 g[u][e][0] = g[u][e][1] = g[u][e][2] = 0.0;
@@ -827,15 +813,6 @@ __global__ void __launch_bounds__(kST) k_solve(SolveArgs A)
             stage_rows(st + c * lc, lm, WT, m, c, m, 0, 0);  // W^T rows
             stage_i(si, A.prow + ro, r);
             break;
-        case kRootX:  // full rows of Z; the assembly of all of f_J
-            stage_rows(st, lc, a.z + a.z_off[s] + static_cast<long long>(r0) * c, c, R, c, 0, 0);
-            stage_i(si, a.contrib_ptr + ro, c + 1);
-            stage_i(si + c + 1, a.contrib_idx + cbeg, nci);
-            stage_i(si + c + 1 + nci, A.prow + ro, c);
-            break;
-        case kSaveB:
-            stage_i(si, A.prow + ro, c);
-            break;
         default:  // kBwdX
             stage_rows(st, lc, XT + static_cast<long long>(r0) * c, c, R, c, 2, r0);
             stage_rows(st + R * lc, lm, WT + static_cast<long long>(r0) * m, m, R, m, 0, 0);
@@ -849,8 +826,6 @@ __global__ void __launch_bounds__(kST) k_solve(SolveArgs A)
             case kFwdFront:
             case kFwdY:
             case kFwdG: ok = wait_ge(cGin + s, tGin[s], err); break;
-            case kRootX: ok = wait_ge(cGin + s, tGin[s], err) && wait_ge(cY + s, 1, err); break;
-            case kSaveB: ok = true; break;
             default: ok = wait_ge(cY + s, tY[s], err) && (p < 0 || wait_ge(cX + p, tX[p], err)); break;
             }
             ok_sh = ok;
@@ -909,30 +884,6 @@ __global__ void __launch_bounds__(kST) k_solve(SolveArgs A)
                 });
                 break;
             }
-            case kSaveB:
-                for (int t = tid; t < c; t += kST) {
-                    double b0, b1, b2;
-                    ld3(A.v + 3LL * si[t], b0, b1, b2);
-                    double* o = A.t + 3LL * (f0 + t);
-                    o[0] = b0;
-                    o[1] = b1;
-                    o[2] = b2;
-                }
-                break;
-            case kRootX: {
-                double* f = wk;  // [c][3]
-                const int* ci = si + c + 1;
-                const int* pr = ci + nci;
-                assemble(A, 0, c, c, si, ci, cbeg, pr, f, A.t + 3LL * f0);
-                __syncthreads();
-                rows_dot(st, lc, f, 0, R, c, 0, 0, [&](int i, double x0, double x1, double x2) {
-                    double* o = A.v + 3LL * pr[r0 + i];
-                    o[0] = x0;
-                    o[1] = x1;
-                    o[2] = x2;
-                });
-                break;
-            }
             case kBwdFront: {
                 double* yj = wk;               // [c][3]
                 double* xr = wk + 3 * c;       // [m][3]
@@ -985,12 +936,11 @@ __global__ void __launch_bounds__(kST) k_solve(SolveArgs A)
                 atomicAdd(cY + s, 1);
                 if (p >= 0) atomicAdd(cGin + p, 1);
                 break;
-            case kFwdY:
-            case kSaveB: atomicAdd(cY + s, 1); break;
+            case kFwdY: atomicAdd(cY + s, 1); break;
             case kFwdG:
                 if (p >= 0) atomicAdd(cGin + p, 1);
                 break;
-            default: atomicAdd(cX + s, 1); break;  // kBwdFront, kBwdX, kRootX
+            default: atomicAdd(cX + s, 1); break;  // kBwdFront, kBwdX
             }
         }
     }
@@ -1208,52 +1158,6 @@ __global__ void __launch_bounds__(kST) k_sub_bwd(SubArgs A)
     }
 }
 
-// Z = X^T X for a root front (X = L_JJ^{-1}, lower triangular, row-major),
-// one 64 x 64 tile of the full symmetric Z per CTA (4 x 4 per thread), the
-// sum over k >= max(i, j) in blocks of 32 rows of X; tile = (front, ti, tj)
-__global__ void __launch_bounds__(256) k_z(FrontArgs a, const int4* __restrict__ tiles)
-{
-    const int4 tl = tiles[blockIdx.x];
-    const int s = tl.x, i0 = tl.y * 64, j0 = tl.z * 64;
-    const int c = a.ncol[s];
-    const double* X = a.dinv + a.dinv_off[s];
-    __shared__ double As[32][64 + 1];  // As[k][i] = X[k0 + k][i0 + i]
-    __shared__ double Bs[32][64 + 1];  // Bs[k][j] = X[k0 + k][j0 + j]
-    const int tid = threadIdx.x, ti = (tid & 15) * 4, tj = (tid >> 4) * 4;
-    double acc[4][4] = {};
-    for (int k0 = (max(i0, j0) / 32) * 32; k0 < c; k0 += 32) {
-        for (int idx = tid; idx < 32 * 64; idx += 256) {
-            const int k = idx >> 6, q = idx & 63;
-            const int gk = k0 + k, gi = i0 + q, gj = j0 + q;
-            As[k][q] = (gk < c && gi < c && gk >= gi) ? X[static_cast<long long>(gk) * c + gi] : 0.0;
-            Bs[k][q] = (gk < c && gj < c && gk >= gj) ? X[static_cast<long long>(gk) * c + gj] : 0.0;
-        }
-        __syncthreads();
-#pragma unroll 8
-        for (int k = 0; k < 32; k++) {
-            double av[4], bv[4];
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                av[q] = As[k][ti + q];
-                bv[q] = Bs[k][tj + q];
-            }
-#pragma unroll
-            for (int x = 0; x < 4; x++)
-#pragma unroll
-                for (int y = 0; y < 4; y++) acc[x][y] += av[x] * bv[y];
-        }
-        __syncthreads();
-    }
-    double* Z = a.z + a.z_off[s];
-#pragma unroll
-    for (int x = 0; x < 4; x++)
-#pragma unroll
-        for (int y = 0; y < 4; y++) {
-            const int gi = i0 + ti + x, gj = j0 + tj + y;
-            if (gi < c && gj < c) Z[static_cast<long long>(gi) * c + gj] = acc[x][y];
-        }
-}
-
 // W = L_RJ L_JJ^{-1} for every front, one 64 x 64 tile of W per CTA (4 x 4
 // per thread), L_RJ from the front's panel and L_JJ^{-1} (lower triangular,
 // entries above the diagonal masked) in blocks of 32; written row-major as W
@@ -1312,8 +1216,7 @@ FrontArgs args_of(Precond& P)
 {
     return FrontArgs { P.d_first, P.d_ncol, P.d_nrow, P.d_rows, P.d_child_ptr, P.d_child_list, P.d_relind,
         P.d_level_list, P.d_contrib_ptr, P.d_contrib_idx, P.d_below_front, P.d_front_off, P.d_rows_off,
-        P.d_relind_off, P.d_dinv_off, P.d_upd_off, P.d_lt_off, P.d_front, P.d_dinv, P.d_dinvT, P.d_w, P.d_wt, P.d_fail,
-        P.d_z, P.d_z_off };
+        P.d_relind_off, P.d_dinv_off, P.d_upd_off, P.d_lt_off, P.d_front, P.d_dinv, P.d_dinvT, P.d_w, P.d_wt, P.d_fail };
 }
 
 // the work buffers of one solve
@@ -1363,9 +1266,6 @@ void free_precond(Model& m)
     dev_free(P.d_chunks);
     dev_free(P.d_syrk);
     dev_free(P.d_wtiles);
-    dev_free(P.d_ztiles);
-    dev_free(P.d_z_off);
-    dev_free(P.d_z);
     for (double** p : { &P.d_front, &P.d_dinv, &P.d_dinvT, &P.d_w, &P.d_wt, &P.d_upd, &P.d_y, &P.d_t, &P.d_vals,
              &P.d_diag_tmp })
         dev_free(*p);
@@ -1584,10 +1484,7 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
     // sized here.
     std::vector<SolveItem> items;
     std::vector<int> tgt(4 * static_cast<size_t>(S.ns), 0);
-    std::vector<char> whole(S.ns, 0), zroot(S.ns, 0);
-    std::vector<long long> z_off(S.ns, -1);
-    std::vector<int4> ztiles;
-    long long z_size = 0;
+    std::vector<char> whole(S.ns, 0);
     size_t stage_d = 1, work_d = 1, ints = 1;
     auto need = [&](size_t sd, size_t wd, size_t ni) {
         stage_d = std::max(stage_d, sd);
@@ -1611,38 +1508,11 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
         if (S.parent[s] >= 0 && !in_sub[s])     // children's g complete (subtree roots finish before k_solve)
             tgt[S.ns + S.parent[s]] += whole[s] ? 1 : ntiles(mm, lc);
         tgt[3 * S.ns + s] = whole[s] ? 1 : ntiles(c, lc + lm);                              // x of s complete
-        // a large root front (no rows below its columns) is solved in one step
-        // from Z = X^T X: kSaveB sets cY, its kRootX tiles set cX
-        zroot[s] = S.parent[s] < 0 && mm == 0 && !whole[s] && !in_sub[s] && c >= kZMinCols;
-        if (zroot[s]) {
-            tgt[s] = 1;
-            tgt[3 * S.ns + s] = ntiles(c, lc);
-            z_off[s] = z_size;
-            z_size += static_cast<long long>(c) * c;
-            for (int ti = 0; ti * 64 < c; ti++)
-                for (int tj = 0; tj * 64 < c; tj++) ztiles.push_back(make_int4(s, ti, tj, 0));
-        }
     }
-    for (int s = 0; s < S.ns; s++)
-        if (zroot[s]) {
-            items.push_back(SolveItem { kSaveB, s, 0, S.ncol[s], 0, 0, 0, 0 });
-            need(1, 1, S.ncol[s]);
-        }
     for (int l = K; l < nlev; l++) {
         for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) {
             const int s = S.level_list[q];
             const int c = S.ncol[s], r = S.nrow[s], mm = r - c, lc = odd_h(c);
-            if (zroot[s]) {
-                const auto cj = crange(s, 0, c);
-                const int tz = tile(lc);
-                for (int o = 0; o < c; o += tz) {
-                    const int i1 = std::min(c, o + tz);
-                    items.push_back(SolveItem { kRootX, s, o, i1, cj.first, cj.second, 0, 0 });
-                    need(static_cast<size_t>(i1 - o) * lc, 3 * static_cast<size_t>(c),
-                        2 * static_cast<size_t>(c) + 1 + (cj.second - cj.first));
-                }
-                continue;
-            }
             if (whole[s]) {
                 const auto cr = crange(s, 0, r);
                 items.push_back(SolveItem { kFwdFront, s, 0, c, cr.first, cr.second, 0, 0 });
@@ -1670,7 +1540,6 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
         for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) {
             const int s = S.level_list[q];
             const int c = S.ncol[s], r = S.nrow[s], mm = r - c, lc = odd_h(c), lm = odd_h(mm);
-            if (zroot[s]) continue;  // solved by its kRootX tiles
             if (whole[s]) {
                 items.push_back(SolveItem { kBwdFront, s, 0, c, 0, 0, 0, 0 });
                 need(static_cast<size_t>(c) * (lc + lm), 3 * static_cast<size_t>(r + c), r);
@@ -1733,12 +1602,6 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
     UP(P.d_inv, inv);
     UP(P.d_oinv, oinv);
     UP(P.d_wtiles, wtiles);
-    P.n_ztiles = static_cast<int>(ztiles.size());
-    if (P.n_ztiles > 0) {
-        UP(P.d_ztiles, ztiles);
-        UP(P.d_z_off, z_off);
-        if ((st = dev_alloc(&P.d_z, static_cast<size_t>(z_size))) != EFEM_OK) return st;
-    }
     UP(P.d_ea, ea);
     UP(P.d_below_front, S.below_front);
     UP(P.d_panel_list, panel_list);
@@ -1814,10 +1677,6 @@ static long long enqueue_factor(Precond& P, cudaStream_t st)
         }
         if (P.n_wtiles > 0) {
             k_w<<<P.n_wtiles, 256, 0, st>>>(a, P.d_wtiles);
-            n++;
-        }
-        if (P.n_ztiles > 0) {
-            k_z<<<P.n_ztiles, 256, 0, st>>>(a, P.d_ztiles);
             n++;
         }
     }
