@@ -54,7 +54,7 @@ class Options(ctypes.Structure):
                 ("host_loop", ctypes.c_int), ("adjoint_tolerance", ctypes.c_double),
                 ("adjoint_max_iterations", ctypes.c_int), ("elem_threads", ctypes.c_int),
                 ("consistent_inertia", ctypes.c_int), ("trace", ctypes.c_int),
-                ("solve_subtree_levels", ctypes.c_int)]
+                ("solve_subtree_levels", ctypes.c_int), ("line_search", ctypes.c_int)]
 
 
 class SolveInfo(ctypes.Structure):

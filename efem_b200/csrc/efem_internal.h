@@ -272,6 +272,7 @@ efem_status adjoint(Model& m, const double* d_u, const double* d_dJdu, double* d
     efem_adjoint_info* info);
 efem_status adjoint_io(Model& m, double** io);  // an n_dof device buffer for host-pointer calls
 efem_status strain_energy_sum(Model& m, const double* d_u, double* energy);  // energy.cu
+efem_status total_potential(Model& m, const double* d_u, double* pi);       // energy.cu: E(u) - f_ext.u
 
 // ------------------------------------------------------------------ preconditioner (chol.cu)
 // Build (once) the scalar approximate Jacobian L and its Cholesky factor.

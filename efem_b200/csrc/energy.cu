@@ -13,6 +13,7 @@
 // added in CTA order.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "efem_internal.h"
@@ -85,7 +86,50 @@ __global__ void __launch_bounds__(kBlock) k_energy(int n, int nen, int ngp, int 
     }
 }
 
+// per-CTA partial sums of f . u
+__global__ void __launch_bounds__(kBlock) k_dot_part(const double* __restrict__ f, const double* __restrict__ u,
+    size_t n, double* __restrict__ part)
+{
+    __shared__ double sh[kBlock / 32];
+    double s = 0.0;
+    for (size_t i = blockIdx.x * static_cast<size_t>(kBlock) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * kBlock)
+        s += f[i] * u[i];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int q = 0; q < kBlock / 32; q++) t += sh[q];
+        part[blockIdx.x] = t;
+    }
+}
+
 }  // namespace
+
+// Total potential of conservative loads, Pi(u) = E(u) - f_ext . u: its
+// gradient is the residual R(u), so the Armijo line search can test it.
+efem_status total_potential(Model& m, const double* d_u, double* pi)
+{
+    double e = 0.0;
+    efem_status s = strain_energy_sum(m, d_u, &e);
+    if (s != EFEM_OK) return s;
+    const size_t n = 3 * static_cast<size_t>(m.n_free);
+    double w = 0.0;
+    if (n > 0) {
+        const int grid = static_cast<int>(std::min<size_t>(296, (n + kBlock - 1) / kBlock));
+        double* part = nullptr;
+        EFEM_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&part), sizeof(double) * grid, m.stream));
+        k_dot_part<<<grid, kBlock, 0, m.stream>>>(m.d_fext, d_u, n, part);
+        m.launches++;
+        std::vector<double> h(grid);
+        EFEM_CUDA(cudaMemcpyAsync(h.data(), part, sizeof(double) * grid, cudaMemcpyDeviceToHost, m.stream));
+        EFEM_CUDA(cudaFreeAsync(part, m.stream));
+        EFEM_CUDA(cudaStreamSynchronize(m.stream));
+        for (double x : h) w += x;
+    }
+    *pi = e - w;
+    return EFEM_OK;
+}
 
 efem_status strain_energy_sum(Model& m, const double* d_u, double* energy)
 {

@@ -285,6 +285,7 @@ efem_status read_json_config(const char* path, ModelInput& in)
                 }
         }
         if (const Json* s = a->find("consistent_inertia"); s && s->is_bool()) in.opts.consistent_inertia = s->b ? 1 : 0;
+        if (const Json* s = a->find("line_search"); s && s->is_string()) in.opts.line_search = s->str == "armijo" ? 1 : 0;
     }
 
     // bodies, src/model/Model.cpp:14-37

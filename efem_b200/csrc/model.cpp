@@ -795,6 +795,7 @@ efem_status efem_default_options(efem_options* o)
     o->consistent_inertia = 0;
     o->trace = 0;
     o->solve_subtree_levels = -1;
+    o->line_search = 0;
     return EFEM_OK;
 }
 
@@ -908,7 +909,7 @@ efem_status efem_set_options(void* model, const efem_options* o)
     if (s != EFEM_OK) return s;
     if (!o || o->m <= 0 || o->max_linesearch <= 0 || o->max_iterations < 0 || o->residual_criterion < 0
         || (o->precision != EFEM_FP64 && o->precision != EFEM_MIXED) || (o->integration != 0 && o->integration != 1)
-        || o->trace < 0) {
+        || o->trace < 0 || (o->line_search != 0 && o->line_search != 1)) {
         efem::set_error("invalid options (NLSolverParam::check_param rules)");
         return EFEM_ERR_ARG;
     }

@@ -1131,6 +1131,40 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
         return EFEM_OK;
     };
 
+    // Line search after a first trial x = xp + d whose residual and r.d are in
+    // the read-back slots: the reference's residual-projection rule
+    // (LineSearchFEA.h:43-67), or with line_search = 1 the Armijo test
+    // Pi(xp + a d) <= Pi(xp) + 1e-4 a r(xp).d on the total potential, halving a.
+    const bool armijo = m.opts.line_search == 1;
+    double pi_prev = 0.0;
+    auto line_search = [&]() -> efem_status {
+        const double dg0 = hr[kRdDg0];
+        double dg = hr[kRdDg], step = 1.0;
+        if (!armijo) {
+            for (int it = 1; it < m.opts.max_linesearch && !(std::fabs(dg) <= std::fabs(dg0)); it++) {
+                step *= dg * dg0 > 0 ? 1.5 : 0.5;
+                efem_status rs = direct_trial(step);
+                if (rs != EFEM_OK) return rs;
+                dg = hr[kRdDg];
+            }
+            return EFEM_OK;
+        }
+        double pi = 0.0;
+        efem_status rs = total_potential(m, x, &pi);
+        if (rs != EFEM_OK) return rs;
+        for (int it = 1; it < m.opts.max_linesearch && !(pi <= pi_prev + 1e-4 * step * dg0); it++) {
+            step *= 0.5;
+            if ((rs = direct_trial(step)) != EFEM_OK) return rs;
+            if ((rs = total_potential(m, x, &pi)) != EFEM_OK) return rs;
+        }
+        pi_prev = pi;
+        return EFEM_OK;
+    };
+    if (armijo && m.n_faces > 0) {
+        set_error("the Armijo line search needs conservative loads: pressure faces have no potential");
+        return EFEM_ERR_UNSUPPORTED;
+    }
+
     // initial residual and early exit (LBFGS.h:110-120); d = 0 so dg = 0 here
     EFEM_CUDA(cudaMemsetAsync(w.d, 0, n * sizeof(double), st));
     k_state_init<<<1, 1, 0, st>>>(w.sc, mm);
@@ -1143,6 +1177,7 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
         converged = true;
         goto done;
     }
+    if (armijo && (s = total_potential(m, x, &pi_prev)) != EFEM_OK) return s;
     // approximate-Jacobian factor, once per solve (LBFGS.h:122-124)
     if (m.opts.nl_solver == 0) {
         int okf = 0;
@@ -1169,7 +1204,7 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
             drop_graphs(w);
             w.epoch = m.epoch;
         }
-        const bool host_loop = m.opts.host_loop != 0;
+        const bool host_loop = m.opts.host_loop != 0 || armijo;  // the Armijo test is applied from the host
         const auto key = std::make_pair(x, (ok ? 1 : 0) | (m.opts.precision << 1) | (host_loop ? 4 : 0)
             | (m.opts.deterministic ? 8 : 0));
         if (!w.graphs.count(key) && w.graphs.size() >= 8) drop_graphs(w);  // many distinct solution pointers
@@ -1189,13 +1224,7 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
         EFEM_CUDA(cudaGraphLaunch(gr.first, st));
         EFEM_CUDA(cudaStreamSynchronize(st));
         m.launches += per_res + 2;
-        const double dg0 = hr[kRdDg0];
-        double dg = hr[kRdDg], step = 1.0;
-        for (int it = 1; it < m.opts.max_linesearch && !(std::fabs(dg) <= std::fabs(dg0)); it++) {
-            step *= dg * dg0 > 0 ? 1.5 : 0.5;
-            if ((s = direct_trial(step)) != EFEM_OK) return s;
-            dg = hr[kRdDg];
-        }
+        if ((s = line_search()) != EFEM_OK) return s;
         rinf = hr[kRdRinf];
         xinf = hr[kRdXinf];
         if (!std::isfinite(rinf) || !std::isfinite(xinf)) goto nan_exit;
@@ -1219,13 +1248,7 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
                     set_error("the triangular solve of the preconditioner gave up waiting for a front");
                     return EFEM_ERR_CUDA;
                 }
-                const double dg0h = hr[kRdDg0];
-                double dgh = hr[kRdDg], steph = 1.0;
-                for (int it = 1; it < m.opts.max_linesearch && !(std::fabs(dgh) <= std::fabs(dg0h)); it++) {
-                    steph *= dgh * dg0h > 0 ? 1.5 : 0.5;
-                    if ((s = direct_trial(steph)) != EFEM_OK) return s;
-                    dgh = hr[kRdDg];
-                }
+                if ((s = line_search()) != EFEM_OK) return s;
                 rinf = hr[kRdRinf];
                 xinf = hr[kRdXinf];
                 if (!std::isfinite(rinf) || !std::isfinite(xinf)) goto nan_exit;

@@ -117,6 +117,11 @@ typedef struct {
     int solve_subtree_levels; /* H0 triangular solves: fronts on the lowest k levels of the elimination
                                  tree are solved one subtree per CTA, the levels above by the dataflow
                                  kernel; 0 or -1 (default) = none, the dataflow kernel for every level */
+    int line_search;          /* 0: the reference's residual-projection test |r.d| <= |r0.d| (default,
+                                 LineSearchFEA.h:43-67); 1: Armijo test on the total potential
+                                 Pi(u) = E(u) - f_ext.u (FP64 strain-energy sum), halving the step;
+                                 needs conservative loads (no pressure faces), runs the iterations
+                                 from the host */
 } efem_options;
 
 enum {

@@ -185,3 +185,11 @@ def test_gravity_strings(tmp_path):
     case.analysis = {"gravity": "non"}
     m = api.Model.from_json(case.write(str(tmp_path / "non")))
     assert np.array_equal(m.external_load(), base)
+
+
+def test_line_search_key(tmp_path):
+    case = mg.small_case("C3D8", "nh", "force")
+    case.analysis = {"line_search": "armijo"}
+    assert api.Model.from_json(case.write(str(tmp_path))).options.line_search == 1
+    case.analysis = {"line_search": "residual"}
+    assert api.Model.from_json(case.write(str(tmp_path / "b"))).options.line_search == 0
