@@ -1251,13 +1251,19 @@ efem_status efem_batch_solve(void** models, int n, double* const* u, efem_solve_
     if (n == 0) return EFEM_OK;
     int nt = max_threads > 0 ? max_threads : static_cast<int>(std::thread::hardware_concurrency());
     nt = std::max(1, std::min(nt, n));
+    // largest models first, so that no large solve starts last and runs alone
+    std::vector<int> order(n);
+    for (int i = 0; i < n; i++) order[i] = i;
+    auto size_of = [&](int i) { return models[i] ? static_cast<const Model*>(models[i])->n_free : 0; };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return size_of(a) > size_of(b); });
     std::atomic<int> next(0);
     std::vector<efem_status> st(n, EFEM_OK);
     std::vector<std::string> err(n);
     auto worker = [&]() {
         for (;;) {
-            const int i = next.fetch_add(1);
-            if (i >= n) return;
+            const int q = next.fetch_add(1);
+            if (q >= n) return;
+            const int i = order[q];
             efem_solve_info local;
             st[i] = efem_solve(models[i], u[i], infos ? &infos[i] : &local);
             if (st[i] != EFEM_OK) err[i] = efem::get_error();
