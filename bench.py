@@ -64,6 +64,21 @@ def config_block(precision, n):
             "parallelism": f"replicas{n}", "l2": "flushed (256 MB write) before every step"}
 
 
+# --------------------------------------------------------------------------- replicas
+def combine_ranks(ms, units, world, device="cpu"):
+    """Whole-job figures over replicas: (the slowest rank's time, the units of
+    all ranks).  Every rank calls it, in the same order (two all-reduces)."""
+    if world <= 1:
+        return float(ms), float(units)
+    import torch
+    import torch.distributed as dist
+    tm = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    tu = torch.tensor([float(units)], dtype=torch.float64, device=device)
+    dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+    dist.all_reduce(tu, op=dist.ReduceOp.SUM)
+    return float(tm[0]), float(tu[0])
+
+
 # --------------------------------------------------------------------------- clocks
 class ClockSampler:
     """nvidia-smi clock / throttle sampling during the timed region."""
@@ -468,14 +483,7 @@ def main():
     step_ms = [a.elapsed_time(b) for a, b in ev]
     total_ms = sum(step_ms)
     iters = sum(i["niter"] for i in infos)
-    t = torch.tensor([total_ms, float(iters)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        tm = t.clone()
-        dist.all_reduce(tm[:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
-        total_ms_max, iters_all = float(tm[0]), float(t[1])
-    else:
-        total_ms_max, iters_all = total_ms, float(iters)
+    total_ms_max, iters_all = combine_ranks(total_ms, iters, world, "cuda")
     value = iters_all / (total_ms_max / 1000.0)
 
     # ---- end to end through the C ABI with host buffers (pinned host input / output)
@@ -492,13 +500,8 @@ def main():
         e2e_iters += info["niter"]
     barrier()
     e2e_ms = sum(a.elapsed_time(b) for a, b in e2e_ev)
-    e2e_value = e2e_iters / (e2e_ms / 1000.0)
-    if world > 1:
-        te = torch.tensor([e2e_ms, float(e2e_iters)], dtype=torch.float64, device="cuda")
-        dist.all_reduce(te[:1], op=dist.ReduceOp.MAX)
-        ti = te[1:].clone()
-        dist.all_reduce(ti, op=dist.ReduceOp.SUM)
-        e2e_value = float(ti[0]) / (float(te[0]) / 1000.0)
+    e2e_ms_max, e2e_iters_all = combine_ranks(e2e_ms, e2e_iters, world, "cuda")
+    e2e_value = e2e_iters_all / (e2e_ms_max / 1000.0)
 
     # ---- roofline of the dominant kernel, measured live on the model's stream
     from efem_b200 import profiling
