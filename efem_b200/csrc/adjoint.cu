@@ -10,7 +10,9 @@
 //               is symmetric, so K_el^T w = K_el w; the pressure part is not
 //               (follower and directed loads are not conservative) and is
 //               transposed face by face: one dual seed per face unknown gives
-//               the column d f_face / d u_j, dotted with w on the face;
+//               the column d f_face / d u_j, dotted with w on the face; an
+//               adjoint solve stores these face blocks once at its u and
+//               applies them in every Krylov iteration;
 //   dR/dtheta   the same kernels with the seed on a material constant
 //               (C10, C01, C20, C30, D1 of one material) or on the scale of one
 //               pressure load;
@@ -57,6 +59,7 @@ namespace {
 constexpr int kBlock = 128;
 constexpr int kVec = 256;        // threads of the vector kernels
 constexpr int kDotBlocks = 128;  // CTAs per dot product
+constexpr size_t kFaceBlockBytes = size_t(4) << 30;  // most device memory the face tangent blocks may take
 
 struct TanElemArgs {
     int n, n_free;
@@ -275,6 +278,62 @@ __global__ void __launch_bounds__(kBlock) k_face_transpose(TanFaceArgs a)
     atomicAdd(a.out + 3 * node[qj] + cj, -s);
 }
 
+// The face tangent blocks at a fixed u: blk[f][i][j] = d f_i / d u_j over the
+// 3 NEN local unknowns (rows i of fixed nodes are 0; columns j of fixed nodes
+// are not written).  One thread per (face, local unknown j), seeded as in
+// k_face_transpose, so each block costs one set of dual passes per adjoint
+// solve instead of one per Krylov iteration.
+template <int NEN>
+__global__ void __launch_bounds__(kBlock) k_face_block(TanFaceArgs a, double* __restrict__ blk)
+{
+    constexpr int ND = 3 * NEN;
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int f = idx / ND, j = idx % ND;
+    if (f >= a.n) return;
+    const int qj = j / 3, cj = j % 3;
+    int node[NEN];
+    Dual uu[NEN][3];
+    for (int q = 0; q < NEN; q++) {
+        node[q] = a.conn[static_cast<size_t>(q) * a.n + f];
+        const bool fr = node[q] < a.n_free;
+#pragma unroll
+        for (int c = 0; c < 3; c++) uu[q][c] = fr ? Dual(a.u[3 * node[q] + c], (q == qj && c == cj) ? 1.0 : 0.0) : Dual(0.0);
+    }
+    if (node[qj] >= a.n_free) return;
+    Dual fq[NEN][3];
+    face_forces<NEN>(a, f, uu, fq);
+    double* b = blk + static_cast<size_t>(f) * ND * ND + j;
+    for (int q = 0; q < NEN; q++) {
+        const bool fr = node[q] < a.n_free;
+#pragma unroll
+        for (int c = 0; c < 3; c++) b[(3 * q + c) * ND] = fr ? fq[q][c].d : 0.0;
+    }
+}
+
+// out_j -= sum_i w_i blk[f][i][j]: the transpose product of k_face_transpose
+// from the stored blocks, one thread per (face, local unknown j); a warp's
+// reads of row i are consecutive in j.
+template <int NEN>
+__global__ void __launch_bounds__(kBlock) k_face_block_apply(TanFaceArgs a, const double* __restrict__ blk)
+{
+    constexpr int ND = 3 * NEN;
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int f = idx / ND, j = idx % ND;
+    if (f >= a.n) return;
+    const int nj = a.conn[static_cast<size_t>(j / 3) * a.n + f];
+    if (nj >= a.n_free) return;
+    const double* b = blk + static_cast<size_t>(f) * ND * ND + j;
+    double s0 = 0.0, s1 = 0.0;
+    for (int q = 0; q < NEN; q++) {
+        const int nq = a.conn[static_cast<size_t>(q) * a.n + f];
+        if (nq >= a.n_free) continue;
+        const double* wq = a.w + 3 * nq;
+        s0 += wq[0] * b[(3 * q) * ND] + wq[2] * b[(3 * q + 2) * ND];
+        s1 += wq[1] * b[(3 * q + 1) * ND];
+    }
+    atomicAdd(a.out + 3 * nj + j % 3, -(s0 + s1));
+}
+
 // ---------------------------------------------------------------- vectors
 // per-CTA partial sums of the dot products x_k . y (k < nk) into part[k][blockIdx.x]
 __global__ void __launch_bounds__(kVec) k_dots(const double* __restrict__ X, size_t ldx, int nk,
@@ -301,9 +360,17 @@ __global__ void __launch_bounds__(kVec) k_axpys(double* __restrict__ y, const do
     const double* __restrict__ c, size_t n)
 {
     for (size_t i = blockIdx.x * (size_t)kVec + threadIdx.x; i < n; i += (size_t)gridDim.x * kVec) {
-        double s = y[i];
-        for (int k = 0; k < nk; k++) s += c[k] * X[k * ldx + i];
-        y[i] = s;
+        // four independent sums keep four loads of X in flight per thread
+        double s0 = y[i], s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        int k = 0;
+        for (; k + 4 <= nk; k += 4) {
+            s0 += c[k] * X[k * ldx + i];
+            s1 += c[k + 1] * X[(k + 1) * ldx + i];
+            s2 += c[k + 2] * X[(k + 2) * ldx + i];
+            s3 += c[k + 3] * X[(k + 3) * ldx + i];
+        }
+        for (; k < nk; k++) s0 += c[k] * X[k * ldx + i];
+        y[i] = (s0 + s1) + (s2 + s3);
     }
 }
 
@@ -363,6 +430,10 @@ struct AdjointWS {
     MatParams<Dual>* mats = nullptr;
     double* dscale = nullptr;
     std::vector<double> h_part;
+    // per face set: the face tangent blocks at u (k_face_block), used for the
+    // transpose products while blocks_ready is set (inside one adjoint solve)
+    std::vector<double*> fblk;
+    bool blocks_ready = false;
 };
 
 void free_adjoint(Model& m)
@@ -373,6 +444,7 @@ void free_adjoint(Model& m)
         dev_free(*p);
     if (w.mats) cudaFree(w.mats);
     if (w.h_hcol) cudaFreeHost(w.h_hcol);
+    for (double*& p : w.fblk) dev_free(p);
     delete m.aws;
     m.aws = nullptr;
 }
@@ -449,32 +521,73 @@ void launch_elem_tangent(Model& m, const double* u, const double* v, double* out
 void launch_face_tangent(Model& m, const double* u, const double* v, const double* dscale, const double* w,
     double* out, bool transpose)
 {
-    for (auto& f : m.faces) {
+    const AdjointWS* ws = m.aws;
+    for (size_t fs = 0; fs < m.faces.size(); fs++) {
+        auto& f = m.faces[fs];
         if (f.n == 0) continue;
         TanFaceArgs a { f.n, m.n_free, f.conn, f.table, f.load_idx, f.A0, f.J0inv, f.load, f.t_ngp, f.t_w, f.t_N,
             f.t_dN, u, v, dscale, w, out };
         const int nthreads = transpose ? f.n * 3 * f.nen : f.n;
         const int grid = (nthreads + kBlock - 1) / kBlock;
+        const double* blk = transpose && ws && ws->blocks_ready ? ws->fblk[fs] : nullptr;
         m.launches++;
         switch (f.nen) {
         case 4:
-            if (transpose) k_face_transpose<4><<<grid, kBlock, 0, m.stream>>>(a);
+            if (blk) k_face_block_apply<4><<<grid, kBlock, 0, m.stream>>>(a, blk);
+            else if (transpose) k_face_transpose<4><<<grid, kBlock, 0, m.stream>>>(a);
             else k_face_tangent<4><<<grid, kBlock, 0, m.stream>>>(a);
             break;
         case 8:
-            if (transpose) k_face_transpose<8><<<grid, kBlock, 0, m.stream>>>(a);
+            if (blk) k_face_block_apply<8><<<grid, kBlock, 0, m.stream>>>(a, blk);
+            else if (transpose) k_face_transpose<8><<<grid, kBlock, 0, m.stream>>>(a);
             else k_face_tangent<8><<<grid, kBlock, 0, m.stream>>>(a);
             break;
         case 10:
-            if (transpose) k_face_transpose<10><<<grid, kBlock, 0, m.stream>>>(a);
+            if (blk) k_face_block_apply<10><<<grid, kBlock, 0, m.stream>>>(a, blk);
+            else if (transpose) k_face_transpose<10><<<grid, kBlock, 0, m.stream>>>(a);
             else k_face_tangent<10><<<grid, kBlock, 0, m.stream>>>(a);
             break;
         case 20:
-            if (transpose) k_face_transpose<20><<<grid, kBlock, 0, m.stream>>>(a);
+            if (blk) k_face_block_apply<20><<<grid, kBlock, 0, m.stream>>>(a, blk);
+            else if (transpose) k_face_transpose<20><<<grid, kBlock, 0, m.stream>>>(a);
             else k_face_tangent<20><<<grid, kBlock, 0, m.stream>>>(a);
             break;
         }
     }
+}
+
+// Face tangent blocks of every face set at u, for the transpose products of
+// one adjoint solve.  Sets blocks_ready only when all of them fit in
+// kFaceBlockBytes; otherwise the transpose products recompute the columns.
+efem_status build_face_blocks(Model& m, const double* u)
+{
+    AdjointWS& w = *m.aws;
+    w.blocks_ready = false;
+    size_t total = 0;
+    for (auto& f : m.faces) total += sizeof(double) * f.n * static_cast<size_t>(9 * f.nen * f.nen);
+    if (total == 0 || total > kFaceBlockBytes) return EFEM_OK;
+    w.fblk.resize(m.faces.size(), nullptr);
+    for (size_t fs = 0; fs < m.faces.size(); fs++) {
+        auto& f = m.faces[fs];
+        if (f.n == 0) continue;
+        if (!w.fblk[fs]) {
+            efem_status s = dev_alloc(&w.fblk[fs], f.n * static_cast<size_t>(9 * f.nen * f.nen));
+            if (s != EFEM_OK) return s;
+        }
+        TanFaceArgs a { f.n, m.n_free, f.conn, f.table, f.load_idx, f.A0, f.J0inv, f.load, f.t_ngp, f.t_w, f.t_N,
+            f.t_dN, u, nullptr, nullptr, nullptr, nullptr };
+        const int grid = (f.n * 3 * f.nen + kBlock - 1) / kBlock;
+        m.launches++;
+        switch (f.nen) {
+        case 4: k_face_block<4><<<grid, kBlock, 0, m.stream>>>(a, w.fblk[fs]); break;
+        case 8: k_face_block<8><<<grid, kBlock, 0, m.stream>>>(a, w.fblk[fs]); break;
+        case 10: k_face_block<10><<<grid, kBlock, 0, m.stream>>>(a, w.fblk[fs]); break;
+        case 20: k_face_block<20><<<grid, kBlock, 0, m.stream>>>(a, w.fblk[fs]); break;
+        }
+    }
+    EFEM_CUDA(cudaGetLastError());
+    w.blocks_ready = true;
+    return EFEM_OK;
 }
 
 // out = K(u) v  (transpose: K(u)^T v); device pointers; dual materials without seeds uploaded
@@ -694,7 +807,10 @@ efem_status adjoint(Model& m, const double* d_u, const double* d_dJdu, double* d
     const int max_it = m.opts.adjoint_max_iterations > 0 ? m.opts.adjoint_max_iterations : 2000;
     int iters = 0;
     double rel = 0.0;
-    if ((s = adjoint_gmres(m, w.u, tol, max_it, &iters, &rel)) != EFEM_OK) return s;
+    if ((s = build_face_blocks(m, w.u)) != EFEM_OK) return s;
+    s = adjoint_gmres(m, w.u, tol, max_it, &iters, &rel);
+    w.blocks_ready = false;  // the blocks hold K at this u only
+    if (s != EFEM_OK) return s;
     info->iterations = iters;
     info->rel_residual = rel;
     if (rel <= tol) info->flags |= EFEM_SOLVE_CONVERGED;
