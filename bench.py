@@ -506,6 +506,9 @@ def main():
     # ---- roofline of the dominant kernel, measured live on the model's stream
     from efem_b200 import profiling
     roof, launches = profiling.roofline_report(model, infos)
+    fp32_res = args.precision == "mixed"
+    roof["residual_compute"] = profiling.residual_compute_roof(
+        model, infos, api.fma_peak(fp32=fp32_res), "FP32" if fp32_res else "FP64")
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps, "higher_is_better": True,

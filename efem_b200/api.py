@@ -37,7 +37,7 @@ EXPORTED = ["efem_default_options", "efem_model_create_from_json", "efem_model_c
             "efem_approx_jacobian_csr", "efem_precond_apply", "efem_precond_apply_noalloc", "efem_solve",
             "efem_set_stream", "efem_last_error", "efem_version", "efem_hvp", "efem_hvp_transpose",
             "efem_residual_param_derivative", "efem_adjoint", "efem_strain_energy", "efem_write_vtk",
-            "efem_batch_solve", "efem_external_load", "efem_solve_trace"]
+            "efem_batch_solve", "efem_external_load", "efem_solve_trace", "efem_fma_peak"]
 
 
 class EfemError(RuntimeError):
@@ -147,6 +147,7 @@ def lib():
             "efem_write_vtk": [vp, vp, ctypes.c_char_p],
             "efem_batch_solve": [ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(vp), ctypes.POINTER(SolveInfo),
                                  ctypes.c_int],
+            "efem_fma_peak": [ctypes.c_int, dp],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -166,6 +167,14 @@ def last_error():
 def check(status):
     if status != OK:
         raise EfemError(status, last_error())
+
+
+def fma_peak(fp32=False):
+    """Measured CUDA-core FMA throughput of the current device, GFLOP/s (FP64,
+    or FP32 with fp32=True): the compute roof of the element residual."""
+    g = ctypes.c_double()
+    check(lib().efem_fma_peak(1 if fp32 else 0, ctypes.byref(g)))
+    return g.value
 
 
 def default_options():

@@ -50,6 +50,29 @@ def measured_traffic(kernel_group):
         return None
 
 
+def residual_compute_roof(model, infos, fma_gflops, fma_kind):
+    """The element residual against its own roofs: achieved GFLOP/s (the
+    library's algorithmic flop count per evaluation over the mean device time
+    of one evaluation) and the attainable min(FMA peak, AI x HBM peak), AI =
+    algorithmic flops / algorithmic bytes."""
+    info = model.info()
+    calls = sum(i["n_residual_evals"] for i in infos)
+    ms = sum(i["ms_residual"] for i in infos)
+    if calls == 0 or ms <= 0.0 or not fma_gflops:
+        return None
+    per_s = (ms / calls) / 1000.0
+    flops, nbytes = float(info["residual_flops"]), float(info["residual_bytes"])
+    hbm, hbm_kind = hbm_peak()
+    ai = flops / nbytes
+    attainable = min(fma_gflops, ai * hbm)
+    achieved = flops / per_s / 1e9
+    return {"kernel": "residual", "bound": "fma" if fma_gflops <= ai * hbm else "hbm",
+            "achieved": achieved, "unit": "GFLOP/s", "fma_peak": fma_gflops,
+            "fma_peak_source": f"measured live ({fma_kind} FMA microbenchmark, efem_fma_peak)",
+            "hbm_peak_source": hbm_kind, "arithmetic_intensity": ai, "attainable": attainable,
+            "frac": achieved / attainable, "mean_launch_us": per_s * 1e6}
+
+
 def roofline_report(model, infos):
     """Return (roofline dict, mean kernel launches per solve)."""
     info = model.info()

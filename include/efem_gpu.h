@@ -316,6 +316,12 @@ efem_status efem_last_error(char* buf, size_t len);
 /* Library version string. */
 const char* efem_version(void);
 
+/* Measured CUDA-core FMA throughput of the current device in GFLOP/s (an FMA
+ * counts 2): FP64 (fp32 = 0) or FP32 (fp32 = 1), the compute roof of the
+ * element residual kernels.  Runs a short microbenchmark (a few ms).  No
+ * reference counterpart; a measurement helper for roofline figures. */
+efem_status efem_fma_peak(int fp32, double* gflops);
+
 #ifdef __cplusplus
 }
 #endif
