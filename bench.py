@@ -225,6 +225,17 @@ def run_adjoint_bench(args):
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
     info = model.info()
+    # whole adjoint solve against HBM: its algorithmic bytes (the library's
+    # count per Krylov iteration) over its time (host clock around the solve,
+    # ended by a stream synchronisation)
+    from efem_b200 import profiling
+    hbm, hbm_kind = profiling.hbm_peak()
+    solve_s = float(np.mean([i["ms_solve"] for i in infos])) / 1000.0
+    nbytes = float(np.mean([i["solve_bytes"] for i in infos]))
+    achieved = nbytes / solve_s / 1e9
+    roof = {"kernel": "adjoint solve (GMRES: k_solve H0, transpose tangent, Gram-Schmidt)", "bound": "hbm",
+            "achieved": achieved, "peak": hbm, "peak_source": hbm_kind, "unit": "GB/s", "frac": achieved / hbm,
+            "traffic": None, "algorithmic_bytes_per_gradient": nbytes}
     line = {"metric": "adjoint gradient time (dJ/dtheta, C3D10 Yeoh finger 50688 el)", "value": float(np.mean(ms)),
             "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(ms)),
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -241,6 +252,8 @@ def run_adjoint_bench(args):
             "setup_s": setup_s,
             "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 2 * 8 * model.n_dof,
                     "d2h_bytes_per_step": 8 * info["n_params"]},
+            "gpu_launches": int(sum(i["n_kernel_launches"] for i in infos)),
+            "roofline": roof,
             "clocks": clocks.summary()}
     print(json.dumps(line))
     model.close()

@@ -70,7 +70,8 @@ class SolveInfo(ctypes.Structure):
 
 class AdjointInfo(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int), ("flags", ctypes.c_int), ("rel_residual", ctypes.c_double),
-                ("ms_total", ctypes.c_double), ("ms_solve", ctypes.c_double), ("ms_params", ctypes.c_double)]
+                ("ms_total", ctypes.c_double), ("ms_solve", ctypes.c_double), ("ms_params", ctypes.c_double),
+                ("n_kernel_launches", ctypes.c_longlong), ("solve_bytes", ctypes.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -12,7 +12,9 @@
 //               transposed face by face: one dual seed per face unknown gives
 //               the column d f_face / d u_j, dotted with w on the face; an
 //               adjoint solve stores these face blocks once at its u and
-//               applies them in every Krylov iteration;
+//               applies them in every Krylov iteration, and likewise the
+//               Gauss-point tangents dP/dH of the elements, so that K_el v
+//               in its iterations is C : grad v without dual numbers;
 //   dR/dtheta   the same kernels with the seed on a material constant
 //               (C10, C01, C20, C30, D1 of one material) or on the scale of one
 //               pressure load;
@@ -59,7 +61,7 @@ namespace {
 constexpr int kBlock = 128;
 constexpr int kVec = 256;        // threads of the vector kernels
 constexpr int kDotBlocks = 128;  // CTAs per dot product
-constexpr size_t kFaceBlockBytes = size_t(4) << 30;  // most device memory the face tangent blocks may take
+constexpr size_t kStoredBytes = size_t(8) << 30;  // most device memory the stored tangents may take
 
 struct TanElemArgs {
     int n, n_free;
@@ -145,6 +147,121 @@ __global__ void __launch_bounds__(kBlock) k_elem_tangent(TanElemArgs a)
             const Dual* S = s_S[el][g];
 #pragma unroll
             for (int c = 0; c < 3; c++) r[c] += S[3 * c].d * d[0] + S[3 * c + 1].d * d[1] + S[3 * c + 2].d * d[2];
+        }
+#pragma unroll
+        for (int c = 0; c < 3; c++) atomicAdd(a.out + 3 * node + c, r[c]);
+    }
+}
+
+// The Gauss-point tangents at a fixed u: C[9 m + p][e NGP + g] = dP_p / dH_m
+// (H = du/dX), one thread per (element, Gauss point, m) with the dual seed
+// on H_m; stored once per adjoint solve so that every Krylov iteration's
+// K_el v is a linear map of grad v instead of a dual-number P(F).
+template <int NEN, int NGP>
+__global__ void __launch_bounds__(kBlock) k_gp_tangent(TanElemArgs a, double* __restrict__ C)
+{
+    const long long idx = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const long long ng = static_cast<long long>(a.n) * NGP;
+    if (idx >= ng * 9) return;
+    const int m = static_cast<int>(idx % 9);
+    const long long eg = idx / 9;
+    const int e = static_cast<int>(eg / NGP), g = static_cast<int>(eg % NGP);
+    double A[9] = { 0, 0, 0, 0, 0, 0, 0, 0, 0 };
+    for (int q = 0; q < NEN; q++) {
+        const int node = a.conn[static_cast<size_t>(q) * a.n + e];
+        if (node >= a.n_free) continue;
+        const double* dN = a.dN + (g * NEN + q) * 3;
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            const double ui = a.u[3 * node + i];
+#pragma unroll
+            for (int k = 0; k < 3; k++) A[3 * i + k] += ui * dN[k];
+        }
+    }
+    const double* Ji = a.J0inv + (static_cast<size_t>(e) * NGP + g) * 9;
+    Dual H[9];
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+            H[3 * i + j] = Dual(A[3 * i] * Ji[j] + A[3 * i + 1] * Ji[3 + j] + A[3 * i + 2] * Ji[6 + j], 3 * i + j == m ? 1.0 : 0.0);
+    const MatParams<Dual> mp = a.mats[a.mat[e]];
+    Dual P[9];
+    piola(mp, H, P);
+#pragma unroll
+    for (int p = 0; p < 9; p++) C[static_cast<size_t>(9 * m + p) * ng + eg] = P[p].d;
+}
+
+// out += K_el v from the stored Gauss-point tangents: the phases of
+// k_elem_tangent with dP = C : dH, dH = grad v, in place of the dual P(F).
+template <int NEN, int NGP>
+__global__ void __launch_bounds__(kBlock) k_elem_tangent_stored(TanElemArgs a, const double* __restrict__ C)
+{
+    constexpr int EPB = tan_epb(NGP);
+    constexpr int SV = (NEN * 3) | 1, SS = 9 | 1;
+    __shared__ double s_v[EPB][SV];
+    __shared__ double s_S[EPB][NGP][SS];
+    __shared__ double s_dN[NGP][NEN][3];
+    __shared__ int s_node[EPB][NEN];
+    const int tid = threadIdx.x;
+    for (int i = tid; i < NGP * NEN * 3; i += kBlock) (&s_dN[0][0][0])[i] = a.dN[i];
+    const int e0 = blockIdx.x * EPB;
+    for (int i = tid; i < EPB * NEN; i += kBlock) {
+        const int el = i % EPB, nd = i / EPB, e = e0 + el;
+        int node = a.n_free;
+        double x[3] = { 0, 0, 0 };
+        if (e < a.n) {
+            node = a.conn[static_cast<size_t>(nd) * a.n + e];
+            if (node < a.n_free)
+#pragma unroll
+                for (int c = 0; c < 3; c++) x[c] = a.v[3 * node + c];
+        }
+        s_node[el][nd] = node;
+#pragma unroll
+        for (int c = 0; c < 3; c++) s_v[el][3 * nd + c] = x[c];
+    }
+    __syncthreads();
+    if (tid < EPB * NGP) {
+        const int el = tid / NGP, g = tid % NGP, e = e0 + el;
+        if (e < a.n) {
+            double A[9] = { 0, 0, 0, 0, 0, 0, 0, 0, 0 };
+            for (int q = 0; q < NEN; q++)
+#pragma unroll
+                for (int i = 0; i < 3; i++)
+#pragma unroll
+                    for (int k = 0; k < 3; k++) A[3 * i + k] += s_v[el][3 * q + i] * s_dN[g][q][k];
+            const double* Ji = a.J0inv + (static_cast<size_t>(e) * NGP + g) * 9;
+            double dH[9];
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+#pragma unroll
+                for (int j = 0; j < 3; j++) dH[3 * i + j] = A[3 * i] * Ji[j] + A[3 * i + 1] * Ji[3 + j] + A[3 * i + 2] * Ji[6 + j];
+            const size_t ng = static_cast<size_t>(a.n) * NGP, eg = static_cast<size_t>(e) * NGP + g;
+            double dP[9] = { 0, 0, 0, 0, 0, 0, 0, 0, 0 };
+#pragma unroll
+            for (int mm = 0; mm < 9; mm++)
+#pragma unroll
+                for (int p = 0; p < 9; p++) dP[p] += C[(9 * mm + p) * ng + eg] * dH[mm];
+            const double wv = a.vol[e] * a.gw[g];
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+#pragma unroll
+                for (int j = 0; j < 3; j++)
+                    s_S[el][g][3 * i + j] = wv * (dP[3 * i] * Ji[3 * j] + dP[3 * i + 1] * Ji[3 * j + 1] + dP[3 * i + 2] * Ji[3 * j + 2]);
+        }
+    }
+    __syncthreads();
+    for (int i = tid; i < EPB * NEN; i += kBlock) {
+        const int el = i % EPB, nd = i / EPB, e = e0 + el;
+        if (e >= a.n) continue;
+        const int node = s_node[el][nd];
+        if (node >= a.n_free) continue;
+        double r[3] = { 0, 0, 0 };
+        for (int g = 0; g < NGP; g++) {
+            const double* d = s_dN[g][nd];
+            const double* S = s_S[el][g];
+#pragma unroll
+            for (int c = 0; c < 3; c++) r[c] += S[3 * c] * d[0] + S[3 * c + 1] * d[1] + S[3 * c + 2] * d[2];
         }
 #pragma unroll
         for (int c = 0; c < 3; c++) atomicAdd(a.out + 3 * node + c, r[c]);
@@ -430,9 +547,10 @@ struct AdjointWS {
     MatParams<Dual>* mats = nullptr;
     double* dscale = nullptr;
     std::vector<double> h_part;
-    // per face set: the face tangent blocks at u (k_face_block), used for the
-    // transpose products while blocks_ready is set (inside one adjoint solve)
-    std::vector<double*> fblk;
+    // stored tangents at u, used while blocks_ready is set (inside one adjoint
+    // solve): per face set the face blocks (k_face_block), per element block
+    // the Gauss-point tangents (k_gp_tangent)
+    std::vector<double*> fblk, gpt;
     bool blocks_ready = false;
 };
 
@@ -445,6 +563,7 @@ void free_adjoint(Model& m)
     if (w.mats) cudaFree(w.mats);
     if (w.h_hcol) cudaFreeHost(w.h_hcol);
     for (double*& p : w.fblk) dev_free(p);
+    for (double*& p : w.gpt) dev_free(p);
     delete m.aws;
     m.aws = nullptr;
 }
@@ -497,23 +616,30 @@ efem_status upload_dual_mats(Model& m, int slot, int k)
     return EFEM_OK;
 }
 
-void launch_elem_tangent(Model& m, const double* u, const double* v, double* out)
+// out += K_el v (dual kernels; from the stored Gauss-point tangents when
+// stored is set, which needs v and blocks_ready), or dR/dtheta with v = nullptr
+void launch_elem_tangent(Model& m, const double* u, const double* v, double* out, bool stored = false)
 {
-    for (auto& b : m.blocks) {
+    for (size_t bi = 0; bi < m.blocks.size(); bi++) {
+        auto& b = m.blocks[bi];
         if (b.n == 0) continue;
         TanElemArgs a { b.n, m.n_free, b.conn, b.mat, b.vol, b.J0inv, b.dN, b.gw, m.aws->mats, u, v, out };
-        auto go = [&](auto kern, int ngp) {
+        const double* C = stored ? m.aws->gpt[bi] : nullptr;
+        auto go = [&](auto kern, auto kern_stored, int ngp) {
             const int epb = tan_epb(ngp);
-            kern<<<(b.n + epb - 1) / epb, kBlock, 0, m.stream>>>(a);
+            if (C) kern_stored<<<(b.n + epb - 1) / epb, kBlock, 0, m.stream>>>(a, C);
+            else kern<<<(b.n + epb - 1) / epb, kBlock, 0, m.stream>>>(a);
             m.launches++;
         };
-        if (b.nen == 4 && b.ngp == 1) go(k_elem_tangent<4, 1>, 1);
-        else if (b.nen == 10 && b.ngp == 4) go(k_elem_tangent<10, 4>, 4);
-        else if (b.nen == 10 && b.ngp == 1) go(k_elem_tangent<10, 1>, 1);
-        else if (b.nen == 8 && b.ngp == 8) go(k_elem_tangent<8, 8>, 8);
-        else if (b.nen == 8 && b.ngp == 1) go(k_elem_tangent<8, 1>, 1);
-        else if (b.nen == 20 && b.ngp == 27) go(k_elem_tangent<20, 27>, 27);
-        else if (b.nen == 20 && b.ngp == 8) go(k_elem_tangent<20, 8>, 8);
+#define EFEM_TAN(NEN, NGP) go(k_elem_tangent<NEN, NGP>, k_elem_tangent_stored<NEN, NGP>, NGP)
+        if (b.nen == 4 && b.ngp == 1) EFEM_TAN(4, 1);
+        else if (b.nen == 10 && b.ngp == 4) EFEM_TAN(10, 4);
+        else if (b.nen == 10 && b.ngp == 1) EFEM_TAN(10, 1);
+        else if (b.nen == 8 && b.ngp == 8) EFEM_TAN(8, 8);
+        else if (b.nen == 8 && b.ngp == 1) EFEM_TAN(8, 1);
+        else if (b.nen == 20 && b.ngp == 27) EFEM_TAN(20, 27);
+        else if (b.nen == 20 && b.ngp == 8) EFEM_TAN(20, 8);
+#undef EFEM_TAN
     }
 }
 
@@ -556,16 +682,39 @@ void launch_face_tangent(Model& m, const double* u, const double* v, const doubl
     }
 }
 
-// Face tangent blocks of every face set at u, for the transpose products of
-// one adjoint solve.  Sets blocks_ready only when all of them fit in
-// kFaceBlockBytes; otherwise the transpose products recompute the columns.
-efem_status build_face_blocks(Model& m, const double* u)
+// The stored tangents at u for the Krylov iterations of one adjoint solve:
+// the face blocks of every face set and the Gauss-point tangents of every
+// element block.  Sets blocks_ready only when all of them fit in
+// kStoredBytes; otherwise every product recomputes them on dual numbers.
+efem_status build_stored_tangents(Model& m, const double* u)
 {
     AdjointWS& w = *m.aws;
     w.blocks_ready = false;
     size_t total = 0;
     for (auto& f : m.faces) total += sizeof(double) * f.n * static_cast<size_t>(9 * f.nen * f.nen);
-    if (total == 0 || total > kFaceBlockBytes) return EFEM_OK;
+    for (auto& b : m.blocks) total += sizeof(double) * b.n * static_cast<size_t>(81 * b.ngp);
+    if (total == 0 || total > kStoredBytes) return EFEM_OK;
+    w.gpt.resize(m.blocks.size(), nullptr);
+    for (size_t bi = 0; bi < m.blocks.size(); bi++) {
+        auto& b = m.blocks[bi];
+        if (b.n == 0) continue;
+        const long long nthreads = 9LL * b.n * b.ngp;
+        if (!w.gpt[bi]) {
+            efem_status s = dev_alloc(&w.gpt[bi], static_cast<size_t>(9 * nthreads));
+            if (s != EFEM_OK) return s;
+        }
+        TanElemArgs a { b.n, m.n_free, b.conn, b.mat, b.vol, b.J0inv, b.dN, b.gw, w.mats, u, nullptr, nullptr };
+        const unsigned grid = static_cast<unsigned>((nthreads + kBlock - 1) / kBlock);
+        double* C = w.gpt[bi];
+        m.launches++;
+        if (b.nen == 4 && b.ngp == 1) k_gp_tangent<4, 1><<<grid, kBlock, 0, m.stream>>>(a, C);
+        else if (b.nen == 10 && b.ngp == 4) k_gp_tangent<10, 4><<<grid, kBlock, 0, m.stream>>>(a, C);
+        else if (b.nen == 10 && b.ngp == 1) k_gp_tangent<10, 1><<<grid, kBlock, 0, m.stream>>>(a, C);
+        else if (b.nen == 8 && b.ngp == 8) k_gp_tangent<8, 8><<<grid, kBlock, 0, m.stream>>>(a, C);
+        else if (b.nen == 8 && b.ngp == 1) k_gp_tangent<8, 1><<<grid, kBlock, 0, m.stream>>>(a, C);
+        else if (b.nen == 20 && b.ngp == 27) k_gp_tangent<20, 27><<<grid, kBlock, 0, m.stream>>>(a, C);
+        else if (b.nen == 20 && b.ngp == 8) k_gp_tangent<20, 8><<<grid, kBlock, 0, m.stream>>>(a, C);
+    }
     w.fblk.resize(m.faces.size(), nullptr);
     for (size_t fs = 0; fs < m.faces.size(); fs++) {
         auto& f = m.faces[fs];
@@ -594,7 +743,7 @@ efem_status build_face_blocks(Model& m, const double* u)
 efem_status tangent(Model& m, const double* u, const double* v, double* out, bool transpose)
 {
     EFEM_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * 3 * m.n_free, m.stream));
-    launch_elem_tangent(m, u, v, out);
+    launch_elem_tangent(m, u, v, out, m.aws->blocks_ready);
     if (transpose)
         launch_face_tangent(m, u, nullptr, nullptr, v, out, true);
     else
@@ -655,11 +804,32 @@ efem_status axpys(Model& m, double* y, const double* X, int nk, const double* c)
 
 // Restarted GMRES(kRestart) for K(u)^T x = b, right-preconditioned with H0
 // (x = H0 z); classical Gram-Schmidt applied twice.  x starts at 0.
-efem_status adjoint_gmres(Model& m, const double* u, double tol, int max_it, int* iters, double* relres)
+efem_status adjoint_gmres(Model& m, const double* u, double tol, int max_it, int* iters, double* relres,
+    double* bytes)
 {
     AdjointWS& w = *m.aws;
     const size_t n = w.n;
     const int R = w.restart;
+    // algorithmic bytes of one Krylov iteration: the basis copy, H0, the
+    // transpose tangent (element part as an FP64 residual plus v and the zeroed
+    // output, plus the stored Gauss-point tangents; the stored face blocks or,
+    // without them, the faces' residual bytes), the norm and the scaling; plus
+    // two Gram-Schmidt passes over the j + 1 basis vectors (dots: the basis and
+    // w; updates: the basis, w read and written)
+    const double nd = 8.0 * static_cast<double>(n);
+    efem_model_info mi {};
+    precond_info(m, &mi);
+    long long rb = 0;
+    double rf = 0.0;
+    residual_work(m, 8, &rb, &rf, !w.blocks_ready);
+    double fb = 0.0;
+    if (w.blocks_ready) {
+        for (auto& f : m.faces) fb += static_cast<double>(f.n) * (72.0 * f.nen * f.nen + 4.0 * f.nen);
+        for (auto& b : m.blocks) fb += static_cast<double>(b.n) * b.ngp * 81.0 * 8.0;
+    }
+    const double it_bytes = 2.0 * nd + 16.0 * static_cast<double>(mi.factor_nnz) + 5.0 * nd + static_cast<double>(rb) +
+        2.0 * nd + fb + 3.0 * nd;
+    *bytes = 0.0;
     double bnorm = 0.0;
     efem_status s = dots(m, w.b, 1, w.b, &bnorm);
     if (s != EFEM_OK) return s;
@@ -686,7 +856,11 @@ efem_status adjoint_gmres(Model& m, const double* u, double tol, int max_it, int
             if ((s = precond_enqueue(m, Zj, m.stream)) != EFEM_OK) return s;
             m.launches++;
             if ((s = tangent(m, u, Zj, w.w, true)) != EFEM_OK) return s;
+            *bytes += it_bytes + 2.0 * (2.0 * (j + 1) * nd + 3.0 * nd);
             // two passes of classical Gram-Schmidt, coefficients kept on the device
+            // (with H0 a good preconditioner, K^T H0 v is close to the basis: the
+            // first pass removes most of w in nearly every iteration, so a
+            // conditional second pass would almost always run)
             for (int pass = 0; pass < 2; pass++) {
                 k_dots<<<dim3(kDotBlocks, j + 1), kVec, 0, m.stream>>>(w.V, n, j + 1, w.w, n, w.part);
                 k_rows_reduce<<<(j + 1 + 7) / 8, 256, 0, m.stream>>>(w.part, j + 1, kDotBlocks, w.hcol, w.coef, pass);
@@ -789,6 +963,7 @@ efem_status adjoint(Model& m, const double* d_u, const double* d_dJdu, double* d
 {
     const auto t0 = std::chrono::steady_clock::now();
     std::memset(info, 0, sizeof(*info));
+    const long long launches0 = m.launches;
     efem_status s = alloc_aws(m);
     if (s != EFEM_OK) return s;
     AdjointWS& w = *m.aws;
@@ -807,8 +982,8 @@ efem_status adjoint(Model& m, const double* d_u, const double* d_dJdu, double* d
     const int max_it = m.opts.adjoint_max_iterations > 0 ? m.opts.adjoint_max_iterations : 2000;
     int iters = 0;
     double rel = 0.0;
-    if ((s = build_face_blocks(m, w.u)) != EFEM_OK) return s;
-    s = adjoint_gmres(m, w.u, tol, max_it, &iters, &rel);
+    if ((s = build_stored_tangents(m, w.u)) != EFEM_OK) return s;
+    s = adjoint_gmres(m, w.u, tol, max_it, &iters, &rel, &info->solve_bytes);
     w.blocks_ready = false;  // the blocks hold K at this u only
     if (s != EFEM_OK) return s;
     info->iterations = iters;
@@ -829,6 +1004,7 @@ efem_status adjoint(Model& m, const double* d_u, const double* d_dJdu, double* d
     EFEM_CUDA(cudaStreamSynchronize(m.stream));
     info->ms_params = ms_since(t1);
     info->ms_total = ms_since(t0);
+    info->n_kernel_launches = m.launches - launches0;
     return EFEM_OK;
 }
 

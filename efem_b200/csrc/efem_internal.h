@@ -240,6 +240,8 @@ void dev_free(T*& p)
 efem_status read_json_config(const char* path, ModelInput& in);
 efem_status build_model(ModelInput& in, Model& m);
 efem_status build_blocks(Model& m);   // (re)build the integration tables for opts.integration (host)
+// one residual evaluation's algorithmic bytes and flops (pressure faces included when faces is set)
+void residual_work(const Model& m, int sz, long long* bytes, double* flops, bool faces);
 efem_status ensure_device(Model& m);  // create the stream and upload everything not yet on the device
 
 // ------------------------------------------------------------------ kernels (residual.cu)

@@ -771,6 +771,36 @@ efem_status vec_in(Model& m, const double* src, double** dst, double* staging)
 }
 }  // namespace
 
+namespace efem {
+
+// algorithmic traffic and work of one residual evaluation with sz-byte
+// geometric factors: every input read once (connectivity, material index,
+// V_e, J0^{-1}, u, f_ext), r written once; flops = 2 per FMA (u.dN, H, P(F),
+// S, and the nodal reduction); the pressure faces' part only when faces is set
+void residual_work(const Model& m, int sz, long long* bytes, double* flops, bool faces)
+{
+    long long b = 3LL * 8 * m.n_free * 3;
+    double f = 0;
+    for (auto& blk : m.blocks) {
+        b += static_cast<long long>(blk.n) * (4LL * blk.nen + 4 + sz + 9LL * sz * blk.ngp);
+        double cmat = 0;
+        for (int e = 0; e < blk.n; e++) {
+            const int t = m.materials_used[blk.h_mat[e]].type;
+            cmat += t == EFEM_MOONEY_RIVLIN ? 510.0 : t == EFEM_YEOH ? 270.0 : 260.0;
+        }
+        f += static_cast<double>(blk.ngp) * (36.0 * blk.nen * blk.n + cmat);
+    }
+    for (auto& fc : m.faces) {
+        if (!faces) break;
+        b += static_cast<long long>(fc.n) * (4LL * fc.nen + 4 + 24 + 32 + 9LL * sz * MAX_FGP);
+        f += static_cast<double>(fc.n) * 9.0 * (24.0 * fc.nen + 120.0);
+    }
+    *bytes = b;
+    *flops = f;
+}
+
+}  // namespace efem
+
 extern "C" {
 
 efem_status efem_default_options(efem_options* o)
@@ -953,25 +983,9 @@ efem_status efem_get_model_info(void* model, efem_model_info* info)
     info->n_faces = m->n_faces;
     info->n_force_nodes = m->n_force_nodes;
     info->n_blocks = static_cast<int>(m->blocks.size());
-    // algorithmic traffic and work of one residual evaluation: every input read
-    // once (connectivity, material index, V_e, J0^{-1}, u, f_ext), r written
-    // once; flops = 2 per FMA (u.dN, H, P(F), S, and the nodal reduction)
-    const long long sz = m->opts.precision == EFEM_MIXED ? 4 : 8;
-    long long bytes = 3LL * 8 * m->n_free * 3;
+    long long bytes = 0;
     double flops = 0;
-    for (auto& b : m->blocks) {
-        bytes += static_cast<long long>(b.n) * (4LL * b.nen + 4 + sz + sz * 9 * b.ngp);
-        double cmat = 0;
-        for (int e = 0; e < b.n; e++) {
-            const int t = m->materials_used[b.h_mat[e]].type;
-            cmat += t == EFEM_MOONEY_RIVLIN ? 510.0 : t == EFEM_YEOH ? 270.0 : 260.0;
-        }
-        flops += static_cast<double>(b.ngp) * (36.0 * b.nen * b.n + cmat);
-    }
-    for (auto& f : m->faces) {
-        bytes += static_cast<long long>(f.n) * (4LL * f.nen + 4 + 24 + 32 + sz * 9 * efem::MAX_FGP);
-        flops += static_cast<double>(f.n) * 9.0 * (24.0 * f.nen + 120.0);
-    }
+    efem::residual_work(*m, m->opts.precision == EFEM_MIXED ? 4 : 8, &bytes, &flops, true);
     info->residual_bytes = bytes;
     info->residual_flops = flops;
     info->n_params = efem::n_params(*m);

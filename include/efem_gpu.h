@@ -171,6 +171,11 @@ typedef struct {
     double ms_total;          /* wall time of the call */
     double ms_solve;          /* the adjoint solve */
     double ms_params;         /* the parameter sensitivities */
+    long long n_kernel_launches; /* kernels the call launched */
+    double solve_bytes;       /* algorithmic bytes of the adjoint solve: per Krylov iteration the basis
+                                 copy, one H0 application (16 nnz(L) + 40 n_dof, as for the solve), the
+                                 transpose tangent (the FP64 residual's bytes, v and the zeroed output,
+                                 the stored tangents) and two Gram-Schmidt passes over the basis */
 } efem_adjoint_info;
 
 /* --------------------------------------------------------------- lifetime */
