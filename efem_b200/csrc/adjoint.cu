@@ -30,6 +30,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <vector>
 
@@ -472,6 +473,38 @@ __global__ void __launch_bounds__(kVec) k_dots(const double* __restrict__ X, siz
     }
 }
 
+// y += sum_k c_k x_k, two entries per thread (16-byte loads; ldx and n even,
+// y and X 16-byte aligned)
+__global__ void __launch_bounds__(kVec) k_axpys2(double* __restrict__ y, const double* __restrict__ X, size_t ldx, int nk,
+    const double* __restrict__ c, size_t n)
+{
+    const size_t n2 = n / 2, ld2 = ldx / 2;
+    const double2* X2 = reinterpret_cast<const double2*>(X);
+    double2* y2 = reinterpret_cast<double2*>(y);
+    for (size_t i = blockIdx.x * (size_t)kVec + threadIdx.x; i < n2; i += (size_t)gridDim.x * kVec) {
+        double2 s0 = y2[i], s1 = make_double2(0.0, 0.0), s2 = s1, s3 = s1;
+        int k = 0;
+        for (; k + 4 <= nk; k += 4) {
+            const double2 a = X2[k * ld2 + i], b = X2[(k + 1) * ld2 + i];
+            const double2 d = X2[(k + 2) * ld2 + i], e = X2[(k + 3) * ld2 + i];
+            s0.x += c[k] * a.x;
+            s0.y += c[k] * a.y;
+            s1.x += c[k + 1] * b.x;
+            s1.y += c[k + 1] * b.y;
+            s2.x += c[k + 2] * d.x;
+            s2.y += c[k + 2] * d.y;
+            s3.x += c[k + 3] * e.x;
+            s3.y += c[k + 3] * e.y;
+        }
+        for (; k < nk; k++) {
+            const double2 a = X2[k * ld2 + i];
+            s0.x += c[k] * a.x;
+            s0.y += c[k] * a.y;
+        }
+        y2[i] = make_double2((s0.x + s1.x) + (s2.x + s3.x), (s0.y + s1.y) + (s2.y + s3.y));
+    }
+}
+
 // y += sum_k c_k x_k (coefficients in device memory)
 __global__ void __launch_bounds__(kVec) k_axpys(double* __restrict__ y, const double* __restrict__ X, size_t ldx, int nk,
     const double* __restrict__ c, size_t n)
@@ -533,6 +566,15 @@ __global__ void __launch_bounds__(kVec) k_scale_copy(double* __restrict__ y, con
 }
 
 int vec_grid(size_t n) { return static_cast<int>(std::min<size_t>(592, std::max<size_t>(1, (n + kVec - 1) / kVec))); }
+
+// y += sum_k c_k X_k (rows of stride ldx): the 16-byte form when the layout allows
+void launch_axpys(cudaStream_t st, double* y, const double* X, size_t ldx, int nk, const double* c, size_t n)
+{
+    const bool v2 = n % 2 == 0 && ldx % 2 == 0 && reinterpret_cast<uintptr_t>(y) % 16 == 0 &&
+        reinterpret_cast<uintptr_t>(X) % 16 == 0;
+    if (v2) k_axpys2<<<vec_grid(n / 2), kVec, 0, st>>>(y, X, ldx, nk, c, n);
+    else k_axpys<<<vec_grid(n), kVec, 0, st>>>(y, X, ldx, nk, c, n);
+}
 
 }  // namespace
 
@@ -796,7 +838,7 @@ efem_status axpys(Model& m, double* y, const double* X, int nk, const double* c)
 {
     AdjointWS& w = *m.aws;
     EFEM_CUDA(cudaMemcpyAsync(w.coef, c, sizeof(double) * nk, cudaMemcpyHostToDevice, m.stream));
-    k_axpys<<<vec_grid(w.n), kVec, 0, m.stream>>>(y, X, w.n, nk, w.coef, w.n);
+    launch_axpys(m.stream, y, X, w.n, nk, w.coef, w.n);
     m.launches++;
     EFEM_CUDA(cudaStreamSynchronize(m.stream));  // c is host memory owned by the caller
     return EFEM_OK;
@@ -864,7 +906,7 @@ efem_status adjoint_gmres(Model& m, const double* u, double tol, int max_it, int
             for (int pass = 0; pass < 2; pass++) {
                 k_dots<<<dim3(kDotBlocks, j + 1), kVec, 0, m.stream>>>(w.V, n, j + 1, w.w, n, w.part);
                 k_rows_reduce<<<(j + 1 + 7) / 8, 256, 0, m.stream>>>(w.part, j + 1, kDotBlocks, w.hcol, w.coef, pass);
-                k_axpys<<<vec_grid(n), kVec, 0, m.stream>>>(w.w, w.V, n, j + 1, w.coef, n);
+                launch_axpys(m.stream, w.w, w.V, n, j + 1, w.coef, n);
                 m.launches += 3;
             }
             k_dots<<<dim3(kDotBlocks, 1), kVec, 0, m.stream>>>(w.w, n, 1, w.w, n, w.part);
