@@ -91,7 +91,7 @@ struct Precond {
     double ms_factor = 0;
     int max_r = 0, max_c = 0, max_m = 0, nlev = 0;
     // solve schedule: the persistent kernel's items, launch shape
-    int n_items = 0, solve_grid = 1;
+    int n_items = 0, solve_grid = 1, solve_grid_full = 1, sms = 1;
     size_t solve_smem = 0;
     SolveItem* d_items = nullptr;
     int *d_tgt = nullptr, *d_parent = nullptr, *d_cnt = nullptr, *d_prow = nullptr;
@@ -1625,7 +1625,9 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
     int per_sm = 0, sms = 0;
     EFEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve, kST, P.solve_smem));
     EFEM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m.device));
-    P.solve_grid = std::max(1, std::min(P.n_items, std::max(per_sm, 1) * sms));
+    P.solve_grid_full = std::max(1, std::min(P.n_items, std::max(per_sm, 1) * sms));
+    P.sms = std::max(1, sms);
+    P.solve_grid = t_batch ? std::max(1, std::min(P.n_items, P.sms)) : P.solve_grid_full;
     if (P.n_subs > 0) {
         EFEM_CUDA(cudaFuncSetAttribute(k_sub_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         EFEM_CUDA(cudaFuncSetAttribute(k_sub_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
@@ -1756,6 +1758,22 @@ static efem_status apply_with(Model& m, double* d_v, const SolveBufs& b)
     }
     EFEM_CUDA(cudaGraphLaunch(it->second, m.stream));
     m.launches += 1;
+    return EFEM_OK;
+}
+
+thread_local bool t_batch = false;
+
+efem_status precond_sync_grid(Model& m)
+{
+    if (!m.precond || !m.precond->ready) return EFEM_OK;
+    Precond& P = *m.precond;
+    const int want = t_batch ? std::max(1, std::min(P.n_items, P.sms)) : P.solve_grid_full;
+    if (want == P.solve_grid) return EFEM_OK;
+    EFEM_CUDA(cudaStreamSynchronize(m.stream));
+    for (auto& kv : P.graphs) cudaGraphExecDestroy(kv.second);
+    P.graphs.clear();
+    P.solve_grid = want;
+    m.epoch++;  // the solver's iteration graphs hold the old grid
     return EFEM_OK;
 }
 

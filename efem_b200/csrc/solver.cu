@@ -1183,6 +1183,7 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
         int okf = 0;
         double msf = 0;
         if ((s = precond_setup(m, true, &okf, &msf)) != EFEM_OK) return s;
+        if ((s = precond_sync_grid(m)) != EFEM_OK) return s;
         ok = okf != 0;
         info->n_jacobian_evals = 1;
         info->ms_factor = msf;

@@ -86,3 +86,18 @@ def test_batch_reports_the_failing_model(cases):
     with pytest.raises(api.EfemError):
         api.check(api.lib().efem_batch_solve(hs, 2, ptrs, None, 2))
     assert "model 1" in api.last_error()
+
+
+def test_model_moves_between_single_and_batch_solves(cases):
+    """A batch solve runs the triangular solve on one CTA per SM and a single
+    solve on every CTA that fits; a model solved alone, then in a batch, then
+    alone again recaptures its graphs at each change and gives the same
+    solution each time."""
+    ms = models(cases[:2], criterion=1e-10)
+    u1, i1 = ms[0].solve()
+    us, infos = api.batch_solve(ms, max_threads=2)
+    u3, i3 = ms[0].solve()
+    for info in (i1, infos[0], infos[1], i3):
+        assert info["flags"] & api.SOLVE_CONVERGED
+    for u in (us[0], u3):
+        assert np.linalg.norm(u - u1) <= 1e-6 * np.linalg.norm(u1)
