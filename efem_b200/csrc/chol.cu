@@ -91,7 +91,7 @@ struct Precond {
     double ms_factor = 0;
     int max_r = 0, max_c = 0, max_m = 0, nlev = 0;
     // solve schedule: the persistent kernel's items, launch shape
-    int n_items = 0, solve_grid = 1, solve_grid_full = 1, sms = 1;
+    int n_items = 0, solve_grid = 1, solve_grid_full = 1, slots = 1;
     size_t solve_smem = 0;
     SolveItem* d_items = nullptr;
     int *d_tgt = nullptr, *d_parent = nullptr, *d_cnt = nullptr, *d_prow = nullptr;
@@ -1288,6 +1288,15 @@ void precond_info(const Model& m, efem_model_info* info)
     info->n_solve_subtrees = m.precond->n_subs;
 }
 
+thread_local int t_batch = 0;
+
+// the persistent solve's grid for the calling thread (see precond_sync_grid)
+static int solve_grid_for(const Precond& P)
+{
+    if (t_batch <= 0) return P.solve_grid_full;
+    return std::max(1, std::min(P.n_items, P.slots / t_batch));
+}
+
 static efem_status precond_factor(Model& m, int* ok, double* ms_factor);
 
 efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
@@ -1625,9 +1634,9 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
     int per_sm = 0, sms = 0;
     EFEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve, kST, P.solve_smem));
     EFEM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m.device));
-    P.solve_grid_full = std::max(1, std::min(P.n_items, std::max(per_sm, 1) * sms));
-    P.sms = std::max(1, sms);
-    P.solve_grid = t_batch ? std::max(1, std::min(P.n_items, P.sms)) : P.solve_grid_full;
+    P.slots = std::max(1, per_sm) * std::max(1, sms);
+    P.solve_grid_full = std::max(1, std::min(P.n_items, P.slots));
+    P.solve_grid = solve_grid_for(P);
     if (P.n_subs > 0) {
         EFEM_CUDA(cudaFuncSetAttribute(k_sub_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         EFEM_CUDA(cudaFuncSetAttribute(k_sub_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
@@ -1761,13 +1770,11 @@ static efem_status apply_with(Model& m, double* d_v, const SolveBufs& b)
     return EFEM_OK;
 }
 
-thread_local bool t_batch = false;
-
 efem_status precond_sync_grid(Model& m)
 {
     if (!m.precond || !m.precond->ready) return EFEM_OK;
     Precond& P = *m.precond;
-    const int want = t_batch ? std::max(1, std::min(P.n_items, P.sms)) : P.solve_grid_full;
+    const int want = solve_grid_for(P);
     if (want == P.solve_grid) return EFEM_OK;
     EFEM_CUDA(cudaStreamSynchronize(m.stream));
     for (auto& kv : P.graphs) cudaGraphExecDestroy(kv.second);

@@ -294,11 +294,12 @@ efem_status precond_check(Model& m);             // wait for the stream and repo
 void free_precond(Model& m);
 void precond_info(const Model& m, efem_model_info* info);
 // The persistent triangular solve's grid: every CTA that fits on the device
-// (one solve at a time), or one CTA per SM while t_batch is set (the batch
-// solve's worker threads: many solves share the device, and CTAs waiting on a
-// front's dependencies would hold the SMs the other solves need).  A change
-// drops the graphs that captured the old grid.
-extern thread_local bool t_batch;
+// (one solve at a time), or, while t_batch > 0 (the batch solve's worker
+// threads, t_batch solves in flight), that many CTAs divided among the
+// solves: CTAs waiting on a front's dependencies would otherwise hold the
+// SMs the other solves need.  A change drops the graphs that captured the
+// old grid.
+extern thread_local int t_batch;
 efem_status precond_sync_grid(Model& m);
 // Host assembly of L in CSR over free nodes (upper and lower triangle).
 void assemble_L_csr(const Model& m, std::vector<int>& rowptr, std::vector<int>& col, std::vector<double>& val);

@@ -1274,7 +1274,7 @@ efem_status efem_batch_solve(void** models, int n, double* const* u, efem_solve_
     std::vector<efem_status> st(n, EFEM_OK);
     std::vector<std::string> err(n);
     auto worker = [&]() {
-        efem::t_batch = true;
+        efem::t_batch = nt;
         for (;;) {
             const int q = next.fetch_add(1);
             if (q >= n) return;
@@ -1287,7 +1287,7 @@ efem_status efem_batch_solve(void** models, int n, double* const* u, efem_solve_
     std::vector<std::thread> pool;
     for (int t = 1; t < nt; t++) pool.emplace_back(worker);
     worker();
-    efem::t_batch = false;
+    efem::t_batch = 0;
     for (auto& t : pool) t.join();
     for (int i = 0; i < n; i++)
         if (st[i] != EFEM_OK) {

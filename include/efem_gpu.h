@@ -303,10 +303,10 @@ efem_status efem_strain_energy(void* model, const double* u, double* energy);
  * pool of max_threads host threads (<= 0: one per hardware thread), so the
  * models' device-driven iteration graphs overlap on the GPU.  u[i] is model
  * i's u_inout (host or device per that model's device_ptrs); infos may be
- * NULL or hold n entries.  Inside a batch each model's persistent triangular
- * solve (the H0 application) runs one CTA per SM instead of every CTA that
- * fits, so that the concurrent solves share the SMs; a model later solved
- * alone goes back to the full grid.  Returns the first failing model's
+ * NULL or hold n entries.  Inside a batch the CTAs that fit on the device are
+ * divided among the solves in flight for each model's persistent triangular
+ * solve (the H0 application), instead of every solve asking for all of them;
+ * a model later solved alone goes back to the full grid.  Returns the first failing model's
  * status, with its index in the error message.  The reference solves one problem per
  * process (Simulator::start, src/simulation/Simulator.cpp:20-41). */
 efem_status efem_batch_solve(void** models, int n, double* const* u, efem_solve_info* infos, int max_threads);
