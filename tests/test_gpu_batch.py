@@ -89,10 +89,10 @@ def test_batch_reports_the_failing_model(cases):
 
 
 def test_model_moves_between_single_and_batch_solves(cases):
-    """A batch solve runs the triangular solve on one CTA per SM and a single
-    solve on every CTA that fits; a model solved alone, then in a batch, then
-    alone again recaptures its graphs at each change and gives the same
-    solution each time."""
+    """A batch solve divides the triangular solve's resident CTAs among the
+    solves in flight and a single solve uses all of them; a model solved
+    alone, then in a batch, then alone again recaptures its graphs at each
+    change and gives the same solution each time."""
     ms = models(cases[:2], criterion=1e-10)
     u1, i1 = ms[0].solve()
     us, infos = api.batch_solve(ms, max_threads=2)
