@@ -131,10 +131,13 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------------------- reference arm
-def reference_sample(steps, warmup, ipstep=2):
+def reference_sample(steps, warmup, ipstep=8):
     """The reference's own solver on bounded samples of the workload: one-time
     factorisation, then `warmup` + `steps` steps of `ipstep` L-BFGS iterations.
-    Returns (iters/s over the timed steps, details)."""
+    Returns (iters/s over the timed steps, details).  The reference's time per
+    iteration grows along the solve (0.21 s per iteration at iterations 3-6,
+    0.7-0.9 s from iteration 7 on this beam), so a step spans several
+    iterations."""
     ref = os.path.join(ROOT, "oracle", "_ref", "efem_ref")
     if not os.path.exists(ref):
         return None, {"why": "oracle/_ref/efem_ref is not built"}
