@@ -112,7 +112,12 @@ def test_adjoint_gradient_matches_finite_differences(etype, mat, load):
     m.set_options(adjoint_tolerance=1e-10)
     grad, lam, info = m.adjoint(u, g, want_lambda=True)
     assert info["flags"] & api.SOLVE_CONVERGED, info
-    # the adjoint equation holds
+    # every Krylov iteration launches kernels and moves at least the basis
+    # vector and one H0 application's factor entries
+    assert info["n_kernel_launches"] >= 5 * info["iterations"]
+    assert info["solve_bytes"] >= info["iterations"] * 16.0 * m.info()["factor_nnz"]
+    # the adjoint equation holds (the stored tangents of the solve against the
+    # dual-number transpose product)
     assert np.linalg.norm(m.hvp(u, lam, transpose=True) - g) <= 1e-8
     fds = []
     for k in range(m.n_params):
