@@ -159,6 +159,33 @@ def reference_sample(steps, warmup, ipstep=8):
     return ips, meta
 
 
+def reference_batch_sample(cases, n_proc, ipstep=8, warmup=1, steps=2):
+    """The reference's own solver on n_proc batch models at once, one process
+    per host core (the reference solves one problem per process): each one
+    factors once (excluded), then runs `warmup` + `steps` steps of `ipstep`
+    L-BFGS iterations.  Returns (aggregate iters/s over the timed steps, the
+    models sampled, details)."""
+    ref = os.path.join(ROOT, "oracle", "_ref", "efem_ref")
+    if not os.path.exists(ref):
+        return None, 0, {"why": "oracle/_ref/efem_ref is not built"}
+    with tempfile.TemporaryDirectory() as td:
+        procs = []
+        for i, c in enumerate(cases[:n_proc]):
+            cfg = c.write(os.path.join(td, f"m{i}"))
+            procs.append(subprocess.Popen([ref, "bench", cfg, str(ipstep), str(warmup), str(steps)],
+                                          stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
+        rate, used = 0.0, 0
+        for p in procs:
+            out, err = p.communicate(timeout=3600)
+            if p.returncode != 0:
+                return None, 0, {"why": err[-300:]}
+            st = json.loads(out.strip().splitlines()[-1])["step_s"]
+            if st:  # a model that converged inside the warm-up adds nothing
+                rate += ipstep * len(st) / sum(st)
+                used += 1
+    return rate, used, {}
+
+
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -413,6 +440,15 @@ def run_batch_bench(args):
             "accuracy_reference": "FP64 solves of the same models converged to residual 1e-10",
             "generate_s": gen_s, "build_s": build_s, "setup_s": setup_s,
             "clocks": clocks.summary()}
+    if not args.no_cpu_baseline:
+        cores = min(len(cases), os.cpu_count() or 1)
+        rate, used, meta = reference_batch_sample(cases, cores)
+        if rate is not None:
+            line["cpu_baseline"] = {"value": rate, "unit": "iters/s (aggregate)", "cores": cores, "kind": "reference",
+                                    "sample": f"reference solver (oracle/_ref), one process per host core on the "
+                                              f"first {cores} batch models at once: one factorisation each "
+                                              f"(excluded), then 2 timed steps of 8 L-BFGS iterations; "
+                                              f"{used} models timed; compare with iterations_per_s"}
     print(json.dumps(line))
 
 
