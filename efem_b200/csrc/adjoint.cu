@@ -724,10 +724,22 @@ void launch_face_tangent(Model& m, const double* u, const double* v, const doubl
     }
 }
 
+// Out of device memory for the stored tangents: free them and go on with the
+// dual-number products (blocks_ready stays unset).
+efem_status drop_stored(AdjointWS& w)
+{
+    cudaGetLastError();  // the failed allocation's error is not sticky
+    for (double*& p : w.fblk) dev_free(p);
+    for (double*& p : w.gpt) dev_free(p);
+    w.blocks_ready = false;
+    return EFEM_OK;
+}
+
 // The stored tangents at u for the Krylov iterations of one adjoint solve:
 // the face blocks of every face set and the Gauss-point tangents of every
 // element block.  Sets blocks_ready only when all of them fit in
-// kStoredBytes; otherwise every product recomputes them on dual numbers.
+// kStoredBytes and in device memory; otherwise every product recomputes them
+// on dual numbers.
 efem_status build_stored_tangents(Model& m, const double* u)
 {
     AdjointWS& w = *m.aws;
@@ -742,8 +754,7 @@ efem_status build_stored_tangents(Model& m, const double* u)
         if (b.n == 0) continue;
         const long long nthreads = 9LL * b.n * b.ngp;
         if (!w.gpt[bi]) {
-            efem_status s = dev_alloc(&w.gpt[bi], static_cast<size_t>(9 * nthreads));
-            if (s != EFEM_OK) return s;
+            if (dev_alloc(&w.gpt[bi], static_cast<size_t>(9 * nthreads)) != EFEM_OK) return drop_stored(w);
         }
         TanElemArgs a { b.n, m.n_free, b.conn, b.mat, b.vol, b.J0inv, b.dN, b.gw, w.mats, u, nullptr, nullptr };
         const unsigned grid = static_cast<unsigned>((nthreads + kBlock - 1) / kBlock);
@@ -762,8 +773,7 @@ efem_status build_stored_tangents(Model& m, const double* u)
         auto& f = m.faces[fs];
         if (f.n == 0) continue;
         if (!w.fblk[fs]) {
-            efem_status s = dev_alloc(&w.fblk[fs], f.n * static_cast<size_t>(9 * f.nen * f.nen));
-            if (s != EFEM_OK) return s;
+            if (dev_alloc(&w.fblk[fs], f.n * static_cast<size_t>(9 * f.nen * f.nen)) != EFEM_OK) return drop_stored(w);
         }
         TanFaceArgs a { f.n, m.n_free, f.conn, f.table, f.load_idx, f.A0, f.J0inv, f.load, f.t_ngp, f.t_w, f.t_N,
             f.t_dN, u, nullptr, nullptr, nullptr, nullptr };
