@@ -38,3 +38,18 @@ def test_two_replicas_combine(tmp_path):
 
 def test_single_rank_is_identity():
     assert bench.combine_ranks(12.5, 7, 1) == (12.5, 7.0)
+
+
+def test_reference_batch_sample_runs_one_process_per_model():
+    """The batch bench's CPU baseline: the reference binary on two small batch
+    models at once gives a positive aggregate rate over both."""
+    import os
+    import bench
+    from efem_b200 import meshgen as mg
+
+    if not os.path.exists(os.path.join(bench.ROOT, "oracle", "_ref", "efem_ref")):
+        pytest.skip("oracle/_ref is not built")
+    cases = mg.batch_beams(n=2, el_max=2000)
+    rate, used, meta = bench.reference_batch_sample(cases, 2, ipstep=2, warmup=1, steps=1)
+    assert rate is not None, meta
+    assert used == 2 and rate > 0.0
