@@ -320,9 +320,11 @@ int main(int argc, char** argv)
         if (trace_path)
             write_raw(trace_path, solver.m_f_benchmark.data(), solver.m_f_benchmark.size() * sizeof(double));
         double rinf = obj.nl_residual.size() ? obj.nl_residual.lpNorm<Eigen::Infinity>() : 0.0;
-        printf("{\"n_dof\": %d, \"niter\": %d, \"r_evals\": %d, \"j_evals\": %d, "
+        // precond_ok: the approximate-Jacobian factorisation succeeded
+        // (LBFGSSolver::updateApproxJacobi, LBFGS.h:65-81); 0 = the H0 = I/theta fallback ran
+        printf("{\"n_dof\": %d, \"niter\": %d, \"r_evals\": %d, \"j_evals\": %d, \"precond_ok\": %d, "
                "\"u_inf\": %.17g, \"r_inf\": %.17g, \"setup_s\": %.6f, \"solve_s\": %.6f}\n",
-            n, niter, obj.r_evalutes, obj.j_evalutes, x.lpNorm<Eigen::Infinity>(), rinf,
+            n, niter, obj.r_evalutes, obj.j_evalutes, solver.m_jacobi_available ? 1 : 0, x.lpNorm<Eigen::Infinity>(), rinf,
             std::chrono::duration<double>(t1 - t0).count(), std::chrono::duration<double>(t3 - t2).count());
         return 0;
     }

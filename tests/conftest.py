@@ -55,3 +55,31 @@ def has_gpu():
         return torch.cuda.is_available()
     except Exception:
         return False
+
+
+def write_sample(path, tmpdir):
+    """Rebuild the files of a fixture made by make_golden.sample_arrays (a
+    config with its mesh and constraint files) under tmpdir, at the relative
+    paths the config names; returns (config path, fixture)."""
+    d = np.load(path, allow_pickle=False)
+    cfg = json.loads(str(d["config"]))
+    files = json.loads(str(d["files"]))
+    for k, f in enumerate(files):
+        out = os.path.join(str(tmpdir), f["path"])
+        os.makedirs(os.path.dirname(out), exist_ok=True)
+        with open(out, "w") as fh:
+            if f["kind"] == "mesh":
+                fh.write("#node\n")
+                np.savetxt(fh, d[f"file{k}_X"], fmt="%.17g", delimiter="    ")
+                fh.write("#element\n")
+                tok, ptr = d[f"file{k}_elem"], d[f"file{k}_elem_ptr"]
+                for i in range(ptr.shape[0] - 1):
+                    fh.write("    ".join(str(int(t)) for t in tok[ptr[i]:ptr[i + 1]]) + "\n")
+            else:
+                tok, ptr = d[f"file{k}_tok"], d[f"file{k}_ptr"]
+                for i in range(ptr.shape[0] - 1):
+                    fh.write("    ".join(str(int(t)) for t in tok[ptr[i]:ptr[i + 1]]) + "\n")
+    cfg_path = os.path.join(str(tmpdir), "case.json")
+    with open(cfg_path, "w") as fh:
+        json.dump(cfg, fh, indent=1)
+    return cfg_path, d

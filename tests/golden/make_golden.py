@@ -7,6 +7,14 @@ the tests never need it):
     python tests/golden/make_golden.py            # everything
     python tests/golden/make_golden.py gravity    # the gravity fixtures only
     python tests/golden/make_golden.py trace      # the solve traces only
+    python tests/golden/make_golden.py samples    # the reference's own sample problems
+    python tests/golden/make_golden.py configs    # converged u of the large benchmark meshes
+    python tests/golden/make_golden.py multibody  # two bodies with pose and model_id routing
+    python tests/golden/make_golden.py failure    # a singular approximate Jacobian (fallback solve)
+
+``samples`` and ``configs`` read the reference tree: its location is the
+EFEM_REFERENCE environment variable, else a ``reference`` directory beside
+this repository.
 
 Each ``case_<etype>_<mat>_<load>.npz`` holds a complete small input (node
 coordinates, connectivity, fixed nodes, loads, material) together with what the
@@ -113,12 +121,235 @@ def trace_cases():
     np.savez_compressed(os.path.join(HERE, "traces.npz"), **out)
 
 
+def reference_root():
+    """The reference tree: $EFEM_REFERENCE, else ``reference`` beside this repository."""
+    return os.environ.get("EFEM_REFERENCE") or os.path.join(os.path.dirname(ROOT), "reference")
+
+
+# The reference's own sample problems (sample/<problem>/<problem>.json); each
+# config names one element variant's files, the others are selected by
+# switching the variant directory in every path (as its README describes).
+REF_SAMPLES = [("beam", "c3d4"), ("beam", "c3d20"), ("cap", "c3d4"), ("cap", "c3d20"),
+               ("finger", "c3d4"), ("finger", "c3d10")]
+
+
+def _ragged(rows):
+    flat = np.array([t for r in rows for t in r], dtype=np.int32)
+    ptr = np.cumsum([0] + [len(r) for r in rows]).astype(np.int64)
+    return flat, ptr
+
+
+def _int_lines(path):
+    """Integer token lists of a constraint file's lines (src/io/IO.cpp:67-96)."""
+    return [[int(t) for t in oracle._split(ln)] for ln in oracle._read_lines(path)]
+
+
+def sample_arrays(cfg_path):
+    """Everything a sample's config reads, as arrays: node coordinates and
+    element token lists of each mesh file, integer token lines of each
+    constraint file, and the config text itself."""
+    wd = os.path.dirname(os.path.abspath(cfg_path))
+    cfg = json.load(open(cfg_path))
+    out = {"config": json.dumps(cfg)}
+    files = []
+    for mj in cfg["model"]:
+        X, raw = oracle.read_mesh(os.path.join(wd, mj["mesh_file"]))
+        k = len(files)
+        files.append({"path": mj["mesh_file"], "kind": "mesh"})
+        out[f"file{k}_X"] = X
+        out[f"file{k}_elem"], out[f"file{k}_elem_ptr"] = _ragged(raw)
+    for cj in cfg["constraint"]:
+        fn = cj.get("constraint_file")
+        if not isinstance(fn, str) or not fn:
+            continue
+        k = len(files)
+        files.append({"path": fn, "kind": "lines"})
+        out[f"file{k}_tok"], out[f"file{k}_ptr"] = _ragged(_int_lines(os.path.join(wd, fn)))
+    out["files"] = json.dumps(files)
+    return out
+
+
+def reference_samples():
+    """``sample_<problem>_<variant>.npz``: the reference's six sample problems
+    (its own meshes, loads and materials, read in place) with the reference's
+    converged displacement at the config's own tolerance (``u_solve``) and at
+    a residual of 1e-10 N (``u_tight``)."""
+    import shutil
+    src = os.path.join(reference_root(), "sample")
+    for prob, var in REF_SAMPLES:
+        cfg = json.load(open(os.path.join(src, prob, f"{prob}.json")))
+        base_var = cfg["model"][0]["mesh_file"].split("/")[0]
+        swap = lambda p: var + p[len(base_var):] if p.startswith(base_var + "/") else p
+        for mj in cfg["model"]:
+            mj["mesh_file"] = swap(mj["mesh_file"])
+        for cj in cfg["constraint"]:
+            if isinstance(cj.get("constraint_file"), str):
+                cj["constraint_file"] = swap(cj["constraint_file"])
+        with tempfile.TemporaryDirectory() as td:
+            os.makedirs(os.path.join(td, var))
+            for fn in os.listdir(os.path.join(src, prob, var)):
+                shutil.copy(os.path.join(src, prob, var, fn), os.path.join(td, var, fn))
+            path = os.path.join(td, f"{prob}.json")
+            json.dump(cfg, open(path, "w"), indent=1)
+            data = sample_arrays(path)
+            meta, us = oracle.run_ref("solve", path)
+            data.update(u_solve=us, solve_meta=json.dumps(meta))
+            cfg["analysis"]["residual_criterion"] = 1e-10
+            json.dump(cfg, open(path, "w"), indent=1)
+            meta_t, ut = oracle.run_ref("solve", path)
+            data.update(u_tight=ut, solve_meta_tight=json.dumps(meta_t))
+        np.savez_compressed(os.path.join(HERE, f"sample_{prob}_{var}.npz"), **data)
+        print("sample", prob, var, meta["niter"], meta_t["niter"], meta["solve_s"], meta_t["solve_s"])
+
+
+def config_case(name):
+    """The large benchmark meshes by name: (case, reduced)."""
+    if name == "beam_c3d8_mr_force":
+        return mg.cantilever_c3d8_force(), False
+    if name == "cap_c3d20r_nh_pressure":
+        return mg.cylinder_cap_c3d20(), True
+    if name == "finger_c3d10_yeoh_pressure":
+        return mg.finger_c3d10()[0], False
+    raise ValueError(name)
+
+
+CONFIG_CASES = ["beam_c3d8_mr_force", "cap_c3d20r_nh_pressure", "finger_c3d10_yeoh_pressure"]
+
+
+def mesh_digest(case):
+    """A short fingerprint of a generated mesh (coordinates, connectivity, fixed nodes)."""
+    import hashlib
+    h = hashlib.sha256()
+    h.update(np.ascontiguousarray(case.mesh.X, dtype=np.float64).tobytes())
+    h.update(np.ascontiguousarray(case.mesh.conn, dtype=np.int64).tobytes())
+    h.update(np.ascontiguousarray(case.fix, dtype=np.int64).tobytes())
+    return h.hexdigest()[:16]
+
+
+def config_cases(names=None, eps=1e-6):
+    """``config_<name>.npz``: the reference's converged displacement (stored
+    as float32, ample for the 1e-6 and 1e-4 relative comparisons) of the
+    generated benchmark meshes -- the C3D8 Mooney-Rivlin beam under tip
+    forces, the C3D20R cylinder cap under 10 kPa and the C3D10 Yeoh finger
+    under 30 kPa -- with the generator's mesh fingerprint.  The meshes are
+    regenerated by the tests from efem_b200.meshgen."""
+    for name in names or CONFIG_CASES:
+        case, red = config_case(name)
+        case.analysis["residual_criterion"] = eps
+        with tempfile.TemporaryDirectory() as td:
+            cfg = case.write(td)
+            meta, us = oracle.run_ref("solve", cfg, reduced=red, timeout=48 * 3600)
+        save_config_fixture(name, case, meta, us, eps)
+
+
+def save_config_fixture(name, case, meta, us, eps):
+    np.savez_compressed(os.path.join(HERE, f"config_{name}.npz"), u_solve=us.astype(np.float32),
+                        u_norm=np.linalg.norm(us), solve_meta=json.dumps(meta), mesh=mesh_digest(case),
+                        epsilon=eps)
+    print("config", name, meta)
+
+
+def multibody_case(td):
+    """Two bodies built from one C3D10 mesh with trailing per-element material
+    ids, placed by ``pose`` (body 1: translation; body 2: Euler angles, scale,
+    axis-angle rotation and translation), with constraints routed by
+    ``model_id``: both bodies fixed at their x = 0 face, a follower pressure on
+    body 2's end face, a nodal force on body 1's end nodes
+    (src/model/Model.cpp:14-37, src/math/Math.cpp:37-99,
+    src/fe/ExternalConstraint.cpp:65-81)."""
+    base = mg.small_case("C3D10", "nh", "pressure", seed=3)
+    m = base.mesh
+    ne = m.conn.shape[0]
+    m.mat = np.where(np.arange(ne) % 3 == 0, 2, 1).astype(np.int64)
+    mg.write_mesh(os.path.join(td, "mesh.txt"), m)
+    mg.write_nodes(os.path.join(td, "fix.txt"), base.fix)
+    mg.write_faces(os.path.join(td, "pressure.txt"), base.pressure[0][1])
+    tip = mg.nodes_where(m, lambda X: np.abs(X[:, 0] - 0.03) < 1e-9)
+    mg.write_nodes(os.path.join(td, "force.txt"), tip)
+    cfg = {
+        "analysis": {"max_solver_iters": 0, "max_line_search": 20, "residual_criterion": 1e-8},
+        "model": [
+            {"id": 1, "type": "soft", "mesh_file": "mesh.txt", "pose": [{"t": [0.0, 0.05, 0.0]}]},
+            {"id": 2, "type": "soft", "mesh_file": "mesh.txt",
+             "pose": [{"r": [10.0, -20.0, 30.0]}, {"s": [1.2, 0.9, 1.1]}, {"r": [1.0, 2.0, 2.0, 45.0]},
+                      {"t": [0.01, -0.02, 0.03]}]},
+        ],
+        "constraint": [
+            {"id": 1, "type": "fix", "constraint_file": "fix.txt", "model_id": [1, 2]},
+            {"id": 2, "type": "pressure", "value": 2.0e4, "constraint_file": "pressure.txt", "model_id": 2},
+            {"id": 3, "type": "force", "value": [0.0, 0.0, -0.05], "constraint_file": "force.txt", "model_id": [1]},
+        ],
+        "material": [
+            {"id": 1, "type": "neo_hookean", "C10": 114000.0, "D1": 1e-6, "density": 1050.0},
+            {"id": 2, "type": "yeoh", "C10": 110000.0, "C20": 20000.0, "C30": -300.0, "D1": 1e-6,
+             "density": 1050.0},
+        ],
+        "output": {"save_frame": False, "show_log": False, "disk_log": False},
+    }
+    path = os.path.join(td, "multibody.json")
+    json.dump(cfg, open(path, "w"), indent=1)
+    return path
+
+
+def multibody():
+    """``multibody_c3d10_pose.npz``: the two-body case's inputs, the
+    reference's R(u) at a seeded u and its converged displacement."""
+    rng = np.random.default_rng(20261205)
+    with tempfile.TemporaryDirectory() as td:
+        cfg = multibody_case(td)
+        data = sample_arrays(cfg)
+        meta, _ = oracle.run_ref("info", cfg)
+        u = rng.normal(size=meta["n_dof"]) * 2e-4
+        _, r = oracle.run_ref("residual", cfg, u)
+        meta, us = oracle.run_ref("solve", cfg)
+        data.update(u=u, r=r, u_solve=us, solve_meta=json.dumps(meta))
+    np.savez_compressed(os.path.join(HERE, "multibody_c3d10_pose.npz"), **data)
+    print("multibody", meta)
+
+
+def failure_cases():
+    """``failure_orphan_node.npz``: the C3D10 Neo-Hookean pressure case with
+    one more node that no element uses.  The node is free, so the scalar
+    approximate Jacobian has a zero row and the reference's factorisation
+    fails; its solve falls back to H0 = I/theta (src/simulation/nlsolver/
+    LBFGS.h:65-81).  Holds the reference's solution at 1e-6 N (``u_solve``)
+    and at 1e-10 N (``u_tight``) and the orphan node's first DOF."""
+    case = mg.small_case("C3D10", "nh", "pressure")
+    X = case.mesh.X
+    case.mesh = mg.Mesh(np.vstack([X, [[0.05, 0.02, 0.02]]]), case.mesh.conn, case.mesh.mat)
+    data = case_arrays(case)
+    with tempfile.TemporaryDirectory() as td:
+        cfg = case.write(td)
+        meta, us = oracle.run_ref("solve", cfg)
+        assert meta["precond_ok"] == 0, meta
+        case.analysis.update(residual_criterion=1e-10)
+        cfg = case.write(td)
+        meta_t, ut = oracle.run_ref("solve", cfg)
+    n_free = X.shape[0] + 1 - len(case.fix)
+    data.update(u_solve=us, solve_meta=json.dumps(meta), u_tight=ut, solve_meta_tight=json.dumps(meta_t),
+                orphan_dof=3 * (n_free - 1))
+    np.savez_compressed(os.path.join(HERE, "failure_orphan_node.npz"), **data)
+    print("failure_orphan_node", meta, meta_t["niter"])
+
+
 def main():
     if sys.argv[1:] == ["gravity"]:
         gravity_cases()
         return
     if sys.argv[1:] == ["trace"]:
         trace_cases()
+        return
+    if sys.argv[1:2] == ["samples"]:
+        reference_samples()
+        return
+    if sys.argv[1:2] == ["configs"]:
+        config_cases(sys.argv[2:] or None)
+        return
+    if sys.argv[1:] == ["multibody"]:
+        multibody()
+        return
+    if sys.argv[1:] == ["failure"]:
+        failure_cases()
         return
     rng = np.random.default_rng(20261203)
     for et in ETYPES:
