@@ -13,15 +13,24 @@ approximate Jacobian (as LBFGSSolver::solve does once per solve); the mesh
 set-up (element tables, symbolic analysis of the factor) happens once, before
 the warm-up steps.
 
+After the timed region the default line also carries, on one GPU, the rest
+of the metric: ``parity_rel_l2_vs_reference`` (the timed solve's u against
+the reference's own solve of the same mesh, a committed fixture),
+``mixed_vs_fp64`` (the C3D20R cylinder cap's time-to-converge in mixed
+precision and in FP64, each solution's error against the reference) and
+``adjoint`` / ``adjoint_ms`` (the finger's gradient time); --no-extras skips
+the last two.
+
 --gpus N: N independent replicas (one process per GPU, the solve does not
 shard); value = iterations of all ranks / max-over-ranks time.
 --impl reference: the reference's own CPU solver (compiled from its sources in
 oracle/_ref), timed on the host cores on bounded samples of the same solve.
 
 --workload batch: the batched time-to-solution of 256 uneven C3D4 beams
-(efem_b200.meshgen.batch_beams, 2.65 M elements in all), mixed precision, all
-solves concurrent (efem_batch_solve), against the plain FP64 path solving the
-same models one after another.
+(efem_b200.meshgen.batch_beams, 2.65 M elements in all), mixed precision, as
+one union model in one iteration graph (efem_batch_solve), next to the same
+batch in FP64 and to the plain FP64 path solving the models one after
+another.
 
 --workload cap: time-to-converge of the closed cylinder cap (C3D20 reduced
 integration, 9088 elements, 10 kPa cavity pressure) in mixed precision next
@@ -210,17 +219,18 @@ def run_reference_arm(args):
 
 
 # --------------------------------------------------------------------------- adjoint gradient
-def run_adjoint_bench(args):
-    """Adjoint gradient time on the pneumatic finger (one GPU)."""
+def measure_adjoint(steps, warmup, stream):
+    """Adjoint gradient time on the pneumatic finger: returns a dict with the
+    mean device time per gradient (CUDA events on the model's stream), the
+    end-to-end time through host buffers, the GMRES iterations and the
+    whole adjoint solve's HBM roofline."""
     import torch
-    from efem_b200 import api, meshgen as mg
-    torch.cuda.set_device(0)
+    from efem_b200 import api, meshgen as mg, profiling
     case, tip = mg.finger_c3d10()
     opts = api.default_options()
     opts.max_iterations = 20000  # a bound for the equilibrium solve
     t_setup = time.time()
     model = api.Model.from_case(case, opts)
-    stream = torch.cuda.current_stream()
     api.check(api.lib().efem_set_stream(model.h, api.ctypes.c_void_p(stream.cuda_stream)))
     model.set_options(device_ptrs=1)
     u = torch.zeros(model.n_dof, dtype=torch.float64, device="cuda")
@@ -229,18 +239,17 @@ def run_adjoint_bench(args):
     dnode = int(np.nonzero(model.dof_map() == tip)[0][0])
     g = torch.zeros(model.n_dof, dtype=torch.float64, device="cuda")
     g[3 * dnode + 2] = 1.0
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         model.adjoint(u, g)
     torch.cuda.synchronize()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     infos = []
-    with ClockSampler(0) as clocks:
-        for a, b in ev:
-            a.record(stream)
-            grad, _, info = model.adjoint(u, g)
-            b.record(stream)
-            infos.append(info)
-        torch.cuda.synchronize()
+    for a, b in ev:
+        a.record(stream)
+        grad, _, info = model.adjoint(u, g)
+        b.record(stream)
+        infos.append(info)
+    torch.cuda.synchronize()
     ms = [a.elapsed_time(b) for a, b in ev]
     # end to end with host buffers: u and dJ/du copied in, dJ/dtheta out
     model.set_options(device_ptrs=0)
@@ -258,45 +267,72 @@ def run_adjoint_bench(args):
     # whole adjoint solve against HBM: its algorithmic bytes (the library's
     # count per Krylov iteration) over its time (host clock around the solve,
     # ended by a stream synchronisation)
-    from efem_b200 import profiling
     hbm, hbm_kind = profiling.hbm_peak()
     solve_s = float(np.mean([i["ms_solve"] for i in infos])) / 1000.0
     nbytes = float(np.mean([i["solve_bytes"] for i in infos]))
     achieved = nbytes / solve_s / 1e9
-    roof = {"kernel": "adjoint solve (GMRES: k_solve H0, transpose tangent, Gram-Schmidt)", "bound": "hbm",
-            "achieved": achieved, "peak": hbm, "peak_source": hbm_kind, "unit": "GB/s", "frac": achieved / hbm,
-            "traffic": None, "algorithmic_bytes_per_gradient": nbytes}
-    line = {"metric": "adjoint gradient time (dJ/dtheta, C3D10 Yeoh finger 50688 el)", "value": float(np.mean(ms)),
-            "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(ms)),
+    out = {"ms": float(np.mean(ms)), "ms_all": ms, "e2e_ms": e2e_ms, "dof": model.n_dof,
+           "elements": info["n_elements"], "parameters": info["n_params"],
+           "gmres_iterations": float(np.mean([i["iterations"] for i in infos])),
+           "adjoint_solve_ms": float(np.mean([i["ms_solve"] for i in infos])),
+           "parameter_sensitivities_ms": float(np.mean([i["ms_params"] for i in infos])),
+           "adjoint_tolerance": model.options.adjoint_tolerance,
+           "equilibrium_solve": {"niter": sinfo["niter"], "ms": sinfo["ms_total"], "r_inf": sinfo["r_inf"]},
+           "setup_s": setup_s, "gpu_launches": int(sum(i["n_kernel_launches"] for i in infos)),
+           "h2d_bytes": 2 * 8 * model.n_dof, "d2h_bytes": 8 * info["n_params"],
+           "roofline": {"kernel": "adjoint solve (GMRES: k_solve H0, transpose tangent, Gram-Schmidt)",
+                        "bound": "hbm", "achieved": achieved, "peak": hbm, "peak_source": hbm_kind, "unit": "GB/s",
+                        "frac": achieved / hbm, "traffic": None, "algorithmic_bytes_per_gradient": nbytes}}
+    model.close()
+    return out
+
+
+def run_adjoint_bench(args):
+    """Adjoint gradient time on the pneumatic finger (one GPU)."""
+    import torch
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream()
+    with ClockSampler(0) as clocks:
+        a = measure_adjoint(args.steps, args.warmup, stream)
+    line = {"metric": "adjoint gradient time (dJ/dtheta, C3D10 Yeoh finger 50688 el)", "value": a["ms"],
+            "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": a["ms"],
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded structured mesh in the reference's input format)",
             "config": {"workload": "pneumatic finger 80x15x15 mm, 8 chambers, 50688 C3D10 (Yeoh), 30 kPa on the "
                                    "chamber walls, J = u_z of the tip node, gradient w.r.t. all material constants "
-                                   "and the pressure at the converged equilibrium", "dof": model.n_dof,
-                       "elements": info["n_elements"], "parameters": info["n_params"],
-                       "adjoint_tolerance": model.options.adjoint_tolerance},
-            "gmres_iterations": float(np.mean([i["iterations"] for i in infos])),
-            "adjoint_solve_ms": float(np.mean([i["ms_solve"] for i in infos])),
-            "parameter_sensitivities_ms": float(np.mean([i["ms_params"] for i in infos])),
-            "equilibrium_solve": {"niter": sinfo["niter"], "ms": sinfo["ms_total"], "r_inf": sinfo["r_inf"]},
-            "setup_s": setup_s,
-            "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 2 * 8 * model.n_dof,
-                    "d2h_bytes_per_step": 8 * info["n_params"]},
-            "gpu_launches": int(sum(i["n_kernel_launches"] for i in infos)),
-            "roofline": roof,
-            "clocks": clocks.summary()}
+                                   "and the pressure at the converged equilibrium", "dof": a["dof"],
+                       "elements": a["elements"], "parameters": a["parameters"],
+                       "adjoint_tolerance": a["adjoint_tolerance"]},
+            "gmres_iterations": a["gmres_iterations"], "adjoint_solve_ms": a["adjoint_solve_ms"],
+            "parameter_sensitivities_ms": a["parameter_sensitivities_ms"],
+            "equilibrium_solve": a["equilibrium_solve"], "setup_s": a["setup_s"],
+            "e2e": {"value": a["e2e_ms"], "unit": "ms", "h2d_bytes_per_step": a["h2d_bytes"],
+                    "d2h_bytes_per_step": a["d2h_bytes"]},
+            "gpu_launches": a["gpu_launches"], "roofline": a["roofline"], "clocks": clocks.summary()}
     print(json.dumps(line))
-    model.close()
 
 
 # --------------------------------------------------------------------------- C3D20R cap, mixed vs FP64
-def run_cap_bench(args):
-    """Time-to-converge of the C3D20R cylinder cap, mixed precision vs FP64 (one GPU)."""
+def reference_fixture(name):
+    """The reference's converged displacement of a generated benchmark mesh
+    (tests/golden/config_<name>.npz, made by tests/golden/make_golden.py from
+    the reference compiled in oracle/_ref), or None."""
+    path = os.path.join(ROOT, "tests", "golden", f"config_{name}.npz")
+    if not os.path.exists(path):
+        return None
+    d = np.load(path, allow_pickle=False)
+    return {"u": d["u_solve"].astype(np.float64), "meta": json.loads(str(d["solve_meta"])),
+            "epsilon": float(d["epsilon"])}
+
+
+def measure_cap(steps, warmup, stream):
+    """Time-to-converge of the C3D20R cylinder cap in mixed precision and in
+    FP64 (same stream, L2 flushed before every solve), each solution's error
+    against the reference's own FP64 solve of the same mesh and against this
+    library's FP64 solve converged to 1e-10 N."""
     import torch
     from efem_b200 import api, meshgen as mg
-    torch.cuda.set_device(0)
     case = mg.cylinder_cap_c3d20()
-    stream = torch.cuda.current_stream()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     def build(precision, criterion=1e-6):
@@ -309,8 +345,8 @@ def run_cap_bench(args):
         m.set_options(device_ptrs=1)
         return m, torch.zeros(m.n_dof, dtype=torch.float64, device="cuda")
 
-    def timed(m, u, steps):
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    def timed(m, u, n):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
         infos = []
         for k, (a, b) in enumerate(ev):
             flush.fill_(float(k))
@@ -324,42 +360,71 @@ def run_cap_bench(args):
     t0 = time.time()
     m32, u32 = build(api.MIXED)
     m64, u64 = build(api.FP64)
-    for _ in range(max(1, args.warmup)):
+    for _ in range(max(1, warmup)):
         timed(m32, u32, 1)
         timed(m64, u64, 1)
     setup_s = time.time() - t0
-    with ClockSampler(0) as clocks:
-        ms32, i32 = timed(m32, u32, args.steps)
-        ms64, i64 = timed(m64, u64, args.steps)
+    ms32, i32 = timed(m32, u32, steps)
+    ms64, i64 = timed(m64, u64, steps)
     mref, uref = build(api.FP64, 1e-10)
     mref.set_options(max_iterations=50000)
     _, iref = mref.solve(uref)
-    rel = lambda a: float(torch.linalg.norm(a - uref) / torch.linalg.norm(uref))  # noqa: E731
+    rel = lambda a, b: float(torch.linalg.norm(a - b) / torch.linalg.norm(b))  # noqa: E731
     r64_at_mixed = float(m64.residual(u32).abs().max())  # device_ptrs: CUDA tensors in and out
+    fx = reference_fixture("cap_c3d20r_nh_pressure")
+    vs_ref = {}
+    if fx is not None:
+        ur = torch.from_numpy(fx["u"]).cuda()
+        vs_ref = {"mixed": rel(u32, ur), "fp64": rel(u64, ur), "fp64_1e-10": rel(uref, ur),
+                  "reference_niter": fx["meta"]["niter"], "reference_epsilon": fx["epsilon"]}
     info = m32.info()
-    line = {"metric": "time-to-converge, mixed precision (C3D20R cylinder cap, 9088 el)", "value": ms32, "unit": "ms",
-            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms32, "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+    n32 = max(1.0, float(np.mean([i["niter"] for i in i32])))
+    n64 = max(1.0, float(np.mean([i["niter"] for i in i64])))
+    out = {"elements": info["n_elements"], "dof": m32.n_dof, "faces": info["n_faces"],
+           "mixed": {"ms": ms32, "niter": n32, "r_inf": i32[-1]["r_inf"],
+                     "refined": bool(i32[-1]["flags"] & api.SOLVE_REFINED),
+                     "rel_l2_vs_fp64_1e-10": rel(u32, uref), "fp64_residual_at_mixed_solution": r64_at_mixed,
+                     "ms_per_iteration": ms32 / n32},
+           "fp64": {"ms": ms64, "niter": n64, "r_inf": i64[-1]["r_inf"],
+                    "rel_l2_vs_fp64_1e-10": rel(u64, uref), "ms_per_iteration": ms64 / n64},
+           "fp64_over_mixed_time": ms64 / ms32,
+           "rel_l2_vs_reference": vs_ref,
+           "fp64_1e-10_solution": {"niter": iref["niter"], "r_inf": iref["r_inf"]},
+           "setup_s": setup_s}
+    for m in (m32, m64, mref):
+        m.close()
+    return out
+
+
+CAP_WORKLOAD = ("hollow cylinder ri 20 mm, ro 25 mm, h 30 mm, 5 mm top plate; 64x4x24 shell + butterfly plate; "
+                "C3D20 reduced integration; NH C10 114 kPa, D1 1e-6; bottom fixed; 10 kPa follower pressure on the "
+                "cavity walls; residual 1e-6")
+
+
+def run_cap_bench(args):
+    """Time-to-converge of the C3D20R cylinder cap, mixed precision vs FP64 (one GPU)."""
+    import torch
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream()
+    with ClockSampler(0) as clocks:
+        c = measure_cap(args.steps, args.warmup, stream)
+    line = {"metric": "time-to-converge, mixed precision (C3D20R cylinder cap, 9088 el)", "value": c["mixed"]["ms"],
+            "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": c["mixed"]["ms"],
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
             "data": "synthetic (seeded structured mesh in the reference's input format)",
-            "config": {"workload": "hollow cylinder ri 20 mm, ro 25 mm, h 30 mm, 5 mm top plate; 64x4x24 shell + "
-                                   "butterfly plate; C3D20 reduced integration; NH C10 114 kPa, D1 1e-6; bottom "
-                                   "fixed; 10 kPa follower pressure on the cavity walls; residual 1e-6",
-                       "elements": info["n_elements"], "dof": m32.n_dof, "faces": info["n_faces"],
+            "config": {"workload": CAP_WORKLOAD, "elements": c["elements"], "dof": c["dof"], "faces": c["faces"],
                        "l2": "flushed (256 MB write) before every solve"},
-            "mixed": {"ms": ms32, "niter": float(np.mean([i["niter"] for i in i32])),
-                      "r_inf": i32[-1]["r_inf"], "rel_l2_vs_fp64_1e-10": rel(u32),
-                      "fp64_residual_at_mixed_solution": r64_at_mixed},
-            "fp64": {"ms": ms64, "niter": float(np.mean([i["niter"] for i in i64])),
-                     "r_inf": i64[-1]["r_inf"], "rel_l2_vs_fp64_1e-10": rel(u64)},
-            "fp64_over_mixed_time": ms64 / ms32,
-            "reference_solution": {"niter": iref["niter"], "r_inf": iref["r_inf"]},
-            "setup_s": setup_s, "clocks": clocks.summary()}
+            **{k: c[k] for k in ("mixed", "fp64", "fp64_over_mixed_time", "rel_l2_vs_reference",
+                                 "fp64_1e-10_solution", "setup_s")},
+            "clocks": clocks.summary()}
     print(json.dumps(line))
 
 
 # --------------------------------------------------------------------------- batched solves
 def run_batch_bench(args):
-    """Mixed-precision batched solves of 256 uneven beams vs the plain FP64 path."""
+    """Mixed-precision batched solves of 256 uneven beams (one union model, one
+    iteration graph) next to the same batch in FP64 and to the plain FP64
+    path solving the models one after another."""
     import torch
     from efem_b200 import api, meshgen as mg
     torch.cuda.set_device(0)
@@ -398,12 +463,14 @@ def run_batch_bench(args):
         torch.cuda.synchronize()
         return time.perf_counter() - a, infos
 
+    rel = lambda a, b: float(torch.linalg.norm(a - b) / torch.linalg.norm(b))  # noqa: E731
     t0 = time.time()
     m32, u32 = build(api.MIXED)
     m64, u64 = build(api.FP64)
     build_s = time.time() - t0
     t0 = time.time()
-    run_batch(m32, u32)          # first solves: symbolic analyses, graph captures
+    run_batch(m32, u32)          # first calls: union set-up, symbolic analyses, graph captures
+    run_batch(m64, u64)
     run_sequential(m64, u64)
     setup_s = time.time() - t0
     for _ in range(max(0, args.warmup - 1)):
@@ -413,12 +480,18 @@ def run_batch_bench(args):
         for _ in range(args.steps):
             t, infos = run_batch(m32, u32)
             times.append(t)
-    t64, infos64 = run_sequential(m64, u64)
-    # accuracy of the mixed solutions against FP64 solutions converged to 1e-10
+        t64b, infos64b = run_batch(m64, u64)
+        u64b = [u.clone() for u in u64]
+        t64, infos64 = run_sequential(m64, u64)
+    # accuracy against FP64 solves converged to 1e-10, at the reference's 1e-6 N and at 1e-9 N
     mref, uref = build(api.FP64, 1e-10)
     api.batch_solve(mref, uref)
-    err = max(float(torch.linalg.norm(a - b) / torch.linalg.norm(b)) for a, b in zip(u32, uref))
-    err64 = max(float(torch.linalg.norm(a - b) / torch.linalg.norm(b)) for a, b in zip(u64, uref))
+    err = max(rel(a, b) for a, b in zip(u32, uref))
+    err64 = max(rel(a, b) for a, b in zip(u64, uref))
+    for m in m32:
+        m.set_options(residual_criterion=1e-9)
+    t_tight, infos_tight = run_batch(m32, u32)
+    err_tight = max(rel(a, b) for a, b in zip(u32, uref))
     iters = sum(i["niter"] for i in infos)
     conv = sum(1 for i in infos if i["flags"] & api.SOLVE_CONVERGED)
     t = float(np.mean(times))
@@ -430,13 +503,22 @@ def run_batch_bench(args):
                                    "elements each), NH or MR, C10 5e4-5e5 Pa, end pressure 1-20 kPa capped at half "
                                    "the Euler buckling load, residual 1e-6",
                        "models": len(cases), "elements": int(sum(c.mesh.conn.shape[0] for c in cases)),
-                       "concurrency": "one CUDA stream and host thread per model (efem_batch_solve)",
+                       "batching": "one union model: one element-kernel launch per element type, one forest "
+                                   "factorisation and triangular solve, segmented L-BFGS kernels, one CUDA graph "
+                                   "of the iteration loop (efem_batch_solve)",
                        "timing": "host clock around the whole batch, device synchronised before and after"},
+            "union": all(bool(i["flags"] & api.SOLVE_BATCHED) for i in infos),
             "batch_iterations": iters, "iterations_per_s": iters / t, "converged": conv,
+            "max_iterations_of_a_member": max(i["niter"] for i in infos),
+            "refined_members": sum(1 for i in infos if i["flags"] & api.SOLVE_REFINED),
+            "fp64_batched_s": t64b, "mixed_speedup_vs_fp64_batched": t64b / t,
             "fp64_sequential_s": t64, "speedup_vs_fp64_sequential": t64 / t,
             "fp64_sequential_iterations": sum(i["niter"] for i in infos64),
+            "fp64_batched_vs_sequential_max_rel_l2": max(rel(a, b) for a, b in zip(u64b, u64)),
             "mixed_vs_fp64_max_rel_l2": err,
             "fp64_at_1e-6_vs_fp64_max_rel_l2": err64,
+            "at_1e-9": {"mixed_s": t_tight, "mixed_vs_fp64_max_rel_l2": err_tight,
+                        "converged": sum(1 for i in infos_tight if i["flags"] & api.SOLVE_CONVERGED)},
             "accuracy_reference": "FP64 solves of the same models converged to residual 1e-10",
             "generate_s": gen_s, "build_s": build_s, "setup_s": setup_s,
             "clocks": clocks.summary()}
@@ -461,6 +543,8 @@ def main():
     ap.add_argument("--impl", default="efem_b200", choices=["efem_b200", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the mixed-vs-FP64 (cap) and adjoint (finger) blocks of the default line")
     ap.add_argument("--host-loop", action="store_true",
                     help="drive the L-BFGS iterations from the host (same kernels; for launch-list profiling)")
     ap.add_argument("--workload", default="beam", choices=["beam", "finger-adjoint", "batch", "cap"])
@@ -579,6 +663,23 @@ def main():
             "gpu_launches": int(launches * args.steps),
             "roofline": roof,
             "clocks": clocks.summary()}
+    # ---- parity of the timed solve's result with the reference's own solve of the same mesh
+    fx = reference_fixture("beam_c3d8_mr_force")
+    if fx is not None:
+        ur = torch.from_numpy(fx["u"]).cuda()
+        line["parity_rel_l2_vs_reference"] = float(torch.linalg.norm(u - ur) / torch.linalg.norm(ur))
+        line["parity"] = {"reference_niter": fx["meta"]["niter"], "reference_r_inf": fx["meta"]["r_inf"],
+                          "epsilon": fx["epsilon"],
+                          "reference": "the reference's LBFGSSolver::solve of the same mesh (oracle/_ref), "
+                                       "tests/golden/config_beam_c3d8_mr_force.npz"}
+    # ---- the rest of the metric, after the timed region: mixed vs FP64 (C3D20R cap) and the adjoint gradient
+    if rank == 0 and world == 1 and not args.no_extras:
+        c = measure_cap(3, 1, stream)
+        line["mixed_vs_fp64"] = {"workload": CAP_WORKLOAD, **c}
+        a = measure_adjoint(3, 1, stream)
+        line["adjoint"] = {"workload": "pneumatic finger, 50688 C3D10 Yeoh, 30 kPa chambers, dJ/dtheta of the "
+                                       "tip node's u_z for every material constant and the pressure", **a}
+        line["adjoint_ms"] = a["ms"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         ips, meta = reference_sample(steps=3, warmup=1)
         if ips is not None:

@@ -30,7 +30,8 @@ LOAD_FIX, LOAD_FORCE, LOAD_PRESSURE, LOAD_DPRESSURE, LOAD_GRAVITY = 0, 1, 2, 3, 
 GRAVITY = {"x": (9.8, 0.0, 0.0), "-x": (-9.8, 0.0, 0.0), "y": (0.0, 9.8, 0.0), "-y": (0.0, -9.8, 0.0),
            "z": (0.0, 0.0, 9.8), "-z": (0.0, 0.0, -9.8)}
 FP64, MIXED = 0, 1
-SOLVE_CONVERGED, SOLVE_PRECOND_FALLBACK, SOLVE_DX_CONVERGED, SOLVE_MAX_ITERS, SOLVE_PDL = 1, 2, 4, 8, 16
+SOLVE_CONVERGED, SOLVE_PRECOND_FALLBACK, SOLVE_DX_CONVERGED, SOLVE_MAX_ITERS, SOLVE_PDL, SOLVE_REFINED = 1, 2, 4, 8, 16, 32
+SOLVE_BATCHED = 64
 
 EXPORTED = ["efem_default_options", "efem_model_create_from_json", "efem_model_create", "efem_model_destroy",
             "efem_get_options", "efem_set_options", "efem_get_model_info", "efem_dof_map", "efem_residual",
@@ -54,7 +55,8 @@ class Options(ctypes.Structure):
                 ("host_loop", ctypes.c_int), ("adjoint_tolerance", ctypes.c_double),
                 ("adjoint_max_iterations", ctypes.c_int), ("elem_threads", ctypes.c_int),
                 ("consistent_inertia", ctypes.c_int), ("trace", ctypes.c_int),
-                ("solve_subtree_levels", ctypes.c_int), ("line_search", ctypes.c_int)]
+                ("solve_subtree_levels", ctypes.c_int), ("line_search", ctypes.c_int),
+                ("wait_limit", ctypes.c_int), ("wait_test", ctypes.c_int)]
 
 
 class SolveInfo(ctypes.Structure):

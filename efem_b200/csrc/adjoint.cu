@@ -27,6 +27,8 @@
 // order (a follower load's pressure value, a directed load's vector scale).
 #include <cuda_runtime.h>
 
+#include <cstdlib>
+
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -728,10 +730,39 @@ void launch_face_tangent(Model& m, const double* u, const double* v, const doubl
 // dual-number products (blocks_ready stays unset).
 efem_status drop_stored(AdjointWS& w)
 {
-    cudaGetLastError();  // the failed allocation's error is not sticky
     for (double*& p : w.fblk) dev_free(p);
     for (double*& p : w.gpt) dev_free(p);
     w.blocks_ready = false;
+    return EFEM_OK;
+}
+
+// Device memory for stored tangents.  Running out of memory is not an error
+// (*oom is set and the caller falls back to the dual-number products); any
+// other failure is.  The environment variable EFEM_TEST_STORED_OOM=1 makes
+// every such allocation report out of memory, so that tests reach the
+// fallback without filling the GPU.
+efem_status stored_alloc(double** p, size_t n, bool* oom)
+{
+    *p = nullptr;
+    *oom = false;
+    if (n == 0) return EFEM_OK;
+    const char* force = std::getenv("EFEM_TEST_STORED_OOM");
+    if (force && force[0] == '1') {
+        *oom = true;
+        return EFEM_OK;
+    }
+    const cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), n * sizeof(double));
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();  // not sticky: clear it so that later checks do not see it
+        *p = nullptr;
+        *oom = true;
+        return EFEM_OK;
+    }
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        set_error(std::string("cudaMalloc of the stored tangents: ") + cudaGetErrorString(e));
+        return EFEM_ERR_CUDA;
+    }
     return EFEM_OK;
 }
 
@@ -754,7 +785,10 @@ efem_status build_stored_tangents(Model& m, const double* u)
         if (b.n == 0) continue;
         const long long nthreads = 9LL * b.n * b.ngp;
         if (!w.gpt[bi]) {
-            if (dev_alloc(&w.gpt[bi], static_cast<size_t>(9 * nthreads)) != EFEM_OK) return drop_stored(w);
+            bool oom = false;
+            const efem_status as = stored_alloc(&w.gpt[bi], static_cast<size_t>(9 * nthreads), &oom);
+            if (as != EFEM_OK) return as;
+            if (oom) return drop_stored(w);
         }
         TanElemArgs a { b.n, m.n_free, b.conn, b.mat, b.vol, b.J0inv, b.dN, b.gw, w.mats, u, nullptr, nullptr };
         const unsigned grid = static_cast<unsigned>((nthreads + kBlock - 1) / kBlock);
@@ -773,7 +807,10 @@ efem_status build_stored_tangents(Model& m, const double* u)
         auto& f = m.faces[fs];
         if (f.n == 0) continue;
         if (!w.fblk[fs]) {
-            if (dev_alloc(&w.fblk[fs], f.n * static_cast<size_t>(9 * f.nen * f.nen)) != EFEM_OK) return drop_stored(w);
+            bool oom = false;
+            const efem_status as = stored_alloc(&w.fblk[fs], f.n * static_cast<size_t>(9 * f.nen * f.nen), &oom);
+            if (as != EFEM_OK) return as;
+            if (oom) return drop_stored(w);
         }
         TanFaceArgs a { f.n, m.n_free, f.conn, f.table, f.load_idx, f.A0, f.J0inv, f.load, f.t_ngp, f.t_w, f.t_N,
             f.t_dN, u, nullptr, nullptr, nullptr, nullptr };

@@ -483,7 +483,7 @@ __global__ void __launch_bounds__(kIT) k_offdiag_inv(FrontArgs a, const Tile* __
 //   kBwdX      x rows of one tile         (waits: own y, parent's x)
 enum ItemKind { kFwdFront = 0, kFwdY = 1, kFwdG = 2, kBwdFront = 3, kBwdX = 5 };
 
-// device counters, one int array: [cY ns][cGin ns][unused ns][cX ns][ticket][error]
+// device counters, one int array: [cY ns][cGin ns][exits, ns - 1 unused][cX ns][ticket][error]
 struct SolveArgs {
     FrontArgs a;
     const int* parent;
@@ -498,9 +498,12 @@ struct SolveArgs {
     double* upd;
     int* cnt;
     unsigned long long* stamp;  // when set: global timer at the start of the solve
+    int spin_limit;             // polls of one wait before the solve gives up
+    int test_wait;              // 1: the last item's wait target is raised by one (it can only run out)
+    int n3;                     // entries of v (3 per free node)
 };
 
-constexpr int kSpinLimit = 1 << 22;  // polls of one wait (about half a second)
+constexpr int kSpinLimit = 1 << 22;  // default polls of one wait (about half a second)
 
 __device__ __forceinline__ int ld_acquire(const int* p)
 {
@@ -509,13 +512,14 @@ __device__ __forceinline__ int ld_acquire(const int* p)
     return v;
 }
 
-// thread 0 only: wait until *c >= target; false on a timeout or an earlier error
-__device__ bool wait_ge(const int* c, int target, int* err)
+// thread 0 only: wait until *c >= target; false after `limit` polls (the
+// error flag is then set) or when another wait has already given up
+__device__ bool wait_ge(const int* c, int target, int* err, int limit)
 {
     for (int it = 0;; it++) {
         if (ld_acquire(c) >= target) return true;
         if (*reinterpret_cast<volatile int*>(err)) return false;
-        if (it >= kSpinLimit) {
+        if (it >= limit) {
             atomicExch(err, 1);
             return false;
         }
@@ -751,6 +755,7 @@ __global__ void __launch_bounds__(kST) k_solve(SolveArgs A)
     const int* tY = A.tgt;
     const int* tGin = A.tgt + ns;
     const int* tX = A.tgt + 3 * ns;
+    int* exits = A.cnt + 2 * ns;
     const int tid = threadIdx.x;
     const FrontArgs& a = A.a;
     int next = 0;  // thread 0: the ticket taken ahead
@@ -770,6 +775,7 @@ __global__ void __launch_bounds__(kST) k_solve(SolveArgs A)
             griddep_launch();  // no more items for this CTA
             break;
         }
+        const int bump = A.test_wait && it == A.n_items - 1 ? 1 : 0;
         const SolveItem d = A.items[it];
         if (tid == 0) next = atomicAdd(ticket, 1);  // in flight while this item runs
         const int kind = d.kind, s = d.s, r0 = d.r0, r1 = d.r1, R = r1 - r0, cbeg = d.cbeg, cend = d.cend;
@@ -825,8 +831,11 @@ __global__ void __launch_bounds__(kST) k_solve(SolveArgs A)
             switch (kind) {
             case kFwdFront:
             case kFwdY:
-            case kFwdG: ok = wait_ge(cGin + s, tGin[s], err); break;
-            default: ok = wait_ge(cY + s, tY[s], err) && (p < 0 || wait_ge(cX + p, tX[p], err)); break;
+            case kFwdG: ok = wait_ge(cGin + s, tGin[s] + bump, err, A.spin_limit); break;
+            default:
+                ok = wait_ge(cY + s, tY[s] + bump, err, A.spin_limit)
+                    && (p < 0 || wait_ge(cX + p, tX[p], err, A.spin_limit));
+                break;
             }
             ok_sh = ok;
         }
@@ -943,6 +952,18 @@ __global__ void __launch_bounds__(kST) k_solve(SolveArgs A)
             default: atomicAdd(cX + s, 1); break;  // kBwdFront, kBwdX
             }
         }
+    }
+    // A solve that gave up leaves v partly overwritten: the last CTA to
+    // leave fills it with NaN, so that a caller who cannot read the error
+    // flag (a replayed graph) still sees that the result is not valid.
+    if (tid == 0) {
+        __threadfence();
+        ok_sh = atomicAdd(exits, 1) == static_cast<int>(gridDim.x) - 1 && *reinterpret_cast<volatile int*>(err);
+    }
+    __syncthreads();
+    if (ok_sh) {
+        __threadfence();
+        for (int i = tid; i < A.n3; i += kST) A.v[i] = __longlong_as_double(0x7ff8000000000000LL);
     }
 }
 
@@ -1227,20 +1248,30 @@ struct SolveBufs {
     int* cnt;     // completion counters, ticket, error flag (4 ns + 2)
 };
 
+// limits of the persistent solve's device-side waits (efem_options.wait_limit, wait_test)
+struct WaitCfg {
+    int limit, test;
+};
+WaitCfg wait_cfg(const Model& m)
+{
+    return WaitCfg { m.opts.wait_limit > 0 ? m.opts.wait_limit : kSpinLimit, m.opts.wait_test ? 1 : 0 };
+}
+
 // enqueue one H0 application (counter reset unless the caller cleared them,
 // then the persistent solve) on stream st
-void enqueue_solve(const Precond& P, const FrontArgs& a, const SolveBufs& b, double* d_v, cudaStream_t st,
-    bool clear = true, unsigned long long* stamp = nullptr)
+efem_status enqueue_solve(const Precond& P, const FrontArgs& a, const SolveBufs& b, double* d_v, cudaStream_t st,
+    WaitCfg wc, bool clear = true, unsigned long long* stamp = nullptr)
 {
     const int ns = P.S.ns;
-    if (clear) cudaMemsetAsync(b.cnt, 0, sizeof(int) * (4 * static_cast<size_t>(ns) + 2), st);
+    if (clear) EFEM_CUDA(cudaMemsetAsync(b.cnt, 0, sizeof(int) * (4 * static_cast<size_t>(ns) + 2), st));
     const SubArgs B { a, P.d_parent, P.d_prow, P.d_perm, P.d_subs, P.d_chunks, P.d_depth, P.d_xidx, P.sub_max_r,
         P.sub_max_cols, P.sub_max_depth, P.sub_max_m, P.sub_max_c, P.sub_max_mroot, d_v, b.y, b.upd, stamp };
     if (P.n_subs > 0) k_sub_fwd<<<P.n_subs, kST, P.sub_smem_f, st>>>(B);
     SolveArgs A { a, P.d_parent, P.d_prow, P.d_items, P.d_tgt, P.n_items, ns, P.stage_d, P.work_d, d_v, b.y, b.t,
-        b.upd, b.cnt, P.n_subs > 0 ? nullptr : stamp };
+        b.upd, b.cnt, P.n_subs > 0 ? nullptr : stamp, wc.limit, wc.test, 3 * P.S.n };
     if (P.n_items > 0) launch_k(k_solve, P.solve_grid, kST, P.solve_smem, st, A);
     if (P.n_subs > 0) k_sub_bwd<<<P.n_subs, kST, P.sub_smem_b, st>>>(B);
+    return EFEM_OK;
 }
 
 }  // namespace
@@ -1759,8 +1790,12 @@ static efem_status apply_with(Model& m, double* d_v, const SolveBufs& b)
         cudaGraphExec_t ge = nullptr;
         std::lock_guard<std::mutex> lock(capture_mutex());
         EFEM_CUDA(cudaStreamBeginCapture(P.capture, cudaStreamCaptureModeThreadLocal));
-        enqueue_solve(P, args_of(P), b, d_v, P.capture);
+        const efem_status es = enqueue_solve(P, args_of(P), b, d_v, P.capture, wait_cfg(m));
         EFEM_CUDA(cudaStreamEndCapture(P.capture, &g));
+        if (es != EFEM_OK) {
+            cudaGraphDestroy(g);
+            return es;
+        }
         EFEM_CUDA(cudaGraphInstantiate(&ge, g, 0));
         cudaGraphDestroy(g);
         it = P.graphs.emplace(key, ge).first;
@@ -1768,6 +1803,15 @@ static efem_status apply_with(Model& m, double* d_v, const SolveBufs& b)
     EFEM_CUDA(cudaGraphLaunch(it->second, m.stream));
     m.launches += 1;
     return EFEM_OK;
+}
+
+void precond_drop_graphs(Model& m)
+{
+    if (!m.precond) return;
+    if (m.on_device) cudaStreamSynchronize(m.stream);
+    for (auto& kv : m.precond->graphs) cudaGraphExecDestroy(kv.second);
+    m.precond->graphs.clear();
+    m.epoch++;  // the solver's iteration graphs hold the persistent solve's arguments too
 }
 
 efem_status precond_sync_grid(Model& m)
@@ -1802,8 +1846,8 @@ efem_status precond_enqueue(Model& m, double* d_v, cudaStream_t stream, bool cle
     }
     Precond& P = *m.precond;
     if (P.S.n == 0) return EFEM_OK;
-    enqueue_solve(P, args_of(P), SolveBufs { P.d_y, P.d_t, P.d_upd, P.d_cnt }, d_v, stream, clear, stamp);
-    return EFEM_OK;
+    return enqueue_solve(P, args_of(P), SolveBufs { P.d_y, P.d_t, P.d_upd, P.d_cnt }, d_v, stream, wait_cfg(m), clear,
+        stamp);
 }
 
 void precond_counters(const Model& m, int** cnt, int* n)
@@ -1830,7 +1874,7 @@ static efem_status check_solve_flag(const int* d_flag, cudaStream_t st)
     EFEM_CUDA(cudaStreamSynchronize(st));
     if (flag) {
         set_error("the triangular solve of the preconditioner gave up waiting for a front");
-        return EFEM_ERR_CUDA;
+        return EFEM_ERR_TIMEOUT;
     }
     return EFEM_OK;
 }
@@ -1903,6 +1947,14 @@ extern "C" efem_status efem_precond_apply_noalloc(void* model, double* d_v)
         return EFEM_ERR_ARG;
     }
     Model& m = *static_cast<Model*>(model);
+    // two vectors of 3 per free node are the least any model needs: refuse
+    // models that cannot fit before asking for anything else
+    if (6 * static_cast<size_t>(m.n_free) > kNoAllocDoubles) {
+        set_error("model needs at least " + std::to_string(6 * static_cast<size_t>(m.n_free))
+            + " doubles of workspace; the static workspace of efem_precond_apply_noalloc holds "
+            + std::to_string(kNoAllocDoubles));
+        return EFEM_ERR_ARG;
+    }
     if (!m.on_device || !m.precond || !m.precond->factored || !m.precond->ok) {
         set_error("efem_precond_apply_noalloc needs an existing positive-definite factor: call efem_solve or "
                   "efem_precond_apply once first");
@@ -1918,14 +1970,33 @@ extern "C" efem_status efem_precond_apply_noalloc(void* model, double* d_v)
             "efem_precond_apply_noalloc holds " + std::to_string(kNoAllocDoubles));
         return EFEM_ERR_ARG;
     }
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    EFEM_CUDA(cudaStreamIsCapturing(m.stream, &cs));
+    const bool capturing = cs != cudaStreamCaptureStatusNone;
     double* scratch = nullptr;
-    efem_status st = noalloc_scratch(m.device, &scratch);
-    if (st != EFEM_OK) return st;
-    EFEM_CUDA(cudaSetDevice(m.device));
+    if (capturing) {  // only a cached address: no CUDA runtime call that a capture forbids
+        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+        scratch = m.device >= 0 && m.device < 256 ? g_noalloc_addr[m.device] : nullptr;
+        if (!scratch) {
+            set_error("efem_precond_apply_noalloc: the first call on a device must come before any stream "
+                      "capture (it looks up the static workspace's device address)");
+            return EFEM_ERR_ARG;
+        }
+    } else {
+        efem_status st = noalloc_scratch(m.device, &scratch);
+        if (st != EFEM_OK) return st;
+        EFEM_CUDA(cudaSetDevice(m.device));
+    }
     if (S.n == 0) return EFEM_OK;
-    cudaStreamCaptureStatus cs0 = cudaStreamCaptureStatusNone;
-    EFEM_CUDA(cudaStreamIsCapturing(m.stream, &cs0));
-    if (cs0 == cudaStreamCaptureStatusNone) {  // d_v must be memory this GPU addresses (not checked while capturing)
+    // This thread's host-side calls below (pointer check, flag read) must not
+    // invalidate a capture that the caller has open on some other stream.
+    cudaStreamCaptureMode mode = cudaStreamCaptureModeRelaxed;
+    EFEM_CUDA(cudaThreadExchangeStreamCaptureMode(&mode));
+    struct Restore {
+        cudaStreamCaptureMode mode;
+        ~Restore() { cudaThreadExchangeStreamCaptureMode(&mode); }
+    } restore { mode };
+    if (!capturing) {  // d_v must be memory this GPU addresses (not checked while capturing)
         cudaPointerAttributes a {};
         const bool ok = cudaPointerGetAttributes(&a, d_v) == cudaSuccess
             && (a.type == cudaMemoryTypeManaged || (a.type == cudaMemoryTypeDevice && a.device == m.device)
@@ -1938,10 +2009,9 @@ extern "C" efem_status efem_precond_apply_noalloc(void* model, double* d_v)
     }
     int* counters = reinterpret_cast<int*>(scratch + 2 * n3 + S.upd_size);
     const SolveBufs b { scratch, scratch + n3, scratch + 2 * n3, counters };
-    enqueue_solve(P, args_of(P), b, d_v, m.stream);
+    efem_status st = enqueue_solve(P, args_of(P), b, d_v, m.stream, wait_cfg(m));
+    if (st != EFEM_OK) return st;
     EFEM_CUDA(cudaGetLastError());
-    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    EFEM_CUDA(cudaStreamIsCapturing(m.stream, &cs));
-    if (cs != cudaStreamCaptureStatusNone) return EFEM_OK;  // recorded into the caller's graph
+    if (capturing) return EFEM_OK;  // recorded into the caller's graph; a give-up shows as NaN in d_v
     return check_solve_flag(counters + 4LL * S.ns + 1, m.stream);
 }

@@ -130,6 +130,7 @@ struct Model {
 
     // element input kept for rebuilding the integration tables
     std::vector<HostBlock> in_blocks;
+    std::vector<HostLoad> in_loads;   // the constraints as given (batch solves rebuild them in a union model)
     int built_integration = -1;
     std::vector<DevBlock> blocks;
     std::vector<DevFaces> faces;
@@ -292,6 +293,14 @@ long long precond_launch_count(const Model& m);  // kernels per H0 application
 const int* precond_error_flag(const Model& m);   // device flag: a solve gave up waiting (nullptr before set-up)
 efem_status precond_check(Model& m);             // wait for the stream and report that flag
 void free_precond(Model& m);
+void precond_drop_graphs(Model& m);  // forget captured H0 solves (new wait limits); the factor stays
+// ------------------------------------------------------------------ batches (batch.cu)
+// Solve n models as one union model (see batch.cu); EFEM_ERR_UNSUPPORTED when
+// the models cannot share one (different devices or options, gravity, an
+// approximate Jacobian that is not positive definite): the caller then solves
+// them one by one.
+efem_status batch_union_solve(Model** models, int n, double* const* u, efem_solve_info* infos);
+void batch_forget(const Model* m);  // drop cached unions that hold m (m is being destroyed)
 void precond_info(const Model& m, efem_model_info* info);
 // The persistent triangular solve's grid: every CTA that fits on the device
 // (one solve at a time), or, while t_batch > 0 (the batch solve's worker

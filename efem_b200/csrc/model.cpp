@@ -170,6 +170,7 @@ const std::string& get_error() { return g_error; }
 
 Model::~Model()
 {
+    batch_forget(this);
     if (device >= 0) cudaSetDevice(device);
     free_solver(*this);
     free_adjoint(*this);
@@ -232,6 +233,7 @@ efem_status build_model(ModelInput& in, Model& m)
         set_error("model has no nodes");
         return EFEM_ERR_MESH;
     }
+    m.in_loads = in.loads;
     // fixed nodes and DOF numbering
     std::vector<char> fixed(m.n_nodes, 0);
     for (auto& L : in.loads)
@@ -939,7 +941,8 @@ efem_status efem_set_options(void* model, const efem_options* o)
     if (s != EFEM_OK) return s;
     if (!o || o->m <= 0 || o->max_linesearch <= 0 || o->max_iterations < 0 || o->residual_criterion < 0
         || (o->precision != EFEM_FP64 && o->precision != EFEM_MIXED) || (o->integration != 0 && o->integration != 1)
-        || o->trace < 0 || (o->line_search != 0 && o->line_search != 1)) {
+        || o->trace < 0 || (o->line_search != 0 && o->line_search != 1) || o->wait_limit < 0
+        || (o->wait_test != 0 && o->wait_test != 1)) {
         efem::set_error("invalid options (NLSolverParam::check_param rules)");
         return EFEM_ERR_ARG;
     }
@@ -947,6 +950,7 @@ efem_status efem_set_options(void* model, const efem_options* o)
     const bool new_history = o->m != m->opts.m;
     const bool new_mass = m->has_gravity && (o->consistent_inertia != 0) != (m->opts.consistent_inertia != 0);
     const bool new_schedule = o->solve_subtree_levels != m->opts.solve_subtree_levels;
+    const bool new_waits = o->wait_limit != m->opts.wait_limit || o->wait_test != m->opts.wait_test;
     const int dev = m->device;
     m->opts = *o;
     if (dev >= 0) m->device = dev;  // the device is fixed once buffers exist
@@ -965,6 +969,7 @@ efem_status efem_set_options(void* model, const efem_options* o)
     }
     if (new_history) efem::free_solver(*m);
     if (new_schedule && !reintegrate) efem::free_precond(*m);  // the solve schedule is rebuilt at the next factorisation
+    else if (new_waits && !reintegrate) efem::precond_drop_graphs(*m);  // captured solves hold the old wait limits
     return EFEM_OK;
 }
 
@@ -1263,6 +1268,20 @@ efem_status efem_batch_solve(void** models, int n, double* const* u, efem_solve_
         return EFEM_ERR_ARG;
     }
     if (n == 0) return EFEM_OK;
+    // One union model for the whole batch when the members can share one
+    // (batch.cu); otherwise the solves run side by side from a thread pool.
+    {
+        std::vector<Model*> ms(n);
+        bool all = true;
+        for (int i = 0; i < n; i++) {
+            ms[i] = static_cast<Model*>(models[i]);
+            all = all && ms[i] && u[i];
+        }
+        if (all) {
+            const efem_status s = efem::batch_union_solve(ms.data(), n, u, infos);
+            if (s != EFEM_ERR_UNSUPPORTED) return s;
+        }
+    }
     int nt = max_threads > 0 ? max_threads : static_cast<int>(std::thread::hardware_concurrency());
     nt = std::max(1, std::min(nt, n));
     // largest models first, so that no large solve starts last and runs alone

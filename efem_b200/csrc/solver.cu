@@ -79,6 +79,10 @@ struct Scalars {
     double* trace;
     int trace_cap, tr_i, tr_evals;
     unsigned long long t_start;
+    // mixed precision's FP32 phase: it ends when the best ||r||_inf has not
+    // halved for stall_iters iterations (0: no such test)
+    double best_rinf;
+    int best_k, stall_iters;
 };
 
 // trace record: seconds since the solve started (GPU global timer), ||r||_2,
@@ -89,7 +93,7 @@ constexpr int kTraceCols = 5;
 enum { kRdDg = 0, kRdRinf, kRdXinf, kRdX2, kRdDg0, kRdPerr, kRdStatus, kRdK, kRdNRes, kRdNExtra, kRdNBody, kRdTRes,
     kRdTPc, kRdTrN, kRdCount };
 // device loop status
-enum { kRunning = 0, kConverged = 1, kMaxIters = 2, kNonFinite = 3, kPrecondFail = 4, kCapReached = 5 };
+enum { kRunning = 0, kConverged = 1, kMaxIters = 2, kNonFinite = 3, kPrecondFail = 4, kCapReached = 5, kStalled = 6 };
 
 __device__ __forceinline__ unsigned long long gtimer()
 {
@@ -718,7 +722,13 @@ __global__ void k_iter_decide(Scalars* S, cudaGraphConditionalHandle h, double* 
         st = kConverged;
     else if (S->max_iter != 0 && S->k >= S->max_iter)
         st = kMaxIters;
+    else if (S->stall_iters > 0 && !(rinf < 0.5 * S->best_rinf) && S->k - S->best_k >= S->stall_iters)
+        st = kStalled;
     else {
+        if (rinf < 0.5 * S->best_rinf) {
+            S->best_rinf = rinf;
+            S->best_k = S->k;
+        }
         S->k++;
         if (++S->launch_iters >= S->cap) st = kCapReached;
     }
@@ -734,8 +744,12 @@ __global__ void k_iter_decide(Scalars* S, cudaGraphConditionalHandle h, double* 
 __global__ void k_loop_start(Scalars* S) { S->launch_iters = 0; }
 
 // options of the device-driven loop, and the iteration number it starts at
-__global__ void k_loop_params(Scalars* S, double eps, int max_iter, int max_ls, int cap, int k)
+__global__ void k_loop_params(Scalars* S, double eps, int max_iter, int max_ls, int cap, int k, int stall_iters,
+    double best_rinf)
 {
+    S->stall_iters = stall_iters;
+    S->best_rinf = best_rinf;
+    S->best_k = k;
     S->eps = eps;
     S->max_iter = max_iter;
     S->max_ls = max_ls;
@@ -746,8 +760,9 @@ __global__ void k_loop_params(Scalars* S, double eps, int max_iter, int max_ls, 
     S->t_pc = 0;
 }
 
-// counters, timers and trace of one solve (the initial residual is trace record 0, step 0)
-__global__ void k_solve_init(Scalars* S, double* trace, int trace_cap)
+// counters, timers and trace of one solve (the initial residual is trace record 0, step 0);
+// keep_trace: a second phase of the same solve, whose records follow the first phase's
+__global__ void k_solve_init(Scalars* S, double* trace, int trace_cap, int keep_trace)
 {
     S->n_res = 0;
     S->t_res = 0;
@@ -756,10 +771,12 @@ __global__ void k_solve_init(Scalars* S, double* trace, int trace_cap)
     S->n_body = 0;
     S->trace = trace;
     S->trace_cap = trace ? trace_cap : 0;
-    S->tr_i = 0;
-    S->tr_evals = 0;
     S->step = 0.0;
-    S->t_start = gtimer();
+    if (!keep_trace) {
+        S->tr_i = 0;
+        S->tr_evals = 0;
+        S->t_start = gtimer();
+    }
 }
 
 // vector kernels are latency-bound at these sizes: about one element per thread
@@ -1084,8 +1101,16 @@ double elapsed_ms(cudaEvent_t a, cudaEvent_t b)
 
 }  // namespace
 
-efem_status run_solve(Model& m, double* x, efem_solve_info* info)
+// One L-BFGS solve from x (LBFGSSolver::solve, LBFGS.h:96-174) with the
+// model's element precision.  refactor: factor the approximate Jacobian
+// (once per solve, LBFGS.h:122-124; a second phase reuses the factor, which
+// does not depend on u).  stall_iters > 0: also end, with *stalled set, when
+// the best ||r||_inf has not halved for that many iterations.  keep_trace:
+// append to the trace of an earlier phase.
+efem_status run_solve_phase(Model& m, double* x, efem_solve_info* info, bool refactor, int stall_iters,
+    bool keep_trace, bool* stalled)
 {
+    *stalled = false;
     efem_status s = alloc_ws(m);
     if (s != EFEM_OK) return s;
     SolverWS& w = *m.ws;
@@ -1112,9 +1137,9 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
             w.trace_cap = m.opts.trace;
         }
     }
-    hr[kRdTrN] = 0.0;
+    if (!keep_trace) hr[kRdTrN] = 0.0;
     EFEM_CUDA(cudaEventRecord(w.ev[0], st));
-    k_solve_init<<<1, 1, 0, st>>>(w.sc, w.trace, w.trace_cap);
+    k_solve_init<<<1, 1, 0, st>>>(w.sc, w.trace, w.trace_cap, keep_trace ? 1 : 0);
     m.launches++;
 
     // host-driven line-search trial: x = xp + step d (step 0: x as is),
@@ -1182,10 +1207,10 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
     if (m.opts.nl_solver == 0) {
         int okf = 0;
         double msf = 0;
-        if ((s = precond_setup(m, true, &okf, &msf)) != EFEM_OK) return s;
+        if ((s = precond_setup(m, refactor, &okf, &msf)) != EFEM_OK) return s;
         if ((s = precond_sync_grid(m)) != EFEM_OK) return s;
         ok = okf != 0;
-        info->n_jacobian_evals = 1;
+        info->n_jacobian_evals = refactor ? 1 : 0;
         info->ms_factor = msf;
         if (!ok) info->flags |= EFEM_SOLVE_PRECOND_FALLBACK;
     }
@@ -1240,6 +1265,8 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
         k++;
         if (host_loop) {  // iterations 2, 3, ... one graph launch each, decisions on the host
             const long long per_step = 4 + (ok ? precond_launch_count(m) : 0) + (per_res - 1) + 1;
+            double best = rinf;
+            int best_k = k;
             for (;;) {
                 EFEM_CUDA(cudaGraphLaunch(gr.step, st));
                 EFEM_CUDA(cudaStreamSynchronize(st));
@@ -1247,7 +1274,7 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
                 if (ok) info->n_precond_applies++;
                 if (hr[kRdPerr] != 0.0) {
                     set_error("the triangular solve of the preconditioner gave up waiting for a front");
-                    return EFEM_ERR_CUDA;
+                    return EFEM_ERR_TIMEOUT;
                 }
                 if ((s = line_search()) != EFEM_OK) return s;
                 rinf = hr[kRdRinf];
@@ -1261,6 +1288,13 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
                     info->flags |= EFEM_SOLVE_MAX_ITERS;
                     break;
                 }
+                if (rinf < 0.5 * best) {
+                    best = rinf;
+                    best_k = k;
+                } else if (stall_iters > 0 && k - best_k >= stall_iters) {
+                    *stalled = true;
+                    break;
+                }
                 k++;
             }
             if (ok) ms_pc += hr[kRdTPc] * 1e-6;
@@ -1268,7 +1302,7 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
         }
         // iterations 2, 3, ... on the device, kIterCap per graph launch
         k_loop_params<<<1, 1, 0, st>>>(w.sc, eps, m.opts.max_iterations, std::max(1, m.opts.max_linesearch),
-            kIterCap, k);
+            kIterCap, k, stall_iters, rinf);
         m.launches++;
         // passes, H0, trial (which starts r), residual, reductions, iteration decision
         // passes (pass 4 starts the first trial), H0, residual, reductions, iteration decision
@@ -1295,11 +1329,12 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
         }
         if (status == kPrecondFail) {
             set_error("the triangular solve of the preconditioner gave up waiting for a front");
-            return EFEM_ERR_CUDA;
+            return EFEM_ERR_TIMEOUT;
         }
         if (status == kNonFinite) goto nan_exit;
         if (status == kConverged) converged = true;
         if (status == kMaxIters) info->flags |= EFEM_SOLVE_MAX_ITERS;
+        if (status == kStalled) *stalled = true;
     }
 done:
     EFEM_CUDA(cudaEventRecord(w.ev[1], st));
@@ -1328,6 +1363,48 @@ nan_exit:
     w.trace_n = static_cast<int>(hr[kRdTrN]);
     set_error("L-BFGS produced a non-finite residual or solution");
     return EFEM_ERR_NAN;
+}
+
+// iterations without a halving of the best ||r||_inf after which the FP32
+// phase of a mixed-precision solve hands over to FP64 element kernels
+constexpr int kStallIters = 24;
+
+// The solve behind efem_solve.  FP64: one phase.  Mixed precision: FP32
+// element kernels until the residual passes the test or stops improving (the
+// FP32 rounding floor of the element forces lies above the tolerance), then
+// FP64 element kernels from that point, with a fresh L-BFGS history and the
+// same factor, so that the residual read by the convergence test that ends
+// the solve is always formed in FP64.  When the FP32 phase has converged the
+// FP64 phase is one residual evaluation (its initial test).
+efem_status run_solve(Model& m, double* x, efem_solve_info* info)
+{
+    bool stalled = false;
+    if (m.opts.precision != EFEM_MIXED) return run_solve_phase(m, x, info, true, 0, false, &stalled);
+    efem_solve_info a {};
+    efem_status s = run_solve_phase(m, x, &a, true, kStallIters, false, &stalled);
+    if (s != EFEM_OK || (a.flags & EFEM_SOLVE_MAX_ITERS)) {
+        *info = a;
+        return s;
+    }
+    const efem_options keep = m.opts;
+    m.opts.precision = EFEM_FP64;
+    if (keep.max_iterations != 0) m.opts.max_iterations = std::max(1, keep.max_iterations - a.niter);
+    efem_solve_info b {};
+    s = run_solve_phase(m, x, &b, false, 0, true, &stalled);
+    m.opts = keep;
+    const bool early = b.n_precond_applies == 0 && b.n_residual_evals <= 1;  // passed its initial test
+    *info = b;
+    info->niter = a.niter + (early ? 0 : b.niter);
+    info->n_residual_evals = a.n_residual_evals + b.n_residual_evals;
+    info->n_jacobian_evals = a.n_jacobian_evals;
+    info->flags = b.flags | (a.flags & (EFEM_SOLVE_PRECOND_FALLBACK | EFEM_SOLVE_PDL)) | (early ? 0 : EFEM_SOLVE_REFINED);
+    info->ms_total = a.ms_total + b.ms_total;
+    info->ms_factor = a.ms_factor;
+    info->ms_residual = a.ms_residual + b.ms_residual;
+    info->ms_precond = a.ms_precond + b.ms_precond;
+    info->n_kernel_launches = a.n_kernel_launches + b.n_kernel_launches;
+    info->n_precond_applies = a.n_precond_applies + b.n_precond_applies;
+    return s;
 }
 
 efem_status solve_trace(Model& m, double* out, int capacity, int* n_records)

@@ -87,6 +87,12 @@ typedef struct {
     double value[3];
 } efem_load_desc;
 
+/* EFEM_MIXED: FP32 element kernels (FP32 arithmetic, FP64 accumulation of
+ * the nodal forces) with the factor, its solves, the L-BFGS vectors and the
+ * norms in FP64.  The FP32 phase runs until the residual passes the test or
+ * stops improving; FP64 element kernels then finish the solve from there
+ * (EFEM_SOLVE_REFINED), so the test that ends every solve reads an FP64
+ * residual. */
 typedef enum { EFEM_FP64 = 0, EFEM_MIXED = 1 } efem_precision;
 
 typedef struct {
@@ -122,6 +128,13 @@ typedef struct {
                                  Pi(u) = E(u) - f_ext.u (FP64 strain-energy sum), halving the step;
                                  needs conservative loads (no pressure faces), runs the iterations
                                  from the host */
+    int wait_limit;           /* polls of one device-side wait of the preconditioner's triangular solve
+                                 (a front waiting for the fronts it depends on) before the solve gives
+                                 up with EFEM_ERR_TIMEOUT and leaves NaN in its output; 0 = default
+                                 (2^22 polls, about half a second) */
+    int wait_test;            /* test aid, 0 = off: 1 makes one wait of every H0 application wait for
+                                 a count that no work item produces, so it runs out after wait_limit
+                                 polls -- the timeout path without a GPU fault */
 } efem_options;
 
 enum {
@@ -129,8 +142,13 @@ enum {
     EFEM_SOLVE_PRECOND_FALLBACK = 2,/* factorisation failed; H0 = I/theta used (LBFGS.h:76-79) */
     EFEM_SOLVE_DX_CONVERGED = 4,   /* ||u||_inf < dx_criterion (the reference's return flag) */
     EFEM_SOLVE_MAX_ITERS = 8,
-    EFEM_SOLVE_PDL = 16            /* the captured iterations chain their kernels with programmatic
+    EFEM_SOLVE_PDL = 16,           /* the captured iterations chain their kernels with programmatic
                                       dependent launch (a capture that refuses it falls back to plain launches) */
+    EFEM_SOLVE_REFINED = 32,       /* mixed precision: the FP32 element kernels stopped short of the
+                                      tolerance (their rounding floor) and FP64 element kernels finished
+                                      the solve from that point */
+    EFEM_SOLVE_BATCHED = 64        /* efem_batch_solve: solved inside one union model with the rest of the
+                                      batch (ms_total, ms_factor and n_kernel_launches are the whole batch's) */
 };
 
 typedef struct {
@@ -234,12 +252,17 @@ efem_status efem_precond_apply(void* model, double* v);
  * device array that every GPU loading this library keeps until exit.
  * Requirements: the model's factor exists (efem_solve or efem_precond_apply
  * ran once) and 6 * free nodes + the factor's update-vector length
- * + 2 * fronts + 1 <= 2^21 doubles (EFEM_ERR_ARG otherwise); d_v is a device
- * pointer, overwritten in place.  Outside a capture the call waits for the
- * result on the model's stream and reports a solve that gave up waiting
- * (EFEM_ERR_CUDA); inside a capture it only records the work.  The first
- * call on a device looks up the array's device address (do it before any
- * stream capture).  All calls share the array: calls that overlap on the GPU
+ * + 2 * fronts + 1 <= 2^21 doubles (EFEM_ERR_ARG otherwise, with the sizes in
+ * efem_last_error; a model with more than 349 525 free nodes is refused
+ * before anything else is checked); d_v is a device pointer, overwritten in
+ * place.  Outside a capture the call waits for the result on the model's
+ * stream and reports a solve that gave up waiting (EFEM_ERR_TIMEOUT).  Inside
+ * a capture it only records the work, and the capture must be on the model's
+ * stream (efem_set_stream with the capturing stream): a replay whose solve
+ * gives up cannot report it, so it leaves NaN in every entry of d_v.  The
+ * first call on a device looks up the array's device address and must come
+ * before any stream capture (a first call inside a capture is refused with
+ * EFEM_ERR_ARG).  All calls share the array: calls that overlap on the GPU
  * race and must be serialised by the caller. */
 efem_status efem_precond_apply_noalloc(void* model, double* d_v);
 
@@ -299,16 +322,24 @@ efem_status efem_write_vtk(void* model, const double* u, const char* path);
 efem_status efem_strain_energy(void* model, const double* u, double* energy);
 
 /* Solve n independent models (load cases, material samples, meshes of any
- * size) concurrently: each model's solve runs on its own CUDA stream from a
- * pool of max_threads host threads (<= 0: one per hardware thread), so the
- * models' device-driven iteration graphs overlap on the GPU.  u[i] is model
- * i's u_inout (host or device per that model's device_ptrs); infos may be
- * NULL or hold n entries.  Inside a batch the CTAs that fit on the device are
- * divided among the solves in flight for each model's persistent triangular
- * solve (the H0 application), instead of every solve asking for all of them;
- * a model later solved alone goes back to the full grid.  Returns the first failing model's
- * status, with its index in the error message.  The reference solves one problem per
- * process (Simulator::start, src/simulation/Simulator.cpp:20-41). */
+ * size) at once.  The reference solves one problem per process
+ * (Simulator::start, src/simulation/Simulator.cpp:20-41).
+ * When the models share their element precision, integration rule, history
+ * length, line-search limit and device, use the approximate-Jacobian
+ * preconditioner, the default line search and no gravity, they are solved as
+ * one union model: one element-kernel launch per element type evaluates
+ * every model's residual, one factorisation and one persistent triangular
+ * solve apply every model's H0, and segmented L-BFGS kernels keep each
+ * model's history, line search and convergence test apart, all inside one
+ * CUDA graph of the iteration loop (EFEM_SOLVE_BATCHED in each info; each
+ * model keeps its own residual_criterion and max_iterations; the union is
+ * cached for further calls with the same models and options).  Otherwise
+ * each model's solve runs on its own CUDA stream from a pool of max_threads
+ * host threads (<= 0: one per hardware thread), and the CTAs of the
+ * persistent triangular solve are divided among the solves in flight.  u[i]
+ * is model i's u_inout (host or device per that model's device_ptrs); infos
+ * may be NULL or hold n entries.  Returns the first failing model's status,
+ * with its index in the error message. */
 efem_status efem_batch_solve(void** models, int n, double* const* u, efem_solve_info* infos, int max_threads);
 
 /* Run the model's device work on the caller's CUDA stream (a cudaStream_t);

@@ -168,3 +168,22 @@ def test_strain_energy_gradient_is_internal_force(etype, mat):
     fint = m.residual(u) - m.residual(np.zeros(m.n_dof))
     assert abs(fd - float(fint @ v)) <= 1e-5 * abs(float(fint @ v))
     assert m.strain_energy(u) > 0
+
+
+@pytest.mark.parametrize("etype,mat,load", [("C3D10", "yeoh", "pressure"), ("C3D8", "mr", "dpressure")])
+def test_adjoint_without_stored_tangents_matches(etype, mat, load, monkeypatch):
+    """When the stored tangents cannot be allocated (forced here with
+    EFEM_TEST_STORED_OOM=1, which makes their allocation report out of
+    memory) the adjoint falls back to dual-number products: same gradient,
+    a successful call and no stale allocation error text."""
+    case = mg.small_case(etype, mat, load)
+    m, u = solved(case)
+    g = np.zeros(m.n_dof)
+    g[-1] = 1.0
+    want, _, info = m.adjoint(u, g)
+    m2, _ = solved(case)
+    monkeypatch.setenv("EFEM_TEST_STORED_OOM", "1")
+    got, _, info2 = m2.adjoint(u, g)
+    assert info2["flags"] & api.SOLVE_CONVERGED, info2
+    assert np.linalg.norm(got - want) <= 1e-8 * np.linalg.norm(want)
+    assert "cudaMalloc" not in api.last_error(), api.last_error()

@@ -2,7 +2,8 @@
 
 Each model of the batch must give the same solution as its own single solve,
 and the mixed-precision batch must stay within 1e-4 relative L2 of the FP64
-solutions (the tolerance stated for the mixed path).
+solutions (the tolerance stated for the mixed path) wherever the tolerance
+of the solve itself allows that accuracy.
 """
 import numpy as np
 import pytest
@@ -40,26 +41,87 @@ def test_batch_matches_single_solves(cases):
     ms = models(cases, criterion=1e-10)
     us, infos = api.batch_solve(ms, max_threads=4)
     for u, ref, info in zip(us, single, infos):
+        assert info["flags"] & api.SOLVE_BATCHED  # one union model, one iteration graph
         assert info["flags"] & api.SOLVE_CONVERGED and info["r_inf"] <= 1e-10 * max(1.0, np.abs(u).max())
         assert np.linalg.norm(u - ref) <= 1e-6 * np.linalg.norm(ref)
 
 
+def test_batch_keeps_each_models_tolerance_and_limits(cases):
+    """Members of one union with different residual criteria and
+    iteration limits: each stops by its own test, as its single solve does."""
+    ms = models(cases[:3], criterion=1e-10)
+    ms[1].set_options(residual_criterion=1e-6)
+    ms[2].set_options(max_iterations=3)
+    us, infos = api.batch_solve(ms)
+    assert all(i["flags"] & api.SOLVE_BATCHED for i in infos)
+    assert infos[0]["r_inf"] <= 1e-10 * max(1.0, np.abs(us[0]).max())
+    assert infos[1]["flags"] & api.SOLVE_CONVERGED and infos[1]["r_inf"] <= 1e-6 * max(1.0, np.abs(us[1]).max())
+    assert infos[2]["flags"] & api.SOLVE_MAX_ITERS and infos[2]["niter"] == 3
+    single = models(cases[2:3], criterion=1e-10)[0]
+    single.set_options(max_iterations=3)
+    u2, i2 = single.solve()
+    assert i2["niter"] == 3
+    assert np.linalg.norm(us[2] - u2) <= 1e-8 * np.linalg.norm(u2)
+
+
+def test_batch_with_gravity_runs_model_by_model(cases):
+    """A member with a gravity load cannot share a union (the acceleration
+    is global to a model): the batch falls back to concurrent single solves
+    and still matches them."""
+    import copy
+    c = copy.deepcopy(cases[0])
+    for mt in c.materials:
+        mt["density"] = 1000.0
+    c.analysis["gravity"] = "-z"
+    ms = models([c, cases[1]], criterion=1e-10)
+    us, infos = api.batch_solve(ms)
+    assert not any(i["flags"] & api.SOLVE_BATCHED for i in infos)
+    for m, u in zip(models([c, cases[1]], criterion=1e-10), us):
+        ref, _ = m.solve()
+        assert np.linalg.norm(u - ref) <= 1e-6 * np.linalg.norm(ref)
+
+
 def test_batch_mixed_solutions_satisfy_the_fp64_problem(cases):
-    """Mixed-precision solves at the reference's residual 1e-6 are solutions
-    of the FP64 problem at that tolerance: the FP64 residual at the mixed
-    solution passes the same test (with 20 % margin for the FP32 evaluation
-    error, a floor of about 1e-7 N on these beams).  Their distance from the
-    FP64 solution converged to 1e-10 is bounded by the tolerance, as for the
-    FP64 path itself (on these slender beams an absolute residual of 1e-6 N
-    allows a few 1e-4 of relative displacement in either precision)."""
+    """Mixed-precision solves at the reference's residual 1e-6 end with the
+    FP64 test (FP64 element kernels finish every mixed solve), so the FP64
+    residual at the mixed solution passes it.  On these slender soft beams an
+    absolute residual of 1e-6 N still allows about 1e-3 of relative
+    displacement in either precision, so at this tolerance the mixed solution
+    is held to the accuracy of the FP64 solve at the same tolerance."""
     uref, _ = api.batch_solve(models(cases, criterion=1e-10))
+    u64, _ = api.batch_solve(models(cases))
     ms32 = models(cases, api.MIXED)
     u32, infos = api.batch_solve(ms32)
-    for m, a, ref, info in zip(models(cases), u32, uref, infos):
+    for m, a, b, ref, info in zip(models(cases), u32, u64, uref, infos):
         assert info["flags"] & api.SOLVE_CONVERGED
         r64 = np.abs(m.residual(a)).max()
-        assert r64 <= 1.2e-6 * max(1.0, np.abs(a).max()), r64
-        assert np.linalg.norm(a - ref) <= 1e-3 * np.linalg.norm(ref)
+        assert r64 <= 1e-6 * max(1.0, np.abs(a).max()), r64
+        own = np.linalg.norm(b - ref) / np.linalg.norm(ref)
+        assert np.linalg.norm(a - ref) <= max(1e-4, 3.0 * own) * np.linalg.norm(ref)
+
+
+def test_batch_mixed_within_1e4_of_fp64(cases):
+    """The mixed path's own error (north_star: <= 1e-4 relative L2 against
+    FP64): at a tolerance tight enough that the solves themselves are
+    accurate (1e-9 N), the mixed solutions are within 1e-4 of the FP64
+    solutions converged to 1e-10."""
+    uref, _ = api.batch_solve(models(cases, criterion=1e-10))
+    u32, infos = api.batch_solve(models(cases, api.MIXED, criterion=1e-9))
+    for a, ref, info in zip(u32, uref, infos):
+        assert info["flags"] & api.SOLVE_CONVERGED, info
+        assert np.linalg.norm(a - ref) <= 1e-4 * np.linalg.norm(ref), np.linalg.norm(a - ref) / np.linalg.norm(ref)
+
+
+def test_single_mixed_solve_ends_on_the_fp64_test(cases):
+    """A single mixed solve at 1e-9 N (below the FP32 floor of these beams):
+    the FP32 phase stalls, FP64 element kernels finish (SOLVE_REFINED), and
+    the result is within 1e-4 of the FP64 solution."""
+    ref, _ = models(cases[:1], criterion=1e-10)[0].solve()
+    m = models(cases[:1], api.MIXED, criterion=1e-9)[0]
+    u, info = m.solve()
+    assert info["flags"] & api.SOLVE_CONVERGED and info["r_inf"] <= 1e-9 * max(1.0, np.abs(u).max()), info
+    assert info["flags"] & api.SOLVE_REFINED, info
+    assert np.linalg.norm(u - ref) <= 1e-4 * np.linalg.norm(ref)
 
 
 def test_batch_device_pointers_and_repeat(cases):
