@@ -22,7 +22,10 @@
 //    runs that member's small recursion, so every member follows exactly the
 //    arithmetic of a single solve.
 //  * One CUDA graph holds the iteration loop: a while node over iterations
-//    whose body holds a while node over line-search trials.  A member that
+//    whose body holds a while node over line-search trials; each condition
+//    is set by a one-CTA kernel that reads every member's state, and both
+//    loops are bounded there (kCap iterations per launch, max_line_search
+//    trials per iteration) whatever that state holds.  A member that
 //    converged (or stopped) is frozen: its x no longer moves and its
 //    counters stop; the loop ends when no member is running.  The host checks
 //    the state every kCap iterations.
@@ -70,8 +73,7 @@ struct Seg {
 };
 
 struct Glob {
-    unsigned int segs_done;  // members done with the current reduction
-    int any;                 // OR over members of "wants another trial"
+    int ls_round;            // line-search trials of the current iteration
     int launch_iters, cap;
     int n_running;
     int pc_fail;
@@ -183,8 +185,7 @@ __global__ void kb_init(Seg* S, const int* c0, const double* eps, const int* max
 
 __global__ void kb_glob_init(Glob* G, int cap)
 {
-    G->segs_done = 0u;
-    G->any = 0;
+    G->ls_round = 0;
     G->launch_iters = 0;
     G->cap = cap;
     G->n_running = 0;
@@ -193,7 +194,11 @@ __global__ void kb_glob_init(Glob* G, int cap)
     G->trials = 0;
 }
 
-__global__ void kb_loop_start(Glob* G) { G->launch_iters = 0; }
+__global__ void kb_loop_start(Glob* G)
+{
+    G->launch_iters = 0;
+    G->ls_round = 0;
+}
 
 // the initial residual's norms and the early exit (LBFGS.h:110-120) of every running member
 __global__ void __launch_bounds__(kT) kb_initial(const double* __restrict__ r, const double* __restrict__ x,
@@ -385,11 +390,9 @@ __global__ void __launch_bounds__(kT) kb_pass4(double* __restrict__ d, const dou
 // After a trial's residual: r.d, ||r||_inf, ||x||_inf, ||x||^2 of every
 // member in its line search, which applies the reference's rule (accept when
 // |r.d| <= |r0.d|, else step x1.5 if (r.d)(r0.d) > 0, x0.5 otherwise, at
-// most max_line_search trials, LineSearchFEA.h:43-67).  The last member to
-// finish sets the trial loop's condition: any member wants another trial.
+// most max_line_search trials, LineSearchFEA.h:43-67).
 __global__ void __launch_bounds__(kT) kb_ls_reduce(const double* __restrict__ r, const double* __restrict__ d,
-    const double* __restrict__ x, const Chunk* __restrict__ ch, Seg* S, int nseg, Glob* G, double* partials,
-    cudaGraphConditionalHandle h)
+    const double* __restrict__ x, const Chunk* __restrict__ ch, Seg* S, double* partials)
 {
     const Chunk c = ch[blockIdx.x];
     Seg* sg = S + c.seg;
@@ -413,17 +416,34 @@ __global__ void __launch_bounds__(kT) kb_ls_reduce(const double* __restrict__ r,
         sg->n_res++;
         const int t = ++sg->ls_t;
         const bool again = !(fabs(v[0]) <= fabs(sg->dg0)) && t < sg->max_ls;
-        if (again) {
-            sg->step *= v[0] * sg->dg0 > 0 ? 1.5 : 0.5;
-            atomicOr(&G->any, 1);
-        }
+        if (again) sg->step *= v[0] * sg->dg0 > 0 ? 1.5 : 0.5;
         sg->trial = again ? 1 : 0;
     }
-    __threadfence();
-    if (atomicAdd(&G->segs_done, 1u) == static_cast<unsigned>(nseg - 1)) {
-        __threadfence();
-        const int any = atomicExch(&G->any, 0);
-        G->segs_done = 0u;
+}
+
+// The trial loop's condition: some member wants another trial.  The loop
+// is also bounded here, whatever the members' state: after max_ls trials of
+// one iteration every line search ends.
+__global__ void __launch_bounds__(1024) kb_ls_decide(Seg* S, int nseg, int max_ls, Glob* G,
+    cudaGraphConditionalHandle h)
+{
+    __shared__ int any;
+    if (threadIdx.x == 0) any = 0;
+    __syncthreads();
+    const bool stop = G->ls_round + 1 >= max_ls;
+    int mine = 0;
+    for (int i = threadIdx.x; i < nseg; i += blockDim.x) {
+        Seg& s = S[i];
+        if (s.state != kRun || !s.trial) continue;
+        if (stop)
+            s.trial = 0;
+        else
+            mine = 1;
+    }
+    if (mine) atomicOr(&any, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        G->ls_round++;
         if (any) G->trials++;
         cudaGraphSetConditional(h, any ? 1u : 0u);
     }
@@ -486,6 +506,7 @@ __global__ void __launch_bounds__(1024) kb_decide(Seg* S, int nseg, Glob* G, con
     if (threadIdx.x == 0) {
         G->n_running = running;
         G->body_iters++;
+        G->ls_round = 0;
         if (pc_fail) G->pc_fail = 1;
         const bool more = running > 0 && ++G->launch_iters < G->cap;
         cudaGraphSetConditional(h, more ? 1u : 0u);
@@ -728,7 +749,8 @@ efem_status capture_union_loop(Union& U, cudaGraphExec_t* out)
         kb_pass4<<<nb, kT, 0, s1>>>(U.d, U.q, U.Sh, U.r, U.x, U.xp, U.rp, M.d_fext, U.n, U.d_chunks, U.d_seg,
             U.partials);
         if ((s = launch_residual_on(M, U.x, U.r, s1, nullptr, false)) != EFEM_OK) break;
-        kb_ls_reduce<<<nb, kT, 0, s1>>>(U.r, U.d, U.x, U.d_chunks, U.d_seg, U.nseg, U.d_glob, U.partials, h_ls);
+        kb_ls_reduce<<<nb, kT, 0, s1>>>(U.r, U.d, U.x, U.d_chunks, U.d_seg, U.partials);
+        kb_ls_decide<<<1, 1024, 0, s1>>>(U.d_seg, U.nseg, std::max(1, M.opts.max_linesearch), U.d_glob, h_ls);
         if ((s = add_while_node(s1, h_ls, &ls_body)) != EFEM_OK) break;
         if (cudaStreamBeginCaptureToGraph(s2, ls_body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
             s = EFEM_ERR_CUDA;
@@ -736,7 +758,8 @@ efem_status capture_union_loop(Union& U, cudaGraphExec_t* out)
         }
         kb_trial<<<nb, kT, 0, s2>>>(U.x, U.xp, U.d, U.r, M.d_fext, U.d_chunks, U.d_seg);
         s = launch_residual_on(M, U.x, U.r, s2, nullptr, false);
-        kb_ls_reduce<<<nb, kT, 0, s2>>>(U.r, U.d, U.x, U.d_chunks, U.d_seg, U.nseg, U.d_glob, U.partials, h_ls);
+        kb_ls_reduce<<<nb, kT, 0, s2>>>(U.r, U.d, U.x, U.d_chunks, U.d_seg, U.partials);
+        kb_ls_decide<<<1, 1024, 0, s2>>>(U.d_seg, U.nseg, std::max(1, M.opts.max_linesearch), U.d_glob, h_ls);
         cudaGraph_t tmp = nullptr;
         if (cudaStreamEndCapture(s2, &tmp) != cudaSuccess && s == EFEM_OK) s = EFEM_ERR_CUDA;
         if (s != EFEM_OK) break;
@@ -804,8 +827,8 @@ efem_status run_union_phase(Union& U, int stall, const std::vector<int>& keep, l
     Glob g {};
     long long body0 = 0, trials0 = 0;
     // per loop body: passes 1-4, H0, residual, reduction, decision; per extra trial: trial, residual, reduction
-    const long long per_body = 6 + precond_launch_count(M) + (U.per_res - 1) + 1;
-    const long long per_trial = 2 + (U.per_res - 1);
+    const long long per_body = 7 + precond_launch_count(M) + (U.per_res - 1) + 1;
+    const long long per_trial = 3 + (U.per_res - 1);
     for (;;) {
         EFEM_CUDA(cudaGraphLaunch(U.loop[slot], st));
         EFEM_CUDA(cudaMemcpyAsync(&g, U.d_glob, sizeof(Glob), cudaMemcpyDeviceToHost, st));
@@ -826,12 +849,16 @@ efem_status run_union_phase(Union& U, int stall, const std::vector<int>& keep, l
 
 void batch_forget(const Model* m)
 {
-    std::lock_guard<std::mutex> lock(g_union_mutex);
-    g_unions.erase(std::remove_if(g_unions.begin(), g_unions.end(),
-                       [&](const std::unique_ptr<Union>& u) {
-                           return std::find(u->members.begin(), u->members.end(), m) != u->members.end();
-                       }),
-        g_unions.end());
+    // Unions that hold m are moved out under the lock and destroyed after it
+    // is released: a union's own model calls this function from its
+    // destructor, and the lock is not recursive.
+    std::vector<std::unique_ptr<Union>> dead;
+    {
+        std::lock_guard<std::mutex> lock(g_union_mutex);
+        for (auto& u : g_unions)
+            if (std::find(u->members.begin(), u->members.end(), m) != u->members.end()) dead.push_back(std::move(u));
+        g_unions.erase(std::remove(g_unions.begin(), g_unions.end(), nullptr), g_unions.end());
+    }
 }
 
 efem_status batch_union_solve(Model** ms, int n, double* const* u, efem_solve_info* infos)
@@ -845,6 +872,7 @@ efem_status batch_union_solve(Model** ms, int n, double* const* u, efem_solve_in
         efem_status s = ensure_device(*ms[i]);
         if (s != EFEM_OK) return s;
     }
+    std::unique_ptr<Union> evicted;  // declared before the lock: destroyed after it is released
     std::lock_guard<std::mutex> lock(g_union_mutex);
     Union* U = nullptr;
     for (auto& cand : g_unions) {
@@ -868,7 +896,10 @@ efem_status batch_union_solve(Model** ms, int n, double* const* u, efem_solve_in
         efem_status s = build_union(*nu);
         if (s == EFEM_OK) s = setup_union(*nu);
         if (s != EFEM_OK) return s;
-        if (g_unions.size() >= 4) g_unions.erase(g_unions.begin());
+        if (g_unions.size() >= 4) {  // the oldest union goes; its destruction must not hold the lock
+            evicted = std::move(g_unions.front());
+            g_unions.erase(g_unions.begin());
+        }
         g_unions.push_back(std::move(nu));
         U = g_unions.back().get();
     }
