@@ -81,6 +81,10 @@ struct Glob {
     long long trials;        // extra line-search trials run
 };
 
+// max that keeps a NaN (fmax drops it): a non-finite residual or solution
+// must show in its infinity norm (Integrator.cpp:28-34 tests for it)
+__device__ __forceinline__ double nan_max(double a, double b) { return (b > a || b != b) ? b : a; }
+
 __device__ __forceinline__ double warp_sum(double v)
 {
 #pragma unroll
@@ -90,7 +94,7 @@ __device__ __forceinline__ double warp_sum(double v)
 __device__ __forceinline__ double warp_max(double v)
 {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    for (int o = 16; o > 0; o >>= 1) v = nan_max(v, __shfl_xor_sync(0xffffffffu, v, o));
     return v;
 }
 
@@ -109,7 +113,7 @@ __device__ void cta_reduce(double* v, unsigned maxmask)
 #pragma unroll
     for (int k = 0; k < NV; k++) {
         double a = 0.0;
-        for (int q = 0; q < kT / 32; q++) a = (maxmask >> k) & 1u ? fmax(a, sh[k][q]) : a + sh[k][q];
+        for (int q = 0; q < kT / 32; q++) a = (maxmask >> k) & 1u ? nan_max(a, sh[k][q]) : a + sh[k][q];
         v[k] = a;
     }
     __syncthreads();
@@ -138,7 +142,7 @@ __device__ bool seg_finish(double* v, unsigned maxmask, Seg* sg, double* partial
     for (int b = sg->c0 + static_cast<int>(threadIdx.x); b < sg->c1; b += kT) {
         const volatile double* pb = partials + static_cast<size_t>(b) * NV;
 #pragma unroll
-        for (int k = 0; k < NV; k++) acc[k] = (maxmask >> k) & 1u ? fmax(acc[k], pb[k]) : acc[k] + pb[k];
+        for (int k = 0; k < NV; k++) acc[k] = (maxmask >> k) & 1u ? nan_max(acc[k], pb[k]) : acc[k] + pb[k];
     }
     cta_reduce<NV>(acc, maxmask);
 #pragma unroll
@@ -208,8 +212,8 @@ __global__ void __launch_bounds__(kT) kb_initial(const double* __restrict__ r, c
     Seg* sg = S + c.seg;
     double v[3] = { 0, 0, 0 };
     for (int i = c.a + threadIdx.x; i < c.b; i += kT) {
-        v[0] = fmax(v[0], fabs(r[i]));
-        v[1] = fmax(v[1], fabs(x[i]));
+        v[0] = nan_max(v[0], fabs(r[i]));
+        v[1] = nan_max(v[1], fabs(x[i]));
         v[2] += x[i] * x[i];
     }
     if (!seg_finish<3>(v, 3u, sg, partials) || threadIdx.x != 0) return;
@@ -402,8 +406,8 @@ __global__ void __launch_bounds__(kT) kb_ls_reduce(const double* __restrict__ r,
         for (int i = c.a + threadIdx.x; i < c.b; i += kT) {
             const double ri = r[i], xi = x[i];
             v[0] += ri * d[i];
-            v[1] = fmax(v[1], fabs(ri));
-            v[2] = fmax(v[2], fabs(xi));
+            v[1] = nan_max(v[1], fabs(ri));
+            v[2] = nan_max(v[2], fabs(xi));
             v[3] += xi * xi;
         }
     if (!seg_finish<4>(v, 6u, sg, partials)) return;

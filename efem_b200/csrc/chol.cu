@@ -745,7 +745,7 @@ __global__ void __launch_bounds__(kST) k_solve(SolveArgs A)
     double* st = sm;                                  // staged factor rows
     double* wk = sm + A.stage_d;                      // work vectors
     int* si = reinterpret_cast<int*>(wk + A.work_d);  // staged index lists
-    __shared__ int item_sh, ok_sh;
+    __shared__ int item_sh, ok_sh, ok2_sh;
     const int ns = A.ns;
     int* cY = A.cnt;
     int* cGin = A.cnt + ns;
@@ -777,7 +777,6 @@ __global__ void __launch_bounds__(kST) k_solve(SolveArgs A)
         }
         const int bump = A.test_wait && it == A.n_items - 1 ? 1 : 0;
         const SolveItem d = A.items[it];
-        if (tid == 0) next = atomicAdd(ticket, 1);  // in flight while this item runs
         const int kind = d.kind, s = d.s, r0 = d.r0, r1 = d.r1, R = r1 - r0, cbeg = d.cbeg, cend = d.cend;
         const int p = A.parent[s];
         const int r = a.nrow[s], c = a.ncol[s], m = r - c, f0 = a.first[s];
@@ -826,19 +825,26 @@ __global__ void __launch_bounds__(kST) k_solve(SolveArgs A)
             break;
         }
         stage_commit();
+        // The next ticket is drawn once this item's dependencies are in (a
+        // few microseconds before the CTA is free), not when the item starts:
+        // a CTA whose item waits on a long chain would otherwise hold up the
+        // item of the ticket it drew.  Backward items wait in two steps: their
+        // own front's forward result first, the parent's solution last.
+        const bool bwd = kind == kBwdFront || kind == kBwdX;
         if (tid == 0) {
-            bool ok;
-            switch (kind) {
-            case kFwdFront:
-            case kFwdY:
-            case kFwdG: ok = wait_ge(cGin + s, tGin[s] + bump, err, A.spin_limit); break;
-            default:
-                ok = wait_ge(cY + s, tY[s] + bump, err, A.spin_limit)
-                    && (p < 0 || wait_ge(cX + p, tX[p], err, A.spin_limit));
-                break;
-            }
+            const bool ok = bwd ? wait_ge(cY + s, tY[s] + bump, err, A.spin_limit)
+                                : wait_ge(cGin + s, tGin[s] + bump, err, A.spin_limit);
             ok_sh = ok;
+            if (!bwd || !ok) next = atomicAdd(ticket, 1);
         }
+        // backward items: thread 0 waits for the parent's x, then draws the next ticket
+        auto parent_wait = [&]() {
+            if (tid == 0) {
+                ok2_sh = p < 0 || wait_ge(cX + p, tX[p], err, A.spin_limit);
+                next = atomicAdd(ticket, 1);
+            }
+            __syncthreads();
+        };
         stage_wait();
         __syncthreads();
         if (ok_sh) {
@@ -898,13 +904,16 @@ __global__ void __launch_bounds__(kST) k_solve(SolveArgs A)
                 double* xr = wk + 3 * c;       // [m][3]
                 double* xs = wk + 3 * r;       // [c][3]
                 copy_cg(yj, A.y + 3LL * f0, 3 * c);
-                gather3(xr, A.v, si + c, m);
                 __syncthreads();
+                // L_JJ^{-T} y_J needs only this front's forward result
                 rows_dot(st, lc, yj, 0, c, c, 2, 0, [&](int i, double x0, double x1, double x2) {
                     xs[3 * i] = x0;
                     xs[3 * i + 1] = x1;
                     xs[3 * i + 2] = x2;
                 });
+                parent_wait();
+                if (!ok2_sh) break;
+                gather3(xr, A.v, si + c, m);
                 __syncthreads();
                 rows_dot(st + c * lc, lm, xr, 0, c, m, 0, 0, [&](int i, double s0, double s1, double s2) {
                     double* o = A.v + 3LL * si[i];
@@ -919,13 +928,15 @@ __global__ void __launch_bounds__(kST) k_solve(SolveArgs A)
                 double* xr = wk + 3 * (c - r0);       // [m][3]
                 double* xs = xr + 3 * m;              // [R][3]
                 copy_cg(yj, A.y + 3LL * (f0 + r0), 3 * (c - r0));
-                gather3(xr, A.v, si + c, m);
                 __syncthreads();
                 rows_dot(st, lc, yj, r0, R, c, 2, r0, [&](int i, double x0, double x1, double x2) {
                     xs[3 * i] = x0;
                     xs[3 * i + 1] = x1;
                     xs[3 * i + 2] = x2;
                 });
+                parent_wait();
+                if (!ok2_sh) break;
+                gather3(xr, A.v, si + c, m);
                 __syncthreads();
                 rows_dot(st + R * lc, lm, xr, 0, R, m, 0, 0, [&](int i, double s0, double s1, double s2) {
                     double* o = A.v + 3LL * si[r0 + i];

@@ -102,6 +102,10 @@ __device__ __forceinline__ unsigned long long gtimer()
     return t;
 }
 
+// max that keeps a NaN (fmax drops it): a non-finite residual or solution
+// must show in its infinity norm (Integrator.cpp:28-34 tests for it)
+__device__ __forceinline__ double nan_max(double a, double b) { return (b > a || b != b) ? b : a; }
+
 __device__ __forceinline__ double warp_sum(double v)
 {
 #pragma unroll
@@ -111,7 +115,7 @@ __device__ __forceinline__ double warp_sum(double v)
 __device__ __forceinline__ double warp_max(double v)
 {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    for (int o = 16; o > 0; o >>= 1) v = nan_max(v, __shfl_xor_sync(0xffffffffu, v, o));
     return v;
 }
 
@@ -161,7 +165,7 @@ __device__ bool grid_finish(double* v, const int* ops, double* partials, unsigne
 #pragma unroll
         for (int k = 0; k < NV; k++) {
             const double p = *(volatile double*)&partials[b * NV + k];
-            acc[k] = ops[k] ? fmax(acc[k], p) : acc[k] + p;
+            acc[k] = ops[k] ? nan_max(acc[k], p) : acc[k] + p;
         }
     block_reduce<NV>(acc, ops);
     if (threadIdx.x == 0) {
@@ -259,8 +263,8 @@ __global__ void __launch_bounds__(kThreads) k_ls_reduce(const double* __restrict
     {
         const double ri = r[i], xi = x[i];
         v[0] += ri * d[i];
-        v[1] = fmax(v[1], fabs(ri));
-        v[2] = fmax(v[2], fabs(xi));
+        v[1] = nan_max(v[1], fabs(ri));
+        v[2] = nan_max(v[2], fabs(xi));
         v[3] += xi * xi;
         v[4] += ri * ri;
     }
