@@ -55,6 +55,7 @@ constexpr int kChunk = 2048;  // vector entries per CTA; a chunk never spans two
 constexpr int kHist = 8;      // largest L-BFGS history of a batch
 constexpr int kCap = 64;      // iterations per launch of the iteration graph
 constexpr int kStall = 24;    // FP32 phase: iterations without halving the best ||r||_inf
+constexpr double kFp32Target = 0.5;  // FP32 phase: residual target as a fraction of the tolerance
 
 enum { kRun = 0, kDone = 1, kMaxIt = 2, kNaN = 3, kStalled = 4, kPcFail = 5 };
 
@@ -159,11 +160,12 @@ struct Chunk {
 __device__ __forceinline__ int ring(int i, int m) { return ((i % m) + m) % m; }
 
 __global__ void kb_init(Seg* S, const int* c0, const double* eps, const int* max_iter, int max_ls, int m, int nseg,
-    int stall, const int* keep)
+    int stall, const int* keep, int* frozen)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nseg) return;
     Seg& s = S[i];
+    frozen[i] = keep && keep[i] ? 1 : 0;
     if (keep && keep[i]) return;  // a member whose earlier phase ended for good
     s.theta = 1.0;
     s.ptr = m;  // ptr % m == 0 on the first correction (LBFGSMat.h:68)
@@ -206,7 +208,7 @@ __global__ void kb_loop_start(Glob* G)
 
 // the initial residual's norms and the early exit (LBFGS.h:110-120) of every running member
 __global__ void __launch_bounds__(kT) kb_initial(const double* __restrict__ r, const double* __restrict__ x,
-    const Chunk* __restrict__ ch, Seg* S, double* partials)
+    const Chunk* __restrict__ ch, Seg* S, double* partials, int* frozen)
 {
     const Chunk c = ch[blockIdx.x];
     Seg* sg = S + c.seg;
@@ -226,6 +228,7 @@ __global__ void __launch_bounds__(kT) kb_initial(const double* __restrict__ r, c
         sg->state = kNaN;
     else if (v[0] <= sg->eps || v[0] <= sg->eps * sqrt(v[2]))
         sg->state = kDone;
+    frozen[c.seg] = sg->state != kRun;
 }
 
 // Pass 1 (LBFGSMat::add_correction, LBFGSMat.h:81-98, and the first loop's
@@ -474,7 +477,7 @@ __global__ void __launch_bounds__(kT) kb_trial(double* __restrict__ x, const dou
 // ||r||_inf has not halved for `stall` iterations; else count the iteration.
 // Sets the iteration loop's condition: some member runs and the launch has
 // iterations left.
-__global__ void __launch_bounds__(1024) kb_decide(Seg* S, int nseg, Glob* G, const int* perr,
+__global__ void __launch_bounds__(1024) kb_decide(Seg* S, int nseg, Glob* G, const int* perr, int* frozen,
     cudaGraphConditionalHandle h)
 {
     __shared__ int running;
@@ -504,6 +507,7 @@ __global__ void __launch_bounds__(1024) kb_decide(Seg* S, int nseg, Glob* G, con
             s.k++;
             mine++;
         }
+        if (s.state != kRun) frozen[i] = 1;  // the triangular solve skips its items from now on
     }
     if (mine) atomicAdd(&running, mine);
     __syncthreads();
@@ -551,6 +555,7 @@ struct Union {
     double* d_eps = nullptr;
     int* d_maxit = nullptr;
     int* d_keep = nullptr;
+    int* d_frozen = nullptr;  // per member: 1 = no longer iterating (the triangular solve skips it)
     Seg* d_seg = nullptr;
     Glob* d_glob = nullptr;
     double *x = nullptr, *xp = nullptr, *r = nullptr, *rp = nullptr, *d = nullptr, *q = nullptr, *Sh = nullptr,
@@ -574,6 +579,7 @@ Union::~Union()
     dev_free(d_c0);
     dev_free(d_maxit);
     dev_free(d_keep);
+    dev_free(d_frozen);
     dev_free(d_seg);
     dev_free(d_glob);
 }
@@ -695,6 +701,7 @@ efem_status setup_union(Union& U)
     if ((s = dev_alloc(&U.d_eps, U.nseg)) != EFEM_OK) return s;
     if ((s = dev_alloc(&U.d_maxit, U.nseg)) != EFEM_OK) return s;
     if ((s = dev_alloc(&U.d_keep, U.nseg)) != EFEM_OK) return s;
+    if ((s = dev_alloc(&U.d_frozen, U.nseg)) != EFEM_OK) return s;
     if ((s = dev_alloc(&U.d_seg, U.nseg)) != EFEM_OK) return s;
     if ((s = dev_alloc(&U.d_glob, 1)) != EFEM_OK) return s;
     EFEM_CUDA(cudaMemset(U.d_seg, 0, sizeof(Seg) * U.nseg));
@@ -767,7 +774,7 @@ efem_status capture_union_loop(Union& U, cudaGraphExec_t* out)
         cudaGraph_t tmp = nullptr;
         if (cudaStreamEndCapture(s2, &tmp) != cudaSuccess && s == EFEM_OK) s = EFEM_ERR_CUDA;
         if (s != EFEM_OK) break;
-        kb_decide<<<1, 1024, 0, s1>>>(U.d_seg, U.nseg, U.d_glob, precond_error_flag(M), h_it);
+        kb_decide<<<1, 1024, 0, s1>>>(U.d_seg, U.nseg, U.d_glob, precond_error_flag(M), U.d_frozen, h_it);
         if (cudaStreamEndCapture(s1, &tmp) != cudaSuccess) s = EFEM_ERR_CUDA;
     } while (false);
     const cudaError_t e = cudaStreamEndCapture(s0, &g);
@@ -798,19 +805,22 @@ efem_status run_union_phase(Union& U, int stall, const std::vector<int>& keep, l
     cudaStream_t st = M.stream;
     std::vector<double> eps(U.nseg);
     std::vector<int> maxit(U.nseg);
+    // the FP32 phase aims below each tolerance, so that the FP64 test that
+    // follows usually passes at once
+    const double target = stall > 0 ? kFp32Target : 1.0;
     for (int i = 0; i < U.nseg; i++) {
-        eps[i] = U.members[i]->opts.residual_criterion;
+        eps[i] = target * U.members[i]->opts.residual_criterion;
         maxit[i] = U.members[i]->opts.max_iterations;
     }
     EFEM_CUDA(cudaMemcpyAsync(U.d_eps, eps.data(), sizeof(double) * U.nseg, cudaMemcpyHostToDevice, st));
     EFEM_CUDA(cudaMemcpyAsync(U.d_maxit, maxit.data(), sizeof(int) * U.nseg, cudaMemcpyHostToDevice, st));
     EFEM_CUDA(cudaMemcpyAsync(U.d_keep, keep.data(), sizeof(int) * U.nseg, cudaMemcpyHostToDevice, st));
     kb_init<<<(U.nseg + 127) / 128, 128, 0, st>>>(U.d_seg, U.d_c0, U.d_eps, U.d_maxit, M.opts.max_linesearch, U.m,
-        U.nseg, stall, U.d_keep);
+        U.nseg, stall, U.d_keep, U.d_frozen);
     kb_glob_init<<<1, 1, 0, st>>>(U.d_glob, kCap);
     efem_status s = launch_residual_on(M, U.x, U.r, st);
     if (s != EFEM_OK) return s;
-    kb_initial<<<U.nchunk, kT, 0, st>>>(U.r, U.x, U.d_chunks, U.d_seg, U.partials);
+    kb_initial<<<U.nchunk, kT, 0, st>>>(U.r, U.x, U.d_chunks, U.d_seg, U.partials, U.d_frozen);
     *launches += 4 + U.per_res;
     // the approximate Jacobian's factor (LBFGS.h:122-124): the forest of the members' trees
     int ok = 0;
@@ -820,6 +830,12 @@ efem_status run_union_phase(Union& U, int stall, const std::vector<int>& keep, l
     if (!ok) {
         set_error("batch union: an approximate Jacobian is not positive definite");
         return EFEM_ERR_UNSUPPORTED;
+    }
+    if (!precond_has_groups(M)) {  // members that stop iterating drop out of the triangular solve
+        std::vector<int> group(M.n_free);
+        for (int i = 0; i < U.nseg; i++)
+            for (size_t q = U.off[i] / 3; q < U.off[i + 1] / 3; q++) group[q] = i;
+        if ((s = precond_set_groups(M, group, U.d_frozen)) != EFEM_OK) return s;
     }
     const int slot = M.opts.precision == EFEM_MIXED ? 1 : 0;
     if (!U.loop[slot] || U.loop_epoch[slot] != M.epoch) {

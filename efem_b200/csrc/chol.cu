@@ -94,6 +94,9 @@ struct Precond {
     int n_items = 0, solve_grid = 1, solve_grid_full = 1, slots = 1;
     size_t solve_smem = 0;
     SolveItem* d_items = nullptr;
+    std::vector<int> h_item_front;  // the front of every item (host)
+    int* d_item_group = nullptr;    // batch unions: member of every item
+    const int* d_frozen = nullptr;  // batch unions: per-member flag, 1 = skip its items
     int *d_tgt = nullptr, *d_parent = nullptr, *d_cnt = nullptr, *d_prow = nullptr;
     // subtree solves below the cut level (sub_levels levels of the tree)
     int sub_levels = 0, n_subs = 0;
@@ -501,6 +504,8 @@ struct SolveArgs {
     int spin_limit;             // polls of one wait before the solve gives up
     int test_wait;              // 1: the last item's wait target is raised by one (it can only run out)
     int n3;                     // entries of v (3 per free node)
+    const int* item_group;      // batch unions: the member each item belongs to
+    const int* frozen;          // batch unions: 1 for a member that no longer iterates (its items are skipped)
 };
 
 constexpr int kSpinLimit = 1 << 22;  // default polls of one wait (about half a second)
@@ -774,6 +779,13 @@ __global__ void __launch_bounds__(kST) k_solve(SolveArgs A)
         if (it >= A.n_items) {
             griddep_launch();  // no more items for this CTA
             break;
+        }
+        if (A.frozen && A.frozen[A.item_group[it]]) {
+            // a batch member that stopped iterating: its tree of fronts (no
+            // other member's items depend on it) is skipped whole
+            if (tid == 0) next = atomicAdd(ticket, 1);
+            __syncthreads();
+            continue;
         }
         const int bump = A.test_wait && it == A.n_items - 1 ? 1 : 0;
         const SolveItem d = A.items[it];
@@ -1279,7 +1291,8 @@ efem_status enqueue_solve(const Precond& P, const FrontArgs& a, const SolveBufs&
         P.sub_max_cols, P.sub_max_depth, P.sub_max_m, P.sub_max_c, P.sub_max_mroot, d_v, b.y, b.upd, stamp };
     if (P.n_subs > 0) k_sub_fwd<<<P.n_subs, kST, P.sub_smem_f, st>>>(B);
     SolveArgs A { a, P.d_parent, P.d_prow, P.d_items, P.d_tgt, P.n_items, ns, P.stage_d, P.work_d, d_v, b.y, b.t,
-        b.upd, b.cnt, P.n_subs > 0 ? nullptr : stamp, wc.limit, wc.test, 3 * P.S.n };
+        b.upd, b.cnt, P.n_subs > 0 ? nullptr : stamp, wc.limit, wc.test, 3 * P.S.n, P.d_item_group,
+        P.d_item_group ? P.d_frozen : nullptr };
     if (P.n_items > 0) launch_k(k_solve, P.solve_grid, kST, P.solve_smem, st, A);
     if (P.n_subs > 0) k_sub_bwd<<<P.n_subs, kST, P.sub_smem_b, st>>>(B);
     return EFEM_OK;
@@ -1304,6 +1317,7 @@ void free_precond(Model& m)
         dev_free(*p);
     for (Tile** p : { &P.d_inv, &P.d_ea, &P.d_oinv }) dev_free(*p);
     dev_free(P.d_items);
+    dev_free(P.d_item_group);
     dev_free(P.d_subs);
     dev_free(P.d_chunks);
     dev_free(P.d_syrk);
@@ -1605,6 +1619,8 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
         }
     }
     P.n_items = static_cast<int>(items.size());
+    P.h_item_front.resize(items.size());
+    for (size_t i = 0; i < items.size(); i++) P.h_item_front[i] = items[i].s;
     P.stage_d = static_cast<int>(stage_d);
     P.work_d = static_cast<int>(work_d);
     P.solve_smem = sizeof(double) * (stage_d + work_d) + sizeof(int) * ints;
@@ -1860,6 +1876,31 @@ efem_status precond_enqueue(Model& m, double* d_v, cudaStream_t stream, bool cle
     return enqueue_solve(P, args_of(P), SolveBufs { P.d_y, P.d_t, P.d_upd, P.d_cnt }, d_v, stream, wait_cfg(m), clear,
         stamp);
 }
+
+efem_status precond_set_groups(Model& m, const std::vector<int>& group_of_free_node, const int* d_frozen)
+{
+    if (!m.precond || !m.precond->ready) {
+        set_error("precond_set_groups: no solve schedule");
+        return EFEM_ERR_ARG;
+    }
+    Precond& P = *m.precond;
+    if (P.n_subs > 0) return EFEM_OK;  // subtree solves do not skip; leave the schedule as it is
+    std::vector<int> g(std::max(1, P.n_items), 0);
+    for (int i = 0; i < P.n_items; i++) {
+        const int s = P.h_item_front[i];
+        g[i] = group_of_free_node[P.S.perm[P.S.first[s]]];
+    }
+    dev_free(P.d_item_group);
+    efem_status st = dev_upload(&P.d_item_group, g);
+    if (st != EFEM_OK) return st;
+    P.d_frozen = d_frozen;
+    for (auto& kv : P.graphs) cudaGraphExecDestroy(kv.second);  // captured solves hold the old arguments
+    P.graphs.clear();
+    m.epoch++;
+    return EFEM_OK;
+}
+
+bool precond_has_groups(const Model& m) { return m.precond && m.precond->d_item_group; }
 
 void precond_counters(const Model& m, int** cnt, int* n)
 {

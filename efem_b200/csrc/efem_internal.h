@@ -289,6 +289,11 @@ efem_status precond_apply(Model& m, double* d_v);
 efem_status precond_enqueue(Model& m, double* d_v, cudaStream_t stream, bool clear = true,
     unsigned long long* stamp = nullptr);
 void precond_counters(const Model& m, int** cnt, int* n);  // the solve's counters, cleared before each H0 v
+// Batch unions: group_of_free_node[i] = the member free node i belongs to;
+// items of member g are skipped while d_frozen[g] != 0 (a member's fronts
+// form trees of their own, so nothing else waits on them).
+efem_status precond_set_groups(Model& m, const std::vector<int>& group_of_free_node, const int* d_frozen);
+bool precond_has_groups(const Model& m);
 long long precond_launch_count(const Model& m);  // kernels per H0 application
 const int* precond_error_flag(const Model& m);   // device flag: a solve gave up waiting (nullptr before set-up)
 efem_status precond_check(Model& m);             // wait for the stream and report that flag

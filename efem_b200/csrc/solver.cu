@@ -1372,6 +1372,8 @@ nan_exit:
 // iterations without a halving of the best ||r||_inf after which the FP32
 // phase of a mixed-precision solve hands over to FP64 element kernels
 constexpr int kStallIters = 24;
+// the FP32 phase's residual target, as a fraction of the tolerance
+constexpr double kFp32Target = 0.5;
 
 // The solve behind efem_solve.  FP64: one phase.  Mixed precision: FP32
 // element kernels until the residual passes the test or stops improving (the
@@ -1385,12 +1387,16 @@ efem_status run_solve(Model& m, double* x, efem_solve_info* info)
     bool stalled = false;
     if (m.opts.precision != EFEM_MIXED) return run_solve_phase(m, x, info, true, 0, false, &stalled);
     efem_solve_info a {};
+    const efem_options keep = m.opts;
+    // the FP32 phase aims below the tolerance, so that the FP64 test that
+    // follows usually passes at once instead of restarting the history
+    m.opts.residual_criterion = kFp32Target * keep.residual_criterion;
     efem_status s = run_solve_phase(m, x, &a, true, kStallIters, false, &stalled);
+    m.opts = keep;
     if (s != EFEM_OK || (a.flags & EFEM_SOLVE_MAX_ITERS)) {
         *info = a;
         return s;
     }
-    const efem_options keep = m.opts;
     m.opts.precision = EFEM_FP64;
     if (keep.max_iterations != 0) m.opts.max_iterations = std::max(1, keep.max_iterations - a.niter);
     efem_solve_info b {};

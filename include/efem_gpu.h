@@ -89,8 +89,8 @@ typedef struct {
 
 /* EFEM_MIXED: FP32 element kernels (FP32 arithmetic, FP64 accumulation of
  * the nodal forces) with the factor, its solves, the L-BFGS vectors and the
- * norms in FP64.  The FP32 phase runs until the residual passes the test or
- * stops improving; FP64 element kernels then finish the solve from there
+ * norms in FP64.  The FP32 phase runs until the residual is below half the
+ * tolerance or stops improving; FP64 element kernels then finish the solve from there
  * (EFEM_SOLVE_REFINED), so the test that ends every solve reads an FP64
  * residual. */
 typedef enum { EFEM_FP64 = 0, EFEM_MIXED = 1 } efem_precision;

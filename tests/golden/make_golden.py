@@ -11,6 +11,7 @@ the tests never need it):
     python tests/golden/make_golden.py configs    # converged u of the large benchmark meshes
     python tests/golden/make_golden.py multibody  # two bodies with pose and model_id routing
     python tests/golden/make_golden.py failure    # a singular approximate Jacobian (fallback solve)
+    python tests/golden/make_golden.py batch      # three members of the benchmark batch
 
 ``samples`` and ``configs`` read the reference tree: its location is the
 EFEM_REFERENCE environment variable, else a ``reference`` directory beside
@@ -332,6 +333,31 @@ def failure_cases():
     print("failure_orphan_node", meta, meta_t["niter"])
 
 
+BATCH_SEED = 20261203
+
+
+def batch_members():
+    """``batch_member_<k>.npz``: three members of the benchmark batch
+    (efem_b200.meshgen.batch_beams(seed=20261203), the three with the fewest
+    elements), the reference's solution of each at 1e-6 N (``u_solve``) and at
+    1e-10 N (``u_tight``), with the member's index in the batch."""
+    cases = mg.batch_beams(seed=BATCH_SEED)
+    order = sorted(range(len(cases)), key=lambda i: cases[i].mesh.conn.shape[0])[:3]
+    for k, i in enumerate(order):
+        case = cases[i]
+        data = case_arrays(case)
+        with tempfile.TemporaryDirectory() as td:
+            cfg = case.write(td)
+            meta, us = oracle.run_ref("solve", cfg)
+            case.analysis.update(residual_criterion=1e-10)
+            cfg = case.write(td)
+            meta_t, ut = oracle.run_ref("solve", cfg)
+        data.update(u_solve=us, solve_meta=json.dumps(meta), u_tight=ut, solve_meta_tight=json.dumps(meta_t),
+                    member=i)
+        np.savez_compressed(os.path.join(HERE, f"batch_member_{k}.npz"), **data)
+        print("batch member", i, case.mesh.conn.shape[0], meta["niter"], meta_t["niter"])
+
+
 def main():
     if sys.argv[1:] == ["gravity"]:
         gravity_cases()
@@ -350,6 +376,9 @@ def main():
         return
     if sys.argv[1:] == ["failure"]:
         failure_cases()
+        return
+    if sys.argv[1:] == ["batch"]:
+        batch_members()
         return
     rng = np.random.default_rng(20261203)
     for et in ETYPES:
