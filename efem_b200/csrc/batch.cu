@@ -705,6 +705,23 @@ efem_status setup_union(Union& U)
     if ((s = dev_alloc(&U.d_seg, U.nseg)) != EFEM_OK) return s;
     if ((s = dev_alloc(&U.d_glob, 1)) != EFEM_OK) return s;
     EFEM_CUDA(cudaMemset(U.d_seg, 0, sizeof(Seg) * U.nseg));
+    EFEM_CUDA(cudaMemset(U.d_frozen, 0, sizeof(int) * U.nseg));
+    // members that stop iterating drop out of the element kernels: the
+    // member of every element, block by block (members' elements are
+    // concatenated in member order within each element type)
+    for (auto& b : M.blocks) {
+        std::vector<int> eg;
+        eg.reserve(b.n);
+        for (int i = 0; i < U.nseg; i++)
+            for (const HostBlock& hb : U.members[i]->in_blocks)
+                if (hb.nen == b.nen) eg.insert(eg.end(), hb.mat_id.size(), i);
+        if (static_cast<int>(eg.size()) != b.n) {
+            set_error("batch union: element count mismatch");
+            return EFEM_ERR_ARG;
+        }
+        if ((s = dev_upload(&b.egroup, eg)) != EFEM_OK) return s;
+    }
+    M.d_frozen_groups = U.d_frozen;
     for (auto& c : U.cap) EFEM_CUDA(cudaStreamCreateWithFlags(&c, cudaStreamNonBlocking));
     U.per_res = 1 + static_cast<long long>(M.blocks.size() + M.faces.size());
     return EFEM_OK;

@@ -78,6 +78,7 @@ struct DevBlock {
     float* dN_f = nullptr;
     double* gw = nullptr;         // [ngp]
     float* gw_f = nullptr;
+    int* egroup = nullptr;        // batch unions: member of every element (null otherwise)
     // host copies used by set-up (Jacobian assembly, tests)
     std::vector<int> h_conn;      // row-major (n, nen), dnode ids
     std::vector<int> h_mat;
@@ -145,6 +146,7 @@ struct Model {
     bool has_gravity = false;
     bool on_device = false;
     double* d_fext = nullptr;         // [3*n_free]
+    const int* d_frozen_groups = nullptr;  // batch unions: per member, 1 = its elements are skipped
     double* d_u = nullptr;            // staging for host-pointer calls
     double* d_r = nullptr;
     // deterministic scatter (opts.deterministic): nodal contributions of every

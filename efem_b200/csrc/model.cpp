@@ -176,6 +176,7 @@ Model::~Model()
     free_adjoint(*this);
     free_precond(*this);
     for (auto& b : blocks) {
+        dev_free(b.egroup);
         dev_free(b.conn);
         dev_free(b.mat);
         dev_free(b.vol);

@@ -48,6 +48,8 @@ struct ElemArgs {
     double* __restrict__ r;           // [3*n_free]
     double* __restrict__ contrib;     // deterministic scatter: [3][n_slots], or null for atomics
     size_t n_slots, slot0;
+    const int* __restrict__ egroup;   // batch unions: the member of every element
+    const int* frozen;                // batch unions: 1 for a member that no longer iterates (null: none)
 };
 
 // where an (element or face, node) pair's nodal force goes
@@ -77,8 +79,17 @@ __global__ void __launch_bounds__(BLK) k_elem_residual(ElemArgs<T> a)
     __shared__ int s_node[EPB][SN];
 
     const int tid = threadIdx.x;
-    for (int i = tid; i < NGP * NEN * 3; i += BLK) s_dN[i / (NEN * 3)][i % (NEN * 3)] = a.dN[i];
     const int e0 = blockIdx.x * EPB;
+    if (a.frozen) {  // a batch union: skip the CTA when every member it covers has stopped iterating
+        const int e1 = min(a.n, e0 + EPB) - 1;
+        bool act = false;
+        for (int g = __ldg(a.egroup + e0); g <= __ldg(a.egroup + e1); g++) act = act || !a.frozen[g];
+        if (!act) {
+            griddep_launch();
+            return;
+        }
+    }
+    for (int i = tid; i < NGP * NEN * 3; i += BLK) s_dN[i / (NEN * 3)][i % (NEN * 3)] = a.dN[i];
 
     // phase 1: stage node displacements relative to the element's first node,
     // formed in FP64 (H only sees differences, since sum_a dN_a = 0, and FP32
@@ -317,9 +328,10 @@ void launch_elem_blk(const ElemArgs<T>& a, cudaStream_t st)
 
 template <int NEN, int NGP, typename T>
 void launch_elem(const DevBlock& b, const MatParams<T>* mats, const T* vol, const T* J0, const T* dN, const T* gw,
-    int n_free, const double* u, double* r, cudaStream_t st, int threads, const Scatter& sc)
+    int n_free, const double* u, double* r, cudaStream_t st, int threads, const Scatter& sc, const int* frozen)
 {
-    ElemArgs<T> a { b.n, n_free, b.conn, b.mat, vol, J0, dN, gw, mats, u, r, sc.contrib, sc.n_slots, sc.slot0 };
+    ElemArgs<T> a { b.n, n_free, b.conn, b.mat, vol, J0, dN, gw, mats, u, r, sc.contrib, sc.n_slots, sc.slot0,
+        b.egroup, b.egroup ? frozen : nullptr };
     if (threads == 64) launch_elem_blk<NEN, NGP, T, 64>(a, st);
     else if (threads == 256) launch_elem_blk<NEN, NGP, T, 256>(a, st);
     else launch_elem_blk<NEN, NGP, T, 128>(a, st);
@@ -327,12 +339,13 @@ void launch_elem(const DevBlock& b, const MatParams<T>* mats, const T* vol, cons
 
 template <typename T>
 void dispatch_elem(const DevBlock& b, const MatParams<T>* mats, const T* vol, const T* J0, const T* dN, const T* gw,
-    int n_free, const double* u, double* r, cudaStream_t st, int threads, const Scatter& sc = Scatter())
+    int n_free, const double* u, double* r, cudaStream_t st, int threads, const Scatter& sc = Scatter(),
+    const int* frozen = nullptr)
 {
-#define CASE(NEN, NGP)                                                                     \
-    if (b.nen == NEN && b.ngp == NGP) {                                                    \
-        launch_elem<NEN, NGP, T>(b, mats, vol, J0, dN, gw, n_free, u, r, st, threads, sc); \
-        return;                                                                            \
+#define CASE(NEN, NGP)                                                                             \
+    if (b.nen == NEN && b.ngp == NGP) {                                                            \
+        launch_elem<NEN, NGP, T>(b, mats, vol, J0, dN, gw, n_free, u, r, st, threads, sc, frozen); \
+        return;                                                                                    \
     }
     CASE(4, 1)
     CASE(10, 4)
@@ -441,9 +454,10 @@ efem_status launch_residual_on(Model& m, const double* d_u, double* d_r, cudaStr
         if (det) sc = Scatter { m.d_contrib, m.n_slots, b.slot0 };
         if (mixed)
             dispatch_elem<float>(b, m.d_mats_f, b.vol_f, b.J0inv_f, b.dN_f, b.gw_f, m.n_free, d_u, d_r, stream,
-                b.threads[1], sc);
+                b.threads[1], sc, m.d_frozen_groups);
         else
-            dispatch_elem<double>(b, m.d_mats, b.vol, b.J0inv, b.dN, b.gw, m.n_free, d_u, d_r, stream, b.threads[0], sc);
+            dispatch_elem<double>(b, m.d_mats, b.vol, b.J0inv, b.dN, b.gw, m.n_free, d_u, d_r, stream, b.threads[0], sc,
+                m.d_frozen_groups);
     }
     for (auto& f : m.faces) {
         if (f.n == 0) continue;
