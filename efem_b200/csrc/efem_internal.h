@@ -67,6 +67,7 @@ constexpr int MAX_MATS = 16;
 struct DevBlock {
     int kind = 0, nen = 0, ngp = 0, n = 0;
     int threads[2] = { 128, 128 };  // element-kernel CTA size per precision (FP64, FP32), from the autotuner
+    int mat_type = -1;            // the one material law of every element, or -1 when they mix laws
     size_t slot0 = 0;             // deterministic scatter: first contribution slot, slot = slot0 + a * n + e
     int* conn = nullptr;          // [nen][n]
     int* mat = nullptr;           // [n]

@@ -83,10 +83,14 @@ __device__ __forceinline__ void kinematics(const T* H, Kin<T>& k)
         for (int j = 0; j < 3; j++) k.B[3 * i + j] = (i == j ? trH : T(0)) - H[3 * j + i] + cH[3 * i + j];
 }
 
-// P(F) for F = I + H, row-major 3x3.
-template <typename T>
+// P(F) for F = I + H, row-major 3x3.  MT: the law when every element of a
+// block has the same one (EFEM_NEO_HOOKEAN, EFEM_MOONEY_RIVLIN, EFEM_YEOH),
+// so that only its code is compiled in; -1: any law, chosen per element.
+template <typename T, int MT = -1>
 __device__ __forceinline__ void piola(const MatParams<T>& mp, const T* H, T* P)
 {
+    const bool yeoh = MT == EFEM_YEOH || (MT < 0 && mp.type == EFEM_YEOH);
+    const bool mr = MT == EFEM_MOONEY_RIVLIN || (MT < 0 && mp.type == EFEM_MOONEY_RIVLIN);
     Kin<T> k;
     kinematics(H, k);
     const T lJ = dlog1p(k.delta);
@@ -95,7 +99,7 @@ __device__ __forceinline__ void piola(const MatParams<T>& mp, const T* H, T* P)
     const T cm1 = (k.a * T(1.0 / 3.0) - k.delta) * inv1pd;  // c - 1
     const T c = T(1) + cm1;
     T coef = mp.C10;
-    if (mp.type == EFEM_YEOH) {
+    if (yeoh) {
         // I1bar - 3 = 3 (J^{-2/3} - 1) + (I1 - 3) J^{-2/3}
         const T t = T(3) * dexpm1(T(-2.0 / 3.0) * lJ) + k.a * Jm23;
         coef = mp.C10 + T(2) * mp.C20 * t + T(3) * mp.C30 * t * t;
@@ -107,7 +111,7 @@ __device__ __forceinline__ void piola(const MatParams<T>& mp, const T* H, T* P)
         const T id = (i % 4 == 0) ? T(1) : T(0);
         P[i] = s1 * (H[i] - cm1 * id - c * k.B[i]) + vol * (id + k.B[i]);
     }
-    if (mp.type == EFEM_MOONEY_RIVLIN) {
+    if (mr) {
         T E[9];
 #pragma unroll
         for (int i = 0; i < 3; i++)

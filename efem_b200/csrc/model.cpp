@@ -543,6 +543,16 @@ efem_status build_blocks(Model& m)
         b.h_conn.resize(hb.conn.size());
         for (size_t i = 0; i < hb.conn.size(); i++) b.h_conn[i] = m.dnode_of_node[hb.conn[i]];
         b.h_mat = hb.mat_id;
+        // one law for the whole block: the element kernel compiles only its code
+        b.mat_type = -1;
+        for (size_t e = 0; e < hb.mat_id.size(); e++) {
+            const int t = m.materials_used[hb.mat_id[e]].type;
+            if (e == 0) b.mat_type = t;
+            else if (t != b.mat_type) {
+                b.mat_type = -1;
+                break;
+            }
+        }
         b.h_vol.resize(b.n);
         b.h_J0inv.resize(static_cast<size_t>(b.n) * b.ngp * 9);
         double Y[3 * MAX_NEN];

@@ -64,7 +64,8 @@ struct Scatter {
 template <int NGP, int BLK>
 constexpr int elems_per_cta() { return (BLK / NGP) < 1 ? 1 : ((BLK / NGP) > 128 ? 128 : BLK / NGP); }
 
-template <int NEN, int NGP, typename T, int BLK>
+// MT: the block's one material law, or -1 when its elements mix laws
+template <int NEN, int NGP, typename T, int BLK, int MT>
 __global__ void __launch_bounds__(BLK) k_elem_residual(ElemArgs<T> a)
 {
     griddep_wait();
@@ -139,24 +140,29 @@ __global__ void __launch_bounds__(BLK) k_elem_residual(ElemArgs<T> a)
                 A[6] += u2 * d0; A[7] += u2 * d1; A[8] += u2 * d2;
             }
             const T* Jp = a.J0inv + (static_cast<size_t>(e) * NGP + g) * 9;
-            T Ji[9];
-#pragma unroll
-            for (int k = 0; k < 9; k++) Ji[k] = __ldg(Jp + k);
             T H[9];
+            {
+                T Ji[9];
 #pragma unroll
-            for (int i = 0; i < 3; i++)
+                for (int k = 0; k < 9; k++) Ji[k] = __ldg(Jp + k);
 #pragma unroll
-                for (int j = 0; j < 3; j++) H[3 * i + j] = A[3 * i] * Ji[j] + A[3 * i + 1] * Ji[3 + j] + A[3 * i + 2] * Ji[6 + j];
+                for (int i = 0; i < 3; i++)
+#pragma unroll
+                    for (int j = 0; j < 3; j++)
+                        H[3 * i + j] = A[3 * i] * Ji[j] + A[3 * i + 1] * Ji[3 + j] + A[3 * i + 2] * Ji[6 + j];
+            }
             const MatParams<T> mp = a.mats[__ldg(a.mat + e)];
             T P[9];
-            piola(mp, H, P);
+            piola<T, MT>(mp, H, P);
             const T wv = __ldg(a.vol + e) * a.gw[g];
-            // S = wv P J0^{-T}
+            // S = wv P J0^{-T}; J0^{-1} read again (an L1 hit) rather than
+            // kept in registers through the stress law
 #pragma unroll
-            for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) {
+                const T j0 = __ldg(Jp + 3 * j), j1 = __ldg(Jp + 3 * j + 1), j2 = __ldg(Jp + 3 * j + 2);
 #pragma unroll
-                for (int j = 0; j < 3; j++)
-                    s_S[el][9 * g + 3 * i + j] = wv * (P[3 * i] * Ji[3 * j] + P[3 * i + 1] * Ji[3 * j + 1] + P[3 * i + 2] * Ji[3 * j + 2]);
+                for (int i = 0; i < 3; i++) s_S[el][9 * g + 3 * i + j] = wv * (P[3 * i] * j0 + P[3 * i + 1] * j1 + P[3 * i + 2] * j2);
+            }
         }
     }
     __syncthreads();
@@ -320,10 +326,16 @@ __global__ void __launch_bounds__(kBlock) k_gather(int n_free, const int* __rest
 }
 
 template <int NEN, int NGP, typename T, int BLK>
-void launch_elem_blk(const ElemArgs<T>& a, cudaStream_t st)
+void launch_elem_blk(const ElemArgs<T>& a, int mt, cudaStream_t st)
 {
     constexpr int EPB = elems_per_cta<NGP, BLK>();
-    launch_k(k_elem_residual<NEN, NGP, T, BLK>, (a.n + EPB - 1) / EPB, BLK, 0, st, a);
+    const int grid = (a.n + EPB - 1) / EPB;
+    switch (mt) {
+    case EFEM_NEO_HOOKEAN: launch_k(k_elem_residual<NEN, NGP, T, BLK, EFEM_NEO_HOOKEAN>, grid, BLK, 0, st, a); break;
+    case EFEM_MOONEY_RIVLIN: launch_k(k_elem_residual<NEN, NGP, T, BLK, EFEM_MOONEY_RIVLIN>, grid, BLK, 0, st, a); break;
+    case EFEM_YEOH: launch_k(k_elem_residual<NEN, NGP, T, BLK, EFEM_YEOH>, grid, BLK, 0, st, a); break;
+    default: launch_k(k_elem_residual<NEN, NGP, T, BLK, -1>, grid, BLK, 0, st, a); break;
+    }
 }
 
 template <int NEN, int NGP, typename T>
@@ -332,9 +344,9 @@ void launch_elem(const DevBlock& b, const MatParams<T>* mats, const T* vol, cons
 {
     ElemArgs<T> a { b.n, n_free, b.conn, b.mat, vol, J0, dN, gw, mats, u, r, sc.contrib, sc.n_slots, sc.slot0,
         b.egroup, b.egroup ? frozen : nullptr };
-    if (threads == 64) launch_elem_blk<NEN, NGP, T, 64>(a, st);
-    else if (threads == 256) launch_elem_blk<NEN, NGP, T, 256>(a, st);
-    else launch_elem_blk<NEN, NGP, T, 128>(a, st);
+    if (threads == 64) launch_elem_blk<NEN, NGP, T, 64>(a, b.mat_type, st);
+    else if (threads == 256) launch_elem_blk<NEN, NGP, T, 256>(a, b.mat_type, st);
+    else launch_elem_blk<NEN, NGP, T, 128>(a, b.mat_type, st);
 }
 
 template <typename T>
