@@ -1,12 +1,21 @@
-"""Benchmark: time-to-converge and L-BFGS iterations/s of the hyperelastic solve.
+"""Benchmark: L-BFGS iterations/s and time-to-converge of the hyperelastic solve.
 
-Workload (one step = one complete solve from u = 0 to ||r||_inf <= 1e-6, the
-reference's JSON-driven call): the C3D8 beam, 0.2 x 0.04 x 0.04 m on an
+Workload (one step = the first 200 L-BFGS iterations of the reference's
+JSON-driven solve from u = 0, criterion ||r||_inf <= 1e-6): the C3D8 beam, 0.2 x 0.04 x 0.04 m on an
 80 x 16 x 16 hexahedral grid (20 480 elements, 23 409 nodes, 69 360 DOF),
 Mooney-Rivlin C10 = 80 kPa, C01 = 20 kPa, D1 = 1e-6, x = 0 fixed, nodal force
 [0, 0, -0.5] N on each of the 289 end-face nodes; FP64 element kernels (or the
 mixed FP32 path with --precision mixed).  Synthetic, seeded mesh in the
 reference's own file formats (efem_b200.meshgen).
+
+The reference's solve of this beam does not converge: at its seventh
+iteration the line search accepts a trial with elements turned inside out
+(its laws stay finite there, J^{-2/3} taken as (J^2)^{-1/3}) and ||r||
+grows without bound, every later iteration exhausting the 20 line-search
+trials.  This library follows the same record (``parity`` below), so a step
+is a fixed count of iterations on that path, the same work on both arms;
+time-to-converge is measured on the cap (``mixed_vs_fp64``), which converges
+in 91 iterations here and in the reference.
 
 Each timed step includes the per-solve numeric factorisation of the
 approximate Jacobian (as LBFGSSolver::solve does once per solve); the mesh
@@ -14,8 +23,8 @@ set-up (element tables, symbolic analysis of the factor) happens once, before
 the warm-up steps.
 
 After the timed region the default line also carries, on one GPU, the rest
-of the metric: ``parity_rel_l2_vs_reference`` (the timed solve's u against
-the reference's own solve of the same mesh, a committed fixture),
+of the metric: ``parity`` (||r||_2 after each of the first line searches
+against the reference's own record of this solve, a committed fixture),
 ``mixed_vs_fp64`` (the C3D20R cylinder cap's time-to-converge in mixed
 precision and in FP64, each solution's error against the reference) and
 ``adjoint`` / ``adjoint_ms`` (the finger's gradient time); --no-extras skips
@@ -57,7 +66,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "L-BFGS iters/s (time-to-converge solve, C3D8 MR beam 20480 el)"
+METRIC = "L-BFGS iters/s (first 200 iterations of the reference's solve, C3D8 MR beam 20480 el)"
+BEAM_ITERS = 200  # iterations per step: the reference's solve of the beam does not converge
 UNIT = "iters/s"
 
 
@@ -68,7 +78,8 @@ def workload_case():
 
 def config_block(precision, n):
     return {"workload": "C3D8 Mooney-Rivlin cantilever, 80x16x16 hex (20480 el, 69360 DOF), tip force, "
-                        "residual 1e-6, one full solve per step",
+                        "residual 1e-6, the first 200 L-BFGS iterations of the solve from u = 0 per step "
+                        "(the reference's solve of this beam does not converge)",
             "precision": precision, "elements": 20480, "dof": 69360, "replicas": n,
             "parallelism": f"replicas{n}", "l2": "flushed (256 MB write) before every step"}
 
@@ -145,8 +156,8 @@ def reference_sample(steps, warmup, ipstep=8):
     factorisation, then `warmup` + `steps` steps of `ipstep` L-BFGS iterations.
     Returns (iters/s over the timed steps, details).  The reference's time per
     iteration grows along the solve (0.21 s per iteration at iterations 3-6,
-    0.7-0.9 s from iteration 7 on this beam), so a step spans several
-    iterations."""
+    0.7-0.9 s from iteration 7 on this beam, where its line search starts to
+    use all 20 trials), so a step spans several iterations."""
     ref = os.path.join(ROOT, "oracle", "_ref", "efem_ref")
     if not os.path.exists(ref):
         return None, {"why": "oracle/_ref/efem_ref is not built"}
@@ -323,6 +334,35 @@ def reference_fixture(name):
     d = np.load(path, allow_pickle=False)
     return {"u": d["u_solve"].astype(np.float64), "meta": json.loads(str(d["solve_meta"])),
             "epsilon": float(d["epsilon"])}
+
+
+BEAM_RECORD_PINNED = 8  # records 0-7: before the divergent iterations amplify rounding
+
+
+def beam_record_parity(model):
+    """||r||_2 after the initial residual and after each line search of a
+    traced solve of the beam, against the reference's own record of the same
+    solve (tests/golden/config_beam_c3d8_mr_force_record.npz, made by
+    tests/golden/make_golden.py from the reference compiled in oracle/_ref).
+    The first eight records agree to rounding; from the ninth on both solves
+    have left every bound (the reference's passes 1e9 N), each along its own
+    rounding, as the reference and its C restatement do as well."""
+    path = os.path.join(ROOT, "tests", "golden", "config_beam_c3d8_mr_force_record.npz")
+    if not os.path.exists(path):
+        return None
+    d = np.load(path, allow_pickle=False)
+    ref = d["r_norm2"]
+    n = len(ref)
+    model.set_options(device_ptrs=0, trace=n, max_iterations=n - 1)
+    model.solve(np.zeros(model.n_dof))
+    tr = model.solve_trace()["r_norm2"]
+    model.set_options(trace=0, max_iterations=BEAM_ITERS)
+    k = min(len(tr), n)
+    rel = np.abs(tr[:k] - ref[:k]) / ref[:k]
+    return {"records": int(k), "max_rel_diff_first_8": float(rel[:BEAM_RECORD_PINNED].max()),
+            "r_norm2": [float(x) for x in tr[:k]], "reference_r_norm2": [float(x) for x in ref[:k]],
+            "reference": "the reference's LBFGSSolver::solve of the same mesh (oracle/_ref): its benchmark "
+                         "record, which does not converge"}
 
 
 def measure_cap(steps, warmup, stream):
@@ -585,9 +625,7 @@ def main():
     opts.precision = api.MIXED if args.precision == "mixed" else api.FP64
     opts.device = local
     opts.host_loop = 1 if args.host_loop else 0
-    # a bound for the timed solves (the FP64 solve converges in about 180
-    # iterations); the FP32 element path stalls above 1e-6 N on this beam
-    opts.max_iterations = 5000
+    opts.max_iterations = BEAM_ITERS
     t_setup = time.time()
     model = api.Model.from_case(case, opts)
     stream = torch.cuda.current_stream()
@@ -651,8 +689,7 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
             "data": "synthetic (seeded structured mesh in the reference's input format)",
             "config": config_block(args.precision, world),
-            "time_to_converge_ms": total_ms_max / args.steps,
-            "iterations_per_solve": iters / args.steps, "residual_evals_per_solve": sum(i["n_residual_evals"] for i in infos) / args.steps,
+            "iterations_per_step": iters / args.steps, "residual_evals_per_solve": sum(i["n_residual_evals"] for i in infos) / args.steps,
             "final_r_inf": infos[-1]["r_inf"], "u_inf": infos[-1]["u_inf"],
             "converged": all(bool(i["flags"] & api.SOLVE_CONVERGED) for i in infos),
             "programmatic_dependent_launch": all(bool(i["flags"] & api.SOLVE_PDL) for i in infos),
@@ -663,15 +700,8 @@ def main():
             "gpu_launches": int(launches * args.steps),
             "roofline": roof,
             "clocks": clocks.summary()}
-    # ---- parity of the timed solve's result with the reference's own solve of the same mesh
-    fx = reference_fixture("beam_c3d8_mr_force")
-    if fx is not None:
-        ur = torch.from_numpy(fx["u"]).cuda()
-        line["parity_rel_l2_vs_reference"] = float(torch.linalg.norm(u - ur) / torch.linalg.norm(ur))
-        line["parity"] = {"reference_niter": fx["meta"]["niter"], "reference_r_inf": fx["meta"]["r_inf"],
-                          "epsilon": fx["epsilon"],
-                          "reference": "the reference's LBFGSSolver::solve of the same mesh (oracle/_ref), "
-                                       "tests/golden/config_beam_c3d8_mr_force.npz"}
+    # ---- parity: ||r||_2 after each line search against the reference's own record of this solve
+    line["parity"] = beam_record_parity(model)
     # ---- the rest of the metric, after the timed region: mixed vs FP64 (C3D20R cap) and the adjoint gradient
     if rank == 0 and world == 1 and not args.no_extras:
         c = measure_cap(3, 1, stream)

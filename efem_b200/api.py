@@ -87,7 +87,8 @@ class ModelInfo(ctypes.Structure):
                 ("factor_dinv_nnz", ctypes.c_longlong), ("residual_bytes", ctypes.c_longlong),
                 ("residual_flops", ctypes.c_double), ("n_params", ctypes.c_int),
                 ("elem_threads_fp64", ctypes.c_int), ("elem_threads_fp32", ctypes.c_int),
-                ("solve_subtree_levels", ctypes.c_int), ("n_solve_subtrees", ctypes.c_int)]
+                ("solve_subtree_levels", ctypes.c_int), ("n_solve_subtrees", ctypes.c_int),
+                ("solve_ctas", ctypes.c_int), ("solve_smem_bytes", ctypes.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

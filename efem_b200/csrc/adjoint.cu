@@ -43,9 +43,9 @@
 namespace efem {
 
 template <>
-__device__ __forceinline__ Dual dlog1p<Dual>(Dual x)
+__device__ __forceinline__ Dual dlogabs1p<Dual>(Dual x)
 {
-    return Dual(log1p(x.v), x.d / (1.0 + x.v));
+    return Dual(dlogabs1p(x.v), x.d / (1.0 + x.v));  // d/dx log|1 + x| = 1 / (1 + x) for either sign
 }
 template <>
 __device__ __forceinline__ Dual dexp<Dual>(Dual x)

@@ -1342,6 +1342,8 @@ void precond_info(const Model& m, efem_model_info* info)
     info->factor_dinv_nnz = dn;
     info->solve_subtree_levels = m.precond->sub_levels;
     info->n_solve_subtrees = m.precond->n_subs;
+    info->solve_ctas = m.precond->solve_grid;
+    info->solve_smem_bytes = static_cast<int>(m.precond->solve_smem);
 }
 
 thread_local int t_batch = 0;
@@ -1547,77 +1549,107 @@ efem_status precond_setup(Model& m, bool refactor, int* ok, double* ms_factor)
     // backward sweep by level (root first).  Each item records the ranges of
     // contributions its rows assemble, and the shared memory it stages is
     // sized here.
-    std::vector<SolveItem> items;
-    std::vector<int> tgt(4 * static_cast<size_t>(S.ns), 0);
+    // Tiles take a multiple of 4 rows, at least 4.  A front with rows longer
+    // than kStageBudget / 4 then stages more than the budget, and on a mesh
+    // like the C3D20 cap that halves the CTAs per SM for every item of the
+    // solve; so the schedule is also built with tiles of 1-3 rows for such
+    // fronts (more items, more repeated assembly), and the one with more CTAs
+    // per SM is kept (the 4-row one on a tie).
+    struct Schedule {
+        std::vector<SolveItem> items;
+        std::vector<int> tgt;
+        size_t stage_d = 1, work_d = 1, ints = 1;
+        size_t smem() const { return sizeof(double) * (stage_d + work_d) + sizeof(int) * ints; }
+    };
     std::vector<char> whole(S.ns, 0);
-    size_t stage_d = 1, work_d = 1, ints = 1;
-    auto need = [&](size_t sd, size_t wd, size_t ni) {
-        stage_d = std::max(stage_d, sd);
-        work_d = std::max(work_d, wd);
-        ints = std::max(ints, ni);
-    };
-    auto tile = [&](int per_row) {  // rows per tile when a row stages per_row doubles
-        const int t = (kStageBudget / per_row) / 4 * 4;
-        return std::max(4, std::min(256, t));
-    };
-    auto ntiles = [&](int n, int per_row) { const int t = tile(per_row); return (n + t - 1) / t; };
-    auto crange = [&](int s, int t0, int t1) {  // contributions of front rows [t0, t1)
-        const long long ro = S.rows_off[s];
-        return t1 > t0 ? std::make_pair(S.contrib_ptr[ro + t0], S.contrib_ptr[ro + t1]) : std::make_pair(0, 0);
-    };
-    for (int s = 0; s < S.ns; s++) {
-        const int c = S.ncol[s], mm = S.nrow[s] - c, r = S.nrow[s];
-        const int lc = odd_h(c), lm = odd_h(mm);
-        whole[s] = static_cast<long long>(r) * lc <= kWholeBudget && static_cast<long long>(c) * (lc + lm) <= kWholeBudget;
-        tgt[s] = whole[s] ? 1 : ntiles(c, lc);  // y of s complete
-        if (S.parent[s] >= 0 && !in_sub[s])     // children's g complete (subtree roots finish before k_solve)
-            tgt[S.ns + S.parent[s]] += whole[s] ? 1 : ntiles(mm, lc);
-        tgt[3 * S.ns + s] = whole[s] ? 1 : ntiles(c, lc + lm);                              // x of s complete
-    }
-    for (int l = K; l < nlev; l++) {
-        for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) {
-            const int s = S.level_list[q];
-            const int c = S.ncol[s], r = S.nrow[s], mm = r - c, lc = odd_h(c);
-            if (whole[s]) {
-                const auto cr = crange(s, 0, r);
-                items.push_back(SolveItem { kFwdFront, s, 0, c, cr.first, cr.second, 0, 0 });
-                need(static_cast<size_t>(r) * lc, 3 * static_cast<size_t>(r), r + 1 + (cr.second - cr.first) + c);
-                continue;
-            }
-            const int ty = tile(lc);
-            for (int o = 0; o < c; o += ty) {
-                const int i1 = std::min(c, o + ty);
-                const auto cr = crange(s, 0, i1);
-                items.push_back(SolveItem { kFwdY, s, o, i1, cr.first, cr.second, 0, 0 });
-                need(static_cast<size_t>(i1 - o) * lc, 3 * static_cast<size_t>(i1), i1 + 1 + (cr.second - cr.first) + i1);
-            }
-            const auto cj = crange(s, 0, c);
-            for (int o = 0; o < mm; o += ty) {
-                const int k1 = std::min(mm, o + ty);
-                const auto cr = crange(s, c + o, c + k1);
-                items.push_back(SolveItem { kFwdG, s, o, k1, cj.first, cj.second, cr.first, cr.second });
-                need(static_cast<size_t>(k1 - o) * lc, 3 * static_cast<size_t>(c + k1 - o),
-                    2 * static_cast<size_t>(c) + 1 + (cj.second - cj.first) + (k1 - o + 1) + (cr.second - cr.first));
+    auto schedule = [&](int min_rows, Schedule& sch) {
+        std::vector<SolveItem>& items = sch.items;
+        std::vector<int>& tgt = sch.tgt;
+        tgt.assign(4 * static_cast<size_t>(S.ns), 0);
+        size_t& stage_d = sch.stage_d;
+        size_t& work_d = sch.work_d;
+        size_t& ints = sch.ints;
+        auto need = [&](size_t sd, size_t wd, size_t ni) {
+            stage_d = std::max(stage_d, sd);
+            work_d = std::max(work_d, wd);
+            ints = std::max(ints, ni);
+        };
+        auto tile = [&](int per_row) {  // rows per tile when a row stages per_row doubles
+            const int t = kStageBudget / per_row;
+            return t >= 4 ? std::min(256, t / 4 * 4) : std::max(min_rows, t);
+        };
+        auto ntiles = [&](int n, int per_row) { const int t = tile(per_row); return (n + t - 1) / t; };
+        auto crange = [&](int s, int t0, int t1) {  // contributions of front rows [t0, t1)
+            const long long ro = S.rows_off[s];
+            return t1 > t0 ? std::make_pair(S.contrib_ptr[ro + t0], S.contrib_ptr[ro + t1]) : std::make_pair(0, 0);
+        };
+        for (int s = 0; s < S.ns; s++) {
+            const int c = S.ncol[s], mm = S.nrow[s] - c, r = S.nrow[s];
+            const int lc = odd_h(c), lm = odd_h(mm);
+            whole[s] = static_cast<long long>(r) * lc <= kWholeBudget && static_cast<long long>(c) * (lc + lm) <= kWholeBudget;
+            tgt[s] = whole[s] ? 1 : ntiles(c, lc);  // y of s complete
+            if (S.parent[s] >= 0 && !in_sub[s])     // children's g complete (subtree roots finish before k_solve)
+                tgt[S.ns + S.parent[s]] += whole[s] ? 1 : ntiles(mm, lc);
+            tgt[3 * S.ns + s] = whole[s] ? 1 : ntiles(c, lc + lm);                              // x of s complete
+        }
+        for (int l = K; l < nlev; l++) {
+            for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) {
+                const int s = S.level_list[q];
+                const int c = S.ncol[s], r = S.nrow[s], mm = r - c, lc = odd_h(c);
+                if (whole[s]) {
+                    const auto cr = crange(s, 0, r);
+                    items.push_back(SolveItem { kFwdFront, s, 0, c, cr.first, cr.second, 0, 0 });
+                    need(static_cast<size_t>(r) * lc, 3 * static_cast<size_t>(r), r + 1 + (cr.second - cr.first) + c);
+                    continue;
+                }
+                const int ty = tile(lc);
+                for (int o = 0; o < c; o += ty) {
+                    const int i1 = std::min(c, o + ty);
+                    const auto cr = crange(s, 0, i1);
+                    items.push_back(SolveItem { kFwdY, s, o, i1, cr.first, cr.second, 0, 0 });
+                    need(static_cast<size_t>(i1 - o) * lc, 3 * static_cast<size_t>(i1), i1 + 1 + (cr.second - cr.first) + i1);
+                }
+                const auto cj = crange(s, 0, c);
+                for (int o = 0; o < mm; o += ty) {
+                    const int k1 = std::min(mm, o + ty);
+                    const auto cr = crange(s, c + o, c + k1);
+                    items.push_back(SolveItem { kFwdG, s, o, k1, cj.first, cj.second, cr.first, cr.second });
+                    need(static_cast<size_t>(k1 - o) * lc, 3 * static_cast<size_t>(c + k1 - o),
+                        2 * static_cast<size_t>(c) + 1 + (cj.second - cj.first) + (k1 - o + 1) + (cr.second - cr.first));
+                }
             }
         }
-    }
-    for (int l = nlev - 1; l >= K; l--) {
-        for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) {
-            const int s = S.level_list[q];
-            const int c = S.ncol[s], r = S.nrow[s], mm = r - c, lc = odd_h(c), lm = odd_h(mm);
-            if (whole[s]) {
-                items.push_back(SolveItem { kBwdFront, s, 0, c, 0, 0, 0, 0 });
-                need(static_cast<size_t>(c) * (lc + lm), 3 * static_cast<size_t>(r + c), r);
-                continue;
-            }
-            const int tx = tile(lc + lm);
-            for (int o = 0; o < c; o += tx) {
-                const int i1 = std::min(c, o + tx);
-                items.push_back(SolveItem { kBwdX, s, o, i1, 0, 0, 0, 0 });
-                need(static_cast<size_t>(i1 - o) * (lc + lm), 3 * static_cast<size_t>(c - o + mm + i1 - o), r);
+        for (int l = nlev - 1; l >= K; l--) {
+            for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; q++) {
+                const int s = S.level_list[q];
+                const int c = S.ncol[s], r = S.nrow[s], mm = r - c, lc = odd_h(c), lm = odd_h(mm);
+                if (whole[s]) {
+                    items.push_back(SolveItem { kBwdFront, s, 0, c, 0, 0, 0, 0 });
+                    need(static_cast<size_t>(c) * (lc + lm), 3 * static_cast<size_t>(r + c), r);
+                    continue;
+                }
+                const int tx = tile(lc + lm);
+                for (int o = 0; o < c; o += tx) {
+                    const int i1 = std::min(c, o + tx);
+                    items.push_back(SolveItem { kBwdX, s, o, i1, 0, 0, 0, 0 });
+                    need(static_cast<size_t>(i1 - o) * (lc + lm), 3 * static_cast<size_t>(c - o + mm + i1 - o), r);
+                }
             }
         }
-    }
+    };
+    Schedule sch4, sch1;
+    schedule(4, sch4);
+    schedule(1, sch1);
+    EFEM_CUDA(cudaFuncSetAttribute(k_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    int per4 = 0, per1 = 0;
+    if (sch4.smem() <= 200 * 1024)
+        EFEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per4, k_solve, kST, sch4.smem()));
+    if (sch1.smem() <= 200 * 1024)
+        EFEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per1, k_solve, kST, sch1.smem()));
+    Schedule& sch = per1 > per4 ? sch1 : sch4;
+    std::vector<SolveItem>& items = sch.items;
+    std::vector<int>& tgt = sch.tgt;
+    const size_t stage_d = sch.stage_d, work_d = sch.work_d, ints = sch.ints;
     P.n_items = static_cast<int>(items.size());
     P.h_item_front.resize(items.size());
     for (size_t i = 0; i < items.size(); i++) P.h_item_front[i] = items[i].s;

@@ -29,7 +29,7 @@ __device__ double strain_energy(const MatParams<double>& mp, const double* H)
 {
     Kin<double> k;
     kinematics(H, k);
-    const double lJ = log1p(k.delta);
+    const double lJ = dlogabs1p(k.delta);  // log|J|: |J|^{-2/3} as in the reference
     const double Jm23 = exp(-2.0 / 3.0 * lJ);
     const double i1 = 3.0 * expm1(-2.0 / 3.0 * lJ) + k.a * Jm23;  // I1bar - 3
     double W = k.delta * k.delta / mp.D1;

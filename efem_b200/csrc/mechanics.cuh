@@ -22,12 +22,16 @@
 
 namespace efem {
 
+// log|1 + x|.  The laws take J^{-2/3} as (J^2)^{-1/3} = |J|^{-2/3}, as the
+// reference does (std::pow(I3, 1/3) with I3 = J^2): an inverted element
+// (J < 0) gets a finite stress, not NaN, so a line-search trial that inverts
+// elements is judged on its residual exactly as in the reference.
 template <typename T>
-__device__ __forceinline__ T dlog1p(T x);
+__device__ __forceinline__ T dlogabs1p(T x);
 template <>
-__device__ __forceinline__ double dlog1p<double>(double x) { return log1p(x); }
+__device__ __forceinline__ double dlogabs1p<double>(double x) { return x > -1.0 ? log1p(x) : log(-(1.0 + x)); }
 template <>
-__device__ __forceinline__ float dlog1p<float>(float x) { return log1pf(x); }
+__device__ __forceinline__ float dlogabs1p<float>(float x) { return x > -1.0f ? log1pf(x) : logf(-(1.0f + x)); }
 template <typename T>
 __device__ __forceinline__ T dexp(T x);
 template <>
@@ -93,7 +97,7 @@ __device__ __forceinline__ void piola(const MatParams<T>& mp, const T* H, T* P)
     const bool mr = MT == EFEM_MOONEY_RIVLIN || (MT < 0 && mp.type == EFEM_MOONEY_RIVLIN);
     Kin<T> k;
     kinematics(H, k);
-    const T lJ = dlog1p(k.delta);
+    const T lJ = dlogabs1p(k.delta);  // log|J|
     const T Jm23 = dexp(T(-2.0 / 3.0) * lJ);
     const T inv1pd = T(1) / (T(1) + k.delta);
     const T cm1 = (k.a * T(1.0 / 3.0) - k.delta) * inv1pd;  // c - 1

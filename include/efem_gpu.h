@@ -180,6 +180,8 @@ typedef struct {
                                              (C10, C01, C20, C30, D1), then 1 per pressure load */
     int elem_threads_fp64, elem_threads_fp32;  /* the first element block's CTA size (autotuner) */
     int solve_subtree_levels, n_solve_subtrees; /* H0 solve schedule: levels solved per subtree, subtrees */
+    int solve_ctas;                             /* CTAs of the persistent triangular solve */
+    int solve_smem_bytes;                       /* its dynamic shared memory per CTA */
 } efem_model_info;
 
 typedef struct {

@@ -358,7 +358,72 @@ def batch_members():
         print("batch member", i, case.mesh.conn.shape[0], meta["niter"], meta_t["niter"])
 
 
+def inverted_cases():
+    """``inverted_<et>_<mat>.npz``: the reference's residual at a displacement
+    that turns every element inside out (x -> -X/2 along the beam axis plus a
+    seeded perturbation, so J is about -1/2 at every Gauss point).  The
+    reference's laws take J^{-2/3} as (J^2)^{-1/3} and stay finite there; a
+    solve whose line search tries such a state (the C3D8 beam under tip forces
+    does at its seventh iteration) takes its next step from these values."""
+    rng = np.random.default_rng(20261204)
+    for et in ("C3D4", "C3D8", "C3D10", "C3D20"):
+        for mat in MATS:
+            case = mg.small_case(et, mat, "force")
+            with tempfile.TemporaryDirectory() as td:
+                cfg = case.write(td)
+                meta, _ = oracle.run_ref("info", cfg)
+                n = meta["n_dof"]
+                # free nodes in the reference's DOF order: the fixture stores u per DOF
+                _, r0 = oracle.run_ref("residual", cfg, None)
+                free = np.setdiff1d(np.arange(case.mesh.X.shape[0]), np.asarray(case.fix))
+                X = case.mesh.X[free]
+                assert 3 * X.shape[0] == n
+                h = np.ptp(case.mesh.X[:, 0]) / 10.0
+                u = np.zeros((X.shape[0], 3))
+                u[:, 0] = -1.5 * X[:, 0]
+                u += rng.normal(scale=0.02 * h, size=u.shape)
+                u = u.ravel()
+                data = case_arrays(case)
+                data.update(u=u)
+                _, r = oracle.run_ref("residual", cfg, u)
+                data["r_full"] = r
+                if et == "C3D20":
+                    _, rr = oracle.run_ref("residual", cfg, u, reduced=True)
+                    data["r_reduced"] = rr
+            assert np.all(np.isfinite(data["r_full"]))
+            np.savez_compressed(os.path.join(HERE, f"inverted_{et}_{mat}.npz"), **data)
+            print("inverted", et, mat, n, float(np.abs(data["r_full"]).max()))
+
+
+def beam_record(iters=12):
+    """``config_beam_c3d8_mr_force_record.npz``: the reference's own solve of
+    the C3D8 Mooney-Rivlin beam under 0.5 N tip forces does not converge: at
+    its seventh iteration the line search accepts a state with elements
+    turned inside out and ||r|| grows without bound (1e93 N by iteration 30).
+    Its converged displacement therefore does not exist; what pins this
+    configuration is its benchmark record (||r||_2 after every line search,
+    initial residual first) over the first iterations, and the steps and
+    residual evaluations of the same solve from the C restatement (oracle),
+    which follows the same record."""
+    case, _ = config_case("beam_c3d8_mr_force")
+    with tempfile.TemporaryDirectory() as td:
+        cfg = case.write(td)
+        meta, _ = oracle.run_ref("solve", cfg, "--max-iters", str(iters), trace=True, timeout=3600)
+        o = oracle.Oracle(oracle.read_case(cfg))
+    _, info = o.solve(max_iterations=iters, trace=iters + 1)
+    rec = np.asarray(meta.pop("trace"))
+    np.savez_compressed(os.path.join(HERE, "config_beam_c3d8_mr_force_record.npz"), r_norm2=rec,
+                        oracle_trace=info["trace"], solve_meta=json.dumps(meta), mesh=mesh_digest(case))
+    print("beam record", meta, rec[:iters + 1])
+
+
 def main():
+    if sys.argv[1:] == ["beamrecord"]:
+        beam_record()
+        return
+    if sys.argv[1:] == ["inverted"]:
+        inverted_cases()
+        return
     if sys.argv[1:] == ["gravity"]:
         gravity_cases()
         return

@@ -38,6 +38,26 @@ def test_residual_mixed_close_to_reference(path, tmp_path):
     assert np.linalg.norm(r - ref) <= 2e-5 * np.linalg.norm(ref)
 
 
+@pytest.mark.parametrize("path", golden_files("inverted_*.npz"), ids=lambda p: p.split("/")[-1][9:-4])
+def test_residual_inverted_elements_match_reference(path, tmp_path):
+    """Every element turned inside out (J about -1/2 at every Gauss point):
+    the reference's laws take J^{-2/3} as (J^2)^{-1/3} and stay finite, and so
+    must R(u) here -- a line search that tries such a state (the C3D8 beam
+    under tip forces does) chooses its next step from these values.  FP64 to
+    1e-12 relative L2 (both integrations for C3D20), FP32 elements to 1e-4."""
+    d0 = np.load(path)
+    for integration in (["full", "reduced"] if "r_reduced" in d0.files else ["full"]):
+        cfg, d = write_golden_case(path, tmp_path, integration)
+        m = api.Model.from_json(cfg)
+        r = m.residual(d["u"])
+        ref = d[f"r_{integration}"]
+        assert np.all(np.isfinite(r))
+        assert np.linalg.norm(r - ref) <= 1e-12 * np.linalg.norm(ref), (integration, np.linalg.norm(r - ref))
+        m.set_options(precision=api.MIXED)
+        rm = m.residual(d["u"])
+        assert np.linalg.norm(rm - ref) <= 1e-4 * np.linalg.norm(ref), (integration, np.linalg.norm(rm - ref))
+
+
 def test_residual_device_pointers():
     import torch
     case = mg.cantilever_c3d4_pressure()

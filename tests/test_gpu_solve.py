@@ -132,15 +132,20 @@ def test_beam_subtree_schedules_agree():
     ref = m.precond_apply(v)
     info = m.info()
     assert info["solve_subtree_levels"] == 0 and info["n_solve_subtrees"] == 0
+    # the persistent solve keeps three CTAs on every SM (registers and shared memory)
+    import torch
+    assert info["solve_ctas"] == 3 * torch.cuda.get_device_properties(0).multi_processor_count, info
     nlev = info["n_levels"]
     for k in (1, 3, nlev - 2, nlev):
         m.set_options(solve_subtree_levels=k)
         hv = m.precond_apply(v)
         assert np.linalg.norm(hv - ref) <= 1e-11 * np.linalg.norm(ref), (k, m.info()["solve_subtree_levels"])
-    # and the whole solve with subtree kernels on the lowest three levels
-    m.set_options(solve_subtree_levels=0)
+    # and the first six iterations of the solve (the beam's solve does not
+    # converge, in the reference either) with subtree kernels on the lowest
+    # three levels
+    m.set_options(solve_subtree_levels=0, max_iterations=6)
     u0, i0 = m.solve()
     m.set_options(solve_subtree_levels=3)
     u1, i1 = m.solve()
-    assert i0["flags"] & api.SOLVE_CONVERGED and i1["flags"] & api.SOLVE_CONVERGED
-    assert np.linalg.norm(u1 - u0) <= 1e-4 * np.linalg.norm(u0)
+    assert i0["niter"] == i1["niter"] == 6
+    assert np.linalg.norm(u1 - u0) <= 1e-8 * np.linalg.norm(u0)
