@@ -1,6 +1,6 @@
 """Benchmark: L-BFGS iterations/s and time-to-converge of the hyperelastic solve.
 
-Workload (one step = the first 200 L-BFGS iterations of the reference's
+Workload (one step = the first 32 L-BFGS iterations of the reference's
 JSON-driven solve from u = 0, criterion ||r||_inf <= 1e-6): the C3D8 beam, 0.2 x 0.04 x 0.04 m on an
 80 x 16 x 16 hexahedral grid (20 480 elements, 23 409 nodes, 69 360 DOF),
 Mooney-Rivlin C10 = 80 kPa, C01 = 20 kPa, D1 = 1e-6, x = 0 fixed, nodal force
@@ -66,8 +66,12 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "L-BFGS iters/s (first 200 iterations of the reference's solve, C3D8 MR beam 20480 el)"
-BEAM_ITERS = 200  # iterations per step: the reference's solve of the beam does not converge
+METRIC = "L-BFGS iters/s (first 32 iterations of the reference's solve, C3D8 MR beam 20480 el)"
+# iterations per step: the reference's solve of the beam does not converge.  32
+# is as far as the reference arm's samples reach (iterations 9-32); further
+# along, ||r|| (about 1e93 N by then) can overflow and end the solve as
+# non-finite, in the reference as here, at a point that varies with rounding
+BEAM_ITERS = 32
 UNIT = "iters/s"
 
 
@@ -78,7 +82,7 @@ def workload_case():
 
 def config_block(precision, n):
     return {"workload": "C3D8 Mooney-Rivlin cantilever, 80x16x16 hex (20480 el, 69360 DOF), tip force, "
-                        "residual 1e-6, the first 200 L-BFGS iterations of the solve from u = 0 per step "
+                        "residual 1e-6, the first 32 L-BFGS iterations of the solve from u = 0 per step "
                         "(the reference's solve of this beam does not converge)",
             "precision": precision, "elements": 20480, "dof": 69360, "replicas": n,
             "parallelism": f"replicas{n}", "l2": "flushed (256 MB write) before every step"}

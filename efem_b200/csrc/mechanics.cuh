@@ -32,6 +32,13 @@ template <>
 __device__ __forceinline__ double dlogabs1p<double>(double x) { return x > -1.0 ? log1p(x) : log(-(1.0 + x)); }
 template <>
 __device__ __forceinline__ float dlogabs1p<float>(float x) { return x > -1.0f ? log1pf(x) : logf(-(1.0f + x)); }
+// J^{-1/3} (negative for J < 0)
+template <typename T>
+__device__ __forceinline__ T drcbrt(T x);
+template <>
+__device__ __forceinline__ double drcbrt<double>(double x) { return rcbrt(x); }
+template <>
+__device__ __forceinline__ float drcbrt<float>(float x) { return rcbrtf(x); }
 template <typename T>
 __device__ __forceinline__ T dexp(T x);
 template <>
@@ -97,15 +104,22 @@ __device__ __forceinline__ void piola(const MatParams<T>& mp, const T* H, T* P)
     const bool mr = MT == EFEM_MOONEY_RIVLIN || (MT < 0 && mp.type == EFEM_MOONEY_RIVLIN);
     Kin<T> k;
     kinematics(H, k);
-    const T lJ = dlogabs1p(k.delta);  // log|J|
-    const T Jm23 = dexp(T(-2.0 / 3.0) * lJ);
-    const T inv1pd = T(1) / (T(1) + k.delta);
+    // J^{-2/3} = rc^2 with rc = J^{-1/3}: the reference's (J^2)^{-1/3}, finite
+    // for an inverted element (rc < 0), with one transcendental call
+    const T J = T(1) + k.delta;
+    const T rc = drcbrt(J);
+    const T Jm23 = rc * rc;
+    const T inv1pd = T(1) / J;
     const T cm1 = (k.a * T(1.0 / 3.0) - k.delta) * inv1pd;  // c - 1
     const T c = T(1) + cm1;
     T coef = mp.C10;
     if (yeoh) {
-        // I1bar - 3 = 3 (J^{-2/3} - 1) + (I1 - 3) J^{-2/3}
-        const T t = T(3) * dexpm1(T(-2.0 / 3.0) * lJ) + k.a * Jm23;
+        // I1bar - 3 = 3 (J^{-2/3} - 1) + (I1 - 3) J^{-2/3}, where with
+        // y = J^{1/3} = J rc^2 (so y - 1 = delta / (y^2 + y + 1)),
+        // J^{-2/3} - 1 = -delta (y + 1) rc^2 / (y^2 + y + 1): no cancellation
+        const T y = J * Jm23;
+        const T jm1 = -k.delta * (y + T(1)) * Jm23 / (y * y + y + T(1));
+        const T t = T(3) * jm1 + k.a * Jm23;
         coef = mp.C10 + T(2) * mp.C20 * t + T(3) * mp.C30 * t * t;
     }
     const T s1 = T(2) * coef * Jm23;
