@@ -343,6 +343,22 @@ def reference_fixture(name):
 BEAM_RECORD_PINNED = 8  # records 0-7: before the divergent iterations amplify rounding
 
 
+def beam_solve(model, u):
+    """One step's solve of the beam: its info dict.  The reference's path on
+    this beam can end non-finite at an iteration that moves with rounding
+    (then the solve stops with EFEM_ERR_NAN and u zeroed, as the reference's
+    Integrator::integral does); the iterations done up to there count."""
+    from efem_b200 import api
+    import ctypes
+    info = api.SolveInfo()
+    st = api.lib().efem_solve(model.h, api._vec_ptr(u), ctypes.byref(info))
+    if st not in (api.OK, api.ERR_NAN):
+        raise api.EfemError(st, api.last_error())
+    d = info.as_dict()
+    d["non_finite"] = st == api.ERR_NAN
+    return d
+
+
 def beam_record_parity(model):
     """||r||_2 after the initial residual and after each line search of a
     traced solve of the beam, against the reference's own record of the same
@@ -358,7 +374,7 @@ def beam_record_parity(model):
     ref = d["r_norm2"]
     n = len(ref)
     model.set_options(device_ptrs=0, trace=n, max_iterations=n - 1)
-    model.solve(np.zeros(model.n_dof))
+    beam_solve(model, np.zeros(model.n_dof))
     tr = model.solve_trace()["r_norm2"]
     model.set_options(trace=0, max_iterations=BEAM_ITERS)
     k = min(len(tr), n)
@@ -640,8 +656,7 @@ def main():
 
     def one_solve():
         u.zero_()
-        _, info = model.solve(u)
-        return info
+        return beam_solve(model, u)
 
     first = one_solve()  # also builds the symbolic factor analysis
     setup_s = time.time() - t_setup
@@ -673,7 +688,7 @@ def main():
     for a, b in e2e_ev:
         u_host[:] = 0.0
         a.record(stream)
-        _, info = model.solve(u_host)
+        info = beam_solve(model, u_host)
         b.record(stream)
         e2e_iters += info["niter"]
     barrier()
@@ -693,7 +708,8 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
             "data": "synthetic (seeded structured mesh in the reference's input format)",
             "config": config_block(args.precision, world),
-            "iterations_per_step": iters / args.steps, "residual_evals_per_solve": sum(i["n_residual_evals"] for i in infos) / args.steps,
+            "iterations_per_step": iters / args.steps,
+            "steps_ended_non_finite": sum(1 for i in infos if i.get("non_finite")), "residual_evals_per_solve": sum(i["n_residual_evals"] for i in infos) / args.steps,
             "final_r_inf": infos[-1]["r_inf"], "u_inf": infos[-1]["u_inf"],
             "converged": all(bool(i["flags"] & api.SOLVE_CONVERGED) for i in infos),
             "programmatic_dependent_launch": all(bool(i["flags"] & api.SOLVE_PDL) for i in infos),

@@ -466,7 +466,7 @@ __global__ void __launch_bounds__(kT) kb_trial(double* __restrict__ x, const dou
     const bool act = sg->state == kRun && sg->trial;
     const double step = sg->step;
     for (int i = c.a + threadIdx.x; i < c.b; i += kT) {
-        if (act) x[i] = xp[i] + step * d[i];
+        if (act) x[i] = __fma_rn(step, d[i], xp[i]);
         r[i] = -fext[i];
     }
 }

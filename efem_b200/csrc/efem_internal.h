@@ -251,6 +251,7 @@ efem_status ensure_device(Model& m);  // create the stream and upload everything
 // ------------------------------------------------------------------ kernels (residual.cu)
 // r = R(u) on the model's stream; u, r device pointers of length 3*n_free.
 efem_status launch_residual(Model& m, const double* d_u, double* d_r);
+int element_tune_key(const Model& m);  // what the element kernels' CTA sizes were tuned for
 efem_status tune_element_blocks(Model& m);  // autotuner of the element kernels' CTA size
 // the same on `stream`; with `stamp`, the GPU's global timer at the start is
 // stored there; init_r = false when the caller has already set r = -f_ext

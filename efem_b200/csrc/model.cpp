@@ -662,7 +662,7 @@ efem_status ensure_device(Model& m)
 #undef UP
     m.on_device = true;
     if (m.opts.deterministic && !m.d_contrib && (s = build_gather(m)) != EFEM_OK) return s;
-    if (m.tuned_threads != m.opts.elem_threads) {
+    if (m.tuned_threads != element_tune_key(m)) {
         // element kernels are tuned before any graph captures them (a retune
         // invalidates captured graphs through the epoch)
         if ((s = tune_element_blocks(m)) != EFEM_OK) return s;

@@ -390,10 +390,14 @@ void dispatch_face(const DevFaces& f, const T* J0, const T* tw, const T* tN, con
 // both precisions, time the 64-, 128- and 256-thread variants (2 warm-up and
 // 5 timed launches each, CUDA events on the model's stream, at u = 0: the
 // kernels' work does not depend on the values) and keep the fastest.
-// opts.elem_threads = 64 / 128 / 256 forces one variant instead.
+// opts.elem_threads = 64 / 128 / 256 forces one variant instead; so does
+// deterministic mode (128 unless forced), so that every model and every solve
+// runs the same instantiation and the results repeat bitwise whatever the
+// timings.
+int element_tune_key(const Model& m) { return m.opts.elem_threads | (m.opts.deterministic ? 0x400 : 0); }
 efem_status tune_element_blocks(Model& m)
 {
-    const int forced = m.opts.elem_threads;
+    const int forced = m.opts.elem_threads ? m.opts.elem_threads : (m.opts.deterministic ? 128 : 0);
     const size_t n = 3 * static_cast<size_t>(std::max(m.n_free, 1));
     EFEM_CUDA(cudaMemsetAsync(m.d_u, 0, n * sizeof(double), m.stream));
     cudaEvent_t e0, e1;
@@ -433,7 +437,7 @@ efem_status tune_element_blocks(Model& m)
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     EFEM_CUDA(cudaGetLastError());
-    m.tuned_threads = forced;
+    m.tuned_threads = element_tune_key(m);
     return EFEM_OK;
 }
 

@@ -236,7 +236,7 @@ __global__ void k_trial(double* __restrict__ x, const double* __restrict__ xp, c
     size_t n, Scalars* S)
 {
     if (blockIdx.x == 0 && threadIdx.x == 0) S->step = step;
-    GRID_STRIDE(i, n) x[i] = xp[i] + step * d[i];
+    GRID_STRIDE(i, n) x[i] = __fma_rn(step, d[i], xp[i]);
 }
 
 // line-search scalars: dg = r.d, rinf = ||r||_inf, xinf = ||x||_inf, x2 = ||x||^2,
@@ -702,7 +702,7 @@ __global__ void k_trial_dev(double* __restrict__ x, const double* __restrict__ x
     const double step = S->step;
     GRID_STRIDE(i, n)
     {
-        x[i] = xp[i] + step * d[i];
+        x[i] = __fma_rn(step, d[i], xp[i]);
         r[i] = -fext[i];
     }
 }
