@@ -25,6 +25,31 @@ def test_residual_matches_reference(path, integration, tmp_path):
     assert np.linalg.norm(r - ref) <= 1e-12 * np.linalg.norm(ref)
 
 
+@pytest.mark.parametrize("path", golden_files("inverted_*.npz"), ids=lambda p: p.split("/")[-1][9:-4])
+def test_residual_inverted_elements_matches_reference(path, tmp_path):
+    """Every element inside out (J about -1/2): the reference's laws stay
+    finite there (J^{-2/3} = (J^2)^{-1/3}), and the restatement follows them."""
+    d0 = np.load(path)
+    for integration in (["full", "reduced"] if "r_reduced" in d0.files else ["full"]):
+        cfg, d = write_golden_case(path, tmp_path, integration)
+        o = oracle.Oracle(oracle.read_case(cfg))
+        r = o.residual(d["u"])
+        ref = d[f"r_{integration}"]
+        assert np.all(np.isfinite(r))
+        assert np.linalg.norm(r - ref) <= 1e-12 * np.linalg.norm(ref), integration
+
+
+def test_beam_record_oracle_follows_reference():
+    """The C3D8 beam's non-converging solve: the restatement's record of
+    ||r||_2 (stored in the fixture by the generator) follows the reference's
+    through the seventh line search."""
+    d = np.load(golden_files("config_beam_c3d8_mr_force_record.npz")[0])
+    ref, ora = d["r_norm2"], d["oracle_trace"][:, 1]
+    rel = np.abs(ora[:8] - ref[:8]) / ref[:8]
+    assert rel.max() <= 1e-6, rel
+    assert ref[8:].min() > 1e8 and ora[8:].min() > 1e8
+
+
 @pytest.mark.parametrize("path", CASES, ids=lambda p: p.split("/")[-1][5:-4])
 @pytest.mark.parametrize("integration", ["full", "reduced"])
 def test_approx_jacobian_matches_reference(path, integration, tmp_path):
