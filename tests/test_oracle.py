@@ -39,6 +39,21 @@ def test_residual_inverted_elements_matches_reference(path, tmp_path):
         assert np.linalg.norm(r - ref) <= 1e-12 * np.linalg.norm(ref), integration
 
 
+@pytest.mark.parametrize("path", golden_files("sample_*.npz"), ids=lambda p: p.split("/")[-1][7:-4])
+def test_residual_vanishes_at_reference_sample_solutions(path, tmp_path):
+    """The reference's own six sample problems (their configs and files, the
+    id -1 Mooney-Rivlin material, directed and follower pressure): at the
+    reference's solution converged to 1e-10 N, the restatement's residual is
+    as small as the reference's own stopping test allows (1.5e-10 N)."""
+    from conftest import write_sample
+    cfg, d = write_sample(path, tmp_path)
+    o = oracle.Oracle(oracle.read_case(cfg))
+    r = o.residual(d["u_tight"])
+    r0 = o.residual(np.zeros_like(d["u_tight"]))
+    assert np.abs(r0).max() > 0.1
+    assert np.abs(r).max() <= 1.5e-10, np.abs(r).max()
+
+
 def test_beam_record_oracle_follows_reference():
     """The C3D8 beam's non-converging solve: the restatement's record of
     ||r||_2 (stored in the fixture by the generator) follows the reference's
