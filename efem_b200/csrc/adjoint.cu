@@ -43,26 +43,10 @@
 namespace efem {
 
 template <>
-__device__ __forceinline__ Dual dlogabs1p<Dual>(Dual x)
-{
-    return Dual(dlogabs1p(x.v), x.d / (1.0 + x.v));  // d/dx log|1 + x| = 1 / (1 + x) for either sign
-}
-template <>
 __device__ __forceinline__ Dual drcbrt<Dual>(Dual x)
 {
     const double r = rcbrt(x.v);
     return Dual(r, -(1.0 / 3.0) * (r * r) * (r * r) * x.d);  // d J^{-1/3} / dJ = -J^{-4/3} / 3
-}
-template <>
-__device__ __forceinline__ Dual dexp<Dual>(Dual x)
-{
-    const double e = exp(x.v);
-    return Dual(e, e * x.d);
-}
-template <>
-__device__ __forceinline__ Dual dexpm1<Dual>(Dual x)
-{
-    return Dual(expm1(x.v), exp(x.v) * x.d);
 }
 
 namespace {

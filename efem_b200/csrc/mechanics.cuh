@@ -39,18 +39,6 @@ template <>
 __device__ __forceinline__ double drcbrt<double>(double x) { return rcbrt(x); }
 template <>
 __device__ __forceinline__ float drcbrt<float>(float x) { return rcbrtf(x); }
-template <typename T>
-__device__ __forceinline__ T dexp(T x);
-template <>
-__device__ __forceinline__ double dexp<double>(double x) { return exp(x); }
-template <>
-__device__ __forceinline__ float dexp<float>(float x) { return expf(x); }
-template <typename T>
-__device__ __forceinline__ T dexpm1(T x);
-template <>
-__device__ __forceinline__ double dexpm1<double>(double x) { return expm1(x); }
-template <>
-__device__ __forceinline__ float dexpm1<float>(float x) { return expm1f(x); }
 
 // cofactor matrix (row-major): cof(A)_ij = A_{i+1,j+1} A_{i+2,j+2} - A_{i+1,j+2} A_{i+2,j+1}
 template <typename T>
